@@ -1,0 +1,288 @@
+"""Throughput of the image-TV prox on B200 (isotropic TV, dual FISTA stopped on
+the duality gap), through libfastprox_b200's C ABI.
+
+Workload (one step = one fp_prox_steps call over one batch): 64 float32 images
+of 512 x 512, each a piecewise-constant phantom (20 rectangles and 10 disks,
+intensities U[0, 1] on 0) plus N(0, 0.1^2) noise; one pixel-weight map
+U[0.5, 1.5] for the batch; steps cycling through gamma = 0.05, 0.1, 0.2 over
+the images; every image stopped at duality gap <= 1e-6 |x|^2 / 2. Seeded
+synthetic data (no dataset is involved).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). ``value`` is images/s with inputs resident in
+HBM; ``e2e`` the same through host (pinned) arrays, copies included;
+``roofline`` the achieved HBM rate of the iteration (algorithmic bytes per
+pixel-iteration x pixel-iterations / time) against the measured copy
+bandwidth; ``cpu_baseline`` the reference C library on the host cores.
+``--impl reference`` times the reference's own CPU implementation (its C
+library, built from its sources into oracle/_ref) on a bounded sample.
+Multi-GPU: replicas (each rank its own batch, no data-path collective).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+B, H, W = 64, 512, 512
+GAMMAS = (0.05, 0.1, 0.2)
+TOL, MAX_ITER = 1e-6, 20000
+BYTES_PER_PIXEL_ITER = 40  # d 4 + u 8 + v 8 in, u 8 + v 8 out, alpha 4 (fp32)
+WORKLOAD = "tv_iso 2D, 64 x 512^2 fp32 phantom+noise(0.1), pixel weights U[0.5,1.5], gamma {0.05,0.1,0.2}, gap<=1e-6"
+
+
+def make_inputs(seed=0):
+    from fastprox_b200 import synth
+    x = synth.phantom(B, H, W, seed=seed, sigma=0.1)
+    alpha = synth.pixel_weights((H, W), seed=seed + 1)
+    steps = np.array([GAMMAS[i % len(GAMMAS)] for i in range(B)], np.float64)
+    return x, alpha, steps
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples (SM clock, throttle reasons) during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+            return self
+
+        def read():
+            for line in self.proc.stdout:
+                self.samples.append([f.strip() for f in line.split(",")])
+        self.thread = threading.Thread(target=read, daemon=True)
+        self.thread.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            if self.thread:
+                self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[0]))
+                mx.append(float(s[1]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, s[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference(x, alpha, steps, nimg, threads=None):
+    """The reference C library (oracle/_ref) on the first nimg images: images/s."""
+    from oracle import ref_capi
+    threads = threads or ref_capi.default_threads()
+    xs = np.ascontiguousarray(x[:nimg])
+    t0 = time.perf_counter()
+    r = ref_capi.solve(xs, 0.0, iso=True, k=2, spatial=alpha, tol=TOL, max_iter=MAX_ITER, threads=threads,
+                       steps=steps[:nimg])
+    dt = time.perf_counter() - t0
+    return nimg / dt, threads, r
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import ref_capi
+    cfg = {"workload": WORKLOAD, "global_batch": B, "image": [H, W], "dtype_in": "float32",
+           "sample_images_per_step": 3}
+    if not ref_capi.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference C library not built (oracle/_ref)"}))
+        return
+    x, alpha, steps = make_inputs()
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, threads, _ = cpu_reference(x, alpha, steps, 3)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {"metric": "TV-prox images/s at gap<=1e-6 (512^2 fp32)", "value": value, "unit": "images/s",
+            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 3 / value * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": "images/s", "cores": threads, "kind": "reference",
+                             "sample": "3 of the 64 images per step (one per gamma), reference fp_prox_steps"},
+            "e2e": {"value": value, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import ctypes as C
+
+    import torch
+    import torch.distributed as dist
+
+    from fastprox_b200 import TVIso, capi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+
+    x, alpha, steps = make_inputs(seed=rank)
+    xt = torch.as_tensor(x, device=dev)
+    st = torch.as_tensor(steps, device=dev)
+    out = torch.empty_like(xt)
+    op = TVIso(2, pixel_weights=alpha)
+    stream = torch.cuda.current_stream(dev)
+    L = capi.lib()
+
+    def device_step():
+        return op.solve(xt, st, tol=TOL, max_iter=MAX_ITER, out=out, with_dual=False)[1]
+
+    for _ in range(max(args.warmup, 3)):
+        info = device_step()
+    ws = op.workspace(xt)
+    kl, sl = C.c_int64(), C.c_int64()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    pix_iters = 0
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            info = device_step()
+            L.fp_b200_workspace_stats(ws, C.byref(kl), C.byref(sl))
+            launches += kl.value
+            pix_iters += int(info.image_iters.sum()) * H * W
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    t = ev0.elapsed_time(ev1) / 1e3
+    if world > 1:
+        tt = torch.tensor([t], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        t = float(tt.item())
+    value = world * B * args.steps / t
+    ms_per_step = t / args.steps * 1e3
+    assert info.converged, "benchmark solve did not converge"
+
+    # end to end through host arrays (pinned), copies in the timed region
+    xh = torch.from_numpy(x).pin_memory()
+    oh = torch.empty_like(xh).pin_memory()
+    xn, on = xh.numpy(), oh.numpy()
+    op_host = TVIso(2, pixel_weights=alpha)
+    for _ in range(2):
+        op_host.solve(xn, steps, tol=TOL, max_iter=MAX_ITER, out=on, with_dual=False)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        op_host.solve(xn, steps, tol=TOL, max_iter=MAX_ITER, out=on, with_dual=False)
+    torch.cuda.synchronize(dev)
+    te = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([te], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    e2e = world * B * e2e_steps / te
+
+    peak, peak_kind = peaks()
+    achieved = BYTES_PER_PIXEL_ITER * pix_iters / args.steps / (t / args.steps) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            from oracle import ref_capi
+            if ref_capi.available():
+                v, threads, _ = cpu_reference(x, alpha, steps, 3)
+                cpu = {"value": v, "unit": "images/s", "cores": threads, "kind": "reference",
+                       "sample": "3 of the 64 images (gamma 0.05, 0.1, 0.2), reference C fp_prox_steps, "
+                                 "all host threads"}
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"value": None, "unit": "images/s", "cores": None, "kind": "reference", "sample": f"failed: {e}"}
+    if rank == 0:
+        iters = info.image_iters
+        line = {
+            "metric": "TV-prox images/s at gap<=1e-6 (512^2 fp32)", "value": value, "unit": "images/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "global_batch": B * world, "image": [H, W], "tol": TOL,
+                       "max_iter": MAX_ITER, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (d, u, v: 604 MB per batch)",
+                       "iters_per_image": {"min": int(iters.min()), "median": float(np.median(iters)),
+                                           "max": int(iters.max())}},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "bytes_per_pixel_iter": BYTES_PER_PIXEL_ITER,
+                         "traffic": None},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "images/s", "h2d_bytes_per_step": int(x.nbytes),
+                    "d2h_bytes_per_step": int(x.nbytes)},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1219 @@
+// The extern "C" boundary of libfastprox_b200: argument checks in the order
+// of the reference's prox_impl (src/api/api.cpp:413-559), the device
+// workspace (all device memory allocated at creation), the host loop that
+// drives the per-iteration launches, and per-image results. No exception
+// crosses the boundary (guard), as in the reference (src/api/api.cpp:28-38).
+#include <cuda_runtime_api.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "../../include/fastprox_b200.h"
+#include "engine.h"
+#include "launch.h"
+#include "workspace.h"
+
+using namespace fpb;
+
+namespace {
+
+constexpr double kMaxScaledStep = 0x1p960;  // the reference's step range (core/op.hpp:48)
+
+template <class F>
+fp_status guard(F &&f) noexcept {
+    try {
+        return f();
+    } catch (const std::bad_alloc &) {
+        return FP_ENOMEM;
+    } catch (...) {
+        return FP_EINTERNAL;
+    }
+}
+
+bool finite_nonneg(double v) { return std::isfinite(v) && v >= 0.0; }
+
+// A validated array descriptor (scalars become shape [1]).
+struct Arr {
+    char *data = nullptr;
+    int dtype = 0;
+    int ndim = 0;
+    int device = 0;
+    int64_t shape[FP_MAX_NDIM] = {};
+    int64_t strides[FP_MAX_NDIM] = {};
+    int64_t numel() const {
+        int64_t n = 1;
+        for (int d = 0; d < ndim; ++d) n *= shape[d];
+        return n;
+    }
+    size_t itemsize() const { return dtype == FP_F32 ? 4 : 8; }
+    bool contiguous() const {
+        int64_t s = 1;
+        for (int d = ndim - 1; d >= 0; --d) {
+            if (shape[d] != 1 && strides[d] != s) return false;
+            s *= shape[d];
+        }
+        return true;
+    }
+};
+
+int enum_bits_dtype(const fp_array *a) {
+    int v;
+    std::memcpy(&v, &a->dtype, sizeof v);
+    return v;
+}
+int enum_bits_device(const fp_array *a) {
+    int v;
+    std::memcpy(&v, &a->device, sizeof v);
+    return v;
+}
+
+constexpr int64_t kMaxElems = (int64_t(1) << 60) - 1;
+
+// src/api/api.cpp:57-110: dtype f32/f64, 0 <= ndim <= 32, extents >= 0,
+// the entry count and offset span below 2^60.
+fp_status to_arr(const fp_array *a, Arr &out) {
+    if (!a) return FP_EINVAL;
+    const int dev = enum_bits_device(a);
+    if (dev != FP_DEVICE_CPU && dev != FP_DEVICE_CUDA) return FP_EINVAL;
+    const int dt = enum_bits_dtype(a);
+    if (dt != FP_F32 && dt != FP_F64) return FP_EDTYPE;
+    if (a->ndim < 0 || a->ndim > FP_MAX_NDIM) return FP_ESHAPE;
+    out.data = static_cast<char *>(a->data);
+    out.dtype = dt;
+    out.device = dev;
+    if (a->ndim == 0) {
+        out.ndim = 1;
+        out.shape[0] = 1;
+        out.strides[0] = 1;
+    } else {
+        if (!a->shape) return FP_EINVAL;
+        out.ndim = a->ndim;
+        double count = 1.0;
+        for (int d = 0; d < a->ndim; ++d) {
+            if (a->shape[d] < 0) return FP_ESHAPE;
+            out.shape[d] = a->shape[d];
+            out.strides[d] = a->strides ? a->strides[d] : 0;
+            if (a->shape[d] > 1) count *= (double)a->shape[d];
+        }
+        if (count > (double)kMaxElems) return FP_ESHAPE;
+        if (!a->strides) {
+            int64_t s = 1;
+            for (int d = a->ndim - 1; d >= 0; --d) {
+                out.strides[d] = s;
+                s *= out.shape[d];
+            }
+        }
+        double span = 0.0;
+        for (int d = 0; d < a->ndim; ++d)
+            if (out.shape[d] > 1) span += (double)(out.shape[d] - 1) * (double)std::llabs(out.strides[d]);
+        if (span > (double)kMaxElems) return FP_ESHAPE;
+    }
+    if (!out.data && out.numel() > 0) return FP_EINVAL;
+    return FP_OK;
+}
+
+// The lowest and highest byte an array touches.
+void byte_range(const Arr &a, intptr_t &lo, intptr_t &hi) {
+    intptr_t l = 0, h = 0;
+    for (int d = 0; d < a.ndim; ++d) {
+        if (a.shape[d] < 2) continue;
+        const intptr_t e = (intptr_t)(a.shape[d] - 1) * (intptr_t)a.strides[d] * (intptr_t)a.itemsize();
+        if (e < 0) l += e;
+        else h += e;
+    }
+    lo = (intptr_t)a.data + l;
+    hi = (intptr_t)a.data + h + (intptr_t)a.itemsize() - 1;
+}
+
+// src/api/api.cpp check_output: out may be x itself; any other overlap, or a
+// stride 0 on an extent > 1 in out, is FP_EINVAL.
+fp_status check_output(const Arr *x, const Arr &out) {
+    if (out.numel() == 0) return FP_OK;
+    for (int d = 0; d < out.ndim; ++d)
+        if (out.shape[d] > 1 && out.strides[d] == 0) return FP_EINVAL;
+    if (!x || out.numel() == 0 || x->numel() == 0) return FP_OK;
+    bool same = x->data == out.data && x->ndim == out.ndim && x->dtype == out.dtype;
+    for (int d = 0; same && d < x->ndim; ++d)
+        same = x->shape[d] == out.shape[d] && (x->shape[d] < 2 || x->strides[d] == out.strides[d]);
+    if (same) return FP_OK;
+    intptr_t xl, xh, ol, oh;
+    byte_range(*x, xl, xh);
+    byte_range(out, ol, oh);
+    return (oh < xl || ol > xh) ? FP_OK : FP_EINVAL;
+}
+
+bool same_shape(const Arr &a, const Arr &b) {
+    if (a.ndim != b.ndim) return false;
+    for (int d = 0; d < a.ndim; ++d)
+        if (a.shape[d] != b.shape[d]) return false;
+    return true;
+}
+
+// A one-dimensional host parameter array of any float dtype and stride.
+fp_status read_vec(const fp_array *a, std::vector<double> &v) {
+    v.clear();
+    if (!a) return FP_OK;
+    Arr x;
+    if (fp_status s = to_arr(a, x)) return s;
+    if (x.device != FP_DEVICE_CPU) return FP_EINVAL;
+    if (a->ndim > 1) return FP_ESHAPE;
+    const int64_t m = x.shape[0];
+    if (m == 0) return FP_ESHAPE;
+    v.resize((size_t)m);
+    for (int64_t i = 0; i < m; ++i) {
+        const char *p = x.data + i * x.strides[0] * (int64_t)x.itemsize();
+        v[(size_t)i] = x.dtype == FP_F32 ? (double)*reinterpret_cast<const float *>(p) : *reinterpret_cast<const double *>(p);
+    }
+    return FP_OK;
+}
+
+// An n-d host parameter array of exactly nd axes, copied in C order.
+fp_status read_nd(const fp_array *a, int nd, std::vector<double> &v, int64_t *shape) {
+    Arr x;
+    if (fp_status s = to_arr(a, x)) return s;
+    if (x.device != FP_DEVICE_CPU) return FP_EINVAL;
+    if (a->ndim != nd) return FP_ESHAPE;
+    const int64_t n = x.numel();
+    if (n == 0) return FP_ESHAPE;
+    for (int d = 0; d < nd; ++d) shape[d] = x.shape[d];
+    v.resize((size_t)n);
+    std::vector<int64_t> idx((size_t)nd, 0);
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t off = 0;
+        for (int d = 0; d < nd; ++d) off += idx[(size_t)d] * x.strides[d];
+        const char *p = x.data + off * (int64_t)x.itemsize();
+        v[(size_t)i] = x.dtype == FP_F32 ? (double)*reinterpret_cast<const float *>(p) : *reinterpret_cast<const double *>(p);
+        for (int d = nd - 1; d >= 0; --d) {
+            if (++idx[(size_t)d] < x.shape[d]) break;
+            idx[(size_t)d] = 0;
+        }
+    }
+    return FP_OK;
+}
+
+fp_options defaults() {
+    fp_options o;
+    o.axis = -1;
+    o.threads = 0;
+    o.tol = 1e-6;
+    o.max_iter = 1000;
+    o.tie = 0;
+    o.keep_structure = 0;
+    return o;
+}
+
+// Restores the caller's current device on scope exit.
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceScope() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// The device an array lives on (-1: host or unknown).
+int pointer_device(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) return at.device;
+    return -1;
+}
+
+bool host_pinned(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Operators
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+FP_API void fp_options_init(fp_options *opt) {
+    if (opt) *opt = defaults();
+}
+
+}  // extern "C"
+
+namespace {
+
+// tv_iso.cpp:1072-1095 and tv_aniso.cpp make_tv_aniso: the parameter rules.
+fp_status make_tv(int kind, int ndim, const std::vector<double> &w, std::vector<double> spatial,
+                  const int64_t *sshape, fp_op **out) {
+    if (ndim != 2 && ndim != 3) return FP_EPARAM;
+    double ww[3] = {1.0, 1.0, 1.0};
+    if (w.size() == 1) {
+        for (int a = 0; a < ndim; ++a) ww[a] = w[0];
+    } else if (!w.empty()) {
+        if ((int)w.size() != ndim) return FP_ESHAPE;
+        for (int a = 0; a < ndim; ++a) ww[a] = w[(size_t)a];
+    }
+    for (int a = 0; a < ndim; ++a)
+        if (!finite_nonneg(ww[a])) return FP_EPARAM;
+    if (!spatial.empty()) {
+        double n = 1.0;
+        for (int a = 0; a < ndim; ++a) n *= (double)sshape[a];
+        if (!(n < 2147483647.0)) return FP_ESHAPE;
+        for (double v : spatial)
+            if (!finite_nonneg(v)) return FP_EPARAM;
+    }
+    auto op = std::make_unique<fp_op>();
+    op->kind = kind;
+    op->k = ndim;
+    for (int a = 0; a < 3; ++a) op->w[a] = a < ndim ? ww[a] : 0.0;
+    op->spatial = std::move(spatial);
+    for (int a = 0; a < 3; ++a) op->sshape[a] = (sshape && a < ndim) ? sshape[a] : 1;
+    op->smax = 0.0;
+    for (double v : op->spatial) op->smax = std::max(op->smax, v);
+    *out = op.release();
+    return FP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+FP_API fp_status fp_op_tv_iso(int ndim, const fp_array *axis_weights, fp_op **out) {
+    return guard([&] {
+        if (!out) return FP_EINVAL;
+        *out = nullptr;
+        std::vector<double> w;
+        if (fp_status s = read_vec(axis_weights, w)) return s;
+        return make_tv(kIso, ndim, w, {}, nullptr, out);
+    });
+}
+
+FP_API fp_status fp_op_tv_aniso(int ndim, const fp_array *axis_weights, fp_op **out) {
+    return guard([&] {
+        if (!out) return FP_EINVAL;
+        *out = nullptr;
+        std::vector<double> w;
+        if (fp_status s = read_vec(axis_weights, w)) return s;
+        return make_tv(kAniso, ndim, w, {}, nullptr, out);
+    });
+}
+
+FP_API fp_status fp_op_tv_iso_weighted(int ndim, const fp_array *axis_weights, const fp_array *pixel_weights,
+                                       fp_op **out) {
+    return guard([&] {
+        if (!out) return FP_EINVAL;
+        *out = nullptr;
+        if (!pixel_weights) return FP_EINVAL;
+        if (ndim != 2 && ndim != 3) return FP_EPARAM;
+        std::vector<double> w, al;
+        int64_t shape[3] = {1, 1, 1};
+        if (fp_status s = read_vec(axis_weights, w)) return s;
+        if (fp_status s = read_nd(pixel_weights, ndim, al, shape)) return s;
+        return make_tv(kIso, ndim, w, std::move(al), shape, out);
+    });
+}
+
+FP_API fp_status fp_op_tv_aniso_weighted(int ndim, const fp_array *axis_weights, const fp_array *edge_weights,
+                                         fp_op **out) {
+    return guard([&] {
+        if (!out) return FP_EINVAL;
+        *out = nullptr;
+        if (!edge_weights) return FP_EINVAL;
+        if (ndim != 2 && ndim != 3) return FP_EPARAM;
+        std::vector<double> w, b;
+        int64_t shape[4] = {1, 1, 1, 1};
+        if (fp_status s = read_vec(axis_weights, w)) return s;
+        if (fp_status s = read_nd(edge_weights, ndim + 1, b, shape)) return s;
+        if (shape[0] != ndim) return FP_ESHAPE;
+        return make_tv(kAniso, ndim, w, std::move(b), shape + 1, out);
+    });
+}
+
+FP_API void fp_op_free(fp_op *op) { delete op; }
+
+FP_API int64_t fp_op_nparams(const fp_op *op) {
+    if (!op) return 0;
+    return op->k + (int64_t)op->spatial.size();
+}
+
+FP_API const char *fp_op_name(const fp_op *op) {
+    if (!op) return "";
+    return op->kind == kIso ? "tv_iso" : "tv_aniso";
+}
+
+FP_API int fp_device_available(fp_device dev) {
+    int n = 0;
+    const int d = (int)dev;
+    if (d != FP_DEVICE_CPU && d != FP_DEVICE_CUDA) return 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n > 0 ? 1 : 0;
+}
+
+FP_API fp_status fp_op_device_check(const fp_op *op, fp_device dev, int *row_parallel_only) {
+    if (!op) return FP_EINVAL;
+    if (row_parallel_only) *row_parallel_only = 0;
+    return fp_device_available(dev) ? FP_OK : FP_EINVAL;
+}
+
+FP_API const char *fp_strerror(fp_status s) {
+    switch ((int)s) {
+    case FP_OK: return "success";
+    case FP_EINVAL: return "invalid argument";
+    case FP_EDTYPE: return "unsupported or mismatched dtype";
+    case FP_ESHAPE: return "mismatched shapes or parameter lengths";
+    case FP_ENOMEM: return "out of memory";
+    case FP_ENOTCONV: return "iterative operator did not converge";
+    case FP_EPARAM: return "invalid operator parameter or step";
+    case FP_EINTERNAL: return "internal error";
+    case FP_EDEVICE: return "device error";
+    default: return "unknown status";
+    }
+}
+
+FP_API int fp_abi_version(void) { return FP_ABI_VERSION; }
+FP_API const char *fp_version_string(void) { return "1.0.6+b200"; }
+FP_API int fp_default_threads(void) { return 1; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Workspaces
+// ---------------------------------------------------------------------------
+
+namespace {
+
+void free_ws_memory(fp_workspace *ws) {
+    DeviceScope ds(ws->device);
+    for (void *p : ws->dev_allocs) cudaFree(p);
+    ws->dev_allocs.clear();
+    for (void *p : ws->host_allocs) cudaFreeHost(p);
+    ws->host_allocs.clear();
+    for (int i = 0; i < 2; ++i)
+        if (ws->ev[i]) cudaEventDestroy(ws->ev[i]);
+    ws->ev[0] = ws->ev[1] = nullptr;
+}
+
+fp_status dev_alloc(fp_workspace *ws, void **p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return FP_ENOMEM;
+    }
+    ws->dev_allocs.push_back(*p);
+    return FP_OK;
+}
+
+fp_status host_alloc(fp_workspace *ws, void **p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cudaHostAlloc(p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return FP_ENOMEM;
+    }
+    ws->host_allocs.push_back(*p);
+    return FP_OK;
+}
+
+// The image plan of x: leading axes are the batch, the last k the image.
+fp_status image_geometry(const fp_op &op, const Arr &x, Geometry &g) {
+    const int k = op.k;
+    if (x.ndim < k) return FP_ESHAPE;
+    g.k = k;
+    g.N = 1;
+    for (int a = 0; a < 3; ++a) g.L[a] = 1;
+    for (int a = 0; a < k; ++a) {
+        g.L[a] = x.shape[x.ndim - k + a];
+        g.N *= g.L[a];
+    }
+    g.B = 1;
+    for (int d = 0; d < x.ndim - k; ++d) g.B *= x.shape[d];
+    return FP_OK;
+}
+
+// tv_iso.cpp:170-177: 32-bit region labels, and the shape of spatial weights.
+fp_status check_image(const fp_op &op, const Arr &x) {
+    const int k = op.k;
+    double n = 1.0;
+    for (int a = 0; a < k; ++a) n *= (double)x.shape[x.ndim - k + a];
+    if (!op.spatial.empty())
+        for (int a = 0; a < k; ++a)
+            if (x.shape[x.ndim - k + a] != op.sshape[a]) return FP_ESHAPE;
+    return n < 2147483647.0 ? FP_OK : FP_ESHAPE;
+}
+
+fp_status cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return FP_OK;
+    if (e == cudaErrorMemoryAllocation) return FP_ENOMEM;
+    return FP_EDEVICE;
+}
+
+}  // namespace
+
+fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o, int device, fp_workspace **out) {
+    Geometry g;
+    if (fp_status s = image_geometry(*op, x, g)) return s;
+    auto ws = std::make_unique<fp_workspace>();
+    ws->op = op;
+    ws->device = device;
+    ws->dtype = x.dtype;
+    ws->ndim = x.ndim;
+    for (int d = 0; d < x.ndim; ++d) ws->shape[d] = x.shape[d];
+    ws->g = g;
+    ws->host_mode = x.device == FP_DEVICE_CPU;
+    ws->keep = o.keep_structure != 0;
+    DeviceScope dsc(device);
+    const size_t T = x.dtype == FP_F32 ? 4 : 8;
+    const int64_t B = std::max<int64_t>(g.B, 1), N = std::max<int64_t>(g.N, 1);
+    const size_t img = (size_t)B * (size_t)N * T;
+    const size_t dualb = img * (size_t)g.k;
+    fp_status s = FP_OK;
+    auto A = [&](void **p, size_t bytes) {
+        if (s == FP_OK) s = dev_alloc(ws.get(), p, bytes);
+    };
+    A(&ws->d, img);
+    A(&ws->stage, img);  // strided or conjugate inputs, strided outputs
+    for (int i = 0; i < 2; ++i) {
+        A(&ws->U[i], dualb);
+        A(&ws->V[i], dualb);
+    }
+    A(&ws->dual, dualb);
+    if (!op->spatial.empty()) {
+        A(&ws->spatial, op->spatial.size() * T);
+        if (s == FP_OK) {
+            std::vector<char> tmp(op->spatial.size() * T);
+            for (size_t i = 0; i < op->spatial.size(); ++i) {
+                if (T == 4) reinterpret_cast<float *>(tmp.data())[i] = (float)op->spatial[i];
+                else reinterpret_cast<double *>(tmp.data())[i] = op->spatial[i];
+            }
+            if (cudaMemcpy(ws->spatial, tmp.data(), tmp.size(), cudaMemcpyHostToDevice) != cudaSuccess) s = FP_EDEVICE;
+        }
+    }
+    // per-image state, partials and tickets
+    ws->shape_ = iso_pick_shape(x.dtype, g, 0, 0);
+    ws->max_part = std::max(iso_setup_blocks(g), ws->shape_.gx * ws->shape_.gy);
+    ws->max_part = std::max(ws->max_part, 4096);
+    A((void **)&ws->img, (size_t)B * sizeof(IsoImage));
+    A((void **)&ws->st, (size_t)B * sizeof(IsoState));
+    A((void **)&ws->gammas, (size_t)B * sizeof(double));
+    A((void **)&ws->part, (size_t)B * (size_t)ws->max_part * 2 * sizeof(double));
+    A((void **)&ws->ticket, (size_t)B * sizeof(unsigned));
+    A((void **)&ws->live, 16);
+    auto H = [&](void **p, size_t bytes) {
+        if (s == FP_OK) s = host_alloc(ws.get(), p, bytes);
+    };
+    H((void **)&ws->h_live, 4 * sizeof(int));
+    H((void **)&ws->h_img, (size_t)B * sizeof(IsoImage));
+    H((void **)&ws->h_st, (size_t)B * sizeof(IsoState));
+    H((void **)&ws->h_gam, (size_t)B * sizeof(double));
+    if (ws->host_mode) H(&ws->h_stage, img);
+    if (s == FP_OK && cudaMemset(ws->ticket, 0, (size_t)B * sizeof(unsigned)) != cudaSuccess) s = FP_EDEVICE;
+    for (int i = 0; i < 2 && s == FP_OK; ++i)
+        if (cudaEventCreateWithFlags(&ws->ev[i], cudaEventDisableTiming) != cudaSuccess) s = FP_EDEVICE;
+    if (s == FP_OK && cudaDeviceSynchronize() != cudaSuccess) s = FP_EDEVICE;
+    if (s != FP_OK) {
+        cudaGetLastError();
+        free_ws_memory(ws.get());
+        return s;
+    }
+    ws->gaps.assign((size_t)B, 0.0);
+    ws->zerrs.assign((size_t)B, 0.0);
+    ws->iters.assign((size_t)B, 0);
+    *out = ws.release();
+    return FP_OK;
+}
+
+extern "C" {
+
+FP_API fp_status fp_workspace_create(const fp_op *op, const fp_array *like, const fp_options *opt,
+                                     fp_workspace **out) {
+    return guard([&] {
+        if (!out) return FP_EINVAL;
+        *out = nullptr;
+        if (!op || !like) return FP_EINVAL;
+        const fp_options o = opt ? *opt : defaults();
+        Arr x;
+        if (fp_status s = to_arr(like, x)) return s;
+        if (x.ndim < op->k) return FP_ESHAPE;
+        if (x.numel() != 0)
+            if (fp_status s = check_image(*op, x)) return s;
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            return FP_EDEVICE;
+        }
+        int device = 0;
+        if (x.device == FP_DEVICE_CUDA) {
+            device = x.data ? pointer_device(x.data) : -1;
+            if (device < 0) {
+                if (x.data) return FP_EINVAL;  // not device memory
+                cudaGetDevice(&device);
+            }
+        } else {
+            cudaGetDevice(&device);
+        }
+        return fpb_workspace_build(op, x, o, device, out);
+    });
+}
+
+FP_API void fp_workspace_free(fp_workspace *ws) {
+    if (!ws) return;
+    free_ws_memory(ws);
+    delete ws;
+}
+
+FP_API fp_status fp_workspace_set_stream(fp_workspace *ws, void *stream) {
+    if (!ws) return FP_EINVAL;
+    if (ws->host_mode) return FP_EINVAL;
+    ws->stream = static_cast<cudaStream_t>(stream);
+    return FP_OK;
+}
+
+FP_API fp_status fp_workspace_get_stream(const fp_workspace *ws, void **stream) {
+    if (!ws || !stream) return FP_EINVAL;
+    if (ws->host_mode) return FP_EINVAL;
+    *stream = ws->stream;
+    return FP_OK;
+}
+
+FP_API fp_status fp_workspace_set_warm(fp_workspace *ws, int on) {
+    if (!ws) return FP_EINVAL;
+    ws->warm = on != 0;
+    return FP_OK;
+}
+
+FP_API fp_status fp_workspace_set_deriv_tol(fp_workspace *ws, double tol, int max_iter) {
+    if (!ws) return FP_EINVAL;
+    if (!(tol >= 0.0) || !std::isfinite(tol) || max_iter < 1) return FP_EPARAM;
+    ws->deriv_tol = tol;
+    ws->deriv_max_iter = max_iter;
+    return FP_OK;
+}
+
+FP_API fp_status fp_workspace_deriv_info(const fp_workspace *ws, double *residual, int *iters) {
+    if (!ws) return FP_EINVAL;
+    if (residual) *residual = ws->deriv_residual;
+    if (iters) *iters = ws->deriv_iters;
+    return FP_OK;
+}
+
+FP_API fp_status fp_workspace_info(const fp_workspace *ws, fp_info *info) {
+    if (!ws || !info) return FP_EINVAL;
+    if (!ws->info_valid) return FP_EINVAL;
+    *info = ws->info;
+    return ws->info_status;
+}
+
+FP_API fp_status fp_workspace_image_info(const fp_workspace *ws, double *gaps, int *iters, double *zerrs,
+                                         int64_t count) {
+    if (!ws) return FP_EINVAL;
+    if (!ws->info_valid) return FP_EINVAL;
+    if (count != ws->g.B) return FP_ESHAPE;
+    for (int64_t i = 0; i < count; ++i) {
+        if (gaps) gaps[i] = ws->gaps[(size_t)i];
+        if (iters) iters[i] = ws->iters[(size_t)i];
+        if (zerrs) zerrs[i] = ws->zerrs[(size_t)i];
+    }
+    return FP_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The dual: get, set (src/api/api.cpp dual_impl; fastprox.h:415-428)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+fp_status dual_io(fp_workspace *ws, const fp_array *arr, bool set) {
+    if (!ws || !arr) return FP_EINVAL;
+    Arr a;
+    if (fp_status s = to_arr(arr, a)) return s;
+    // shape (k, *x.shape)
+    if (a.ndim != ws->ndim + 1 || a.shape[0] != ws->g.k) return FP_ESHAPE;
+    for (int d = 0; d < ws->ndim; ++d)
+        if (a.shape[d + 1] != ws->shape[d]) return FP_ESHAPE;
+    if (!set && !ws->dual_valid) return FP_EINVAL;
+    const int64_t n = a.numel();
+    if (n == 0) {
+        if (set) {
+            ws->seeded = true;
+            ws->dual_valid = true;
+        }
+        return FP_OK;
+    }
+    DeviceScope dsc(ws->device);
+    const size_t T = ws->dtype == FP_F32 ? 4 : 8;
+    int64_t cst[FP_MAX_NDIM];
+    {
+        int64_t s = 1;
+        for (int d = a.ndim - 1; d >= 0; --d) {
+            cst[d] = s;
+            s *= a.shape[d];
+        }
+    }
+    cudaStream_t st = ws->stream;
+    if (a.device == FP_DEVICE_CUDA) {
+        if (pointer_device(a.data) != ws->device) return FP_EINVAL;
+        if (set) {
+            // Inf entries are rejected, NaN entries stored as 0.
+            std::vector<char> hostcopy((size_t)n * a.itemsize());
+            cudaError_t e = cudaSuccess;
+            if (a.contiguous()) {
+                e = cudaMemcpyAsync(ws->dual, a.data, (size_t)n * T, cudaMemcpyDeviceToDevice, st);
+                if (a.dtype != ws->dtype) {
+                    e = strided_copy(a.data, a.dtype, a.shape, a.strides, a.ndim, ws->dual, ws->dtype, cst, st);
+                }
+            } else {
+                e = strided_copy(a.data, a.dtype, a.shape, a.strides, a.ndim, ws->dual, ws->dtype, cst, st);
+            }
+            if (e != cudaSuccess) return cuda_status(e);
+            // validate on the host
+            std::vector<char> h((size_t)n * T);
+            if (cudaMemcpyAsync(h.data(), ws->dual, h.size(), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return FP_EDEVICE;
+            bool bad = false;
+            for (int64_t i = 0; i < n; ++i) {
+                double v = T == 4 ? (double)reinterpret_cast<float *>(h.data())[i] : reinterpret_cast<double *>(h.data())[i];
+                if (std::isinf(v)) bad = true;
+                if (std::isnan(v)) {
+                    if (T == 4) reinterpret_cast<float *>(h.data())[i] = 0.0f;
+                    else reinterpret_cast<double *>(h.data())[i] = 0.0;
+                }
+            }
+            if (bad) return FP_EINVAL;
+            if (cudaMemcpy(ws->dual, h.data(), h.size(), cudaMemcpyHostToDevice) != cudaSuccess) return FP_EDEVICE;
+            ws->seeded = true;
+            ws->dual_valid = true;
+            return FP_OK;
+        }
+        cudaError_t e = strided_copy(ws->dual, ws->dtype, a.shape, cst, a.ndim, a.data, a.dtype, a.strides, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        return cuda_status(e);
+    }
+    // host array
+    std::vector<char> h((size_t)n * T);
+    if (set) {
+        std::vector<int64_t> idx((size_t)a.ndim, 0);
+        bool bad = false;
+        for (int64_t i = 0; i < n; ++i) {
+            int64_t off = 0;
+            for (int d = 0; d < a.ndim; ++d) off += idx[(size_t)d] * a.strides[d];
+            const char *p = a.data + off * (int64_t)a.itemsize();
+            double v = a.dtype == FP_F32 ? (double)*reinterpret_cast<const float *>(p) : *reinterpret_cast<const double *>(p);
+            if (std::isinf(v)) bad = true;
+            if (std::isnan(v)) v = 0.0;
+            if (T == 4) reinterpret_cast<float *>(h.data())[i] = (float)v;
+            else reinterpret_cast<double *>(h.data())[i] = v;
+            for (int d = a.ndim - 1; d >= 0; --d) {
+                if (++idx[(size_t)d] < a.shape[d]) break;
+                idx[(size_t)d] = 0;
+            }
+        }
+        if (bad) return FP_EINVAL;
+        if (cudaStreamSynchronize(st) != cudaSuccess) return FP_EDEVICE;
+        if (cudaMemcpy(ws->dual, h.data(), h.size(), cudaMemcpyHostToDevice) != cudaSuccess) return FP_EDEVICE;
+        ws->seeded = true;
+        ws->dual_valid = true;
+        return FP_OK;
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return FP_EDEVICE;
+    if (cudaMemcpy(h.data(), ws->dual, h.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return FP_EDEVICE;
+    std::vector<int64_t> idx((size_t)a.ndim, 0);
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t off = 0;
+        for (int d = 0; d < a.ndim; ++d) off += idx[(size_t)d] * a.strides[d];
+        char *p = a.data + off * (int64_t)a.itemsize();
+        const double v = T == 4 ? (double)reinterpret_cast<float *>(h.data())[i] : reinterpret_cast<double *>(h.data())[i];
+        if (a.dtype == FP_F32) *reinterpret_cast<float *>(p) = (float)v;
+        else *reinterpret_cast<double *>(p) = v;
+        for (int d = a.ndim - 1; d >= 0; --d) {
+            if (++idx[(size_t)d] < a.shape[d]) break;
+            idx[(size_t)d] = 0;
+        }
+    }
+    return FP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+FP_API fp_status fp_workspace_get_dual(const fp_workspace *ws, fp_array *out) {
+    return guard([&] { return dual_io(const_cast<fp_workspace *>(ws), out, false); });
+}
+
+FP_API fp_status fp_workspace_set_dual(fp_workspace *ws, const fp_array *dual) {
+    return guard([&] { return dual_io(ws, dual, true); });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// prox
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// Per-image certified relative error of the returned z (driver.hpp:1187-1237):
+// r + round (u (1 + r) + a / |x|), r = sqrt(2 gap) / |x|, at the solved scale.
+double certified_error(double gap_s, double dd_s, int64_t N, int e, int dtype, int round) {
+    if (std::isnan(gap_s)) return gap_s;
+    if (!(dd_s > 0.0)) return 0.0;
+    const double u = 0.5 * (dtype == FP_F32 ? (double)std::numeric_limits<float>::epsilon()
+                                            : std::numeric_limits<double>::epsilon());
+    const double eta = 0.5 * (dtype == FP_F32 ? (double)std::numeric_limits<float>::denorm_min()
+                                              : std::numeric_limits<double>::denorm_min());
+    const double n = std::sqrt(dd_s);
+    const double r = std::sqrt(2.0 * std::max(gap_s, 0.0)) / n;
+    const double a = std::ldexp(eta, -e) * std::sqrt((double)N) / n;
+    return r + round * (u * (1.0 + r) + a);
+}
+
+fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zdst, double tol, int max_iter,
+                  bool warm) {
+    const Geometry &g = ws->g;
+    cudaStream_t s = ws->stream;
+    IsoCall c{};
+    // Active axes (tv_iso.cpp:350-358) for a positive step
+    double wmax_all = 0.0;
+    for (int a = 0; a < g.k; ++a)
+        if (g.L[a] > 1) wmax_all = std::max(wmax_all, op->w[a]);
+    double wa[3] = {0.0, 0.0, 0.0};
+    int na = 0, act = -1;
+    for (int a = 0; a < g.k; ++a)
+        if (op->w[a] > 0.0 && g.L[a] > 1 && op->w[a] >= 1e-100 * wmax_all) {
+            wa[a] = op->w[a];
+            ++na;
+            act = a;
+        }
+    c.na = na;
+    c.act_axis = act < 0 ? 0 : act;
+    c.w_act = act < 0 ? 1.0 : op->w[act];
+    double wmax = 0.0;
+    for (int a = 0; a < g.k; ++a) wmax = std::max(wmax, wa[a]);
+    c.wmax = wmax > 0.0 ? wmax : 1.0;
+    double whmin = 1.0, L2 = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        c.wh[a] = (a < g.k && wa[a] != 0.0) ? wa[a] / c.wmax : 0.0;
+        if (a < g.k && wa[a] != 0.0) whmin = std::min(whmin, c.wh[a]);
+        L2 += 4.0 * c.wh[a] * c.wh[a];
+    }
+    c.whmin = whmin;
+    c.tau = L2 > 0.0 ? 1.0 / L2 : 0.0;
+    c.tol = tol;
+    c.max_iter = max_iter;
+    c.has_alpha = op->spatial.empty() ? 0 : 1;
+    c.alpha_stride = 0;
+    c.alpha_max = op->smax;
+    c.step_scale = std::max({op->w[0], op->w[1], op->w[2]}) * (op->spatial.empty() ? 1.0 : op->smax);
+
+    IsoBuffers bf;
+    bf.d = ws->d;
+    for (int i = 0; i < 2; ++i) {
+        bf.U[i] = ws->U[i];
+        bf.V[i] = ws->V[i];
+    }
+    bf.dual = ws->dual;
+    bf.alpha = ws->spatial;
+    bf.img = ws->img;
+    bf.st = ws->st;
+    bf.gammas = ws->gammas;
+    bf.part = ws->part;
+    bf.ticket = ws->ticket;
+    bf.live = ws->live;
+    bf.max_part = ws->max_part;
+
+    cudaError_t e = cudaMemsetAsync(ws->live, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = iso_setup(ws->dtype, g, c, bf, xsrc, warm ? 1 : 0, 0, s);
+    if (e != cudaSuccess) return cuda_status(e);
+    // The iteration: chunks of launches, each followed by a read of the live
+    // count; two chunks in flight so the device never waits for the host.
+    const int chunk = ws->chunk > 0 ? ws->chunk : 8;
+    int par = 0, slot = 0, inflight = 0;
+    int64_t launched = 0;
+    const int64_t cap = (int64_t)max_iter + 1 + 2 * chunk;
+    bool done = false;
+    while (!done) {
+        for (int j = 0; j < chunk; ++j) {
+            e = iso_step(ws->dtype, g, c, bf, ws->shape_, par, s);
+            if (e != cudaSuccess) return cuda_status(e);
+            par ^= 1;
+            ++launched;
+        }
+        e = cudaMemcpyAsync(ws->h_live + slot, ws->live, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaEventRecord(ws->ev[slot], s);
+        if (e != cudaSuccess) return cuda_status(e);
+        slot ^= 1;
+        ++inflight;
+        if (inflight == 2) {
+            e = cudaEventSynchronize(ws->ev[slot]);
+            if (e != cudaSuccess) return cuda_status(e);
+            --inflight;
+            if (ws->h_live[slot] == 0) done = true;
+        }
+        if (launched >= cap) done = true;
+    }
+    ws->launches = launched;
+    ws->kernel_launches += launched + 3 + (warm ? 1 : 0) + 1 + ((c.na == 1 && !c.has_alpha) ? 1 : 0);
+    e = iso_finalize(ws->dtype, g, c, bf, zdst, s);
+    return cuda_status(e);
+}
+
+fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *oa, const fp_options *opt,
+                    fp_workspace *ws, fp_info *info, bool conj, const fp_array *sa) {
+    if (!op || !xa || !oa) return FP_EINVAL;
+    if (!std::isfinite(step) || step < 0) return FP_EPARAM;
+    const fp_options o = opt ? *opt : defaults();
+    if (o.tie != 0 && o.tie != 1) return FP_EINVAL;
+    Arr x, out;
+    if (fp_status s = to_arr(xa, x)) return s;
+    if (fp_status s = to_arr(oa, out)) return s;
+    if (x.dtype != out.dtype) return FP_EDTYPE;
+    if (!same_shape(x, out)) return FP_ESHAPE;
+    if (x.device != out.device) return FP_EINVAL;
+    if (fp_status s = check_output(&x, out)) return s;
+    const bool keep = o.keep_structure != 0;
+    if (keep && !ws) return FP_EINVAL;
+    if (ws) {
+        if (ws->op != op || ws->dtype != x.dtype || ws->ndim != x.ndim) return FP_EINVAL;
+        for (int d = 0; d < x.ndim; ++d)
+            if (ws->shape[d] != x.shape[d]) return FP_ESHAPE;
+        if (keep && !ws->keep) return FP_EINVAL;
+        if (ws->host_mode != (x.device == FP_DEVICE_CPU)) return FP_EINVAL;
+    }
+    if (info) {
+        info->gap = 0.0;
+        info->iters = 0;
+        info->ties = 0;
+    }
+    const int k = op->k;
+    if (x.ndim < k) return FP_ESHAPE;
+    if (!(o.tol >= 0.0) || !std::isfinite(o.tol) || o.max_iter < 1) return FP_EPARAM;
+    const double step_scale = std::max({op->w[0], op->w[1], op->w[2]}) * (op->spatial.empty() ? 1.0 : op->smax);
+    const bool identity = conj && step == 0.0;
+    const double gamma = conj ? 1.0 : step;  // TV is positively homogeneous (api.cpp:463-469)
+    Arr st;
+    Geometry g0;
+    if (fp_status s = image_geometry(*op, x, g0)) return s;
+    std::vector<double> host_steps;
+    bool device_steps = false;
+    if (sa) {
+        if (fp_status s = to_arr(sa, st)) return s;
+        if (sa->ndim != x.ndim - k) return FP_ESHAPE;
+        for (int d = 0; d < sa->ndim; ++d)
+            if (st.shape[d] != x.shape[d]) return FP_ESHAPE;
+        if (fp_status s = check_output(&st, out)) return s;
+        // every step checked before any work
+        const int64_t B = g0.B;
+        host_steps.resize((size_t)B);
+        if (st.device == FP_DEVICE_CPU) {
+            std::vector<int64_t> idx((size_t)std::max(1, (int)sa->ndim), 0);
+            for (int64_t i = 0; i < B; ++i) {
+                int64_t off = 0;
+                for (int d = 0; d < sa->ndim; ++d) off += idx[(size_t)d] * st.strides[d];
+                const char *p = st.data + off * (int64_t)st.itemsize();
+                host_steps[(size_t)i] = st.dtype == FP_F32 ? (double)*reinterpret_cast<const float *>(p)
+                                                           : *reinterpret_cast<const double *>(p);
+                for (int d = sa->ndim - 1; d >= 0; --d) {
+                    if (++idx[(size_t)d] < st.shape[d]) break;
+                    idx[(size_t)d] = 0;
+                }
+            }
+        } else {
+            device_steps = true;  // read into the workspace below, checked before any work
+        }
+        if (!device_steps)
+            for (double v : host_steps) {
+                if (!std::isfinite(v) || v < 0) return FP_EPARAM;
+                if (step_scale > 0.0 && !(v * step_scale <= kMaxScaledStep)) return FP_EPARAM;
+            }
+    } else if (!identity && step_scale > 0.0 && !(gamma * step_scale <= kMaxScaledStep)) {
+        return FP_EPARAM;
+    }
+    if (x.numel() != 0)
+        if (fp_status s = check_image(*op, x)) return s;
+    if (ws) {
+        ws->valid = false;
+        ws->info_valid = false;
+    }
+    if (x.numel() == 0) {
+        if (ws) {
+            ws->dual_valid = true;
+            ws->info = fp_info{0.0, 0, 0};
+            ws->info_status = FP_OK;
+            ws->info_valid = true;
+        }
+        return FP_OK;
+    }
+    // The device: the workspace's, or that of the arrays.
+    std::unique_ptr<fp_workspace, void (*)(fp_workspace *)> local(nullptr, fp_workspace_free);
+    if (!ws) {
+        int device = 0;
+        if (x.device == FP_DEVICE_CUDA) {
+            device = pointer_device(x.data);
+            if (device < 0) return FP_EINVAL;
+        } else {
+            int n = 0;
+            if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+                cudaGetLastError();
+                return FP_EDEVICE;
+            }
+            cudaGetDevice(&device);
+        }
+        fp_workspace *w = nullptr;
+        if (fp_status s = fpb_workspace_build(op, x, o, device, &w)) return s;
+        local.reset(w);
+        ws = w;
+    }
+    DeviceScope dsc(ws->device);
+    if (x.device == FP_DEVICE_CUDA) {
+        if (pointer_device(x.data) != ws->device || pointer_device(out.data) != ws->device) return FP_EINVAL;
+    }
+    if (op->kind != kIso) return FP_EINVAL;  // anisotropic TV: see aniso.cu
+    if (device_steps) {
+        // the steps into the workspace (as doubles), read back and checked
+        if (pointer_device(st.data) != ws->device) return FP_EINVAL;
+        int64_t one[FP_MAX_NDIM];
+        int64_t sz = 1;
+        for (int d = sa->ndim - 1; d >= 0; --d) {
+            one[d] = sz;
+            sz *= st.shape[d];
+        }
+        cudaError_t e0 = strided_copy(st.data, st.dtype, st.shape, st.strides, std::max(1, sa->ndim), ws->gammas,
+                                      FP_F64, one, ws->stream);
+        if (e0 == cudaSuccess)
+            e0 = cudaMemcpyAsync(ws->h_gam, ws->gammas, (size_t)ws->g.B * sizeof(double), cudaMemcpyDeviceToHost,
+                                 ws->stream);
+        if (e0 == cudaSuccess) e0 = cudaStreamSynchronize(ws->stream);
+        if (e0 != cudaSuccess) return cuda_status(e0);
+        host_steps.assign(ws->h_gam, ws->h_gam + ws->g.B);
+        for (double v : host_steps) {
+            if (!std::isfinite(v) || v < 0) return FP_EPARAM;
+            if (step_scale > 0.0 && !(v * step_scale <= kMaxScaledStep)) return FP_EPARAM;
+        }
+    }
+    cudaStream_t s = ws->stream;
+    const Geometry &g = ws->g;
+    const size_t T = x.itemsize();
+    const int64_t total = g.B * g.N;
+    int64_t cst[FP_MAX_NDIM];
+    {
+        int64_t sz = 1;
+        for (int d = x.ndim - 1; d >= 0; --d) {
+            cst[d] = sz;
+            sz *= x.shape[d];
+        }
+    }
+    ws->kernel_launches = 1;  // the steps fill (or strided copies, counted below)
+    cudaError_t e = cudaSuccess;
+    // Stage x: the kernels read a contiguous batch. The conjugate keeps y
+    // in the staging buffer for out = y - z.
+    const void *xsrc = nullptr;
+    const void *ysave = nullptr;
+    if (ws->host_mode) {
+        if (x.contiguous() && host_pinned(x.data)) {
+            e = cudaMemcpyAsync(ws->d, x.data, (size_t)total * T, cudaMemcpyHostToDevice, s);
+        } else {
+            // pack through the pinned staging buffer
+            if (cudaStreamSynchronize(s) != cudaSuccess) return FP_EDEVICE;
+            std::vector<int64_t> idx((size_t)x.ndim, 0);
+            char *hs = static_cast<char *>(ws->h_stage);
+            for (int64_t i = 0; i < total; ++i) {
+                int64_t off = 0;
+                for (int d = 0; d < x.ndim; ++d) off += idx[(size_t)d] * x.strides[d];
+                std::memcpy(hs + i * (int64_t)T, x.data + off * (int64_t)T, T);
+                for (int d = x.ndim - 1; d >= 0; --d) {
+                    if (++idx[(size_t)d] < x.shape[d]) break;
+                    idx[(size_t)d] = 0;
+                }
+            }
+            e = cudaMemcpyAsync(ws->d, hs, (size_t)total * T, cudaMemcpyHostToDevice, s);
+        }
+        xsrc = ws->d;
+        if (conj && e == cudaSuccess) {
+            e = cudaMemcpyAsync(ws->stage, ws->d, (size_t)total * T, cudaMemcpyDeviceToDevice, s);
+            ysave = ws->stage;
+        }
+    } else if (x.contiguous()) {
+        xsrc = x.data;
+        if (conj) {
+            e = cudaMemcpyAsync(ws->stage, x.data, (size_t)total * T, cudaMemcpyDeviceToDevice, s);
+            ysave = ws->stage;
+        }
+    } else {
+        void *dst = conj ? ws->stage : ws->d;
+        e = strided_copy(x.data, x.dtype, x.shape, x.strides, x.ndim, dst, x.dtype, cst, s);
+        xsrc = dst;
+        if (conj) ysave = dst;
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    // Steps per image
+    if (sa && !device_steps) {
+        std::memcpy(ws->h_gam, host_steps.data(), host_steps.size() * sizeof(double));
+        e = cudaMemcpyAsync(ws->gammas, ws->h_gam, host_steps.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+    } else if (!sa) {
+        e = fill_double(ws->gammas, identity ? 0.0 : gamma, g.B, s);
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    const bool warm = ws->dual_valid && (ws->warm || ws->seeded);
+    // z: straight into a contiguous device out, else a device buffer free
+    // at the end of the solve (stage, or V[1] when stage holds y)
+    const bool direct_out = !ws->host_mode && out.contiguous();
+    void *zdst = direct_out ? out.data : (conj ? ws->V[1] : ws->stage);
+    if (fp_status st2 = run_iso(ws, op, xsrc, zdst, o.tol, o.max_iter, warm)) return st2;
+    if (conj) {
+        e = conj_finish(ws->dtype, ysave, zdst, total, s);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    // Results back to the host
+    e = cudaMemcpyAsync(ws->h_img, ws->img, (size_t)g.B * sizeof(IsoImage), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ws->h_st, ws->st, (size_t)g.B * sizeof(IsoState), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (!direct_out) {
+        if (ws->host_mode) {
+            if (out.contiguous() && host_pinned(out.data)) {
+                e = cudaMemcpyAsync(out.data, zdst, (size_t)total * T, cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            } else {
+                e = cudaMemcpyAsync(ws->h_stage, zdst, (size_t)total * T, cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                if (e == cudaSuccess) {
+                    std::vector<int64_t> idx((size_t)out.ndim, 0);
+                    const char *hs = static_cast<const char *>(ws->h_stage);
+                    for (int64_t i = 0; i < total; ++i) {
+                        int64_t off = 0;
+                        for (int d = 0; d < out.ndim; ++d) off += idx[(size_t)d] * out.strides[d];
+                        std::memcpy(out.data + off * (int64_t)T, hs + i * (int64_t)T, T);
+                        for (int d = out.ndim - 1; d >= 0; --d) {
+                            if (++idx[(size_t)d] < out.shape[d]) break;
+                            idx[(size_t)d] = 0;
+                        }
+                    }
+                }
+            }
+        } else {
+            e = strided_copy(zdst, out.dtype, out.shape, cst, out.ndim, out.data, out.dtype, out.strides, s);
+        }
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e);
+    // Per-image results (driver.hpp:1303-1341)
+    bool inf = false, notconv = false;
+    double gsum = 0.0;
+    int imax = 0;
+    for (int64_t b = 0; b < g.B; ++b) {
+        const IsoImage &im = ws->h_img[b];
+        const IsoState &sst = ws->h_st[b];
+        double gap = 0.0, gap_s = 0.0;
+        int it = 0;
+        if (im.mode == kModeInf) {
+            inf = true;
+        } else if (im.mode == kModeNan) {
+            gap = gap_s = std::numeric_limits<double>::quiet_NaN();
+        } else if (im.mode == kModeFdpg) {
+            gap_s = std::max(sst.gp, 0.0);
+            if (std::isnan(sst.gp)) gap_s = sst.gp;
+            gap = im.e ? std::ldexp(gap_s, 2 * im.e) : gap_s;
+            it = sst.it;
+            if (sst.status != kConverged) notconv = true;
+        }
+        ws->gaps[(size_t)b] = gap;
+        ws->iters[(size_t)b] = it;
+        ws->zerrs[(size_t)b] = certified_error(gap_s, im.dd, g.N, im.e, ws->dtype, conj ? 2 : 1);
+        gsum += gap;
+        imax = std::max(imax, it);
+    }
+    ws->seeded = false;
+    if (inf) return FP_EINVAL;
+    ws->dual_valid = true;
+    if (keep) ws->valid = true;
+    ws->info = fp_info{gsum, imax, 0};
+    ws->info_status = notconv ? FP_ENOTCONV : FP_OK;
+    ws->info_valid = true;
+    if (info) *info = ws->info;
+    return ws->info_status;
+}
+
+}  // namespace
+
+extern "C" {
+
+FP_API fp_status fp_prox(const fp_op *op, double gamma, const fp_array *x, fp_array *out, const fp_options *opt,
+                         fp_workspace *ws, fp_info *info) {
+    return guard([&] { return prox_impl(op, gamma, x, out, opt, ws, info, false, nullptr); });
+}
+
+FP_API fp_status fp_prox_steps(const fp_op *op, const fp_array *gamma, const fp_array *x, fp_array *out,
+                               const fp_options *opt, fp_workspace *ws) {
+    return guard([&] {
+        if (!gamma) return FP_EINVAL;
+        return prox_impl(op, 0.0, x, out, opt, ws, nullptr, false, gamma);
+    });
+}
+
+FP_API fp_status fp_prox_conj(const fp_op *op, double sigma, const fp_array *y, fp_array *out,
+                              const fp_options *opt, fp_workspace *ws, fp_info *info) {
+    return guard([&] { return prox_impl(op, sigma, y, out, opt, ws, info, true, nullptr); });
+}
+
+FP_API fp_status fp_b200_workspace_stats(const fp_workspace *ws, int64_t *kernel_launches, int64_t *step_launches) {
+    if (!ws || !ws->info_valid) return FP_EINVAL;
+    if (kernel_launches) *kernel_launches = ws->kernel_launches;
+    if (step_launches) *step_launches = ws->launches;
+    return FP_OK;
+}
+
+FP_API fp_status fp_jvp(const fp_op *op, const fp_workspace *ws, const fp_array *dx, double dgamma,
+                        const fp_array *dparams, fp_array *dout) {
+    (void)dx;
+    (void)dgamma;
+    (void)dparams;
+    (void)dout;
+    if (!op || !ws || !ws->valid) return FP_EINVAL;
+    return FP_EINVAL;
+}
+
+FP_API fp_status fp_vjp(const fp_op *op, const fp_workspace *ws, const fp_array *g, fp_array *gx, double *ggamma,
+                        fp_array *gparams) {
+    (void)g;
+    (void)gx;
+    (void)ggamma;
+    (void)gparams;
+    if (!op || !ws || !ws->valid) return FP_EINVAL;
+    return FP_EINVAL;
+}
+
+FP_API fp_status fp_vjp_device(const fp_op *op, const fp_workspace *ws, const fp_array *g, fp_array *gx,
+                               fp_array *ggamma, fp_array *gparams) {
+    (void)g;
+    (void)gx;
+    (void)ggamma;
+    (void)gparams;
+    if (!op || !ws || !ws->valid) return FP_EINVAL;
+    return FP_EINVAL;
+}
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+// Kernel launchers of the image-TV engine, callable from plain C++ (api.cpp).
+// Every pointer is device memory owned by the workspace unless noted.
+#pragma once
+
+#include <cuda_runtime_api.h>
+
+#include "engine.h"
+
+namespace fpb {
+
+// Device buffers of an isotropic solve (see engine.h for the layout).
+struct IsoBuffers {
+    void *d = nullptr;          // B x N of T
+    void *U[2] = {nullptr, nullptr};
+    void *V[2] = {nullptr, nullptr};
+    void *dual = nullptr;       // k x B x N of T
+    const void *alpha = nullptr;  // pixel weights (T), N or B x N, or null
+    IsoImage *img = nullptr;
+    IsoState *st = nullptr;
+    double *gammas = nullptr;   // B steps
+    double *part = nullptr;     // B x max_part x 2
+    unsigned *ticket = nullptr; // B
+    int *live = nullptr;        // images still iterating
+    int max_part = 0;
+};
+
+// Launch shape of the step kernel, picked per geometry (and by the tuner).
+struct StepShape {
+    int kind = 0;   // 0: 2D row-marching, 1: generic (one thread per pixel)
+    int vec = 1;    // pixels per thread along the contiguous axis (march)
+    int bx = 128;   // threads per block
+    int rows = 16;  // rows per block (march)
+    int gx = 1, gy = 1;  // blocks per image = gx * gy
+};
+
+StepShape iso_pick_shape(int dtype, const Geometry &g, int rows_hint, int bx_hint);
+int iso_setup_blocks(const Geometry &g);
+
+// Set-up: stage x (contiguous, device) into d, per-image scans, state
+// initialisation, and the warm-start projection of the stored dual.
+cudaError_t iso_setup(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const void *x,
+                      int warm, int par, cudaStream_t s);
+// One dual-FISTA iteration (and the gap / restart tests it carries) for
+// every live image, reading buffers par and writing par ^ 1.
+cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh,
+                     int par, cudaStream_t s);
+// z = x - G^T q into out (contiguous, device, x's dtype), the dual into
+// bf.dual, for every image by its mode; exact 1D TV for single-axis images.
+cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, void *out,
+                         cudaStream_t s);
+
+// Fills gammas[i] = v for i < n.
+cudaError_t fill_double(double *dst, double v, int64_t n, cudaStream_t s);
+// Gathers a strided array of n_dims dims into a contiguous one (element
+// strides, dtype 1 = f32, 2 = f64; the destination dtype may differ: it
+// converts). Used for strided inputs, outputs and per-image steps.
+cudaError_t strided_copy(const void *src, int src_dtype, const int64_t *shape, const int64_t *src_strides,
+                         int ndim, void *dst, int dst_dtype, const int64_t *dst_strides, cudaStream_t s);
+// out = y - out (the conjugate's y - prox(y)), contiguous, n entries.
+cudaError_t conj_finish(int dtype, const void *y, void *out, int64_t n, cudaStream_t s);
+
+}  // namespace fpb

@@ -1,0 +1,908 @@
+// Isotropic image TV by dual FISTA on sm_100a: the set-up scans, the fused
+// iteration, the per-image stopping and restart logic, and the finalisation.
+//
+// The schedule is the reference's TVIso::fdpg (src/ops/tv_iso.cpp:424-543),
+// replayed per image on the device: the restart test of O'Donoghue and
+// Candes at every iteration it with it % 4 == 0 (tv_iso.cpp:498, 528-534),
+// the duality gap after every fourth iteration and at max_iter
+// (tv_iso.cpp:536), with FP64 accumulation of the gap and of the restart
+// dot. Iterates are kept in the array's dtype (FP32 for float32 input).
+//
+// One launch is one iteration of every live image. The gap of the state an
+// iteration starts from is evaluated in that same launch (its stencil reads
+// the same rows), and the last block of each image decides: converged (the
+// launch's update is dropped: it wrote the other ping-pong buffer), max_iter
+// reached, or go on, with the restart folded into the next launch's reads
+// (v = u) instead of a copy.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+
+#include "common.cuh"
+#include "launch.h"
+
+namespace fpb {
+namespace {
+
+constexpr int kScanThreads = 256;
+#define FP_MAX_NDIM_DEV 32
+constexpr double kMaxScaledStepLog2 = 960.0;  // the reference's kMaxScaledStep = 2^960 (core/op.hpp:48)
+
+template <class T>
+__device__ __forceinline__ T ldexp_t(T v, int e);
+template <>
+__device__ __forceinline__ float ldexp_t<float>(float v, int e) { return ldexpf(v, e); }
+template <>
+__device__ __forceinline__ double ldexp_t<double>(double v, int e) { return ldexp(v, e); }
+
+__device__ __forceinline__ float sqrt_t(float v) { return sqrtf(v); }
+__device__ __forceinline__ double sqrt_t(double v) { return sqrt(v); }
+
+// ---------------------------------------------------------------------------
+// Set-up scans (tv_iso.cpp:342-366, 369-377, 435-452, 479-483)
+// ---------------------------------------------------------------------------
+
+// Pass 1: copy x into d (unless it is already there), max |x|, NaN and Inf
+// flags; the last block picks the rescaling exponent and the image's mode.
+template <class T>
+__global__ void __launch_bounds__(kScanThreads) scan1_kernel(const T *__restrict__ x, T *__restrict__ d, Geometry g,
+                                                             IsoCall c, IsoBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const T *xb = x + (int64_t)b * N;
+    T *db = d + (int64_t)b * N;
+    double m = 0.0;
+    int fl = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const T v = xb[i];
+        if (xb != db) db[i] = v;
+        const double a = fabs((double)v);
+        if (isnan(a)) fl |= 1;
+        else if (isinf(a)) fl |= 2;
+        else m = fmax(m, a);
+    }
+    // the two flag bits are reduced apart: a max cannot OR them
+    const double mb = block_max(m, sh);
+    const double f1 = block_max((double)(fl & 1), sh);
+    const double f2 = block_max((double)((fl >> 1) & 1), sh);
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 2 + 0] = mb;
+        part[blockIdx.x * 2 + 1] = f1 + 2.0 * f2;
+    }
+    if (!arrive_last(bf.ticket + b, gridDim.x, &flag)) return;
+    const double mx = max_partials(part, gridDim.x, 2, 0, sh);
+    // OR of the flag codes: max over bit 0 and bit 1 separately
+    double o1 = 0.0, o2 = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+        const int code = (int)__ldcg(part + i * 2 + 1);
+        o1 = fmax(o1, (double)(code & 1));
+        o2 = fmax(o2, (double)((code >> 1) & 1));
+    }
+    o1 = block_max(o1, sh);
+    o2 = block_max(o2, sh);
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoImage im;
+    im.gamma_in = bf.gammas[b];
+    im.maxabs = mx;
+    im.flags = (o1 > 0.0 ? 1 : 0) | (o2 > 0.0 ? 2 : 0);
+    im.mean = 0.0;
+    im.dd = 0.0;
+    im.target = 0.0;
+    im.bound = 0.0;
+    im.radius = 0.0;
+    im.pad = 0;
+    int e = 0;
+    const bool act = im.gamma_in > 0.0 && c.na > 0;
+    if (im.flags & 2) im.mode = kModeInf;
+    else if (im.flags & 1) im.mode = kModeNan;
+    else if (!act) im.mode = kModeIdentity;
+    else im.mode = (c.na == 1 && !c.has_alpha) ? kModeTv1d : kModeFdpg;
+    if (im.mode == kModeFdpg || im.mode == kModeTv1d) {
+        // rescale_exponent (src/ops/image_util.hpp:56-65)
+        const double gamma = im.gamma_in;
+        if (mx > 0.0) {
+            e = ilogb(mx);
+            if (e >= -64 && e <= 64) {
+                e = 0;
+            } else {
+                const double top = fmax(gamma, gamma * c.step_scale);
+                if (e < 0 && top > 0.0) e = min(0, max(e, ilogb(top) + 1 - (int)kMaxScaledStepLog2));
+            }
+        }
+        // unless an active step would underflow there (tv_iso.cpp:371-372)
+        for (int a = 0; a < g.k && e; ++a) {
+            const double wa = c.wh[a] * c.wmax;
+            if (wa > 0.0 && !(ldexp(gamma * wa, -e) > 0.0)) e = 0;
+        }
+    }
+    im.e = e;
+    bf.img[b] = im;
+    IsoState st;
+    st.it = 0;
+    st.since = 0;
+    st.last = 0;
+    st.status = kFinished;
+    st.vsel = 0;
+    st.zero_in = 1;
+    st.warm = 0;
+    st.fin_par = 0;
+    st.tn = fista_t(1.0);
+    st.beta = 0.0;
+    st.gp = CUDART_INF;
+    st.dot = 0.0;
+    bf.st[b] = st;
+}
+
+// Pass 2: d *= 2^-e, sum d and sum d^2 (mean and the stopping target).
+template <class T>
+__global__ void __launch_bounds__(kScanThreads) scan2_kernel(T *__restrict__ d, Geometry g, IsoCall c, IsoBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const int mode = bf.img[b].mode;
+    if (mode == kModeNan || mode == kModeInf) return;
+    const int e = bf.img[b].e;  // 0 unless the image is solved (fdpg, tv1d)
+    const int64_t N = g.N;
+    T *db = d + (int64_t)b * N;
+    double s = 0.0, s2 = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        T v = db[i];
+        if (e) {
+            v = ldexp_t(v, -e);
+            db[i] = v;
+        }
+        const double dv = (double)v;
+        s += dv;
+        s2 += dv * dv;
+    }
+    const double sb = block_sum(s, sh);
+    const double s2b = block_sum(s2, sh);
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 2 + 0] = sb;
+        part[blockIdx.x * 2 + 1] = s2b;
+    }
+    if (!arrive_last(bf.ticket + b, gridDim.x, &flag)) return;
+    const double tot = sum_partials(part, gridDim.x, 2, 0, sh);
+    const double tot2 = sum_partials(part, gridDim.x, 2, 1, sh);
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    bf.img[b].mean = tot / (double)N;
+    bf.img[b].dd = tot2;
+    bf.img[b].target = c.tol * 0.5 * tot2;
+}
+
+// Pass 3: the imbalance sum |d - mean| -> bound and radius; state set-up.
+template <class T>
+__global__ void __launch_bounds__(kScanThreads) scan3_kernel(const T *__restrict__ d, Geometry g, IsoCall c,
+                                                             IsoBuffers bf, int warm) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    if (bf.img[b].mode != kModeFdpg) return;
+    const double mean = bf.img[b].mean;
+    const int64_t N = g.N;
+    const T *db = d + (int64_t)b * N;
+    double s = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        s += fabs((double)db[i] - mean);
+    const double sb = block_sum(s, sh);
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) part[blockIdx.x * 2 + 0] = sb;
+    if (!arrive_last(bf.ticket + b, gridDim.x, &flag)) return;
+    const double imb = sum_partials(part, gridDim.x, 2, 0, sh);
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoImage &im = bf.img[b];
+    const double gamma_s = ldexp(im.gamma_in, -im.e);
+    double gamma = gamma_s * c.wmax;  // tv_iso.cpp:445-447
+    const double bound = 2.0 * imb / c.whmin + DBL_MIN;
+    if (!(gamma <= bound) && !c.has_alpha) gamma = bound;
+    im.bound = bound;
+    im.radius = gamma;
+    IsoState &st = bf.st[b];
+    st.status = kLive;
+    st.zero_in = warm ? 0 : 1;
+    st.warm = warm ? 1 : 0;
+    atomicAdd(bf.live, 1);
+}
+
+// The radius of pixel p: gamma alpha_p capped at bound, 0 where alpha_p = 0
+// (tv_iso.cpp:180-185); gamma itself without pixel weights.
+template <class T, bool ALPHA>
+__device__ __forceinline__ T pixel_radius(T rad, T bnd, const T *al, int64_t p) {
+    if (!ALPHA) return rad;
+    const T a = al[p];
+    if (a == T(0)) return T(0);
+    const T r = rad * a;
+    return r <= bnd ? r : bnd;
+}
+
+// Warm start: u = q 2^-e wmax, zero on inactive axes, at the last entry
+// along each axis and where not finite, projected onto the balls
+// (tv_iso.cpp:456-478); v = u.
+template <class T, bool ALPHA>
+__global__ void warm_kernel(Geometry g, IsoCall c, IsoBuffers bf, int par) {
+    const int b = blockIdx.y;
+    const IsoImage &im = bf.img[b];
+    if (im.mode != kModeFdpg) return;
+    const int64_t N = g.N, B = g.B;
+    const T *q = static_cast<const T *>(bf.dual);
+    T *U = static_cast<T *>(bf.U[par]) + (int64_t)b * g.k * N;
+    T *V = static_cast<T *>(bf.V[par]) + (int64_t)b * g.k * N;
+    const T *al = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
+    const T rad = (T)im.radius, bnd = (T)im.bound;
+    int64_t S[3];
+    S[g.k - 1] = 1;
+    for (int a = g.k - 2; a >= 0; --a) S[a] = S[a + 1] * g.L[a + 1];
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        T u[3] = {T(0), T(0), T(0)};
+        T nn = T(0);
+        for (int a = 0; a < g.k; ++a) {
+            const bool has = ((p / S[a]) % g.L[a]) + 1 < g.L[a];
+            T v = ldexp_t(q[((int64_t)a * B + b) * N + p], -im.e) * (T)c.wmax;
+            if (c.wh[a] == 0.0 || !has || !isfinite(v)) v = T(0);
+            u[a] = v;
+            nn += v * v;
+        }
+        const T rp = pixel_radius<T, ALPHA>(rad, bnd, al, p);
+        const T nr = sqrt_t(nn);
+        if (nr > rp) {
+            const T sc = rp / nr;
+            for (int a = 0; a < g.k; ++a) u[a] *= sc;
+        }
+        for (int a = 0; a < g.k; ++a) {
+            U[a * N + p] = u[a];
+            V[a * N + p] = u[a];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-image control: the scalar part of one fdpg iteration (tv_iso.cpp:528-537)
+// ---------------------------------------------------------------------------
+
+// Runs in thread 0 of the last block of an image after a step launch that
+// started from iteration st.it. gap: the gap of that starting state, when
+// do_gap; dot: the restart test's <v - u+, u+ - u>, when test.
+__device__ void control(IsoState &st, const IsoImage &im, int max_iter, bool do_gap, bool test, double gap,
+                        double dot, int par_in, int *live) {
+    if (do_gap) {
+        st.gp = gap;
+        if (gap <= im.target) {  // the loop condition of tv_iso.cpp:491
+            st.status = kConverged;
+            st.fin_par = par_in;
+            atomicSub(live, 1);
+            return;
+        }
+        if (st.it >= max_iter) {
+            st.status = kNotConv;
+            st.fin_par = par_in;
+            atomicSub(live, 1);
+            return;
+        }
+    }
+    // The update of this launch stands.
+    st.dot = dot;
+    st.since += 1;
+    const bool restart = test && dot > 0.0 && st.since >= st.last;
+    double t = st.tn;
+    if (restart) {
+        t = 1.0;
+        st.last = st.since;
+        st.since = 0;
+    }
+    st.vsel = restart ? 1 : 0;
+    st.zero_in = 0;
+    st.it += 1;
+    const double tn = fista_t(t);
+    st.beta = (t - 1.0) / tn;
+    st.tn = tn;
+    st.fin_par = par_in ^ 1;
+}
+
+struct StepArgs {
+    Geometry g;
+    int max_iter;
+    int par;
+    int rows;
+};
+
+// ---------------------------------------------------------------------------
+// The 2D row-marching step: a warp spans 32 * VEC consecutive columns, a
+// block BX * VEC of them, and each thread walks down `rows` rows keeping the
+// current and next rows of z, u and v in registers, so every array is read
+// from HBM once per iteration (36 B per pixel in FP32: d, u, v in; u, v out).
+// Horizontal neighbours come from the next lane by shuffle; lane 31 reads
+// the first column of the next warp's span itself.
+// ---------------------------------------------------------------------------
+
+template <class T, int VEC>
+struct Row {
+    T v[VEC];
+};
+
+template <class T, int VEC, bool ALPHA>
+__global__ void __launch_bounds__(256) iso2d_march_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.z;
+    const IsoState st = bf.st[b];
+    if (st.status != kLive) return;
+    const IsoImage im = bf.img[b];
+    const int64_t H = A.g.L[0], W = A.g.L[1], N = A.g.N;
+    const int it = st.it;
+    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == A.max_iter)) || (it == 0 && st.warm);
+    const bool do_upd = it < A.max_iter;
+    const bool test = do_upd && (it & 3) == 0;
+    const bool zin = st.zero_in != 0;
+    const int pin = A.par, pout = A.par ^ 1;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *U0 = static_cast<const T *>(bf.U[pin]) + (int64_t)b * 2 * N;
+    const T *U1 = U0 + N;
+    const T *V0 = st.vsel ? U0 : static_cast<const T *>(bf.V[pin]) + (int64_t)b * 2 * N;
+    const T *V1 = V0 + N;
+    T *UO0 = static_cast<T *>(bf.U[pout]) + (int64_t)b * 2 * N;
+    T *UO1 = UO0 + N;
+    T *VO0 = static_cast<T *>(bf.V[pout]) + (int64_t)b * 2 * N;
+    T *VO1 = VO0 + N;
+    const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
+    const T wh0 = (T)c.wh[0], wh1 = (T)c.wh[1], tau = (T)c.tau, beta = (T)st.beta;
+    const T rad = (T)im.radius, bnd = (T)im.bound;
+    const int lane = threadIdx.x & 31;
+    const int64_t cb = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * VEC;
+    const bool colok = cb < W;
+    const int64_t r0 = (int64_t)blockIdx.y * A.rows;
+    const int64_t r1 = min(H, r0 + (int64_t)A.rows);
+
+    auto LD = [&](const T *P, int64_t r, bool zero, T(&o)[VEC]) {
+        if (zero || r < 0 || r >= H || !colok) {
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) o[j] = T(0);
+        } else {
+            load_pack<T, VEC>(P + r * W + cb, o);
+        }
+    };
+    auto LS = [&](const T *P, int64_t r, int64_t col, bool zero) -> T {
+        if (zero || r < 0 || r >= H || col < 0 || col >= W) return T(0);
+        return P[r * W + col];
+    };
+    // z at (r, col) from d and a dual field (P0, P1), for one point.
+    auto zpoint = [&](const T *P0, const T *P1, int64_t r, int64_t col, T left1) -> T {
+        const T dd = LS(D, r, col, false);
+        const T a0 = LS(P0, r, col, zin), a0p = LS(P0, r - 1, col, zin);
+        const T a1 = LS(P1, r, col, zin);
+        return dd + wh0 * (a0 - a0p) + wh1 * (a1 - left1);
+    };
+    // z on a row: d + wh0 (p0 - p0prev) + wh1 (p1 - p1 shifted right by one)
+    auto zrow = [&](const T(&dd)[VEC], const T(&p0)[VEC], const T(&p0p)[VEC], const T(&p1)[VEC], T p1l,
+                    T(&z)[VEC]) {
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            const T left = j == 0 ? p1l : p1[j - 1];
+            z[j] = dd[j] + wh0 * (p0[j] - p0p[j]) + wh1 * (p1[j] - left);
+        }
+    };
+
+    T v0c[VEC], v1c[VEC], u0c[VEC], u1c[VEC], zc[VEC], zuc[VEC];
+    {
+        T v0p[VEC], dc[VEC];
+        LD(V0, r0 - 1, zin, v0p);
+        LD(V0, r0, zin, v0c);
+        LD(V1, r0, zin, v1c);
+        LD(D, r0, false, dc);
+        zrow(dc, v0c, v0p, v1c, LS(V1, r0, cb - 1, zin), zc);
+        LD(U0, r0, zin, u0c);
+        LD(U1, r0, zin, u1c);
+        if (do_gap) {
+            T u0p[VEC];
+            LD(U0, r0 - 1, zin, u0p);
+            zrow(dc, u0c, u0p, u1c, LS(U1, r0, cb - 1, zin), zuc);
+        } else {
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) zuc[j] = T(0);
+        }
+    }
+    double gap_acc = 0.0, dot_acc = 0.0;
+    for (int64_t i = r0; i < r1; ++i) {
+        const bool hasn = i + 1 < H;
+        T dn[VEC], v0n[VEC], v1n[VEC], u0n[VEC], u1n[VEC], zn[VEC], zun[VEC];
+        LD(D, i + 1, false, dn);
+        LD(V0, i + 1, zin, v0n);
+        LD(V1, i + 1, zin, v1n);
+        LD(U0, i + 1, zin, u0n);
+        LD(U1, i + 1, zin, u1n);
+        T al[VEC];
+        if (ALPHA) {
+            if (colok) load_pack<T, VEC>(AL + i * W + cb, al);
+            else
+#pragma unroll
+                for (int j = 0; j < VEC; ++j) al[j] = T(0);
+        }
+        zrow(dn, v0n, v0c, v1n, LS(V1, i + 1, cb - 1, zin), zn);
+        // right neighbour of the last column
+        T zr = __shfl_down_sync(0xffffffffu, zc[0], 1);
+        if (lane == 31 && cb + VEC < W) zr = zpoint(V0, V1, i, cb + VEC, v1c[VEC - 1]);
+        T zur = T(0);
+        if (do_gap) {
+            zrow(dn, u0n, u0c, u1n, LS(U1, i + 1, cb - 1, zin), zun);
+            zur = __shfl_down_sync(0xffffffffu, zuc[0], 1);
+            if (lane == 31 && cb + VEC < W) zur = zpoint(U0, U1, i, cb + VEC, u1c[VEC - 1]);
+        }
+        T uo0[VEC], uo1[VEC], vo0[VEC], vo1[VEC];
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            const int64_t col = cb + j;
+            const bool hasr = col + 1 < W;
+            const T zright = j + 1 < VEC ? zc[j + 1] : zr;
+            const T g0 = hasn ? wh0 * (zn[j] - zc[j]) : T(0);
+            const T g1 = hasr ? wh1 * (zright - zc[j]) : T(0);
+            const T cv0 = wh0 != T(0) ? v0c[j] + tau * g0 : T(0);
+            const T cv1 = wh1 != T(0) ? v1c[j] + tau * g1 : T(0);
+            const T nr = sqrt_t(cv0 * cv0 + cv1 * cv1);
+            T rp = rad;
+            if (ALPHA) rp = al[j] == T(0) ? T(0) : (rad * al[j] <= bnd ? rad * al[j] : bnd);
+            const T sc = nr > rp ? rp / nr : T(1);
+            const T un0 = cv0 * sc, un1 = cv1 * sc;
+            if (test && colok)
+                dot_acc += (double)((v0c[j] - un0) * (un0 - u0c[j])) + (double)((v1c[j] - un1) * (un1 - u1c[j]));
+            vo0[j] = un0 + beta * (un0 - u0c[j]);
+            vo1[j] = un1 + beta * (un1 - u1c[j]);
+            uo0[j] = un0;
+            uo1[j] = un1;
+            if (do_gap && colok) {
+                const T zuright = j + 1 < VEC ? zuc[j + 1] : zur;
+                const double gu0 = hasn ? (double)(wh0 * (zun[j] - zuc[j])) : 0.0;
+                const double gu1 = hasr ? (double)(wh1 * (zuright - zuc[j])) : 0.0;
+                gap_acc += (double)rp * sqrt(gu0 * gu0 + gu1 * gu1) - (gu0 * (double)u0c[j] + gu1 * (double)u1c[j]);
+            }
+        }
+        if (do_upd && colok) {
+            store_pack<T, VEC>(UO0 + i * W + cb, uo0);
+            store_pack<T, VEC>(UO1 + i * W + cb, uo1);
+            store_pack<T, VEC>(VO0 + i * W + cb, vo0);
+            store_pack<T, VEC>(VO1 + i * W + cb, vo1);
+        }
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            v0c[j] = v0n[j];
+            v1c[j] = v1n[j];
+            u0c[j] = u0n[j];
+            u1c[j] = u1n[j];
+            zc[j] = zn[j];
+            zuc[j] = do_gap ? zun[j] : T(0);
+        }
+    }
+    const unsigned nblk = gridDim.x * gridDim.y;
+    const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
+    const double gsum = (do_gap ? block_sum(gap_acc, sh) : 0.0);
+    const double dsum = (test ? block_sum(dot_acc, sh) : 0.0);
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[blk * 2 + 0] = gsum;
+        part[blk * 2 + 1] = dsum;
+    }
+    if (!arrive_last(bf.ticket + b, nblk, &flag)) return;
+    const double gap = do_gap ? sum_partials(part, nblk, 2, 0, sh) : 0.0;
+    const double dot = test ? sum_partials(part, nblk, 2, 1, sh) : 0.0;
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2 = st;
+    control(s2, im, A.max_iter, do_gap, test, gap, dot, pin, bf.live);
+    bf.st[b] = s2;
+}
+
+// ---------------------------------------------------------------------------
+// Generic step: one thread per pixel, 2D or 3D, any extents. Neighbours are
+// read through the caches.
+// ---------------------------------------------------------------------------
+
+template <class T, int K, bool ALPHA>
+__global__ void __launch_bounds__(256) iso_generic_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const IsoState st = bf.st[b];
+    if (st.status != kLive) return;
+    const IsoImage im = bf.img[b];
+    const int64_t N = A.g.N;
+    const int it = st.it;
+    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == A.max_iter)) || (it == 0 && st.warm);
+    const bool do_upd = it < A.max_iter;
+    const bool test = do_upd && (it & 3) == 0;
+    const bool zin = st.zero_in != 0;
+    const int pin = A.par, pout = A.par ^ 1;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *U = static_cast<const T *>(bf.U[pin]) + (int64_t)b * K * N;
+    const T *V = st.vsel ? U : static_cast<const T *>(bf.V[pin]) + (int64_t)b * K * N;
+    T *UO = static_cast<T *>(bf.U[pout]) + (int64_t)b * K * N;
+    T *VO = static_cast<T *>(bf.V[pout]) + (int64_t)b * K * N;
+    const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
+    T wh[K];
+    int64_t L[K], S[K];
+    for (int a = 0; a < K; ++a) {
+        wh[a] = (T)c.wh[a];
+        L[a] = A.g.L[a];
+    }
+    S[K - 1] = 1;
+    for (int a = K - 2; a >= 0; --a) S[a] = S[a + 1] * L[a + 1];
+    const T tau = (T)c.tau, beta = (T)st.beta, rad = (T)im.radius, bnd = (T)im.bound;
+
+    // z(P) at q, with the coordinates of q
+    auto zat = [&](const T *P, int64_t q, const int64_t *co) -> T {
+        T z = D[q];
+        for (int a = 0; a < K; ++a) {
+            if (wh[a] == T(0)) continue;
+            const T cur = zin ? T(0) : P[a * N + q];
+            const T prev = (zin || co[a] == 0) ? T(0) : P[a * N + q - S[a]];
+            z += wh[a] * (cur - prev);
+        }
+        return z;
+    };
+    double gap_acc = 0.0, dot_acc = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        int64_t co[K];
+        for (int a = 0; a < K; ++a) co[a] = (p / S[a]) % L[a];
+        const T z0 = zat(V, p, co);
+        T gv[K];
+        for (int a = 0; a < K; ++a) {
+            gv[a] = T(0);
+            if (wh[a] != T(0) && co[a] + 1 < L[a]) {
+                int64_t cn[K];
+                for (int e = 0; e < K; ++e) cn[e] = co[e];
+                cn[a] += 1;
+                gv[a] = wh[a] * (zat(V, p + S[a], cn) - z0);
+            }
+        }
+        T cv[K], uc[K], vc[K];
+        T nn = T(0);
+        for (int a = 0; a < K; ++a) {
+            uc[a] = zin ? T(0) : U[a * N + p];
+            vc[a] = zin ? T(0) : V[a * N + p];
+            cv[a] = wh[a] != T(0) ? vc[a] + tau * gv[a] : T(0);
+            nn += cv[a] * cv[a];
+        }
+        const T nr = sqrt_t(nn);
+        const T rp = pixel_radius<T, ALPHA>(rad, bnd, AL, p);
+        const T sc = nr > rp ? rp / nr : T(1);
+        for (int a = 0; a < K; ++a) {
+            const T un = cv[a] * sc;
+            if (test) dot_acc += (double)((vc[a] - un) * (un - uc[a]));
+            if (do_upd) {
+                VO[a * N + p] = un + beta * (un - uc[a]);
+                UO[a * N + p] = un;
+            }
+        }
+        if (do_gap) {
+            const T zu0 = zat(U, p, co);
+            double gg = 0.0, gu = 0.0;
+            for (int a = 0; a < K; ++a) {
+                if (wh[a] != T(0) && co[a] + 1 < L[a]) {
+                    int64_t cn[K];
+                    for (int e = 0; e < K; ++e) cn[e] = co[e];
+                    cn[a] += 1;
+                    const double ga = (double)(wh[a] * (zat(U, p + S[a], cn) - zu0));
+                    gg += ga * ga;
+                    gu += ga * (double)uc[a];
+                }
+            }
+            gap_acc += (double)rp * sqrt(gg) - gu;
+        }
+    }
+    const unsigned nblk = gridDim.x;
+    const double gsum = do_gap ? block_sum(gap_acc, sh) : 0.0;
+    const double dsum = test ? block_sum(dot_acc, sh) : 0.0;
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 2 + 0] = gsum;
+        part[blockIdx.x * 2 + 1] = dsum;
+    }
+    if (!arrive_last(bf.ticket + b, nblk, &flag)) return;
+    const double gap = do_gap ? sum_partials(part, nblk, 2, 0, sh) : 0.0;
+    const double dot = test ? sum_partials(part, nblk, 2, 1, sh) : 0.0;
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2 = st;
+    control(s2, im, A.max_iter, do_gap, test, gap, dot, pin, bf.live);
+    bf.st[b] = s2;
+}
+
+// ---------------------------------------------------------------------------
+// Finalisation: z = d - G^T u (tv_iso.cpp:484-487, 539) back at the input's
+// scale (tv_iso.cpp:403-413), the dual q = u / wmax 2^e into bf.dual.
+// ---------------------------------------------------------------------------
+
+template <class T>
+__global__ void finalize_kernel(Geometry g, IsoCall c, IsoBuffers bf, T *__restrict__ out) {
+    const int b = blockIdx.y;
+    const IsoImage im = bf.img[b];
+    if (im.mode == kModeTv1d || im.mode == kModeInf) return;
+    const IsoState st = bf.st[b];
+    const int64_t N = g.N, B = g.B;
+    const int K = g.k;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *U = static_cast<const T *>(bf.U[st.fin_par]) + (int64_t)b * K * N;
+    T *Q = static_cast<T *>(bf.dual);
+    T *O = out + (int64_t)b * N;
+    int64_t S[3], L[3];
+    for (int a = 0; a < K; ++a) L[a] = g.L[a];
+    S[K - 1] = 1;
+    for (int a = K - 2; a >= 0; --a) S[a] = S[a + 1] * L[a + 1];
+    const T inv = (T)(1.0 / c.wmax);
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        if (im.mode == kModeNan) {
+            O[p] = (T)CUDART_NAN;
+            for (int a = 0; a < K; ++a) Q[((int64_t)a * B + b) * N + p] = (T)CUDART_NAN;
+            continue;
+        }
+        if (im.mode == kModeIdentity) {
+            O[p] = D[p];
+            for (int a = 0; a < K; ++a) Q[((int64_t)a * B + b) * N + p] = T(0);
+            continue;
+        }
+        T z = D[p];
+        for (int a = 0; a < K; ++a) {
+            const T wa = (T)c.wh[a];
+            if (wa == T(0)) continue;
+            const bool first = ((p / S[a]) % L[a]) == 0;
+            z += wa * (U[a * N + p] - (first ? T(0) : U[a * N + p - S[a]]));
+        }
+        O[p] = im.e ? ldexp_t(z, im.e) : z;
+        for (int a = 0; a < K; ++a) {
+            T q = U[a * N + p] * inv;
+            if (im.e) q = ldexp_t(q, im.e);
+            Q[((int64_t)a * B + b) * N + p] = q;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One active axis without pixel weights: exact 1D TV along it (tv_iso.cpp:381-398)
+// ---------------------------------------------------------------------------
+}  // namespace
+
+}  // namespace fpb
+
+#include "tv1d.cuh"
+
+namespace fpb {
+namespace {
+
+template <class T>
+__global__ void iso_tv1d_kernel(Geometry g, IsoCall c, IsoBuffers bf, T *__restrict__ out) {
+    const int b = blockIdx.y;
+    const IsoImage im = bf.img[b];
+    if (im.mode != kModeTv1d) return;
+    const int a = c.act_axis;
+    const int64_t N = g.N, B = g.B;
+    const int K = g.k;
+    int64_t S[3];
+    S[K - 1] = 1;
+    for (int x = K - 2; x >= 0; --x) S[x] = S[x + 1] * g.L[x + 1];
+    const int64_t L = g.L[a], s = S[a];
+    const int64_t nfib = N / L;
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nfib) return;
+    const int64_t base = (f / s) * L * s + (f % s);
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    T *Z = static_cast<T *>(bf.U[0]) + (int64_t)b * K * N;  // solved-scale z, scratch
+    T *O = out + (int64_t)b * N;
+    T *Q = static_cast<T *>(bf.dual);
+    const double lam = ldexp(im.gamma_in, -im.e) * c.w_act;
+    tv1d_fiber<T>(D + base, s, Z + base, s, L, lam, nullptr, 0);
+    double cs = 0.0;
+    for (int64_t i = 0; i < L; ++i) {
+        const int64_t o = base + i * s;
+        const T z = Z[o];
+        cs += (double)D[o] - (double)z;
+        O[o] = im.e ? ldexp_t(z, im.e) : z;
+        for (int x = 0; x < K; ++x) {
+            double q = 0.0;
+            if (x == a && i + 1 < L) q = -cs / c.w_act;
+            if (im.e) q = ldexp(q, im.e);
+            Q[((int64_t)x * B + b) * N + o] = (T)q;
+        }
+    }
+}
+
+template <class T>
+__global__ void conj_kernel(const T *__restrict__ y, T *__restrict__ out, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = y[i] - out[i];
+}
+
+__global__ void fill_double_kernel(double *dst, double v, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = v;
+}
+
+struct StridedDesc {
+    int ndim;
+    int64_t shape[FP_MAX_NDIM_DEV];
+    int64_t ss[FP_MAX_NDIM_DEV];
+    int64_t ds[FP_MAX_NDIM_DEV];
+};
+
+template <class S, class D>
+__global__ void strided_kernel(const S *__restrict__ src, D *__restrict__ dst, StridedDesc sd, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = i, so = 0, doff = 0;
+        for (int d = sd.ndim - 1; d >= 0; --d) {
+            const int64_t ext = sd.shape[d];
+            const int64_t c = r % ext;
+            r /= ext;
+            so += c * sd.ss[d];
+            doff += c * sd.ds[d];
+        }
+        dst[doff] = (D)src[so];
+    }
+}
+
+int grid_for(int64_t n, int threads) {
+    int64_t g = (n + threads - 1) / threads;
+    if (g > 148 * 32) g = 148 * 32;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+template <class T>
+cudaError_t setup_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const void *x, int warm, int par,
+                    cudaStream_t s) {
+    const int nb = iso_setup_blocks(g);
+    const dim3 grid(nb, (unsigned)g.B);
+    scan1_kernel<T><<<grid, kScanThreads, 0, s>>>(static_cast<const T *>(x), static_cast<T *>(bf.d), g, c, bf);
+    scan2_kernel<T><<<grid, kScanThreads, 0, s>>>(static_cast<T *>(bf.d), g, c, bf);
+    scan3_kernel<T><<<grid, kScanThreads, 0, s>>>(static_cast<const T *>(bf.d), g, c, bf, warm);
+    if (warm) {
+        const dim3 wg((unsigned)std::min<int64_t>((g.N + 255) / 256, 4096), (unsigned)g.B);
+        if (c.has_alpha) warm_kernel<T, true><<<wg, 256, 0, s>>>(g, c, bf, par);
+        else warm_kernel<T, false><<<wg, 256, 0, s>>>(g, c, bf, par);
+    }
+    return cudaGetLastError();
+}
+
+template <class T, int VEC>
+void launch_march(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
+    const dim3 grid(sh.gx, sh.gy, (unsigned)A.g.B);
+    if (c.has_alpha) iso2d_march_kernel<T, VEC, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
+    else iso2d_march_kernel<T, VEC, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
+}
+
+template <class T>
+cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh, int par,
+                   cudaStream_t s) {
+    StepArgs A;
+    A.g = g;
+    A.max_iter = c.max_iter;
+    A.par = par;
+    A.rows = sh.rows;
+    if (sh.kind == 0) {
+        if (sh.vec == 4) launch_march<T, 4>(sh, A, c, bf, s);
+        else if (sh.vec == 2) launch_march<T, 2>(sh, A, c, bf, s);
+        else launch_march<T, 1>(sh, A, c, bf, s);
+    } else {
+        const dim3 grid(sh.gx, (unsigned)g.B);
+        if (g.k == 2) {
+            if (c.has_alpha) iso_generic_kernel<T, 2, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
+            else iso_generic_kernel<T, 2, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
+        } else {
+            if (c.has_alpha) iso_generic_kernel<T, 3, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
+            else iso_generic_kernel<T, 3, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
+        }
+    }
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t finalize_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, void *out, cudaStream_t s) {
+    const dim3 grid((unsigned)std::min<int64_t>((g.N + 255) / 256, 2048), (unsigned)g.B);
+    finalize_kernel<T><<<grid, 256, 0, s>>>(g, c, bf, static_cast<T *>(out));
+    if (c.na == 1 && !c.has_alpha) {
+        const int64_t nfib = g.N / g.L[c.act_axis];
+        const dim3 g1((unsigned)((nfib + 127) / 128), (unsigned)g.B);
+        iso_tv1d_kernel<T><<<g1, 128, 0, s>>>(g, c, bf, static_cast<T *>(out));
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int iso_setup_blocks(const Geometry &g) {
+    int64_t nb = (g.N + kScanThreads * 8 - 1) / (kScanThreads * 8);
+    if (nb > 128) nb = 128;
+    if (nb < 1) nb = 1;
+    return (int)nb;
+}
+
+StepShape iso_pick_shape(int dtype, const Geometry &g, int rows_hint, int bx_hint) {
+    StepShape sh;
+    const int64_t W = g.k == 2 ? g.L[1] : 0;
+    const int vmax = dtype == 1 ? 4 : 2;
+    if (g.k == 2 && W >= 32) {
+        sh.kind = 0;
+        sh.vec = (W % vmax == 0) ? vmax : ((W % 2 == 0) ? 2 : 1);
+        const int64_t cols = (W + sh.vec - 1) / sh.vec;
+        int bx = bx_hint > 0 ? bx_hint : (int)std::min<int64_t>(128, ((cols + 31) / 32) * 32);
+        sh.bx = bx;
+        sh.gx = (int)((cols + bx - 1) / bx);
+        const int64_t H = g.L[0];
+        // The block partition of an image depends on its shape only, so an
+        // image gives the same bits alone and in any batch.
+        int rows = rows_hint;
+        if (rows <= 0) rows = (int)std::max<int64_t>(4, std::min<int64_t>(16, H / 32));
+        sh.rows = rows;
+        sh.gy = (int)((H + rows - 1) / rows);
+    } else {
+        sh.kind = 1;
+        sh.vec = 1;
+        sh.bx = bx_hint > 0 ? bx_hint : 256;
+        int64_t gx = (g.N + sh.bx - 1) / sh.bx;
+        if (gx > 1024) gx = 1024;  // shape-only, as above
+        sh.gx = (int)std::max<int64_t>(1, gx);
+        sh.gy = 1;
+    }
+    return sh;
+}
+
+cudaError_t iso_setup(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const void *x, int warm,
+                      int par, cudaStream_t s) {
+    return dtype == 1 ? setup_t<float>(g, c, bf, x, warm, par, s) : setup_t<double>(g, c, bf, x, warm, par, s);
+}
+
+cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh,
+                     int par, cudaStream_t s) {
+    return dtype == 1 ? step_t<float>(g, c, bf, sh, par, s) : step_t<double>(g, c, bf, sh, par, s);
+}
+
+cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, void *out,
+                         cudaStream_t s) {
+    return dtype == 1 ? finalize_t<float>(g, c, bf, out, s) : finalize_t<double>(g, c, bf, out, s);
+}
+
+cudaError_t fill_double(double *dst, double v, int64_t n, cudaStream_t s) {
+    fill_double_kernel<<<grid_for(n, 256), 256, 0, s>>>(dst, v, n);
+    return cudaGetLastError();
+}
+
+cudaError_t conj_finish(int dtype, const void *y, void *out, int64_t n, cudaStream_t s) {
+    if (dtype == 1)
+        conj_kernel<float><<<grid_for(n, 256), 256, 0, s>>>(static_cast<const float *>(y), static_cast<float *>(out), n);
+    else
+        conj_kernel<double>
+            <<<grid_for(n, 256), 256, 0, s>>>(static_cast<const double *>(y), static_cast<double *>(out), n);
+    return cudaGetLastError();
+}
+
+cudaError_t strided_copy(const void *src, int src_dtype, const int64_t *shape, const int64_t *src_strides, int ndim,
+                         void *dst, int dst_dtype, const int64_t *dst_strides, cudaStream_t s) {
+    if (ndim > FP_MAX_NDIM_DEV) return cudaErrorInvalidValue;
+    StridedDesc sd;
+    sd.ndim = ndim;
+    int64_t n = 1;
+    for (int d = 0; d < ndim; ++d) {
+        sd.shape[d] = shape[d];
+        sd.ss[d] = src_strides[d];
+        sd.ds[d] = dst_strides[d];
+        n *= shape[d];
+    }
+    if (n == 0) return cudaSuccess;
+    const int grid = grid_for(n, 256);
+    if (src_dtype == 1 && dst_dtype == 1)
+        strided_kernel<float, float><<<grid, 256, 0, s>>>(static_cast<const float *>(src), static_cast<float *>(dst), sd, n);
+    else if (src_dtype == 1)
+        strided_kernel<float, double><<<grid, 256, 0, s>>>(static_cast<const float *>(src), static_cast<double *>(dst), sd, n);
+    else if (dst_dtype == 1)
+        strided_kernel<double, float><<<grid, 256, 0, s>>>(static_cast<const double *>(src), static_cast<float *>(dst), sd, n);
+    else
+        strided_kernel<double, double>
+            <<<grid, 256, 0, s>>>(static_cast<const double *>(src), static_cast<double *>(dst), sd, n);
+    return cudaGetLastError();
+}
+
+}  // namespace fpb

@@ -1,0 +1,74 @@
+// The opaque fp_op and fp_workspace of the C ABI (host side).
+#pragma once
+
+#include <cuda_runtime_api.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/fastprox_b200.h"
+#include "engine.h"
+#include "launch.h"
+
+namespace fpb {
+enum OpKind : int { kIso = 1, kAniso = 2 };
+}
+
+// Immutable and shareable: device copies of its parameters live in the
+// workspaces (the reference's fp_op, src/core/op.hpp).
+struct fp_op {
+    int kind = 0;                 // fpb::OpKind
+    int k = 2;                    // image axes
+    double w[3] = {0, 0, 0};      // axis weights
+    std::vector<double> spatial;  // pixel weights (iso, N) or edge weights (aniso, k N), C order
+    int64_t sshape[3] = {1, 1, 1};
+    double smax = 0.0;
+};
+
+// One array shape, dtype and device; calls on it must not overlap. Every
+// device byte is allocated in fp_workspace_create.
+struct fp_workspace {
+    const fp_op *op = nullptr;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int dtype = 0;
+    int ndim = 0;
+    int64_t shape[FP_MAX_NDIM] = {};
+    fpb::Geometry g{};
+    bool host_mode = false;  // created with a host `like`: host arrays staged through here
+    bool keep = false;
+    // device memory
+    void *d = nullptr, *stage = nullptr, *dual = nullptr, *spatial = nullptr;
+    void *U[2] = {nullptr, nullptr}, *V[2] = {nullptr, nullptr};
+    fpb::IsoImage *img = nullptr;
+    fpb::IsoState *st = nullptr;
+    double *gammas = nullptr;
+    double *part = nullptr;
+    unsigned *ticket = nullptr;
+    int *live = nullptr;
+    int max_part = 0;
+    // pinned host memory
+    int *h_live = nullptr;
+    fpb::IsoImage *h_img = nullptr;
+    fpb::IsoState *h_st = nullptr;
+    double *h_gam = nullptr;
+    void *h_stage = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    std::vector<void *> dev_allocs, host_allocs;
+    // launch shape and polling
+    fpb::StepShape shape_{};
+    int chunk = 8;
+    int64_t launches = 0;         // step launches of the last call
+    int64_t kernel_launches = 0;  // all kernels of the last call
+    // results of the last call
+    std::vector<double> gaps, zerrs;
+    std::vector<int> iters;
+    fp_info info{0.0, 0, 0};
+    fp_status info_status = FP_OK;
+    bool info_valid = false;
+    bool warm = false, seeded = false, dual_valid = false, valid = false;
+    double deriv_tol = 0.0;
+    int deriv_max_iter = 10000;
+    double deriv_residual = 0.0;
+    int deriv_iters = 0;
+};

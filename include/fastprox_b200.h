@@ -1,0 +1,189 @@
+/*
+ * fastprox_b200.h -- the image total-variation entry points of fastprox's
+ * plain-C ABI (ABI version 1), served by sm_100a CUDA kernels.
+ *
+ * A drop-in for the image-TV subset of the reference library: the types,
+ * enum values, structure layouts and function signatures below are those of
+ * the reference's include/fastprox.h, so a caller compiled against that
+ * header links against libfastprox_b200.so unchanged. Arrays on a CUDA
+ * device (FP_DEVICE_CUDA, DLPack's kDLCUDA) are solved in place on that
+ * device; arrays in host memory (FP_DEVICE_CPU) are staged through the
+ * workspace's device buffers and solved on the GPU as well. There is no CPU
+ * solver behind these entry points: without a usable GPU they return
+ * FP_EDEVICE.
+ *
+ * Every function is extern "C", returns fp_status (or a plain value), and
+ * lets no C++ exception escape.
+ */
+#ifndef FASTPROX_B200_H
+#define FASTPROX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#define FP_VERSION_MAJOR 1
+#define FP_VERSION_MINOR 0
+#define FP_VERSION_PATCH 6
+#define FP_ABI_VERSION 1
+#define FP_MAX_NDIM 32
+
+#define FP_API __attribute__((visibility("default")))
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same values as the reference's fp_dtype / fp_device / fp_status
+ * (include/fastprox.h:52-80). */
+typedef enum { FP_F32 = 1, FP_F64 = 2, FP_I8 = 3, FP_I32 = 4, FP_I64 = 5 } fp_dtype;
+typedef enum { FP_DEVICE_CPU = 0, FP_DEVICE_CUDA = 2 } fp_device;
+
+/* Strided n-d array; strides in elements (NULL = C order); never freed by
+ * the library (include/fastprox.h:61-68). */
+typedef struct {
+    void          *data;
+    fp_dtype       dtype;
+    int            ndim;
+    const int64_t *shape;
+    const int64_t *strides;
+    fp_device      device;
+} fp_array;
+
+typedef enum {
+    FP_OK = 0,
+    FP_EINVAL,
+    FP_EDTYPE,
+    FP_ESHAPE,
+    FP_ENOMEM,
+    FP_ENOTCONV,
+    FP_EPARAM,
+    FP_EINTERNAL,
+    FP_EDEVICE
+} fp_status;
+
+typedef struct fp_op fp_op;
+typedef struct fp_workspace fp_workspace;
+
+/* include/fastprox.h:93-103. threads is ignored on the device. */
+typedef struct {
+    int    axis;
+    int    threads;
+    double tol;
+    int    max_iter;
+    int    tie;
+    int    keep_structure;
+} fp_options;
+
+/* include/fastprox.h:105-109. */
+typedef struct {
+    double  gap;
+    int     iters;
+    int64_t ties;
+} fp_info;
+
+/* Replaces fp_options_init, include/fastprox.h:113. Defaults: axis -1,
+ * threads 0, tol 1e-6, max_iter 1000, tie 0, keep_structure 0. */
+FP_API void fp_options_init(fp_options *opt);
+
+/* Operator constructors: replace include/fastprox.h:322, :332, :343, :352
+ * (fp_op_tv_aniso, fp_op_tv_aniso_weighted, fp_op_tv_iso,
+ * fp_op_tv_iso_weighted). Same parameter rules and errors: ndim 2 or 3
+ * (FP_EPARAM otherwise); axis_weights NULL, length 1 or ndim, finite and
+ * >= 0; pixel weights of the image shape, edge weights of shape
+ * (ndim, image shape), finite and >= 0. Parameter arrays must be host
+ * arrays (they are copied). */
+FP_API fp_status fp_op_tv_aniso(int ndim, const fp_array *axis_weights, fp_op **out);
+FP_API fp_status fp_op_tv_aniso_weighted(int ndim, const fp_array *axis_weights,
+                                         const fp_array *edge_weights, fp_op **out);
+FP_API fp_status fp_op_tv_iso(int ndim, const fp_array *axis_weights, fp_op **out);
+FP_API fp_status fp_op_tv_iso_weighted(int ndim, const fp_array *axis_weights,
+                                       const fp_array *pixel_weights, fp_op **out);
+
+/* Replace include/fastprox.h:392-394. */
+FP_API void        fp_op_free(fp_op *op);
+FP_API int64_t     fp_op_nparams(const fp_op *op);
+FP_API const char *fp_op_name(const fp_op *op);
+
+/* Replaces include/fastprox.h:411-413. Every byte of device memory the
+ * calls on this workspace use is allocated here, on the calling thread's
+ * current device (FP_DEVICE_CUDA like) or on device 0 (FP_DEVICE_CPU like,
+ * whose calls then stage host arrays through it). */
+FP_API fp_status fp_workspace_create(const fp_op *op, const fp_array *like,
+                                     const fp_options *opt, fp_workspace **out);
+FP_API void      fp_workspace_free(fp_workspace *ws);
+
+/* Replace include/fastprox.h:426-428: the dual (ndim, *x.shape) of the last
+ * call, a seed for the next one, and warm starts from the previous call. */
+FP_API fp_status fp_workspace_get_dual(const fp_workspace *ws, fp_array *out);
+FP_API fp_status fp_workspace_set_dual(fp_workspace *ws, const fp_array *dual);
+FP_API fp_status fp_workspace_set_warm(fp_workspace *ws, int on);
+
+/* Replace include/fastprox.h:437-438 (derivative conjugate gradients). */
+FP_API fp_status fp_workspace_set_deriv_tol(fp_workspace *ws, double tol, int max_iter);
+FP_API fp_status fp_workspace_deriv_info(const fp_workspace *ws, double *residual, int *iters);
+
+/* Replaces include/fastprox.h:599-601. Stops each image when its duality gap
+ * is at most tol |x|^2 / 2; FP_ENOTCONV after max_iter with the last iterate
+ * written. Waits for the stream (it reads per-image flags between groups of
+ * iterations). */
+FP_API fp_status fp_prox(const fp_op *op, double gamma, const fp_array *x,
+                         fp_array *out, const fp_options *opt,
+                         fp_workspace *ws, fp_info *info);
+
+/* Replaces include/fastprox.h:613-614: one step per image (gamma has x's
+ * batch shape, host or device memory). */
+FP_API fp_status fp_prox_steps(const fp_op *op, const fp_array *gamma, const fp_array *x,
+                               fp_array *out, const fp_options *opt, fp_workspace *ws);
+
+/* Replaces include/fastprox.h:637-639 for the TV operators (positively
+ * homogeneous: the result is y - prox_g(y), for every sigma > 0; y for
+ * sigma = 0). */
+FP_API fp_status fp_prox_conj(const fp_op *op, double sigma, const fp_array *y,
+                              fp_array *out, const fp_options *opt,
+                              fp_workspace *ws, fp_info *info);
+
+/* Replace include/fastprox.h:646-654 and :779-780: derivatives at the point
+ * kept by the last prox call with keep_structure. */
+FP_API fp_status fp_jvp(const fp_op *op, const fp_workspace *ws,
+                        const fp_array *dx, double dgamma,
+                        const fp_array *dparams, fp_array *dout);
+FP_API fp_status fp_vjp(const fp_op *op, const fp_workspace *ws,
+                        const fp_array *g, fp_array *gx, double *ggamma,
+                        fp_array *gparams);
+FP_API fp_status fp_vjp_device(const fp_op *op, const fp_workspace *ws, const fp_array *g,
+                               fp_array *gx, fp_array *ggamma, fp_array *gparams);
+
+/* Replace include/fastprox.h:712 and :718. */
+FP_API int       fp_device_available(fp_device dev);
+FP_API fp_status fp_op_device_check(const fp_op *op, fp_device dev, int *row_parallel_only);
+
+/* Replace include/fastprox.h:724-725. */
+FP_API fp_status fp_workspace_set_stream(fp_workspace *ws, void *stream);
+FP_API fp_status fp_workspace_get_stream(const fp_workspace *ws, void **stream);
+
+/* Replace include/fastprox.h:732 and :773-774. */
+FP_API fp_status fp_workspace_info(const fp_workspace *ws, fp_info *info);
+FP_API fp_status fp_workspace_image_info(const fp_workspace *ws, double *gaps, int *iters,
+                                         double *zerrs, int64_t count);
+
+/* Replace include/fastprox.h:782-789. */
+FP_API const char *fp_strerror(fp_status s);
+FP_API int         fp_abi_version(void);
+FP_API const char *fp_version_string(void);
+FP_API int         fp_default_threads(void);
+
+/* ------------------------------------------------------------------------
+ * Extensions of this library (no counterpart in the reference ABI).
+ * ---------------------------------------------------------------------- */
+
+/* Counters of the last prox call on ws: the kernels it launched (set-up,
+ * iterations, finalisation) and the step launches alone. For benchmarks and
+ * tests; FP_EINVAL before a call. */
+FP_API fp_status fp_b200_workspace_stats(const fp_workspace *ws, int64_t *kernel_launches,
+                                         int64_t *step_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTPROX_B200_H */
