@@ -1,0 +1,91 @@
+// Host-visible structures of the anisotropic engine (tv_aniso.cu).
+#pragma once
+
+#include <cuda_runtime_api.h>
+
+#include <cstdint>
+
+namespace fpb {
+
+enum AnMode : int { kAnAdbpg = 0, kAnFdpg3 = 1, kAnSingle = 2, kAnIdentity = 3, kAnNan = 4, kAnInf = 5 };
+enum AnStage : int { kStIter = 0, kStCheck = 1, kStPolish = 2, kStFinal = 3, kStDone = 4 };
+
+struct AnGeom {
+    int k;
+    int64_t L[3];
+    int64_t S[3];
+    int64_t N, B;
+};
+
+struct AnCall {
+    double w[3];
+    double tol;
+    int max_iter;
+    double step_scale;
+    int has_beta;
+    double beta_max;
+    int64_t N;
+    int has_adbpg, has_fdpg3;
+};
+
+struct AnImage {
+    double gamma_in;
+    double lam[3];   // gamma w_a 2^-e on active axes, else 0
+    double target;   // tol |d|^2 / 2 at the solved scale
+    double dd;
+    double maxabs;
+    int e, mode, flags, na, a1, a2, fx_shift, pad;
+};
+
+// The scalars of TVAniso::adbpg / fdpg3 (src/ops/tv_aniso.cpp:429-616).
+struct AnState {
+    int status, stage, it, since, last, restart, warm, polished, zsel, pol_accept;
+    int chk_next, chk_prev_it;
+    double tn, beta, gp, gz, accept, chk_prev, pol_next;
+};
+
+struct AnBuffers {
+    void *d = nullptr, *z = nullptr, *u = nullptr, *y = nullptr, *wv = nullptr, *zp = nullptr, *scratch = nullptr;
+    void *dual = nullptr;
+    const void *beta = nullptr;  // edge weights (T), k x N, or null
+    uint8_t *flag = nullptr;
+    int *parent = nullptr;
+    unsigned long long *sum = nullptr;
+    int *cnt = nullptr;
+    AnImage *img = nullptr;
+    AnState *st = nullptr;
+    double *gammas = nullptr;
+    double *part = nullptr;
+    unsigned *ticket = nullptr;
+    int *live = nullptr;
+    int *err = nullptr;
+    int max_part = 0;
+};
+
+// CheckSchedule::done (src/ops/tv_aniso.cpp:400-413): after the first two
+// checks, every 4 iterations, sooner when the rate of the gap's fall
+// predicts the target.
+#ifdef __CUDACC__
+__device__ __forceinline__ void check_done(AnState &s, double gp, double target) {
+    int step = 1;
+    if (s.chk_prev_it >= 0) {
+        step = 4;
+        if (gp < s.chk_prev && gp > target) {
+            const double n = log(target / gp) / log(gp / s.chk_prev) * (double)(s.it - s.chk_prev_it);
+            if (n < 4.0) step = n > 1.0 ? (int)n : 1;
+        }
+    }
+    s.chk_prev_it = s.it;
+    s.chk_prev = gp;
+    s.chk_next = s.it + step;
+}
+#endif
+
+int an_pixel_blocks(const AnGeom &g);
+cudaError_t aniso_setup(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, const void *x,
+                        cudaStream_t s);
+cudaError_t aniso_round(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s,
+                        int64_t *launches);
+cudaError_t aniso_output(int dtype, const AnGeom &g, const AnBuffers &bf, void *out, cudaStream_t s);
+
+}  // namespace fpb

@@ -508,16 +508,40 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
             if (cudaMemcpy(ws->spatial, tmp.data(), tmp.size(), cudaMemcpyHostToDevice) != cudaSuccess) s = FP_EDEVICE;
         }
     }
-    // per-image state, partials and tickets
-    ws->shape_ = iso_pick_shape(x.dtype, g, 0, 0);
+    // per-image state, partials and tickets; launch shape (tuning hints from
+    // the environment: FASTPROX_B200_ROWS, FASTPROX_B200_BX, FASTPROX_B200_VEC)
+    auto env_int = [](const char *n) {
+        const char *v = std::getenv(n);
+        return v ? std::atoi(v) : 0;
+    };
+    ws->shape_ = iso_pick_shape(x.dtype, g, env_int("FASTPROX_B200_ROWS"), env_int("FASTPROX_B200_BX"),
+                                env_int("FASTPROX_B200_KIND"));
+    if (const int vh = env_int("FASTPROX_B200_VEC")) {
+        if (ws->shape_.kind == 0 && vh > 0 && vh <= ws->shape_.vec && g.L[1] % vh == 0) {
+            const int64_t cols = (g.L[1] + vh - 1) / vh;
+            ws->shape_.vec = vh;
+            ws->shape_.gx = (int)((cols + ws->shape_.bx - 1) / ws->shape_.bx);
+        }
+    }
+    if (const int ch = env_int("FASTPROX_B200_CHUNK")) ws->chunk = ch;
     ws->max_part = std::max(iso_setup_blocks(g), ws->shape_.gx * ws->shape_.gy);
     ws->max_part = std::max(ws->max_part, 4096);
+    if (op->kind == kAniso) {
+        A((void **)&ws->an_img, (size_t)B * sizeof(AnImage));
+        A((void **)&ws->an_st, (size_t)B * sizeof(AnState));
+        A(&ws->an_scratch, img);
+        A((void **)&ws->an_flag, (size_t)B * (size_t)N);
+        A((void **)&ws->an_parent, (size_t)B * (size_t)N * sizeof(int));
+        A((void **)&ws->an_cnt, (size_t)B * (size_t)N * sizeof(int));
+        A((void **)&ws->an_sum, (size_t)B * (size_t)N * sizeof(unsigned long long));
+    }
     A((void **)&ws->img, (size_t)B * sizeof(IsoImage));
     A((void **)&ws->st, (size_t)B * sizeof(IsoState));
     A((void **)&ws->gammas, (size_t)B * sizeof(double));
     A((void **)&ws->part, (size_t)B * (size_t)ws->max_part * 2 * sizeof(double));
     A((void **)&ws->ticket, (size_t)B * sizeof(unsigned));
     A((void **)&ws->live, 16);
+    A((void **)&ws->err, 16);
     auto H = [&](void **p, size_t bytes) {
         if (s == FP_OK) s = host_alloc(ws.get(), p, bytes);
     };
@@ -525,8 +549,13 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     H((void **)&ws->h_img, (size_t)B * sizeof(IsoImage));
     H((void **)&ws->h_st, (size_t)B * sizeof(IsoState));
     H((void **)&ws->h_gam, (size_t)B * sizeof(double));
+    if (op->kind == kAniso) {
+        H((void **)&ws->h_an_img, (size_t)B * sizeof(AnImage));
+        H((void **)&ws->h_an_st, (size_t)B * sizeof(AnState));
+    }
     if (ws->host_mode) H(&ws->h_stage, img);
     if (s == FP_OK && cudaMemset(ws->ticket, 0, (size_t)B * sizeof(unsigned)) != cudaSuccess) s = FP_EDEVICE;
+    if (s == FP_OK && cudaMemset(ws->err, 0, 16) != cudaSuccess) s = FP_EDEVICE;
     for (int i = 0; i < 2 && s == FP_OK; ++i)
         if (cudaEventCreateWithFlags(&ws->ev[i], cudaEventDisableTiming) != cudaSuccess) s = FP_EDEVICE;
     if (s == FP_OK && cudaDeviceSynchronize() != cudaSuccess) s = FP_EDEVICE;
@@ -842,6 +871,7 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     bf.part = ws->part;
     bf.ticket = ws->ticket;
     bf.live = ws->live;
+    bf.err = ws->err;
     bf.max_part = ws->max_part;
 
     cudaError_t e = cudaMemsetAsync(ws->live, 0, sizeof(int), s);
@@ -856,7 +886,7 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     bool done = false;
     while (!done) {
         for (int j = 0; j < chunk; ++j) {
-            e = iso_step(ws->dtype, g, c, bf, ws->shape_, par, s);
+            e = iso_step(ws->dtype, g, c, bf, ws->shape_, par, iso_variant(launched, max_iter, warm), s);
             if (e != cudaSuccess) return cuda_status(e);
             par ^= 1;
             ++launched;
@@ -877,6 +907,90 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     ws->launches = launched;
     ws->kernel_launches += launched + 3 + (warm ? 1 : 0) + 1 + ((c.na == 1 && !c.has_alpha) ? 1 : 0);
     e = iso_finalize(ws->dtype, g, c, bf, zdst, s);
+    return cuda_status(e);
+}
+
+fp_status run_aniso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zdst, double tol, int max_iter) {
+    const Geometry &g0 = ws->g;
+    cudaStream_t s = ws->stream;
+    const size_t T = ws->dtype == FP_F32 ? 4 : 8;
+    AnGeom g{};
+    g.k = g0.k;
+    for (int a = 0; a < 3; ++a) g.L[a] = g0.L[a];
+    g.S[g.k - 1] = 1;
+    for (int a = g.k - 2; a >= 0; --a) g.S[a] = g.S[a + 1] * g.L[a + 1];
+    for (int a = g.k; a < 3; ++a) g.S[a] = 1;
+    g.N = g0.N;
+    g.B = g0.B;
+    AnCall c{};
+    int na = 0;
+    for (int a = 0; a < 3; ++a) {
+        c.w[a] = a < g.k ? op->w[a] : 0.0;
+        if (a < g.k && op->w[a] > 0.0 && g.L[a] > 1) ++na;
+    }
+    c.tol = tol;
+    c.max_iter = max_iter;
+    c.has_beta = op->spatial.empty() ? 0 : 1;
+    c.beta_max = op->spatial.empty() ? 1.0 : op->smax;
+    c.step_scale = std::max({op->w[0], op->w[1], op->w[2]}) * (op->spatial.empty() ? 1.0 : op->smax);
+    c.N = g.N;
+    c.has_adbpg = na == 2;
+    c.has_fdpg3 = na == 3;
+    AnBuffers bf;
+    const size_t bn = (size_t)g.B * (size_t)g.N;
+    bf.d = ws->d;
+    bf.y = ws->U[0];
+    bf.wv = ws->V[0];
+    bf.z = ws->U[1];
+    bf.zp = static_cast<char *>(ws->U[1]) + bn * T;
+    bf.u = ws->V[1];
+    bf.scratch = ws->an_scratch;
+    bf.dual = ws->dual;
+    bf.beta = ws->spatial;
+    bf.flag = ws->an_flag;
+    bf.parent = ws->an_parent;
+    bf.sum = ws->an_sum;
+    bf.cnt = ws->an_cnt;
+    bf.img = ws->an_img;
+    bf.st = ws->an_st;
+    bf.gammas = ws->gammas;
+    bf.part = ws->part;
+    bf.ticket = ws->ticket;
+    bf.live = ws->live;
+    bf.err = ws->err;
+    bf.max_part = ws->max_part;
+    cudaError_t e = cudaMemsetAsync(ws->live, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws->U[0], 0, (size_t)g.k * bn * T, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws->V[0], 0, (size_t)g.k * bn * T, s);
+    if (e == cudaSuccess) e = aniso_setup(ws->dtype, g, c, bf, xsrc, s);
+    if (e != cudaSuccess) return cuda_status(e);
+    int64_t launches = 5;
+    // rounds of launches (an iteration each, with its check, polish and
+    // retirement), the live count read back behind two rounds in flight
+    int slot = 0, inflight = 0;
+    int64_t rounds = 0;
+    const int64_t cap = (int64_t)max_iter + 4;
+    bool done = false;
+    while (!done) {
+        e = aniso_round(ws->dtype, g, c, bf, s, &launches);
+        if (e != cudaSuccess) return cuda_status(e);
+        ++rounds;
+        e = cudaMemcpyAsync(ws->h_live + slot, ws->live, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaEventRecord(ws->ev[slot], s);
+        if (e != cudaSuccess) return cuda_status(e);
+        slot ^= 1;
+        ++inflight;
+        if (inflight == 2) {
+            e = cudaEventSynchronize(ws->ev[slot]);
+            if (e != cudaSuccess) return cuda_status(e);
+            --inflight;
+            if (ws->h_live[slot] == 0) done = true;
+        }
+        if (rounds >= cap) done = true;
+    }
+    ws->launches = rounds;
+    ws->kernel_launches += launches + 1;
+    e = aniso_output(ws->dtype, g, bf, zdst, s);
     return cuda_status(e);
 }
 
@@ -990,7 +1104,6 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
     if (x.device == FP_DEVICE_CUDA) {
         if (pointer_device(x.data) != ws->device || pointer_device(out.data) != ws->device) return FP_EINVAL;
     }
-    if (op->kind != kIso) return FP_EINVAL;  // anisotropic TV: see aniso.cu
     if (device_steps) {
         // the steps into the workspace (as doubles), read back and checked
         if (pointer_device(st.data) != ws->device) return FP_EINVAL;
@@ -1081,15 +1194,26 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
     // at the end of the solve (stage, or V[1] when stage holds y)
     const bool direct_out = !ws->host_mode && out.contiguous();
     void *zdst = direct_out ? out.data : (conj ? ws->V[1] : ws->stage);
-    if (fp_status st2 = run_iso(ws, op, xsrc, zdst, o.tol, o.max_iter, warm)) return st2;
+    if (op->kind == kIso) {
+        if (fp_status st2 = run_iso(ws, op, xsrc, zdst, o.tol, o.max_iter, warm)) return st2;
+    } else {
+        // anisotropic warm starts restart cold (the dual seed is not read)
+        if (fp_status st2 = run_aniso(ws, op, xsrc, zdst, o.tol, o.max_iter)) return st2;
+    }
     if (conj) {
         e = conj_finish(ws->dtype, ysave, zdst, total, s);
         if (e != cudaSuccess) return cuda_status(e);
     }
     // Results back to the host
-    e = cudaMemcpyAsync(ws->h_img, ws->img, (size_t)g.B * sizeof(IsoImage), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(ws->h_st, ws->st, (size_t)g.B * sizeof(IsoState), cudaMemcpyDeviceToHost, s);
+    if (op->kind == kIso) {
+        e = cudaMemcpyAsync(ws->h_img, ws->img, (size_t)g.B * sizeof(IsoImage), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ws->h_st, ws->st, (size_t)g.B * sizeof(IsoState), cudaMemcpyDeviceToHost, s);
+    } else {
+        e = cudaMemcpyAsync(ws->h_an_img, ws->an_img, (size_t)g.B * sizeof(AnImage), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ws->h_an_st, ws->an_st, (size_t)g.B * sizeof(AnState), cudaMemcpyDeviceToHost, s);
+    }
     if (e != cudaSuccess) return cuda_status(e);
     if (!direct_out) {
         if (ws->host_mode) {
@@ -1120,11 +1244,41 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
     }
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e);
+    {
+        int herr = 0;
+        if (cudaMemcpy(&herr, ws->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return FP_EDEVICE;
+        if (herr) {
+            cudaMemset(ws->err, 0, sizeof(int));
+            return FP_EDEVICE;
+        }
+    }
     // Per-image results (driver.hpp:1303-1341)
     bool inf = false, notconv = false;
     double gsum = 0.0;
     int imax = 0;
     for (int64_t b = 0; b < g.B; ++b) {
+        if (op->kind == kAniso) {
+            const AnImage &im = ws->h_an_img[b];
+            const AnState &sst = ws->h_an_st[b];
+            double gap = 0.0, gap_s = 0.0;
+            int it = 0;
+            if (im.mode == kAnInf) {
+                inf = true;
+            } else if (im.mode == kAnNan) {
+                gap = gap_s = std::numeric_limits<double>::quiet_NaN();
+            } else if (im.mode == kAnAdbpg || im.mode == kAnFdpg3) {
+                gap_s = std::isnan(sst.gp) ? sst.gp : std::max(sst.gp, 0.0);
+                gap = im.e ? std::ldexp(gap_s, 2 * im.e) : gap_s;
+                it = sst.it;
+                if (sst.status != kConverged) notconv = true;
+            }
+            ws->gaps[(size_t)b] = gap;
+            ws->iters[(size_t)b] = it;
+            ws->zerrs[(size_t)b] = certified_error(gap_s, im.dd, g.N, im.e, ws->dtype, conj ? 2 : 1);
+            gsum += gap;
+            imax = std::max(imax, it);
+            continue;
+        }
         const IsoImage &im = ws->h_img[b];
         const IsoState &sst = ws->h_st[b];
         double gap = 0.0, gap_s = 0.0;

@@ -21,19 +21,20 @@ struct IsoBuffers {
     double *part = nullptr;     // B x max_part x 2
     unsigned *ticket = nullptr; // B
     int *live = nullptr;        // images still iterating
+    int *err = nullptr;         // set by a kernel whose copies never completed
     int max_part = 0;
 };
 
 // Launch shape of the step kernel, picked per geometry (and by the tuner).
 struct StepShape {
-    int kind = 0;   // 0: 2D row-marching, 1: generic (one thread per pixel)
+    int kind = 0;   // 0: 2D row-marching, 1: generic (one thread per pixel), 2: 2D TMA row pipeline
     int vec = 1;    // pixels per thread along the contiguous axis (march)
     int bx = 128;   // threads per block
     int rows = 16;  // rows per block (march)
     int gx = 1, gy = 1;  // blocks per image = gx * gy
 };
 
-StepShape iso_pick_shape(int dtype, const Geometry &g, int rows_hint, int bx_hint);
+StepShape iso_pick_shape(int dtype, const Geometry &g, int rows_hint, int bx_hint, int kind_hint = 0);
 int iso_setup_blocks(const Geometry &g);
 
 // Set-up: stage x (contiguous, device) into d, per-image scans, state
@@ -42,8 +43,14 @@ cudaError_t iso_setup(int dtype, const Geometry &g, const IsoCall &c, const IsoB
                       int warm, int par, cudaStream_t s);
 // One dual-FISTA iteration (and the gap / restart tests it carries) for
 // every live image, reading buffers par and writing par ^ 1.
+// variant (the lean kernel, chosen from the launch index k of a call):
+// 1 the cold first iteration (u = v = 0), 2 a launch carrying a gap check, 0 otherwise.
 cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh,
-                     int par, cudaStream_t s);
+                     int par, int variant, cudaStream_t s);
+inline int iso_variant(int64_t k, int max_iter, bool warm) {
+    if (k == 0) return warm ? 2 : 1;
+    return (k % 4 == 0 || k == max_iter) ? 2 : 0;
+}
 // z = x - G^T q into out (contiguous, device, x's dtype), the dual into
 // bf.dual, for every image by its mode; exact 1D TV for single-axis images.
 cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, void *out,

@@ -1,0 +1,924 @@
+// Anisotropic image TV on sm_100a: the reference's own method, replayed per
+// image on the device.
+//
+// Two active axes: the accelerated dual block proximal gradient method
+// (ADBPG) of TVAniso::adbpg (src/ops/tv_aniso.cpp:429-530): per iteration an
+// exact 1D TV prox of every fibre along the axis of smaller stride (a1) and
+// then along the other (a2), the dual update with extrapolation, the gradient
+// restart every 4 iterations (Restart, :357-367), gap checks on the adaptive
+// CheckSchedule (:396-414), and the polish on the PolishSchedule (:382-391)
+// that reads the flat regions off the dual and solves on them exactly
+// (try_polish, :886-953). Three active axes: FDPG for three terms
+// (TVAniso::fdpg3, :534-616). One active axis: a single exact pass.
+//
+// Each image carries a stage (iterate, check, polish, final, done); every
+// kernel acts only on the images in its stage, and the last block of an
+// image (a ticket per image) advances the stage with the scalar logic of the
+// reference in FP64. The host issues the same round of launches until no
+// image is live. The 1D steps are Condat's algorithm, one thread per fibre
+// (tv1d.cuh). Components of the polish are found by union-find with atomic
+// hooking of the larger root to the smaller (so every root is the smallest
+// index of its component, whatever the order), and region sums use 64-bit
+// fixed point, so every result is the same bit for bit on every run.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+
+#include "aniso.h"
+#include "common.cuh"
+#include "tv1d.cuh"
+
+namespace fpb {
+namespace {
+
+constexpr int kCheck = 4;               // tv_aniso.cpp:76
+constexpr double kPolishDrop = 0.1;     // :78
+constexpr double kPolishEta = 1e-9;     // :81, for FP64 duals
+// FP32 duals carry rounding near 1e-7 of the bound: the margin of the
+// reference's own device path for float32, max(1e-9, 64 eps)
+// (bindings/python/fastprox/_tv_torch.py dual_eta).
+template <class T>
+__device__ __forceinline__ double polish_eta() {
+    return sizeof(T) == 4 ? 64.0 * 1.1920928955078125e-07 : kPolishEta;
+}
+constexpr double kPolishRatio = 0.01;   // :86
+constexpr int kThreads = 256;
+
+template <class T>
+__device__ __forceinline__ T ldexp_t(T v, int e);
+template <>
+__device__ __forceinline__ float ldexp_t<float>(float v, int e) { return ldexpf(v, e); }
+template <>
+__device__ __forceinline__ double ldexp_t<double>(double v, int e) { return ldexp(v, e); }
+
+struct Fib {
+    int64_t s, L, nfib;
+    __device__ __forceinline__ int64_t base(int64_t f) const { return (f / s) * L * s + (f % s); }
+};
+
+__device__ __forceinline__ Fib fibers(const AnGeom &g, int a) {
+    Fib f;
+    f.s = g.S[a];
+    f.L = g.L[a];
+    f.nfib = g.N / g.L[a];
+    return f;
+}
+
+__device__ __forceinline__ double *img_part(const AnBuffers &bf, int b) { return bf.part + (int64_t)b * bf.max_part * 2; }
+
+// Ends a per-image reduction: block partial (two sums) to part, and in the
+// last block of the image the totals. Returns true in thread 0 of that block.
+__device__ __forceinline__ bool reduce2(const AnBuffers &bf, int b, unsigned blk, unsigned nblk, double a0,
+                                        double a1, double *sh, int *flag, double &t0, double &t1) {
+    const double s0 = block_sum(a0, sh);
+    const double s1 = block_sum(a1, sh);
+    double *part = img_part(bf, b);
+    if (threadIdx.x == 0) {
+        part[blk * 2 + 0] = s0;
+        part[blk * 2 + 1] = s1;
+    }
+    if (!arrive_last(bf.ticket + b, nblk, flag)) return false;
+    t0 = sum_partials(part, nblk, 2, 0, sh);
+    t1 = sum_partials(part, nblk, 2, 1, sh);
+    if (threadIdx.x != 0) return false;
+    bf.ticket[b] = 0;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Set-up (tv_aniso.cpp:260-340)
+// ---------------------------------------------------------------------------
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) an_scan1(const T *__restrict__ x, AnGeom g, AnCall c, AnBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const T *xb = x + (int64_t)b * N;
+    T *db = static_cast<T *>(bf.d) + (int64_t)b * N;
+    double m = 0.0;
+    int fl = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const T v = xb[i];
+        if (xb != db) db[i] = v;
+        const double a = fabs((double)v);
+        if (isnan(a)) fl |= 1;
+        else if (isinf(a)) fl |= 2;
+        else m = fmax(m, a);
+    }
+    const double mb = block_max(m, sh);
+    const double f1 = block_max((double)(fl & 1), sh);
+    const double f2 = block_max((double)((fl >> 1) & 1), sh);
+    double *part = img_part(bf, b);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 2 + 0] = mb;
+        part[blockIdx.x * 2 + 1] = f1 + 2.0 * f2;
+    }
+    if (!arrive_last(bf.ticket + b, gridDim.x, &flag)) return;
+    const double mx = max_partials(part, gridDim.x, 2, 0, sh);
+    double o1 = 0.0, o2 = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+        const int code = (int)__ldcg(part + i * 2 + 1);
+        o1 = fmax(o1, (double)(code & 1));
+        o2 = fmax(o2, (double)((code >> 1) & 1));
+    }
+    o1 = block_max(o1, sh);
+    o2 = block_max(o2, sh);
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    AnImage im{};
+    im.gamma_in = bf.gammas[b];
+    im.maxabs = mx;
+    im.flags = (o1 > 0.0 ? 1 : 0) | (o2 > 0.0 ? 2 : 0);
+    int na = 0;
+    for (int a = 0; a < 3; ++a) {
+        im.lam[a] = 0.0;
+        if (a < g.k) {
+            const double l = im.gamma_in * c.w[a];
+            if (l > 0.0 && g.L[a] > 1) {
+                im.lam[a] = l;
+                ++na;
+            }
+        }
+    }
+    im.na = na;
+    if (im.flags & 2) im.mode = kAnInf;
+    else if (im.flags & 1) im.mode = kAnNan;
+    else if (na == 0) im.mode = kAnIdentity;
+    else if (na == 1) im.mode = kAnSingle;
+    else im.mode = na == 2 ? kAnAdbpg : kAnFdpg3;
+    int e = 0;
+    if (na > 0 && mx > 0.0) {  // rescale_exponent (src/ops/image_util.hpp:56-65)
+        const double gamma = im.gamma_in;
+        e = ilogb(mx);
+        if (e >= -64 && e <= 64) {
+            e = 0;
+        } else {
+            const double top = fmax(gamma, gamma * c.step_scale);
+            if (e < 0 && top > 0.0) e = min(0, max(e, ilogb(top) + 1 - 960));
+        }
+        for (int a = 0; a < 3 && e; ++a)
+            if (im.lam[a] > 0.0 && !(ldexp(im.lam[a], -e) > 0.0)) e = 0;
+    }
+    im.e = e;
+    for (int a = 0; a < 3; ++a) im.lam[a] = e ? ldexp(im.lam[a], -e) : im.lam[a];
+    // the active axes of ADBPG: a1 of the smaller stride (tv_aniso.cpp:432-433)
+    int act[3], n = 0;
+    for (int a = 0; a < g.k; ++a)
+        if (im.lam[a] > 0.0) act[n++] = a;
+    im.a1 = n >= 2 ? (g.S[act[0]] < g.S[act[1]] ? act[0] : act[1]) : (n ? act[0] : 0);
+    im.a2 = n >= 2 ? (im.a1 == act[0] ? act[1] : act[0]) : 0;
+    // the fixed-point scale of the polish's region sums: |zp| <= max|d| + 2 k lam_max beta_max
+    double lmax = 0.0;
+    for (int a = 0; a < 3; ++a) lmax = fmax(lmax, im.lam[a]);
+    const double zb = ldexp(mx, -e) + 2.0 * g.k * lmax * c.beta_max + 1e-300;
+    int lgN = 0;
+    while ((1LL << lgN) <= g.N) ++lgN;
+    im.fx_shift = 61 - lgN - (ilogb(zb) + 1);
+    bf.img[b] = im;
+    AnState st{};
+    st.status = (im.mode == kAnAdbpg || im.mode == kAnFdpg3) ? kLive : kFinished;
+    st.stage = kStIter;
+    st.tn = fista_t(1.0);
+    st.beta = 0.0;
+    st.gp = CUDART_INF;
+    st.chk_next = 1;
+    st.chk_prev_it = -1;
+    st.pol_next = CUDART_INF;
+    bf.st[b] = st;
+    if (st.status == kLive) atomicAdd(bf.live, 1);
+}
+
+// d *= 2^-e, |d|^2 -> target (tv_aniso.cpp:329-337)
+template <class T>
+__global__ void __launch_bounds__(kThreads) an_scan2(AnGeom g, AnCall c, AnBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const int mode = bf.img[b].mode;
+    if (mode == kAnNan || mode == kAnInf) return;
+    const int e = bf.img[b].e;
+    T *db = static_cast<T *>(bf.d) + (int64_t)b * g.N;
+    double s2 = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.N; i += (int64_t)gridDim.x * blockDim.x) {
+        T v = db[i];
+        if (e) {
+            v = ldexp_t(v, -e);
+            db[i] = v;
+        }
+        s2 += (double)v * (double)v;
+    }
+    double t0, t1;
+    if (!reduce2(bf, b, blockIdx.x, gridDim.x, s2, 0.0, sh, &flag, t0, t1)) return;
+    bf.img[b].dd = t0;
+    bf.img[b].target = c.tol * 0.5 * t0;
+}
+
+// ---------------------------------------------------------------------------
+// Fibre passes of the iteration
+// ---------------------------------------------------------------------------
+
+// Edge weight of the edge (o, o + S[a]) times nothing (beta), or 1.
+template <class T>
+struct BetaW {
+    const T *p;
+    int64_t s;
+    __device__ __forceinline__ double operator()(int64_t i) const { return (double)p[i * s]; }
+};
+
+// One exact 1D TV prox on fibre f of axis a of image b: in(i) -> out(i, v).
+template <class T, class In, class Out>
+__device__ __forceinline__ void fibre_prox(const AnCall &c, const AnBuffers &bf, int a, int64_t base, const Fib &fb,
+                                           double lam, const In &in, const Out &out) {
+    if (c.has_beta) {
+        const T *bw = static_cast<const T *>(bf.beta) + (int64_t)a * c.N + base;
+        tv1d_fiber(in, out, fb.L, lam, true, BetaW<T>{bw, fb.s});
+    } else {
+        tv1d_fiber(in, out, fb.L, lam, false, NoWeight{});
+    }
+}
+
+// ADBPG first block step: u = prox_{g1}(d + w) along a1 (tv_aniso.cpp:459-460).
+template <class T>
+__global__ void __launch_bounds__(128) an_pass1(AnGeom g, AnCall c, AnBuffers bf) {
+    const int b = blockIdx.y;
+    const AnState &st = bf.st[b];
+    if (st.status != kLive || st.stage != kStIter) return;
+    const AnImage &im = bf.img[b];
+    if (im.mode != kAnAdbpg) return;
+    const int a = im.a1;
+    const Fib fb = fibers(g, a);
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= fb.nfib) return;
+    const int64_t N = g.N, base = fb.base(f), s = fb.s;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N + base;
+    const T *Wv = static_cast<const T *>(bf.wv) + (int64_t)b * g.k * N + base;
+    T *U = static_cast<T *>(bf.u) + (int64_t)b * N + base;
+    auto in = [D, Wv, s](int64_t i) -> double { return (double)(D[i * s] + Wv[i * s]); };
+    auto out = [U, s](int64_t i, double v) { U[i * s] = (T)v; };
+    fibre_prox<T>(c, bf, a, base, fb, im.lam[a], in, out);
+}
+
+// ADBPG second block step along a2 with the dual update and extrapolation
+// (tv_aniso.cpp:461-80); the last block runs the restart test, advances the
+// iteration and decides whether a gap check is due.
+template <class T>
+__global__ void __launch_bounds__(128) an_pass2(AnGeom g, AnCall c, AnBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const AnState st = bf.st[b];
+    if (st.status != kLive || st.stage != kStIter) return;
+    const AnImage &im = bf.img[b];
+    if (im.mode != kAnAdbpg) return;
+    const int a = im.a2;
+    const Fib fb = fibers(g, a);
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t N = g.N;
+    const bool test = st.it % kCheck == 0;
+    const T beta = (T)st.beta;
+    double up = 0.0;
+    if (f < fb.nfib) {
+        const int64_t base = fb.base(f), s = fb.s;
+        const T *U = static_cast<const T *>(bf.u) + (int64_t)b * N + base;
+        T *Wv = static_cast<T *>(bf.wv) + (int64_t)b * g.k * N + base;
+        T *Y = static_cast<T *>(bf.y) + (int64_t)b * g.k * N + base;
+        T *Z = static_cast<T *>(bf.z) + (int64_t)b * N + base;
+        auto in = [U, Wv, s](int64_t i) -> double { return (double)(U[i * s] - Wv[i * s]); };
+        auto out = [Z, s](int64_t i, double v) { Z[i * s] = (T)v; };
+        fibre_prox<T>(c, bf, a, base, fb, im.lam[a], in, out);
+        for (int64_t i = 0; i < fb.L; ++i) {
+            const int64_t o = i * s;
+            const T v = U[o] - Wv[o];
+            const T yn = Z[o] - v;
+            const T y = Y[o], w = Wv[o];
+            if (test) up += (double)((w - yn) * (yn - y));
+            Wv[o] = yn + beta * (yn - y);
+            Y[o] = yn;
+        }
+    }
+    double dot, unused;
+    if (!reduce2(bf, b, blockIdx.x, gridDim.x, test ? up : 0.0, 0.0, sh, &flag, dot, unused)) return;
+    AnState s2 = st;
+    // Restart (tv_aniso.cpp:357-367): ++since; restart when test && up > 0 && since >= last
+    s2.since += 1;
+    double t = s2.tn;
+    if (test && dot > 0.0 && s2.since >= s2.last) {
+        s2.last = s2.since;
+        s2.since = 0;
+        s2.restart = 1;
+        t = 1.0;
+    } else {
+        s2.restart = 0;
+    }
+    s2.it += 1;
+    const double tn = fista_t(t);
+    s2.beta = (t - 1.0) / tn;
+    s2.tn = tn;
+    if (s2.it == s2.chk_next || s2.it == c.max_iter) s2.stage = kStCheck;
+    bf.st[b] = s2;
+}
+
+// After a restart the extrapolated dual restarts from y (tv_aniso.cpp:474-477).
+template <class T>
+__global__ void an_restart_copy(AnGeom g, AnBuffers bf) {
+    const int b = blockIdx.y;
+    const AnState &st = bf.st[b];
+    if (st.status != kLive || !st.restart) return;
+    const int64_t n = (int64_t)g.k * g.N;
+    const T *Y = static_cast<const T *>(bf.y) + (int64_t)b * n;
+    T *Wv = static_cast<T *>(bf.wv) + (int64_t)b * n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        Wv[i] = Y[i];
+}
+
+// FDPG-3 (tv_aniso.cpp:534-616): u = d + w0 + w1 + w2, then for each axis a
+// y_a+ = (prox_{3 g_a}(u - 3 w_a) - (u - 3 w_a)) / 3 and the extrapolation.
+template <class T>
+__global__ void an_fdpg3_u(AnGeom g, AnBuffers bf) {
+    const int b = blockIdx.y;
+    const AnState &st = bf.st[b];
+    if (st.status != kLive || st.stage != kStIter || bf.img[b].mode != kAnFdpg3) return;
+    const int64_t N = g.N;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *Wv = static_cast<const T *>(bf.wv) + (int64_t)b * 3 * N;
+    T *U = static_cast<T *>(bf.u) + (int64_t)b * N;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        U[i] = D[i] + Wv[i] + Wv[N + i] + Wv[2 * N + i];
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) an_fdpg3_pass(AnGeom g, AnCall c, AnBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.z;
+    const AnState st = bf.st[b];
+    if (st.status != kLive || st.stage != kStIter) return;
+    const AnImage &im = bf.img[b];
+    if (im.mode != kAnFdpg3) return;
+    const int64_t N = g.N;
+    const bool test = st.it % kCheck == 0;
+    const T beta = (T)st.beta;
+    double up = 0.0;
+    // blockIdx.y = axis; the fibres of all three axes in one launch
+    const int a = blockIdx.y;
+    const Fib fb = fibers(g, a);
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < fb.nfib) {
+        const int64_t base = fb.base(f), s = fb.s;
+        const T *U = static_cast<const T *>(bf.u) + (int64_t)b * N + base;
+        T *Wa = static_cast<T *>(bf.wv) + ((int64_t)b * 3 + a) * N + base;
+        T *Ya = static_cast<T *>(bf.y) + ((int64_t)b * 3 + a) * N + base;
+        T *Zs = static_cast<T *>(bf.zp) + (int64_t)b * N;  // scratch: z of this axis' fibres
+        T *Za = Zs + base;
+        // the three axes write disjoint scratch: zp (a = 0), z (a = 1), dual slot (a = 2)
+        if (a == 1) Za = static_cast<T *>(bf.z) + (int64_t)b * N + base;
+        if (a == 2) Za = static_cast<T *>(bf.scratch) + (int64_t)b * N + base;
+        auto in = [U, Wa, s](int64_t i) -> double { return (double)(U[i * s] - T(3) * Wa[i * s]); };
+        auto out = [Za, s](int64_t i, double v) { Za[i * s] = (T)v; };
+        fibre_prox<T>(c, bf, a, base, fb, 3.0 * im.lam[a], in, out);
+        for (int64_t i = 0; i < fb.L; ++i) {
+            const int64_t o = i * s;
+            const T v = U[o] - T(3) * Wa[o];
+            const T yn = (Za[o] - v) / T(3);
+            const T y = Ya[o], w = Wa[o];
+            if (test) up += (double)((w - yn) * (yn - y));
+            Wa[o] = yn + beta * (yn - y);
+            Ya[o] = yn;
+        }
+    }
+    double dot, unused;
+    const unsigned nblk = gridDim.x * gridDim.y;
+    const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
+    if (!reduce2(bf, b, blk, nblk, test ? up : 0.0, 0.0, sh, &flag, dot, unused)) return;
+    AnState s2 = st;
+    s2.since += 1;
+    double t = s2.tn;
+    if (test && dot > 0.0 && s2.since >= s2.last) {
+        s2.last = s2.since;
+        s2.since = 0;
+        s2.restart = 1;
+        t = 1.0;
+    } else {
+        s2.restart = 0;
+    }
+    s2.it += 1;
+    const double tn = fista_t(t);
+    s2.beta = (t - 1.0) / tn;
+    s2.tn = tn;
+    if (s2.it % kCheck == 0 || s2.it == c.max_iter) s2.stage = kStCheck;
+    bf.st[b] = s2;
+}
+
+// FDPG-3's primal at a check: z = prox_{g_c}(d + y_0 + y_1) along the
+// contiguous axis c = 2 (tv_aniso.cpp:118-123).
+template <class T>
+__global__ void __launch_bounds__(128) an_fdpg3_primal(AnGeom g, AnCall c, AnBuffers bf, int stage) {
+    const int b = blockIdx.y;
+    const AnState &st = bf.st[b];
+    if (st.status != kLive || st.stage != stage) return;
+    const AnImage &im = bf.img[b];
+    if (im.mode != kAnFdpg3) return;
+    const Fib fb = fibers(g, 2);
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= fb.nfib) return;
+    const int64_t N = g.N, base = fb.base(f), s = fb.s;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N + base;
+    const T *Y0 = static_cast<const T *>(bf.y) + (int64_t)b * 3 * N + base;
+    const T *Y1 = Y0 + N;
+    T *Z = static_cast<T *>(bf.z) + (int64_t)b * N + base;
+    auto in = [D, Y0, Y1, s](int64_t i) -> double { return (double)(D[i * s] + Y0[i * s] + Y1[i * s]); };
+    auto out = [Z, s](int64_t i, double v) { Z[i * s] = (T)v; };
+    fibre_prox<T>(c, bf, 2, base, fb, im.lam[2], in, out);
+}
+
+// ---------------------------------------------------------------------------
+// The gap of a point: sum_a lam_e |z_j - z_i| - <z, d - z> (tv_aniso.cpp:192-226)
+// ---------------------------------------------------------------------------
+
+template <class T>
+__device__ __forceinline__ double tv_at(const AnGeom &g, const AnCall &c, const AnBuffers &bf, const AnImage &im,
+                                        const T *Z, int64_t p, int64_t Nimg) {
+    double s = 0.0;
+    for (int a = 0; a < g.k; ++a) {
+        const double l = im.lam[a];
+        if (l == 0.0) continue;
+        const int64_t co = (p / g.S[a]) % g.L[a];
+        if (co + 1 >= g.L[a]) continue;
+        double le = l;
+        if (c.has_beta) le = l * (double)static_cast<const T *>(bf.beta)[(int64_t)a * Nimg + p];
+        s += le * fabs((double)Z[p + g.S[a]] - (double)Z[p]);
+    }
+    return s;
+}
+
+// stage kStCheck: the gap of z; kStFinal: the gap of zp (the final rebuild).
+template <class T>
+__global__ void __launch_bounds__(kThreads) an_gap(AnGeom g, AnCall c, AnBuffers bf, int stage) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const AnState st = bf.st[b];
+    if (st.status != kLive || st.stage != stage) return;
+    if (stage == kStFinal && (st.polished || st.it == 0 || bf.img[b].mode != kAnAdbpg)) return;
+    const AnImage im = bf.img[b];
+    const int64_t N = g.N;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *Z = static_cast<const T *>(stage == kStCheck ? bf.z : bf.zp) + (int64_t)b * N;
+    double acc = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const double z = (double)Z[p];
+        acc += tv_at<T>(g, c, bf, im, Z, p, N) - z * ((double)D[p] - z);
+    }
+    double gz, unused;
+    if (!reduce2(bf, b, blockIdx.x, gridDim.x, acc, 0.0, sh, &flag, gz, unused)) return;
+    AnState s2 = st;
+    if (stage == kStFinal) {
+        // d - q1 - q2 in place of the iterate, unless rounding alone takes its
+        // gap over the target (tv_aniso.cpp:87-96)
+        if (gz <= im.target || !(s2.gp <= im.target)) {
+            s2.zsel = 1;
+            s2.gp = gz;
+        }
+        s2.stage = kStDone;
+        bf.st[b] = s2;
+        return;
+    }
+    const bool last = s2.it == c.max_iter;
+    s2.gz = gz;
+    if (gz <= im.target) {
+        s2.gp = gz;
+        s2.stage = kStFinal;
+    } else if (last ? !s2.polished
+                    : (im.mode == kAnAdbpg ? ((s2.warm || s2.it >= kCheck) && gz <= s2.pol_next) : gz <= s2.pol_next)) {
+        s2.accept = last ? gz : im.target;
+        s2.stage = kStPolish;
+    } else {
+        s2.gp = gz;
+        if (im.mode == kAnAdbpg) check_done(s2, gz, im.target);
+        s2.stage = last ? kStFinal : kStIter;
+    }
+    bf.st[b] = s2;
+}
+
+// ---------------------------------------------------------------------------
+// The polish (tv_aniso.cpp:630-953)
+// ---------------------------------------------------------------------------
+
+// dual(z) (tv_aniso.cpp:443-449, 124-131) into the dual, and the polish's
+// scratch reset: zp = d, flags 0, parent = self, sums 0.
+// stage kStPolish: for a polish; kStFinal: the final rebuild zp = d - q1 - q2.
+template <class T>
+__global__ void an_dual(AnGeom g, AnBuffers bf, int stage) {
+    const int b = blockIdx.y;
+    const AnState &st = bf.st[b];
+    if (st.status != kLive || st.stage != stage) return;
+    if (stage == kStFinal && (st.polished || st.it == 0)) return;
+    const AnImage &im = bf.img[b];
+    const int64_t N = g.N, B = g.B;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *Z = static_cast<const T *>(bf.z) + (int64_t)b * N;
+    const T *Y = static_cast<const T *>(bf.y) + (int64_t)b * g.k * N;
+    T *Q = static_cast<T *>(bf.dual);
+    T *ZP = static_cast<T *>(bf.zp) + (int64_t)b * N;
+    uint8_t *F = bf.flag + (int64_t)b * N;
+    int *P = bf.parent + (int64_t)b * N;
+    unsigned long long *S = bf.sum + (int64_t)b * N;
+    int *C = bf.cnt + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        T q[3] = {T(0), T(0), T(0)};
+        if (im.mode == kAnAdbpg) {
+            q[im.a1] = D[p] + Y[p] - Z[p];
+            q[im.a2] = -Y[p];
+        } else {
+            q[0] = -Y[p];
+            q[1] = -Y[N + p];
+            q[2] = D[p] + Y[p] + Y[N + p] - Z[p];
+        }
+        for (int a = 0; a < g.k; ++a) Q[((int64_t)a * B + b) * N + p] = q[a];
+        if (stage == kStFinal) {
+            if (im.mode == kAnAdbpg) {
+                T s = T(0);
+                for (int a = 0; a < g.k; ++a) s += q[a];
+                ZP[p] = D[p] - s;
+            }
+        } else {
+            ZP[p] = D[p];
+            F[p] = 0;
+            P[p] = (int)p;
+            S[p] = 0ull;
+            C[p] = 0;
+        }
+    }
+}
+
+// mark_edges (tv_aniso.cpp:256-297) along axis a: the 1D dual of each edge
+// from the running sum of q_a along its fibre; an edge strictly inside its
+// bound is flat (bit a), the others move lam_e sign(p_e) from j to i in zp.
+template <class T>
+__global__ void __launch_bounds__(128) an_mark(AnGeom g, AnCall c, AnBuffers bf, int a) {
+    const int b = blockIdx.y;
+    const AnState &st = bf.st[b];
+    if (st.status != kLive || st.stage != kStPolish) return;
+    const AnImage &im = bf.img[b];
+    const double lam = im.lam[a];
+    if (lam == 0.0) return;
+    const Fib fb = fibers(g, a);
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= fb.nfib) return;
+    const int64_t N = g.N, base = fb.base(f), s = fb.s;
+    const T *Q = static_cast<const T *>(bf.dual) + ((int64_t)a * g.B + b) * N + base;
+    const T *Bw = c.has_beta ? static_cast<const T *>(bf.beta) + (int64_t)a * N + base : nullptr;
+    T *ZP = static_cast<T *>(bf.zp) + (int64_t)b * N + base;
+    uint8_t *F = bf.flag + (int64_t)b * N + base;
+    const uint8_t bit = (uint8_t)(1u << a);
+    double acc = 0.0;
+    for (int64_t l = 0; l + 1 < fb.L; ++l) {
+        const int64_t o = l * s;
+        acc += (double)Q[o];
+        const double pe = -acc;
+        const double lb = Bw ? lam * (double)Bw[o] : lam;
+        const bool inside = fabs(pe) < lb * (1.0 - polish_eta<T>());
+        if (inside) {
+            F[o] |= bit;
+        } else {
+            const double ls = copysign(lb, pe);
+            ZP[o] = (T)((double)ZP[o] + ls);
+            ZP[o + s] = (T)((double)ZP[o + s] - ls);
+        }
+    }
+}
+
+__device__ __forceinline__ int uf_find(int *P, int i) {
+    // parents point to smaller indices, so the walk ends; path halving
+    for (int n = 0; n < (1 << 30); ++n) {
+        const int p = P[i];
+        if (p == i) return i;
+        const int q = P[p];
+        if (q != p) P[i] = q;
+        i = p;
+    }
+    return i;
+}
+
+// components (tv_aniso.cpp:324-439) by union-find: the flat edges join
+// their ends, the larger root hooked under the smaller by compare-and-swap,
+// so each root is the smallest index of its component.
+__global__ void an_union(AnGeom g, AnBuffers bf) {
+    const int b = blockIdx.y;
+    const AnState &st = bf.st[b];
+    if (st.status != kLive || st.stage != kStPolish) return;
+    const int64_t N = g.N;
+    const uint8_t *F = bf.flag + (int64_t)b * N;
+    int *P = bf.parent + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const uint8_t fl = F[p];
+        if (!fl) continue;
+        for (int a = 0; a < g.k; ++a) {
+            if (!(fl & (1u << a))) continue;
+            int x = (int)p, y = (int)(p + g.S[a]);
+            int tries = 0;
+            for (;;) {
+                x = uf_find(P, x);
+                y = uf_find(P, y);
+                if (x == y) break;
+                const int hi = x > y ? x : y, lo = x > y ? y : x;
+                const int old = atomicCAS(P + hi, hi, lo);
+                if (old == hi) break;
+                x = old;  // hi was hooked meanwhile: retry from there
+                y = lo;
+                if (++tries > (1 << 24)) {
+                    atomicExch(bf.err, 2);
+                    break;
+                }
+            }
+        }
+    }
+}
+
+// every entry to its root; the region sums of zp (64-bit fixed point) and sizes
+template <class T>
+__global__ void an_region_sum(AnGeom g, AnBuffers bf) {
+    const int b = blockIdx.y;
+    const AnState &st = bf.st[b];
+    if (st.status != kLive || st.stage != kStPolish) return;
+    const int64_t N = g.N;
+    const int sh = bf.img[b].fx_shift;
+    int *P = bf.parent + (int64_t)b * N;
+    const T *ZP = static_cast<const T *>(bf.zp) + (int64_t)b * N;
+    unsigned long long *S = bf.sum + (int64_t)b * N;
+    int *C = bf.cnt + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const int r = uf_find(P, (int)p);
+        P[p] = r;
+        const long long fx = llrint(ldexp((double)ZP[p], sh));
+        atomicAdd(S + r, (unsigned long long)fx);
+        atomicAdd(C + r, 1);
+    }
+}
+
+// zp = the region means; the polished gap P(zp) - D(q) (tv_aniso.cpp:504-523);
+// the last block accepts or schedules the next attempt (:520-523, :382-391).
+template <class T>
+__global__ void __launch_bounds__(kThreads) an_polish_gap(AnGeom g, AnCall c, AnBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const AnState st = bf.st[b];
+    if (st.status != kLive || st.stage != kStPolish) return;
+    const AnImage im = bf.img[b];
+    const int64_t N = g.N, B = g.B;
+    const int shf = im.fx_shift;
+    const int *P = bf.parent + (int64_t)b * N;
+    const unsigned long long *S = bf.sum + (int64_t)b * N;
+    const int *C = bf.cnt + (int64_t)b * N;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *Q = static_cast<const T *>(bf.dual);
+    T *ZP = static_cast<T *>(bf.zp) + (int64_t)b * N;
+    auto mean = [&](int64_t p) -> double {
+        const int r = P[p];
+        return ldexp((double)(long long)S[r], -shf) / (double)C[r];
+    };
+    double acc = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const double zp = mean(p);
+        const double d = (double)D[p];
+        const double e = zp - d;
+        double sj = 0.0;
+        for (int a = 0; a < g.k; ++a) sj += (double)Q[((int64_t)a * B + b) * N + p];
+        double tv = 0.0;
+        for (int a = 0; a < g.k; ++a) {
+            const double l = im.lam[a];
+            if (l == 0.0) continue;
+            const int64_t co = (p / g.S[a]) % g.L[a];
+            if (co + 1 >= g.L[a]) continue;
+            double le = l;
+            if (c.has_beta) le = l * (double)static_cast<const T *>(bf.beta)[(int64_t)a * N + p];
+            tv += le * fabs(mean(p + g.S[a]) - zp);
+        }
+        acc += 0.5 * e * e - (d * sj - 0.5 * sj * sj) + tv;
+    }
+    // write the means after every block of this image has read them: the
+    // last block does it (below); here only the gap
+    double pz, unused;
+    if (!reduce2(bf, b, blockIdx.x, gridDim.x, acc, 0.0, sh, &flag, pz, unused)) return;
+    (void)ZP;
+    AnState s2 = st;
+    const double gz = s2.gz;
+    const bool last = s2.it == c.max_iter;
+    if (pz <= s2.accept && pz <= kPolishRatio * gz) {
+        s2.polished = 1;
+        s2.zsel = 1;
+        s2.gp = pz;
+        s2.pol_accept = 1;
+    } else {
+        // PolishSchedule::done (tv_aniso.cpp:386-390)
+        const bool eager = im.mode == kAnFdpg3;
+        double next = gz * kPolishDrop;
+        if (pz > 0.0 && pz < (eager ? 1.0 : kPolishRatio) * gz) next = fmax(next, im.target * gz / pz);
+        s2.pol_next = next;
+        s2.gp = gz;
+        s2.pol_accept = 0;
+    }
+    if (im.mode == kAnAdbpg) check_done(s2, s2.gp, im.target);
+    s2.stage = (s2.gp <= im.target || last) ? kStFinal : kStIter;
+    bf.st[b] = s2;
+}
+
+// the accepted candidate: zp = region means
+template <class T>
+__global__ void an_polish_write(AnGeom g, AnBuffers bf) {
+    const int b = blockIdx.y;
+    const AnState &st = bf.st[b];
+    if (st.status != kLive || !st.pol_accept) return;
+    const int64_t N = g.N;
+    const int shf = bf.img[b].fx_shift;
+    const int *P = bf.parent + (int64_t)b * N;
+    const unsigned long long *S = bf.sum + (int64_t)b * N;
+    const int *C = bf.cnt + (int64_t)b * N;
+    T *ZP = static_cast<T *>(bf.zp) + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const int r = P[p];
+        ZP[p] = (T)(ldexp((double)(long long)S[r], -shf) / (double)C[r]);
+    }
+}
+
+// images whose stage is done leave the live set
+__global__ void an_retire(AnGeom g, AnBuffers bf) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= g.B) return;
+    AnState &st = bf.st[b];
+    st.pol_accept = 0;
+    if (st.status == kLive && (st.stage == kStDone || (st.stage == kStFinal && bf.img[b].mode == kAnFdpg3))) {
+        st.status = st.gp <= bf.img[b].target ? kConverged : kNotConv;
+        atomicSub(bf.live, 1);
+    }
+}
+
+// a final rebuild is not needed after a polish or at it = 0: done
+__global__ void an_final_skip(AnGeom g, AnBuffers bf) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= g.B) return;
+    AnState &st = bf.st[b];
+    if (st.status == kLive && st.stage == kStFinal && (st.polished || st.it == 0)) st.stage = kStDone;
+}
+
+// ---------------------------------------------------------------------------
+// Single active axis, identity, NaN; the output at the input's scale
+// ---------------------------------------------------------------------------
+
+template <class T>
+__global__ void __launch_bounds__(128) an_single(AnGeom g, AnCall c, AnBuffers bf) {
+    const int b = blockIdx.y;
+    const AnImage &im = bf.img[b];
+    if (im.mode != kAnSingle) return;
+    int a = 0;
+    for (int x = 0; x < g.k; ++x)
+        if (im.lam[x] > 0.0) a = x;
+    const Fib fb = fibers(g, a);
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= fb.nfib) return;
+    const int64_t N = g.N, base = fb.base(f), s = fb.s;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N + base;
+    T *Z = static_cast<T *>(bf.z) + (int64_t)b * N + base;
+    auto in = [D, s](int64_t i) -> double { return (double)D[i * s]; };
+    auto out = [Z, s](int64_t i, double v) { Z[i * s] = (T)v; };
+    fibre_prox<T>(c, bf, a, base, fb, im.lam[a], in, out);
+}
+
+template <class T>
+__global__ void an_output(AnGeom g, AnBuffers bf, T *__restrict__ out) {
+    const int b = blockIdx.y;
+    const AnImage im = bf.img[b];
+    if (im.mode == kAnInf) return;
+    const AnState st = bf.st[b];
+    const int64_t N = g.N, B = g.B;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *Z = static_cast<const T *>(st.zsel ? bf.zp : bf.z) + (int64_t)b * N;
+    T *Q = static_cast<T *>(bf.dual);
+    T *O = out + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        if (im.mode == kAnNan) {
+            O[p] = (T)CUDART_NAN;
+            for (int a = 0; a < g.k; ++a) Q[((int64_t)a * B + b) * N + p] = (T)CUDART_NAN;
+        } else if (im.mode == kAnIdentity) {
+            O[p] = D[p];
+            for (int a = 0; a < g.k; ++a) Q[((int64_t)a * B + b) * N + p] = T(0);
+        } else if (im.mode == kAnSingle) {
+            const T z = Z[p];
+            O[p] = im.e ? ldexp_t(z, im.e) : z;
+            for (int a = 0; a < g.k; ++a) {
+                T q = im.lam[a] > 0.0 ? D[p] - z : T(0);  // q_a = v - z (tv_aniso.cpp:321-323)
+                Q[((int64_t)a * B + b) * N + p] = im.e ? ldexp_t(q, im.e) : q;
+            }
+        } else {
+            const T z = Z[p];
+            O[p] = im.e ? ldexp_t(z, im.e) : z;
+            if (im.e)
+                for (int a = 0; a < g.k; ++a) {
+                    T &q = Q[((int64_t)a * B + b) * N + p];
+                    q = ldexp_t(q, im.e);
+                }
+        }
+    }
+}
+
+int grid1(int64_t n, int t) {
+    int64_t g = (n + t - 1) / t;
+    if (g > 4096) g = 4096;
+    return (int)std::max<int64_t>(1, g);
+}
+
+template <class T>
+cudaError_t setup_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, const void *x, cudaStream_t s) {
+    const int nb = (int)std::min<int64_t>(128, std::max<int64_t>(1, (g.N + kThreads * 8 - 1) / (kThreads * 8)));
+    const dim3 grid(nb, (unsigned)g.B);
+    an_scan1<T><<<grid, kThreads, 0, s>>>(static_cast<const T *>(x), g, c, bf);
+    an_scan2<T><<<grid, kThreads, 0, s>>>(g, c, bf);
+    // single-axis images are solved here
+    int64_t nfmax = 0;
+    for (int a = 0; a < g.k; ++a) nfmax = std::max<int64_t>(nfmax, g.N / g.L[a]);
+    an_single<T><<<dim3((unsigned)((nfmax + 127) / 128), (unsigned)g.B), 128, 0, s>>>(g, c, bf);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s, int64_t *launches) {
+    const unsigned B = (unsigned)g.B;
+    int64_t nl = 0;
+    const int pb = an_pixel_blocks(g);
+    const dim3 pg(pb, B);
+    // the iteration: ADBPG's two passes, or FDPG-3's three
+    int64_t nf[3] = {1, 1, 1};
+    for (int a = 0; a < g.k; ++a) nf[a] = g.N / g.L[a];
+    int64_t nfmax = 0;
+    for (int a = 0; a < g.k; ++a) nfmax = std::max(nfmax, nf[a]);
+    const unsigned fbk = (unsigned)((nfmax + 127) / 128);
+    if (c.has_adbpg) {
+        an_pass1<T><<<dim3(fbk, B), 128, 0, s>>>(g, c, bf);
+        an_pass2<T><<<dim3(fbk, B), 128, 0, s>>>(g, c, bf);
+        nl += 2;
+    }
+    if (c.has_fdpg3) {
+        an_fdpg3_u<T><<<pg, kThreads, 0, s>>>(g, bf);
+        an_fdpg3_pass<T><<<dim3(fbk, 3, B), 128, 0, s>>>(g, c, bf);
+        nl += 2;
+    }
+    an_restart_copy<T><<<pg, kThreads, 0, s>>>(g, bf);
+    ++nl;
+    // gap check (FDPG-3 forms its primal first)
+    if (c.has_fdpg3) {
+        an_fdpg3_primal<T><<<dim3((unsigned)((nf[2] + 127) / 128), B), 128, 0, s>>>(g, c, bf, kStCheck);
+        ++nl;
+    }
+    an_gap<T><<<pg, kThreads, 0, s>>>(g, c, bf, kStCheck);
+    ++nl;
+    // polish
+    an_dual<T><<<pg, kThreads, 0, s>>>(g, bf, kStPolish);
+    for (int a = 0; a < g.k; ++a) an_mark<T><<<dim3((unsigned)((nf[a] + 127) / 128), B), 128, 0, s>>>(g, c, bf, a);
+    an_union<<<pg, kThreads, 0, s>>>(g, bf);
+    an_region_sum<T><<<pg, kThreads, 0, s>>>(g, bf);
+    an_polish_gap<T><<<pg, kThreads, 0, s>>>(g, c, bf);
+    an_polish_write<T><<<pg, kThreads, 0, s>>>(g, bf);
+    nl += 5 + g.k;
+    // final rebuild, then retirement
+    an_final_skip<<<(B + 127) / 128, 128, 0, s>>>(g, bf);
+    an_dual<T><<<pg, kThreads, 0, s>>>(g, bf, kStFinal);
+    an_gap<T><<<pg, kThreads, 0, s>>>(g, c, bf, kStFinal);
+    an_retire<<<(B + 127) / 128, 128, 0, s>>>(g, bf);
+    nl += 4;
+    if (launches) *launches += nl;
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t output_t(const AnGeom &g, const AnBuffers &bf, void *out, cudaStream_t s) {
+    an_output<T><<<dim3(an_pixel_blocks(g), (unsigned)g.B), kThreads, 0, s>>>(g, bf, static_cast<T *>(out));
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int an_pixel_blocks(const AnGeom &g) {
+    int64_t nb = (g.N + kThreads * 4 - 1) / (kThreads * 4);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(nb, 256));
+}
+
+cudaError_t aniso_setup(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, const void *x,
+                        cudaStream_t s) {
+    return dtype == 1 ? setup_t<float>(g, c, bf, x, s) : setup_t<double>(g, c, bf, x, s);
+}
+
+cudaError_t aniso_round(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s,
+                        int64_t *launches) {
+    return dtype == 1 ? round_t<float>(g, c, bf, s, launches) : round_t<double>(g, c, bf, s, launches);
+}
+
+cudaError_t aniso_output(int dtype, const AnGeom &g, const AnBuffers &bf, void *out, cudaStream_t s) {
+    return dtype == 1 ? output_t<float>(g, bf, out, s) : output_t<double>(g, bf, out, s);
+}
+
+}  // namespace fpb

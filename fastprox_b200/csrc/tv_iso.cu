@@ -499,6 +499,514 @@ __global__ void __launch_bounds__(256) iso2d_march_kernel(StepArgs A, IsoCall c,
 }
 
 // ---------------------------------------------------------------------------
+// The lean 2D step: the row-marching scheme above with the per-pixel work
+// cut to the arithmetic of the iteration. Offsets are 32-bit within an image
+// (images have fewer than 2^31 pixels), row pointers advance by W, the gap
+// and the cold start are compile-time variants (one per block: every live
+// image of a launch shares its branch), the projection multiplies by a
+// reciprocal square root, and lane 31 carries the three scalars of the next
+// warp's first column instead of re-reading them.
+// ---------------------------------------------------------------------------
+
+template <class T>
+__device__ __forceinline__ T rsqrt_t(T v);
+template <>
+__device__ __forceinline__ float rsqrt_t<float>(float v) { return rsqrtf(v); }
+template <>
+__device__ __forceinline__ double rsqrt_t<double>(double v) { return rsqrt(v); }
+
+template <class T, int VEC, bool ALPHA, bool GAP, bool ZIN>
+__device__ __forceinline__ void lean_rows(const T *__restrict__ D, const T *__restrict__ U0, const T *__restrict__ U1,
+                                          const T *__restrict__ V0, const T *__restrict__ V1, T *__restrict__ UO0,
+                                          T *__restrict__ UO1, T *__restrict__ VO0, T *__restrict__ VO1,
+                                          const T *__restrict__ AL, int H, int W, int cb, int r0, int r1, T wh0, T wh1,
+                                          T tau, T beta, T rad, T bnd, bool test, bool store, double &gap_acc,
+                                          double &dot_acc) {
+    const int lane = threadIdx.x & 31;
+    const bool colok = cb < W;
+    const bool ext = lane == 31 && cb + VEC < W;  // the next warp's first column
+    const int cx = cb + VEC;
+    auto ld = [&](const T *P, int off, T(&o)[VEC]) {
+        if (!ZIN && colok) load_pack<T, VEC>(P + off, o);
+        else
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) o[j] = T(0);
+    };
+    auto ldd = [&](int off, T(&o)[VEC]) {
+        if (colok) load_pack<T, VEC>(D + off, o);
+        else
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) o[j] = T(0);
+    };
+    auto zrow = [&](const T(&dd)[VEC], const T(&p0)[VEC], const T(&p0p)[VEC], const T(&p1)[VEC], T left, T(&z)[VEC]) {
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            z[j] = dd[j] + wh0 * (p0[j] - p0p[j]) + wh1 * (p1[j] - left);
+            left = p1[j];
+        }
+    };
+    int off = r0 * W + cb;
+    // row r0 and the part of row r0 - 1 it needs
+    T v0c[VEC], v1c[VEC], u0c[VEC], u1c[VEC], zc[VEC], zuc[VEC];
+    T dc[VEC], v0p[VEC], u0p[VEC];
+    ldd(off, dc);
+    ld(V0, off, v0c);
+    ld(V1, off, v1c);
+    ld(U0, off, u0c);
+    ld(U1, off, u1c);
+    if (r0 > 0) {
+        ld(V0, off - W, v0p);
+        if (GAP) ld(U0, off - W, u0p);
+    } else {
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) v0p[j] = u0p[j] = T(0);
+    }
+    const T v1l = (!ZIN && colok && cb > 0) ? V1[off - 1] : T(0);
+    zrow(dc, v0c, v0p, v1c, v1l, zc);
+    if (GAP) zrow(dc, u0c, u0p, u1c, (colok && cb > 0) ? U1[off - 1] : T(0), zuc);
+    // lane 31: z at (r0, cx) of v (and u)
+    T x_v0 = T(0), x_u0 = T(0), x_z = T(0), x_zu = T(0);
+    if (ext) {
+        const T dx = D[off + VEC];
+        if (!ZIN) {
+            x_v0 = V0[off + VEC];
+            x_u0 = U0[off + VEC];
+        }
+        const T pv = (!ZIN && r0 > 0) ? V0[off + VEC - W] : T(0);
+        x_z = dx + wh0 * (x_v0 - pv) + wh1 * ((ZIN ? T(0) : V1[off + VEC]) - v1c[VEC - 1]);
+        if (GAP) {
+            const T pu = r0 > 0 ? U0[off + VEC - W] : T(0);
+            x_zu = dx + wh0 * (x_u0 - pu) + wh1 * (U1[off + VEC] - u1c[VEC - 1]);
+        }
+    }
+    for (int i = r0; i < r1; ++i) {
+        const bool hasn = i + 1 < H;
+        const int offn = off + W;
+        T dn[VEC], v0n[VEC], v1n[VEC], u0n[VEC], u1n[VEC], zn[VEC], zun[VEC];
+        T nx_v0 = T(0), nx_u0 = T(0), nx_z = T(0), nx_zu = T(0);
+        if (hasn) {
+            ldd(offn, dn);
+            ld(V0, offn, v0n);
+            ld(V1, offn, v1n);
+            ld(U0, offn, u0n);
+            ld(U1, offn, u1n);
+            zrow(dn, v0n, v0c, v1n, (!ZIN && colok && cb > 0) ? V1[offn - 1] : T(0), zn);
+            if (GAP) zrow(dn, u0n, u0c, u1n, (colok && cb > 0) ? U1[offn - 1] : T(0), zun);
+            if (ext) {
+                const T dx = D[offn + VEC];
+                if (!ZIN) {
+                    nx_v0 = V0[offn + VEC];
+                    nx_u0 = U0[offn + VEC];
+                }
+                nx_z = dx + wh0 * (nx_v0 - x_v0) + wh1 * ((ZIN ? T(0) : V1[offn + VEC]) - v1n[VEC - 1]);
+                if (GAP) nx_zu = dx + wh0 * (nx_u0 - x_u0) + wh1 * (U1[offn + VEC] - u1n[VEC - 1]);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) zn[j] = zun[j] = u0n[j] = u1n[j] = v0n[j] = v1n[j] = T(0);
+        }
+        T al[VEC];
+        if (ALPHA) {
+            if (colok) load_pack<T, VEC>(AL + off, al);
+            else
+#pragma unroll
+                for (int j = 0; j < VEC; ++j) al[j] = T(0);
+        }
+        T zr = __shfl_down_sync(0xffffffffu, zc[0], 1);
+        if (lane == 31) zr = x_z;
+        T zur = T(0);
+        if (GAP) {
+            zur = __shfl_down_sync(0xffffffffu, zuc[0], 1);
+            if (lane == 31) zur = x_zu;
+        }
+        if (colok) {
+            T uo0[VEC], uo1[VEC], vo0[VEC], vo1[VEC];
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) {
+                const bool hasr = cb + j + 1 < W;
+                const T zright = j + 1 < VEC ? zc[j + 1] : zr;
+                const T g0 = hasn ? wh0 * (zn[j] - zc[j]) : T(0);
+                const T g1 = hasr ? wh1 * (zright - zc[j]) : T(0);
+                const T cv0 = v0c[j] + tau * g0;  // wh = 0 gives g = 0 and v = 0 on that axis
+                const T cv1 = v1c[j] + tau * g1;
+                const T nn = cv0 * cv0 + cv1 * cv1;
+                T rp = rad;
+                if (ALPHA) {
+                    const T r = rad * al[j];
+                    rp = al[j] == T(0) ? T(0) : (r <= bnd ? r : bnd);
+                }
+                const T sc = nn > rp * rp ? rp * rsqrt_t(nn) : T(1);
+                const T un0 = cv0 * sc, un1 = cv1 * sc;
+                if (test) dot_acc += (double)((v0c[j] - un0) * (un0 - u0c[j]) + (v1c[j] - un1) * (un1 - u1c[j]));
+                vo0[j] = un0 + beta * (un0 - u0c[j]);
+                vo1[j] = un1 + beta * (un1 - u1c[j]);
+                uo0[j] = un0;
+                uo1[j] = un1;
+                if (GAP) {
+                    const T zuright = j + 1 < VEC ? zuc[j + 1] : zur;
+                    const T gu0 = hasn ? wh0 * (zun[j] - zuc[j]) : T(0);
+                    const T gu1 = hasr ? wh1 * (zuright - zuc[j]) : T(0);
+                    gap_acc += (double)(rp * sqrt_t(gu0 * gu0 + gu1 * gu1) - (gu0 * u0c[j] + gu1 * u1c[j]));
+                }
+            }
+            if (store) {
+                store_pack<T, VEC>(UO0 + off, uo0);
+                store_pack<T, VEC>(UO1 + off, uo1);
+                store_pack<T, VEC>(VO0 + off, vo0);
+                store_pack<T, VEC>(VO1 + off, vo1);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            v0c[j] = v0n[j];
+            v1c[j] = v1n[j];
+            u0c[j] = u0n[j];
+            u1c[j] = u1n[j];
+            zc[j] = zn[j];
+            if (GAP) zuc[j] = zun[j];
+        }
+        x_v0 = nx_v0;
+        x_u0 = nx_u0;
+        x_z = nx_z;
+        x_zu = nx_zu;
+        off = offn;
+    }
+}
+
+// GAP and ZIN are chosen by the host from the launch index (every live image
+// of a call is at the same iteration); an image at another iteration (which
+// a single call never has) is flagged as an error rather than solved wrongly.
+template <class T, int VEC, bool ALPHA, bool GAP, bool ZIN>
+__global__ void __launch_bounds__(128) iso2d_lean_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.z;
+    const IsoState st = bf.st[b];
+    if (st.status != kLive) return;
+    const int it = st.it;
+    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == A.max_iter)) || (it == 0 && st.warm);
+    const bool zin = st.zero_in != 0;
+    if (do_gap != GAP || zin != ZIN) {
+        if (threadIdx.x == 0) atomicExch(bf.err, 3);
+        return;
+    }
+    const IsoImage im = bf.img[b];
+    const int H = (int)A.g.L[0], W = (int)A.g.L[1];
+    const int64_t N = A.g.N;
+    const bool do_upd = it < A.max_iter;
+    const bool test = do_upd && (it & 3) == 0;
+    const int pin = A.par, pout = A.par ^ 1;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *U0 = static_cast<const T *>(bf.U[pin]) + (int64_t)b * 2 * N;
+    const T *V0 = st.vsel ? U0 : static_cast<const T *>(bf.V[pin]) + (int64_t)b * 2 * N;
+    T *UO0 = static_cast<T *>(bf.U[pout]) + (int64_t)b * 2 * N;
+    T *VO0 = static_cast<T *>(bf.V[pout]) + (int64_t)b * 2 * N;
+    const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
+    const int cb = (blockIdx.x * blockDim.x + threadIdx.x) * VEC;
+    const int r0 = blockIdx.y * A.rows;
+    const int r1 = min(H, r0 + A.rows);
+    double gap_acc = 0.0, dot_acc = 0.0;
+    lean_rows<T, VEC, ALPHA, GAP, ZIN>(D, U0, U0 + N, V0, V0 + N, UO0, UO0 + N, VO0, VO0 + N, AL, H, W, cb, r0, r1,
+                                       (T)c.wh[0], (T)c.wh[1], (T)c.tau, (T)st.beta, (T)im.radius, (T)im.bound, test,
+                                       do_upd, gap_acc, dot_acc);
+    const unsigned nblk = gridDim.x * gridDim.y;
+    const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
+    const double gsum = GAP ? block_sum(gap_acc, sh) : 0.0;
+    const double dsum = test ? block_sum(dot_acc, sh) : 0.0;
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[blk * 2 + 0] = gsum;
+        part[blk * 2 + 1] = dsum;
+    }
+    if (!arrive_last(bf.ticket + b, nblk, &flag)) return;
+    const double gap = GAP ? sum_partials(part, nblk, 2, 0, sh) : 0.0;
+    const double dot = test ? sum_partials(part, nblk, 2, 1, sh) : 0.0;
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2 = st;
+    control(s2, im, A.max_iter, GAP, test, gap, dot, pin, bf.live);
+    bf.st[b] = s2;
+}
+
+// ---------------------------------------------------------------------------
+// The 2D step with a TMA row pipeline (sm_100a): one elected thread streams
+// whole row segments of d, v, u (and the pixel weights) from HBM into a ring
+// of shared-memory slots with bulk asynchronous copies (cp.async.bulk,
+// completion counted on an mbarrier per slot), several rows ahead of the
+// rows being computed, so the loads in flight are not bounded by registers.
+// The threads compute z for the next row into shared memory, then update the
+// current row with every neighbour read from shared memory, and store u and
+// v straight to HBM. Same arithmetic and control as the kernels above.
+//
+// A block owns a span of SPAN = blockDim.x * VEC columns (plus a halo of one
+// 16-byte vector each side) and walks `rows` rows. Slot s holds row r with
+// (r - r0 + 1) % SLOTS == s; the row a slot holds is known to every thread.
+// Rows outside the image are never copied: they read as zeros.
+// ---------------------------------------------------------------------------
+
+constexpr int kSlots = 4;
+constexpr int kArrays = 6;  // d, v0, v1, u0, u1, alpha
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Waits for the phase of parity `par` of a slot's barrier; false after
+// about a second of polling (the caller then records an error).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned par) {
+    const uint32_t a = smem_addr(bar);
+    for (int i = 0; i < (1 << 22); ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(a), "r"(par)
+            : "memory");
+        if (ok) return true;
+        if (i > 16) __nanosleep(64);
+    }
+    return false;
+}
+
+template <class T, int VEC, bool ALPHA>
+__global__ void __launch_bounds__(128) iso2d_tma_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ uint64_t bars[kSlots];
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.z;
+    const IsoState st = bf.st[b];
+    if (st.status != kLive) return;
+    const IsoImage im = bf.img[b];
+    const int64_t H = A.g.L[0], W = A.g.L[1], N = A.g.N;
+    const int it = st.it;
+    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == A.max_iter)) || (it == 0 && st.warm);
+    const bool do_upd = it < A.max_iter;
+    const bool test = do_upd && (it & 3) == 0;
+    const bool zin = st.zero_in != 0;
+    const bool vsel = st.vsel != 0;
+    const int pin = A.par, pout = A.par ^ 1;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *U0 = static_cast<const T *>(bf.U[pin]) + (int64_t)b * 2 * N;
+    const T *V0 = static_cast<const T *>(bf.V[pin]) + (int64_t)b * 2 * N;
+    T *UO0 = static_cast<T *>(bf.U[pout]) + (int64_t)b * 2 * N;
+    T *VO0 = static_cast<T *>(bf.V[pout]) + (int64_t)b * 2 * N;
+    const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
+    const T wh0 = (T)c.wh[0], wh1 = (T)c.wh[1], tau = (T)c.tau, beta = (T)st.beta;
+    const T rad = (T)im.radius, bnd = (T)im.bound;
+
+    constexpr int HALO = 16 / sizeof(T);
+    const int span = blockDim.x * VEC;
+    const int RW = span + 2 * HALO;                    // row width in shared memory (elements)
+    const int64_t cs = (int64_t)blockIdx.x * span;     // first column of the span
+    const int64_t c0 = cs - HALO > 0 ? cs - HALO : 0;  // loaded columns [c0, c1)
+    const int64_t c1 = cs + span + HALO < W ? cs + span + HALO : W;
+    const unsigned seg_bytes = (unsigned)((c1 - c0) * (int64_t)sizeof(T));
+    const int soff = (int)(c0 - (cs - HALO));          // shared index of column c0
+    T *slots = reinterpret_cast<T *>(smem_raw);        // [kSlots][kArrays][RW]
+    T *zrow = slots + (size_t)kSlots * kArrays * RW;   // [2][RW] z of v, then [2][RW] z of u
+    const int64_t r0 = (int64_t)blockIdx.y * A.rows;
+    const int64_t r1 = min(H, r0 + (int64_t)A.rows);
+    const bool load_v = !zin && !vsel;
+    const bool load_u = !zin;
+    const unsigned row_bytes = seg_bytes * (1u + (load_v ? 2u : 0u) + (load_u ? 2u : 0u) + (ALPHA ? 1u : 0u));
+    const int tid = threadIdx.x;
+
+    auto slot_of = [&](int64_t r) { return (int)((r - r0 + 1) % kSlots); };
+    auto parity = [&](int64_t r) { return (unsigned)(((r - r0 + 1) / kSlots) & 1); };
+    auto arr = [&](int s, int a) { return slots + ((size_t)s * kArrays + a) * RW; };
+    // the shared row of array a (d 0, v0 1, v1 2, u0 3, u1 4, alpha 5) holding row r,
+    // or null where it reads as zeros (outside the image; u = v = 0 on a cold
+    // start; v = u after a restart)
+    auto row = [&](int64_t r, int a) -> const T * {
+        if (r < 0 || r >= H) return nullptr;
+        if ((a >= 1 && a <= 4) && zin) return nullptr;
+        if ((a == 1 || a == 2) && vsel) a += 2;
+        return arr(slot_of(r), a);
+    };
+    int64_t last_prod = r0 - 2;
+    auto produce = [&](int64_t r) {  // thread 0 only
+        const int s = slot_of(r);
+        uint64_t *bar = &bars[s];
+        last_prod = r;
+        if (r < 0 || r >= H) {
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+            return;
+        }
+        mbar_expect_tx(bar, row_bytes);
+        const int64_t g = r * W + c0;
+        bulk_load(arr(s, 0) + soff, D + g, seg_bytes, bar);
+        if (load_v) {
+            bulk_load(arr(s, 1) + soff, V0 + g, seg_bytes, bar);
+            bulk_load(arr(s, 2) + soff, V0 + N + g, seg_bytes, bar);
+        }
+        if (load_u) {
+            bulk_load(arr(s, 3) + soff, U0 + g, seg_bytes, bar);
+            bulk_load(arr(s, 4) + soff, U0 + N + g, seg_bytes, bar);
+        }
+        if (ALPHA) bulk_load(arr(s, 5) + soff, AL + g, seg_bytes, bar);
+    };
+    if (tid == 0) {
+        for (int i = 0; i < kSlots; ++i) mbar_init(&bars[i], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int64_t r = r0 - 1; r < r0 - 1 + kSlots && r <= r1; ++r) produce(r);
+
+    const int64_t cb = cs + (int64_t)tid * VEC;
+    const bool colok = cb < W;
+    const int ib = HALO + tid * VEC;  // shared index of column cb
+    auto ldv = [&](const T *p, T(&o)[VEC]) {
+        if (p && colok) load_pack<T, VEC>(p + ib, o);
+        else
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) o[j] = T(0);
+    };
+    auto lds = [&](const T *p, int64_t col) -> T {  // one column, zero outside
+        if (!p || col < 0 || col >= W) return T(0);
+        return p[col - cs + HALO];
+    };
+    // z of a dual pair (p = 1: v, p = 3: u) on row r, for this thread's columns
+    // and (the last thread) the right halo column
+    auto zfill = [&](int64_t r, int p, T *zdst) {
+        if (r < 0 || r >= H) {
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) zdst[ib + j] = T(0);
+            if (tid == blockDim.x - 1) zdst[HALO + span] = T(0);
+            return;
+        }
+        const T *dr = row(r, 0), *a0 = row(r, p), *a0p = row(r - 1, p), *a1 = row(r, p + 1);
+        T dd[VEC], x0[VEC], x0p[VEC], x1[VEC], z[VEC];
+        ldv(dr, dd);
+        ldv(a0, x0);
+        ldv(a0p, x0p);
+        ldv(a1, x1);
+        T left = lds(a1, cb - 1);
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            z[j] = colok ? dd[j] + wh0 * (x0[j] - x0p[j]) + wh1 * (x1[j] - left) : T(0);
+            left = x1[j];
+        }
+        if (colok) store_pack<T, VEC>(zdst + ib, z);
+        else
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) zdst[ib + j] = T(0);
+        if (tid == blockDim.x - 1) {
+            const int64_t col = cs + span;
+            zdst[HALO + span] = col < W ? lds(dr, col) + wh0 * (lds(a0, col) - lds(a0p, col)) +
+                                              wh1 * (lds(a1, col) - lds(a1, col - 1))
+                                        : T(0);
+        }
+    };
+    auto zv = [&](int64_t r) { return zrow + (size_t)(r & 1) * RW; };
+    auto zu = [&](int64_t r) { return zrow + (size_t)(2 + (r & 1)) * RW; };
+
+    bool ok = mbar_wait(&bars[slot_of(r0 - 1)], parity(r0 - 1));
+    ok = mbar_wait(&bars[slot_of(r0)], parity(r0)) && ok;
+    zfill(r0, 1, zv(r0));
+    if (do_gap) zfill(r0, 3, zu(r0));
+    double gap_acc = 0.0, dot_acc = 0.0;
+    for (int64_t i = r0; i < r1; ++i) {
+        ok = mbar_wait(&bars[slot_of(i + 1)], parity(i + 1)) && ok;
+        zfill(i + 1, 1, zv(i + 1));
+        if (do_gap) zfill(i + 1, 3, zu(i + 1));
+        ok = __syncthreads_and(ok) != 0;  // block-uniform from here
+        if (!ok) break;
+        if (colok) {
+            const T *zc = zv(i), *zn = zv(i + 1), *zuc = zu(i), *zun = zu(i + 1);
+            T v0[VEC], v1[VEC], u0[VEC], u1[VEC], al[VEC], zcv[VEC], znv[VEC];
+            ldv(row(i, 1), v0);
+            ldv(row(i, 2), v1);
+            ldv(row(i, 3), u0);
+            ldv(row(i, 4), u1);
+            if (ALPHA) ldv(row(i, 5), al);
+            load_pack<T, VEC>(zc + ib, zcv);
+            load_pack<T, VEC>(zn + ib, znv);
+            const T zright = zc[ib + VEC];
+            const bool hasn = i + 1 < H;
+            T uo0[VEC], uo1[VEC], vo0[VEC], vo1[VEC];
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) {
+                const bool hasr = cb + j + 1 < W;
+                const T zr = j + 1 < VEC ? zcv[j + 1] : zright;
+                const T g0 = hasn ? wh0 * (znv[j] - zcv[j]) : T(0);
+                const T g1 = hasr ? wh1 * (zr - zcv[j]) : T(0);
+                const T cv0 = wh0 != T(0) ? v0[j] + tau * g0 : T(0);
+                const T cv1 = wh1 != T(0) ? v1[j] + tau * g1 : T(0);
+                const T nr = sqrt_t(cv0 * cv0 + cv1 * cv1);
+                T rp = rad;
+                if (ALPHA) rp = al[j] == T(0) ? T(0) : (rad * al[j] <= bnd ? rad * al[j] : bnd);
+                const T sc = nr > rp ? rp / nr : T(1);
+                const T un0 = cv0 * sc, un1 = cv1 * sc;
+                if (test) dot_acc += (double)((v0[j] - un0) * (un0 - u0[j])) + (double)((v1[j] - un1) * (un1 - u1[j]));
+                vo0[j] = un0 + beta * (un0 - u0[j]);
+                vo1[j] = un1 + beta * (un1 - u1[j]);
+                uo0[j] = un0;
+                uo1[j] = un1;
+                if (do_gap) {
+                    const T zur = j + 1 < VEC ? zuc[ib + j + 1] : zuc[ib + VEC];
+                    const double gu0 = hasn ? (double)(wh0 * (zun[ib + j] - zuc[ib + j])) : 0.0;
+                    const double gu1 = hasr ? (double)(wh1 * (zur - zuc[ib + j])) : 0.0;
+                    gap_acc += (double)rp * sqrt(gu0 * gu0 + gu1 * gu1) - (gu0 * (double)u0[j] + gu1 * (double)u1[j]);
+                }
+            }
+            if (do_upd) {
+                store_pack<T, VEC>(UO0 + i * W + cb, uo0);
+                store_pack<T, VEC>(UO0 + N + i * W + cb, uo1);
+                store_pack<T, VEC>(VO0 + i * W + cb, vo0);
+                store_pack<T, VEC>(VO0 + N + i * W + cb, vo1);
+            }
+        }
+        __syncthreads();  // rows i - 1 and i and z row i are free
+        if (tid == 0 && i + kSlots - 1 <= r1) produce(i + kSlots - 1);
+    }
+    if (!ok) {
+        // a copy never completed: record it, wait (bounded) for whatever this
+        // block still has in flight, and leave the image's state unchanged
+        if (tid == 0) {
+            atomicExch(bf.err, 1);
+            for (int64_t r = r0 - 1; r <= last_prod; ++r) mbar_wait(&bars[slot_of(r)], parity(r));
+        }
+        return;
+    }
+    const unsigned nblk = gridDim.x * gridDim.y;
+    const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
+    const double gsum = do_gap ? block_sum(gap_acc, sh) : 0.0;
+    const double dsum = test ? block_sum(dot_acc, sh) : 0.0;
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[blk * 2 + 0] = gsum;
+        part[blk * 2 + 1] = dsum;
+    }
+    if (!arrive_last(bf.ticket + b, nblk, &flag)) return;
+    const double gap = do_gap ? sum_partials(part, nblk, 2, 0, sh) : 0.0;
+    const double dot = test ? sum_partials(part, nblk, 2, 1, sh) : 0.0;
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2 = st;
+    control(s2, im, A.max_iter, do_gap, test, gap, dot, pin, bf.live);
+    bf.st[b] = s2;
+}
+
+// ---------------------------------------------------------------------------
 // Generic step: one thread per pixel, 2D or 3D, any extents. Neighbours are
 // read through the caches.
 // ---------------------------------------------------------------------------
@@ -695,7 +1203,11 @@ __global__ void iso_tv1d_kernel(Geometry g, IsoCall c, IsoBuffers bf, T *__restr
     T *O = out + (int64_t)b * N;
     T *Q = static_cast<T *>(bf.dual);
     const double lam = ldexp(im.gamma_in, -im.e) * c.w_act;
-    tv1d_fiber<T>(D + base, s, Z + base, s, L, lam, nullptr, 0);
+    const T *Db = D + base;
+    T *Zb = Z + base;
+    auto fin = [Db, s](int64_t i) -> double { return (double)Db[i * s]; };
+    auto fout = [Zb, s](int64_t i, double v) { Zb[i * s] = (T)v; };
+    tv1d_fiber(fin, fout, L, lam, false, NoWeight{});
     double cs = 0.0;
     for (int64_t i = 0; i < L; ++i) {
         const int64_t o = base + i * s;
@@ -767,6 +1279,22 @@ cudaError_t setup_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, c
     return cudaGetLastError();
 }
 
+template <class T, int VEC, bool ALPHA>
+void launch_lean_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s,
+                   int variant) {
+    const dim3 grid(sh.gx, sh.gy, (unsigned)A.g.B);
+    if (variant == 1) iso2d_lean_kernel<T, VEC, ALPHA, false, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
+    else if (variant == 2) iso2d_lean_kernel<T, VEC, ALPHA, true, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
+    else iso2d_lean_kernel<T, VEC, ALPHA, false, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
+}
+
+template <class T, int VEC>
+void launch_lean(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s,
+                 int variant) {
+    if (c.has_alpha) launch_lean_a<T, VEC, true>(sh, A, c, bf, s, variant);
+    else launch_lean_a<T, VEC, false>(sh, A, c, bf, s, variant);
+}
+
 template <class T, int VEC>
 void launch_march(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
     const dim3 grid(sh.gx, sh.gy, (unsigned)A.g.B);
@@ -774,15 +1302,37 @@ void launch_march(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBu
     else iso2d_march_kernel<T, VEC, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
 }
 
+template <class T, int VEC, bool ALPHA>
+void launch_tma(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
+    constexpr int HALO = 16 / sizeof(T);
+    const int RW = sh.bx * VEC + 2 * HALO;
+    const size_t smem = (size_t)(kSlots * kArrays + 4) * RW * sizeof(T);
+    static size_t configured = 0;
+    if (configured < smem) {
+        cudaFuncSetAttribute(iso2d_tma_kernel<T, VEC, ALPHA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        configured = smem;
+    }
+    const dim3 grid(sh.gx, sh.gy, (unsigned)A.g.B);
+    iso2d_tma_kernel<T, VEC, ALPHA><<<grid, sh.bx, smem, s>>>(A, c, bf);
+}
+
 template <class T>
 cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh, int par,
-                   cudaStream_t s) {
+                   int variant, cudaStream_t s) {
     StepArgs A;
     A.g = g;
     A.max_iter = c.max_iter;
     A.par = par;
     A.rows = sh.rows;
-    if (sh.kind == 0) {
+    if (sh.kind == 4) {
+        if (sh.vec == 4) launch_lean<T, 4>(sh, A, c, bf, s, variant);
+        else if (sh.vec == 2) launch_lean<T, 2>(sh, A, c, bf, s, variant);
+        else launch_lean<T, 1>(sh, A, c, bf, s, variant);
+    } else if (sh.kind == 2) {
+        constexpr int V = 16 / sizeof(T);
+        if (c.has_alpha) launch_tma<T, V, true>(sh, A, c, bf, s);
+        else launch_tma<T, V, false>(sh, A, c, bf, s);
+    } else if (sh.kind == 0) {
         if (sh.vec == 4) launch_march<T, 4>(sh, A, c, bf, s);
         else if (sh.vec == 2) launch_march<T, 2>(sh, A, c, bf, s);
         else launch_march<T, 1>(sh, A, c, bf, s);
@@ -820,12 +1370,25 @@ int iso_setup_blocks(const Geometry &g) {
     return (int)nb;
 }
 
-StepShape iso_pick_shape(int dtype, const Geometry &g, int rows_hint, int bx_hint) {
+StepShape iso_pick_shape(int dtype, const Geometry &g, int rows_hint, int bx_hint, int kind_hint) {
     StepShape sh;
     const int64_t W = g.k == 2 ? g.L[1] : 0;
     const int vmax = dtype == 1 ? 4 : 2;
-    if (g.k == 2 && W >= 32) {
-        sh.kind = 0;
+    const int vfull = dtype == 1 ? 4 : 2;  // one 16-byte vector per thread
+    if (g.k == 2 && W >= 32 && W % vfull == 0 && kind_hint == 2) {
+        // TMA row pipeline: spans of at most 512 columns (fp32), 128 threads
+        sh.kind = 2;
+        sh.vec = vfull;
+        const int64_t cols = W / vfull;
+        sh.bx = bx_hint > 0 ? bx_hint : (int)std::min<int64_t>(128, ((cols + 31) / 32) * 32);
+        sh.gx = (int)((cols + sh.bx - 1) / sh.bx);
+        const int64_t H = g.L[0];
+        int rows = rows_hint;
+        if (rows <= 0) rows = (int)std::max<int64_t>(8, std::min<int64_t>(32, H / 16));
+        sh.rows = rows;
+        sh.gy = (int)((H + rows - 1) / rows);
+    } else if (g.k == 2 && W >= 32 && kind_hint != 1) {
+        sh.kind = kind_hint == 3 ? 0 : 4;
         sh.vec = (W % vmax == 0) ? vmax : ((W % 2 == 0) ? 2 : 1);
         const int64_t cols = (W + sh.vec - 1) / sh.vec;
         int bx = bx_hint > 0 ? bx_hint : (int)std::min<int64_t>(128, ((cols + 31) / 32) * 32);
@@ -856,8 +1419,8 @@ cudaError_t iso_setup(int dtype, const Geometry &g, const IsoCall &c, const IsoB
 }
 
 cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh,
-                     int par, cudaStream_t s) {
-    return dtype == 1 ? step_t<float>(g, c, bf, sh, par, s) : step_t<double>(g, c, bf, sh, par, s);
+                     int par, int variant, cudaStream_t s) {
+    return dtype == 1 ? step_t<float>(g, c, bf, sh, par, variant, s) : step_t<double>(g, c, bf, sh, par, variant, s);
 }
 
 cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, void *out,

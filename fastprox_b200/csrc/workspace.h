@@ -8,6 +8,7 @@
 
 #include "../../include/fastprox_b200.h"
 #include "engine.h"
+#include "aniso.h"
 #include "launch.h"
 
 namespace fpb {
@@ -42,15 +43,25 @@ struct fp_workspace {
     void *U[2] = {nullptr, nullptr}, *V[2] = {nullptr, nullptr};
     fpb::IsoImage *img = nullptr;
     fpb::IsoState *st = nullptr;
+    // anisotropic TV: per-image state, the polish's scratch, FDPG-3's scratch
+    fpb::AnImage *an_img = nullptr;
+    fpb::AnState *an_st = nullptr;
+    void *an_scratch = nullptr;
+    uint8_t *an_flag = nullptr;
+    int *an_parent = nullptr, *an_cnt = nullptr;
+    unsigned long long *an_sum = nullptr;
     double *gammas = nullptr;
     double *part = nullptr;
     unsigned *ticket = nullptr;
     int *live = nullptr;
+    int *err = nullptr;
     int max_part = 0;
     // pinned host memory
     int *h_live = nullptr;
     fpb::IsoImage *h_img = nullptr;
     fpb::IsoState *h_st = nullptr;
+    fpb::AnImage *h_an_img = nullptr;
+    fpb::AnState *h_an_st = nullptr;
     double *h_gam = nullptr;
     void *h_stage = nullptr;
     cudaEvent_t ev[2] = {nullptr, nullptr};
