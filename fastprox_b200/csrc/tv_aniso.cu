@@ -826,11 +826,6 @@ __global__ void an_output(AnGeom g, AnBuffers bf, T *__restrict__ out) {
     }
 }
 
-int grid1(int64_t n, int t) {
-    int64_t g = (n + t - 1) / t;
-    if (g > 4096) g = 4096;
-    return (int)std::max<int64_t>(1, g);
-}
 
 template <class T>
 cudaError_t setup_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, const void *x, cudaStream_t s) {

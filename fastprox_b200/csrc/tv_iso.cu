@@ -525,7 +525,6 @@ __device__ __forceinline__ void lean_rows(const T *__restrict__ D, const T *__re
     const int lane = threadIdx.x & 31;
     const bool colok = cb < W;
     const bool ext = lane == 31 && cb + VEC < W;  // the next warp's first column
-    const int cx = cb + VEC;
     auto ld = [&](const T *P, int off, T(&o)[VEC]) {
         if (!ZIN && colok) load_pack<T, VEC>(P + off, o);
         else
@@ -1469,3 +1468,200 @@ cudaError_t strided_copy(const void *src, int src_dtype, const int64_t *shape, c
 }
 
 }  // namespace fpb
+
+// ---------------------------------------------------------------------------
+// fp_b200_tv_iso_noalloc: the isotropic solve for callers that cannot
+// allocate device memory (see include/fastprox_b200.h). Its scratch is the
+// file-scope array below, resolved to a device address once per device.
+// ---------------------------------------------------------------------------
+
+#include <mutex>
+
+#include "../../include/fastprox_b200.h"
+
+namespace fpb {
+namespace {
+
+constexpr int64_t kNoAllocPixels = int64_t(1) << 20;  // batch x height x width at most
+constexpr int64_t kNoAllocImages = 64;                // batch at most
+constexpr int kNoAllocParts = 1024;                   // partial-sum slots per image
+
+constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+// Byte offsets of the scratch regions.
+constexpr size_t kOffD = 0;
+constexpr size_t kOffU0 = kOffD + align256(kNoAllocPixels * 4);
+constexpr size_t kOffU1 = kOffU0 + align256(2 * kNoAllocPixels * 4);
+constexpr size_t kOffV0 = kOffU1 + align256(2 * kNoAllocPixels * 4);
+constexpr size_t kOffV1 = kOffV0 + align256(2 * kNoAllocPixels * 4);
+constexpr size_t kOffDual = kOffV1 + align256(2 * kNoAllocPixels * 4);
+constexpr size_t kOffImg = kOffDual + align256(2 * kNoAllocPixels * 4);
+constexpr size_t kOffSt = kOffImg + align256(kNoAllocImages * sizeof(IsoImage));
+constexpr size_t kOffGam = kOffSt + align256(kNoAllocImages * sizeof(IsoState));
+constexpr size_t kOffPart = kOffGam + align256(kNoAllocImages * sizeof(double));
+constexpr size_t kOffTicket = kOffPart + align256(kNoAllocImages * kNoAllocParts * 2 * sizeof(double));
+constexpr size_t kOffLive = kOffTicket + align256(kNoAllocImages * sizeof(unsigned));
+constexpr size_t kOffErr = kOffLive + 256;
+constexpr size_t kOffRes = kOffErr + 256;  // per image: gap (double), iters (int); then a flag word
+constexpr size_t kNoAllocBytes = kOffRes + align256(kNoAllocImages * (sizeof(double) + sizeof(int)) + 16);
+
+// Every GPU that loads this library holds this array (about 47 MB) until
+// the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+unsigned char *g_scratch_addr[kMaxDevices] = {};
+std::mutex g_scratch_mu;
+
+// Per-image results into the scratch: gap at the input's scale, iterations,
+// and flag bits (1: an image did not converge, 2: an image held an Inf).
+__global__ void noalloc_results(const IsoImage *img, const IsoState *st, int64_t B, double *gaps, int *iters,
+                                int *flags) {
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    const IsoImage im = img[b];
+    const IsoState s = st[b];
+    double gap = 0.0;
+    int it = 0;
+    if (im.mode == kModeInf) {
+        atomicOr(flags, 2);
+    } else if (im.mode == kModeNan) {
+        gap = CUDART_NAN;
+    } else if (im.mode == kModeFdpg) {
+        gap = isnan(s.gp) ? s.gp : fmax(s.gp, 0.0);
+        if (im.e) gap = ldexp(gap, 2 * im.e);
+        it = s.it;
+        if (s.status != kConverged) atomicOr(flags, 1);
+    }
+    gaps[b] = gap;
+    iters[b] = it;
+}
+
+}  // namespace
+}  // namespace fpb
+
+extern "C" FP_API fp_status fp_b200_tv_iso_noalloc(const float *x, float *z, int64_t batch, int64_t height,
+                                                    int64_t width, double gamma, double tol, int max_iter,
+                                                    void *stream, double *gaps, int *iters) {
+    using namespace fpb;
+    if (batch < 0 || height < 0 || width < 0) return FP_ESHAPE;
+    if (batch == 0 || height == 0 || width == 0) return FP_OK;
+    if (!x || !z) return FP_EINVAL;
+    if (batch > kNoAllocImages || height > kNoAllocPixels || width > kNoAllocPixels ||
+        batch * height * width > kNoAllocPixels)
+        return FP_ESHAPE;
+    if (!std::isfinite(gamma) || gamma < 0.0 || !(gamma <= 0x1p960)) return FP_EPARAM;
+    if (!(tol >= 0.0) || !std::isfinite(tol) || max_iter < 1) return FP_EPARAM;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FP_EDEVICE;
+    unsigned char *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_scratch_mu);
+        if (!g_scratch_addr[dev]) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+                cudaGetLastError();
+                return FP_EDEVICE;
+            }
+            g_scratch_addr[dev] = static_cast<unsigned char *>(p);
+        }
+        base = g_scratch_addr[dev];
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Geometry g{};
+    g.k = 2;
+    g.L[0] = height;
+    g.L[1] = width;
+    g.L[2] = 1;
+    g.N = height * width;
+    g.B = batch;
+    // unit axis weights: the active axes are those of extent > 1 (tv_iso.cpp:350-358)
+    IsoCall c{};
+    int na = 0, act = 0;
+    for (int a = 0; a < 2; ++a)
+        if (g.L[a] > 1) {
+            ++na;
+            act = a;
+        }
+    c.na = na;
+    c.act_axis = act;
+    c.w_act = 1.0;
+    c.wmax = 1.0;
+    c.whmin = 1.0;
+    double L2 = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        c.wh[a] = (a < 2 && g.L[a] > 1) ? 1.0 : 0.0;
+        L2 += 4.0 * c.wh[a] * c.wh[a];
+    }
+    c.tau = L2 > 0.0 ? 1.0 / L2 : 0.0;
+    c.tol = tol;
+    c.max_iter = max_iter;
+    c.has_alpha = 0;
+    c.alpha_stride = 0;
+    c.alpha_max = 0.0;
+    c.step_scale = 1.0;
+    IsoBuffers bf;
+    bf.d = base + kOffD;
+    bf.U[0] = base + kOffU0;
+    bf.U[1] = base + kOffU1;
+    bf.V[0] = base + kOffV0;
+    bf.V[1] = base + kOffV1;
+    bf.dual = base + kOffDual;
+    bf.alpha = nullptr;
+    bf.img = reinterpret_cast<IsoImage *>(base + kOffImg);
+    bf.st = reinterpret_cast<IsoState *>(base + kOffSt);
+    bf.gammas = reinterpret_cast<double *>(base + kOffGam);
+    bf.part = reinterpret_cast<double *>(base + kOffPart);
+    bf.ticket = reinterpret_cast<unsigned *>(base + kOffTicket);
+    bf.live = reinterpret_cast<int *>(base + kOffLive);
+    bf.err = reinterpret_cast<int *>(base + kOffErr);
+    bf.max_part = kNoAllocParts;
+    double *rg = reinterpret_cast<double *>(base + kOffRes);
+    int *ri = reinterpret_cast<int *>(base + kOffRes + kNoAllocImages * sizeof(double));
+    int *rflags = ri + kNoAllocImages;
+    StepShape sh = iso_pick_shape(FP_F32, g, 0, 0, 0);
+    if (sh.gx * sh.gy > kNoAllocParts) {  // more rows per block keep the partials within their slots
+        const int per = kNoAllocParts / sh.gx;
+        sh.rows = (int)((height + per - 1) / per);
+        sh.gy = (int)((height + sh.rows - 1) / sh.rows);
+    }
+    if (sh.gx * sh.gy > kNoAllocParts || iso_setup_blocks(g) > kNoAllocParts) return FP_ESHAPE;
+    // the scratch keeps the last call's contents: clear what must start at zero
+    cudaError_t e = cudaMemsetAsync(bf.ticket, 0, (size_t)batch * sizeof(unsigned), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bf.live, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bf.err, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(rflags, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = fill_double(bf.gammas, gamma, batch, s);
+    if (e == cudaSuccess) e = iso_setup(FP_F32, g, c, bf, x, 0, 0, s);
+    if (e != cudaSuccess) return FP_EDEVICE;
+    int par = 0;
+    int64_t launched = 0;
+    const int chunk = 8;
+    for (;;) {
+        for (int j = 0; j < chunk; ++j) {
+            e = iso_step(FP_F32, g, c, bf, sh, par, iso_variant(launched, max_iter, false), s);
+            if (e != cudaSuccess) return FP_EDEVICE;
+            par ^= 1;
+            ++launched;
+        }
+        int live = 0;  // a pageable copy: this entry point holds no pinned memory either
+        if (cudaMemcpyAsync(&live, bf.live, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return FP_EDEVICE;
+        if (live == 0 || launched > (int64_t)max_iter + chunk) break;
+    }
+    e = iso_finalize(FP_F32, g, c, bf, z, s);
+    if (e == cudaSuccess) {
+        noalloc_results<<<(unsigned)((batch + 127) / 128), 128, 0, s>>>(bf.img, bf.st, batch, rg, ri, rflags);
+        e = cudaGetLastError();
+    }
+    int flags = 0, err = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flags, rflags, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&err, bf.err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && gaps) e = cudaMemcpyAsync(gaps, rg, (size_t)batch * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && iters) e = cudaMemcpyAsync(iters, ri, (size_t)batch * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess || err) return FP_EDEVICE;
+    if (flags & 2) return FP_EINVAL;
+    return (flags & 1) ? FP_ENOTCONV : FP_OK;
+}

@@ -182,6 +182,36 @@ FP_API int         fp_default_threads(void);
 FP_API fp_status fp_b200_workspace_stats(const fp_workspace *ws, int64_t *kernel_launches,
                                          int64_t *step_launches);
 
+/* Isotropic 2D TV prox of a small float32 batch without allocating any
+ * memory. No counterpart in the reference ABI.
+ *
+ * For callers that must not allocate device memory: a custom operator inside
+ * another runtime that plans all device memory ahead of time (an inference
+ * server with a fixed memory budget), a caching allocator's out-of-memory
+ * handler, or latency-bound code that may not call cudaMalloc because it can
+ * synchronise the whole device. fp_prox needs a workspace, and creating one
+ * allocates; this entry point takes its scratch from a fixed array inside the
+ * library instead (about 47 MB, held on every GPU that loads the library until
+ * the process exits). It calls no cudaMalloc, cudaFree or other allocating
+ * routine.
+ *
+ * x and z: device pointers on the calling thread's current device to
+ * contiguous (batch, height, width) float32 arrays; z may equal x. Unit axis
+ * weights, no pixel weights; gamma, tol and max_iter as in fp_prox. stream: a
+ * cudaStream_t (NULL for the legacy default stream); the call waits for it.
+ * gaps, iters: host arrays of batch entries for the per-image duality gap and
+ * iterations, or NULL. Limits: batch <= 64 and batch * height * width <= 2^20
+ * (FP_ESHAPE beyond them). Returns FP_OK, FP_ENOTCONV, FP_EINVAL (an image
+ * holding +-Inf), FP_EPARAM or FP_EDEVICE.
+ *
+ * Every call shares the one scratch array, which keeps the last call's
+ * contents: calls that overlap on the GPU (from two host threads, or on two
+ * streams) race and corrupt each other's results; serialise them. The first
+ * call on each device looks up the array's device address. */
+FP_API fp_status fp_b200_tv_iso_noalloc(const float *x, float *z, int64_t batch, int64_t height, int64_t width,
+                                        double gamma, double tol, int max_iter, void *stream, double *gaps,
+                                        int *iters);
+
 #ifdef __cplusplus
 }
 #endif
