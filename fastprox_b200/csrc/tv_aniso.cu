@@ -639,6 +639,19 @@ __global__ void an_union(AnGeom g, AnBuffers bf) {
     }
 }
 
+// The root of i by a walk that writes nothing (parents point to smaller
+// indices, so it ends). After the unions, each thread stores its own
+// entry's root only: a halving write here could put a stale, non-root
+// ancestor over an entry whose root another thread has already stored.
+__device__ __forceinline__ int uf_root(const int *P, int i) {
+    for (int n = 0; n < (1 << 30); ++n) {
+        const int p = P[i];
+        if (p == i) return i;
+        i = p;
+    }
+    return i;
+}
+
 // every entry to its root; the region sums of zp (64-bit fixed point) and sizes
 template <class T>
 __global__ void an_region_sum(AnGeom g, AnBuffers bf) {
@@ -652,7 +665,7 @@ __global__ void an_region_sum(AnGeom g, AnBuffers bf) {
     unsigned long long *S = bf.sum + (int64_t)b * N;
     int *C = bf.cnt + (int64_t)b * N;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
-        const int r = uf_find(P, (int)p);
+        const int r = uf_root(P, (int)p);
         P[p] = r;
         const long long fx = llrint(ldexp((double)ZP[p], sh));
         atomicAdd(S + r, (unsigned long long)fx);
