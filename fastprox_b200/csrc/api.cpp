@@ -535,6 +535,19 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
         A((void **)&ws->an_cnt, (size_t)B * (size_t)N * sizeof(int));
         A((void **)&ws->an_sum, (size_t)B * (size_t)N * sizeof(unsigned long long));
     }
+    if (ws->keep && op->kind == kIso) {
+        const size_t bn = (size_t)B * (size_t)N, kk = (size_t)g.k;
+        A((void **)&ws->v_flat, bn);
+        A((void **)&ws->v_root, bn * sizeof(int));
+        A((void **)&ws->v_cnt, bn * sizeof(int));
+        A((void **)&ws->v_gz, kk * bn * sizeof(double));
+        A((void **)&ws->v_h, kk * bn * sizeof(double));
+        A((void **)&ws->v_vec, 7 * bn * sizeof(double));
+        A((void **)&ws->v_acc, 2 * bn * sizeof(unsigned long long));
+        A((void **)&ws->v_img, (size_t)B * sizeof(VjpImage));
+        A((void **)&ws->v_cg, (size_t)B * sizeof(CgState));
+        A((void **)&ws->v_ggam, (size_t)B * sizeof(double));
+    }
     A((void **)&ws->img, (size_t)B * sizeof(IsoImage));
     A((void **)&ws->st, (size_t)B * sizeof(IsoState));
     A((void **)&ws->gammas, (size_t)B * sizeof(double));
@@ -549,6 +562,11 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     H((void **)&ws->h_img, (size_t)B * sizeof(IsoImage));
     H((void **)&ws->h_st, (size_t)B * sizeof(IsoState));
     H((void **)&ws->h_gam, (size_t)B * sizeof(double));
+    if (ws->keep && op->kind == kIso) {
+        H((void **)&ws->h_vimg, (size_t)B * sizeof(VjpImage));
+        H((void **)&ws->h_cg, (size_t)B * sizeof(CgState));
+        H((void **)&ws->h_ggam, (size_t)B * sizeof(double));
+    }
     if (op->kind == kAniso) {
         H((void **)&ws->h_an_img, (size_t)B * sizeof(AnImage));
         H((void **)&ws->h_an_st, (size_t)B * sizeof(AnState));
@@ -1070,6 +1088,8 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
     if (ws) {
         ws->valid = false;
         ws->info_valid = false;
+        ws->struct_valid = false;
+        ws->conj = conj;
     }
     if (x.numel() == 0) {
         if (ws) {
@@ -1313,6 +1333,207 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
 
 }  // namespace
 
+namespace {
+
+// The derivative at the kept point (the reference's vjp_impl,
+// src/api/api.cpp:693-738, and image_vjp_driver, src/core/driver.hpp:1505-1560):
+// gx = J^T g and the step's gradient summed over the batch. Isotropic TV.
+fp_status vjp_impl(const fp_op *op, fp_workspace *ws, const fp_array *ga, fp_array *gxa, double *ggamma,
+                   fp_array *ggdev, fp_array *gpa) {
+    if (!op || !ws || !ga || !gxa) return FP_EINVAL;
+    if (ws->op != op || !ws->valid) return FP_EINVAL;
+    if (op->kind != kIso) return FP_EINVAL;  // anisotropic derivatives: not on the device yet
+    if (gpa) return FP_EINVAL;               // parameter gradients: not on the device yet
+    Arr g, gx;
+    if (fp_status s = to_arr(ga, g)) return s;
+    if (fp_status s = to_arr(gxa, gx)) return s;
+    if (g.dtype != ws->dtype || gx.dtype != ws->dtype) return FP_EDTYPE;
+    if (g.ndim != ws->ndim || gx.ndim != ws->ndim) return FP_ESHAPE;
+    for (int d = 0; d < ws->ndim; ++d)
+        if (g.shape[d] != ws->shape[d] || gx.shape[d] != ws->shape[d]) return FP_ESHAPE;
+    if (fp_status s = check_output(&g, gx)) return s;
+    if (g.device != gx.device || ws->host_mode != (g.device == FP_DEVICE_CPU)) return FP_EINVAL;
+    Arr gg;
+    if (ggdev) {
+        if (fp_status s = to_arr(ggdev, gg)) return s;
+        if (gg.device != FP_DEVICE_CUDA || gg.numel() != 1) return FP_EINVAL;
+    }
+    const Geometry &g0 = ws->g;
+    if (g0.B * g0.N == 0) {
+        if (ggamma) *ggamma = 0.0;
+        return FP_OK;
+    }
+    DeviceScope dsc(ws->device);
+    cudaStream_t s = ws->stream;
+    const size_t T = ws->dtype == FP_F32 ? 4 : 8;
+    const int64_t total = g0.B * g0.N;
+    // geometry and the forward's weights
+    VjpGeom vg{};
+    vg.k = g0.k;
+    for (int a = 0; a < 3; ++a) vg.L[a] = g0.L[a];
+    vg.S[g0.k - 1] = 1;
+    for (int a = g0.k - 2; a >= 0; --a) vg.S[a] = vg.S[a + 1] * vg.L[a + 1];
+    for (int a = g0.k; a < 3; ++a) vg.S[a] = 1;
+    vg.N = g0.N;
+    vg.B = g0.B;
+    double wmax_all = 0.0;
+    for (int a = 0; a < g0.k; ++a)
+        if (g0.L[a] > 1) wmax_all = std::max(wmax_all, op->w[a]);
+    double wmax = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        const bool act = a < g0.k && op->w[a] > 0.0 && g0.L[a] > 1 && op->w[a] >= 1e-100 * wmax_all;
+        vg.wa[a] = act ? op->w[a] : 0.0;
+        wmax = std::max(wmax, vg.wa[a]);
+    }
+    vg.wmax = wmax > 0.0 ? wmax : 1.0;
+    for (int a = 0; a < 3; ++a) vg.wh[a] = vg.wa[a] / vg.wmax;
+    const double eps = ws->dtype == FP_F32 ? (double)std::numeric_limits<float>::epsilon() : 2.2e-16;
+    // the flat margin below the radius: the reference's 1e-9, or 64 eps where
+    // the iterates are float32 (its device path's dual_eta)
+    vg.eta = ws->dtype == FP_F32 ? 64.0 * eps : 1e-9;
+    VjpBuffers bf;
+    bf.d = ws->d;
+    bf.U[0] = ws->U[0];
+    bf.U[1] = ws->U[1];
+    bf.img = ws->img;
+    bf.st = ws->st;
+    bf.alpha = ws->spatial;
+    bf.alpha_stride = 0;
+    bf.dtype = ws->dtype;
+    bf.flat = ws->v_flat;
+    bf.root = ws->v_root;
+    bf.cnt = ws->v_cnt;
+    bf.gz = ws->v_gz;
+    bf.acc = ws->v_acc;
+    const size_t bn = (size_t)total;
+    bf.b = ws->v_vec;
+    bf.x = ws->v_vec + bn;
+    bf.r = ws->v_vec + 2 * bn;
+    bf.pv = ws->v_vec + 3 * bn;
+    bf.qv = ws->v_vec + 4 * bn;
+    bf.dinv = ws->v_vec + 5 * bn;
+    bf.y = ws->v_vec + 6 * bn;
+    bf.h = ws->v_h;
+    bf.vimg = ws->v_img;
+    bf.cg = ws->v_cg;
+    bf.ggam = ws->v_ggam;
+    bf.part = ws->part;
+    bf.ticket = ws->ticket;
+    bf.live = ws->live;
+    bf.err = ws->err;
+    bf.max_part = ws->max_part;
+    if (!bf.flat) return FP_EINVAL;
+    cudaError_t e = cudaSuccess;
+    if (!ws->struct_valid) {
+        // per image, from the forward (tv_iso.cpp:559-570), at the solved scale
+        for (int64_t b = 0; b < g0.B; ++b) {
+            const IsoImage &im = ws->h_img[b];
+            const IsoState &st = ws->h_st[b];
+            VjpImage &vi = ws->h_vimg[b];
+            const bool from_dual = im.mode == kModeFdpg;
+            const double gap_s = im.mode == kModeFdpg ? std::max(st.gp, 0.0) : 0.0;
+            vi.gs = std::ldexp(im.gamma_in, -im.e);
+            vi.rel = im.dd > 0.0 ? std::sqrt(2.0 * gap_s / im.dd) : 0.0;
+            vi.mu = from_dual ? 0.1 * vg.wmax * std::sqrt(2.0 * gap_s / (double)g0.N) : 0.0;
+            vi.thr = from_dual ? vg.wmax * 64.0 * eps * std::ldexp(im.maxabs, -im.e) : 0.0;
+        }
+        e = cudaMemcpyAsync(ws->v_img, ws->h_vimg, (size_t)g0.B * sizeof(VjpImage), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = vjp_structure(ws->dtype, vg, bf, s);
+        if (e != cudaSuccess) return cuda_status(e);
+        ws->struct_valid = true;
+    }
+    // the cotangent and the output, contiguous on the device (V buffers are
+    // free after the solve)
+    const void *gsrc = nullptr;
+    int64_t cst[FP_MAX_NDIM];
+    {
+        int64_t sz = 1;
+        for (int d = g.ndim - 1; d >= 0; --d) {
+            cst[d] = sz;
+            sz *= g.shape[d];
+        }
+    }
+    if (ws->host_mode) {
+        std::vector<char> tmp((size_t)total * T);
+        std::vector<int64_t> idx((size_t)g.ndim, 0);
+        for (int64_t i = 0; i < total; ++i) {
+            int64_t off = 0;
+            for (int d = 0; d < g.ndim; ++d) off += idx[(size_t)d] * g.strides[d];
+            std::memcpy(tmp.data() + i * (int64_t)T, g.data + off * (int64_t)T, T);
+            for (int d = g.ndim - 1; d >= 0; --d) {
+                if (++idx[(size_t)d] < g.shape[d]) break;
+                idx[(size_t)d] = 0;
+            }
+        }
+        e = cudaMemcpyAsync(ws->V[0], tmp.data(), tmp.size(), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        gsrc = ws->V[0];
+    } else if (g.contiguous()) {
+        if (pointer_device(g.data) != ws->device) return FP_EINVAL;
+        gsrc = g.data;
+    } else {
+        e = strided_copy(g.data, g.dtype, g.shape, g.strides, g.ndim, ws->V[0], g.dtype, cst, s);
+        gsrc = ws->V[0];
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    const bool direct = !ws->host_mode && gx.contiguous();
+    void *gdst = direct ? gx.data : ws->V[1];
+    if (direct && pointer_device(gx.data) != ws->device) return FP_EINVAL;
+    int64_t nl = 0;
+    e = vjp_solve(ws->dtype, vg, bf, gsrc, gdst, ws->deriv_tol, ws->deriv_max_iter, ws->conj ? 1 : 0, s, ws->h_live,
+                  ws->ev[0], &nl);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (!direct) {
+        if (ws->host_mode) {
+            std::vector<char> tmp((size_t)total * T);
+            e = cudaMemcpyAsync(tmp.data(), gdst, tmp.size(), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) return cuda_status(e);
+            std::vector<int64_t> idx((size_t)gx.ndim, 0);
+            for (int64_t i = 0; i < total; ++i) {
+                int64_t off = 0;
+                for (int d = 0; d < gx.ndim; ++d) off += idx[(size_t)d] * gx.strides[d];
+                std::memcpy(gx.data + off * (int64_t)T, tmp.data() + i * (int64_t)T, T);
+                for (int d = gx.ndim - 1; d >= 0; --d) {
+                    if (++idx[(size_t)d] < gx.shape[d]) break;
+                    idx[(size_t)d] = 0;
+                }
+            }
+        } else {
+            e = strided_copy(gdst, gx.dtype, gx.shape, cst, gx.ndim, gx.data, gx.dtype, gx.strides, s);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+    }
+    e = cudaMemcpyAsync(ws->h_ggam, ws->v_ggam, (size_t)g0.B * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ws->h_cg, ws->v_cg, (size_t)g0.B * sizeof(CgState), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e);
+    double tot = 0.0, res = 0.0;
+    int its = 0;
+    for (int64_t b = 0; b < g0.B; ++b) {
+        tot += ws->h_ggam[b];
+        res = std::max(res, ws->h_cg[b].res);
+        its = std::max(its, ws->h_cg[b].it);
+    }
+    ws->deriv_residual = res;
+    ws->deriv_iters = its;
+    ws->kernel_launches = nl;
+    if (ggamma) *ggamma = tot;
+    if (ggdev) {
+        if (gg.dtype == FP_F32) {
+            const float v = (float)tot;
+            e = cudaMemcpy(gg.data, &v, sizeof v, cudaMemcpyHostToDevice);
+        } else {
+            e = cudaMemcpy(gg.data, &tot, sizeof tot, cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    return FP_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 FP_API fp_status fp_prox(const fp_op *op, double gamma, const fp_array *x, fp_array *out, const fp_options *opt,
@@ -1352,22 +1573,12 @@ FP_API fp_status fp_jvp(const fp_op *op, const fp_workspace *ws, const fp_array 
 
 FP_API fp_status fp_vjp(const fp_op *op, const fp_workspace *ws, const fp_array *g, fp_array *gx, double *ggamma,
                         fp_array *gparams) {
-    (void)g;
-    (void)gx;
-    (void)ggamma;
-    (void)gparams;
-    if (!op || !ws || !ws->valid) return FP_EINVAL;
-    return FP_EINVAL;
+    return guard([&] { return vjp_impl(op, const_cast<fp_workspace *>(ws), g, gx, ggamma, nullptr, gparams); });
 }
 
 FP_API fp_status fp_vjp_device(const fp_op *op, const fp_workspace *ws, const fp_array *g, fp_array *gx,
                                fp_array *ggamma, fp_array *gparams) {
-    (void)g;
-    (void)gx;
-    (void)ggamma;
-    (void)gparams;
-    if (!op || !ws || !ws->valid) return FP_EINVAL;
-    return FP_EINVAL;
+    return guard([&] { return vjp_impl(op, const_cast<fp_workspace *>(ws), g, gx, nullptr, ggamma, gparams); });
 }
 
 }  // extern "C"

@@ -1,0 +1,698 @@
+// The vector-Jacobian product of isotropic TV on sm_100a, by implicit
+// differentiation at the point a prox call kept (keep_structure).
+//
+// The reference's TVIso::save / Sys / cg / vjp_img (src/ops/tv_iso.cpp:551-631,
+// 672-934, 1000-1067), per image on the device:
+//   * structure: a pixel is flat when it has no active forward neighbour, when
+//     its gradient |(W D z)_p| is at the rounding level of the data, or when
+//     its dual is strictly inside its ball (complementary slackness); flat
+//     pixels join their forward neighbours into regions (union-find, each
+//     region named by its smallest pixel index, its "root");
+//   * the system (M^T (I + G_A^T H G_A) M) c = M^T g on the regions, with
+//     H_p = r_p / max(|g_p|, mu) (I - n_p n_p^T) on the non-flat pixels, solved
+//     by conjugate gradients preconditioned by its diagonal (Jacobi), each
+//     image stopping at its own tolerance (the relative error of z that its gap
+//     certifies, at least 1e-10, or the caller's);
+//   * gx = M c (every pixel takes its region's value), and the step's gradient
+//     -sum over non-flat pixels of alpha_p <(G gx)_p, n_p>.
+// Region vectors live at the roots' slots of pixel-sized arrays, so nothing
+// is compacted. Every region sum (the right-hand side, each product with the
+// matrix, the diagonal) is accumulated in 128-bit fixed point with integer
+// atomics: exact, so the result is the same bit for bit on every run.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+
+#include "common.cuh"
+#include "vjp.h"
+
+namespace fpb {
+namespace {
+
+constexpr int kT = 256;
+
+__device__ __forceinline__ int uf_find_h(int *P, int i) {
+    for (int n = 0; n < (1 << 30); ++n) {
+        const int p = P[i];
+        if (p == i) return i;
+        const int q = P[p];
+        if (q != p) P[i] = q;
+        i = p;
+    }
+    return i;
+}
+
+__device__ __forceinline__ int uf_root_r(const int *P, int i) {
+    for (int n = 0; n < (1 << 30); ++n) {
+        const int p = P[i];
+        if (p == i) return i;
+        i = p;
+    }
+    return i;
+}
+
+// ---- 128-bit fixed point -------------------------------------------------
+
+struct I128 {
+    unsigned long long lo;
+    long long hi;
+};
+
+// v 2^s as a 128-bit integer (|v 2^s| < 2^126)
+__device__ __forceinline__ I128 to_fixed(double v, int s) {
+    const double t = ldexp(v, s);
+    const double h = floor(ldexp(t, -64));
+    const double rem = t - ldexp(h, 64);  // in [0, 2^64)
+    I128 r;
+    r.hi = (long long)h;
+    double rr = rint(rem);
+    if (rr >= 18446744073709551616.0) {
+        rr = 0.0;
+        r.hi += 1;
+    }
+    r.lo = (unsigned long long)rr;
+    return r;
+}
+
+__device__ __forceinline__ double from_fixed(unsigned long long lo, long long hi, int s) {
+    return ldexp(ldexp((double)hi, 64) + (double)lo, -s);
+}
+
+__device__ __forceinline__ I128 add128(I128 a, I128 b) {
+    I128 r;
+    r.lo = a.lo + b.lo;
+    r.hi = a.hi + b.hi + (r.lo < a.lo ? 1 : 0);
+    return r;
+}
+
+// acc[2 slot] (lo) and acc[2 slot + 1] (hi) += v 2^s; a warp whose lanes all
+// add to one slot sums first and adds once.
+__device__ __forceinline__ void racc(unsigned long long *acc, int slot, double v, int s, bool active) {
+    const unsigned mask = __activemask();
+    I128 x = active ? to_fixed(v, s) : I128{0ull, 0ll};
+    const int lead_slot = __shfl_sync(mask, active ? slot : -1, __ffs(mask) - 1);
+    const bool uniform = __all_sync(mask, !active || slot == lead_slot) && lead_slot >= 0 && mask == 0xffffffffu;
+    if (uniform) {
+        for (int o = 16; o > 0; o >>= 1) {
+            I128 y;
+            y.lo = __shfl_down_sync(mask, x.lo, o);
+            y.hi = __shfl_down_sync(mask, x.hi, o);
+            if ((threadIdx.x & 31) + o < 32) x = add128(x, y);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            const unsigned long long old = atomicAdd(acc + 2 * (int64_t)lead_slot, x.lo);
+            const unsigned long long carry = (old + x.lo < old) ? 1ull : 0ull;
+            atomicAdd(acc + 2 * (int64_t)lead_slot + 1, (unsigned long long)x.hi + carry);
+        }
+        return;
+    }
+    if (!active) return;
+    const unsigned long long old = atomicAdd(acc + 2 * (int64_t)slot, x.lo);
+    const unsigned long long carry = (old + x.lo < old) ? 1ull : 0ull;
+    atomicAdd(acc + 2 * (int64_t)slot + 1, (unsigned long long)x.hi + carry);
+}
+
+// the fixed-point exponent for values below 2^E in magnitude over N terms
+__device__ __forceinline__ int fixed_exp(double maxabs, int64_t N) {
+    if (!(maxabs > 0.0) || !isfinite(maxabs)) return 0;
+    int lg = 0;
+    while ((1LL << lg) <= N) ++lg;
+    return 124 - lg - (ilogb(maxabs) + 1);
+}
+
+// ---- per-image bookkeeping --------------------------------------------------
+
+__device__ __forceinline__ bool img_reduce(const VjpBuffers &bf, int b, unsigned blk, unsigned nblk, double a0,
+                                           double a1, double *sh, int *flag, double &t0, double &t1, bool mx) {
+    const double s0 = mx ? block_max(a0, sh) : block_sum(a0, sh);
+    const double s1 = block_sum(a1, sh);
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[blk * 2 + 0] = s0;
+        part[blk * 2 + 1] = s1;
+    }
+    if (!arrive_last(bf.ticket + b, nblk, flag)) return false;
+    t0 = mx ? max_partials(part, nblk, 2, 0, sh) : sum_partials(part, nblk, 2, 0, sh);
+    t1 = sum_partials(part, nblk, 2, 1, sh);
+    if (threadIdx.x != 0) return false;
+    bf.ticket[b] = 0;
+    return true;
+}
+
+struct Px {  // a pixel's coordinates and its forward neighbours
+    int64_t co[3];
+    bool has[3];
+};
+
+__device__ __forceinline__ Px pix_of(const VjpGeom &g, int64_t p) {
+    Px x;
+    for (int a = 0; a < 3; ++a) {
+        x.co[a] = a < g.k ? (p / g.S[a]) % g.L[a] : 0;
+        x.has[a] = a < g.k && g.wa[a] != 0.0 && x.co[a] + 1 < g.L[a];
+    }
+    return x;
+}
+
+// z at the solved scale of image b at pixel q: from the dual of the solve
+// (d - G^T u, tv_iso.cpp:251-270), or the stored z of a single-axis solve
+template <class T>
+__device__ __forceinline__ double z_at(const VjpGeom &g, const VjpBuffers &bf, int b, int64_t q) {
+    const int mode = bf.img[b].mode;
+    const int64_t N = g.N;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    if (mode == kModeTv1d) return (double)static_cast<const T *>(bf.U[0])[(int64_t)b * g.k * N + q];
+    if (mode != kModeFdpg) return (double)D[q];
+    const T *U = static_cast<const T *>(bf.U[bf.st[b].fin_par]) + (int64_t)b * g.k * N;
+    double z = (double)D[q];
+    for (int a = 0; a < g.k; ++a) {
+        const double wh = g.wh[a];
+        if (wh == 0.0) continue;
+        const int64_t co = (q / g.S[a]) % g.L[a];
+        const double cur = (double)U[a * N + q];
+        const double prev = co > 0 ? (double)U[a * N + q - g.S[a]] : 0.0;
+        z += wh * (cur - prev);
+    }
+    return z;
+}
+
+// ---- structure (tv_iso.cpp:551-631) ---------------------------------------------
+
+template <class T>
+__global__ void __launch_bounds__(kT) st_flat(VjpGeom g, VjpBuffers bf) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const VjpImage &vi = bf.vimg[b];
+    const int mode = bf.img[b].mode;
+    const bool from_dual = mode == kModeFdpg;
+    const T *U = from_dual ? static_cast<const T *>(bf.U[bf.st[b].fin_par]) + (int64_t)b * g.k * N : nullptr;
+    const T *AL = bf.alpha ? static_cast<const T *>(bf.alpha) + (int64_t)b * bf.alpha_stride : nullptr;
+    double *GZ = bf.gz + (int64_t)b * g.k * N;
+    uint8_t *F = bf.flat + (int64_t)b * N;
+    int *P = bf.root + (int64_t)b * N;
+    int *C = bf.cnt + (int64_t)b * N;
+    unsigned long long *A = bf.acc + (int64_t)b * 2 * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const Px x = pix_of(g, p);
+        const double z0 = z_at<T>(g, bf, b, p);
+        double nn = 0.0;
+        bool any = false;
+        for (int a = 0; a < g.k; ++a) {
+            double gv = 0.0;
+            if (x.has[a]) {
+                gv = g.wa[a] * (z_at<T>(g, bf, b, p + g.S[a]) - z0);
+                nn += gv * gv;
+                any = true;
+            }
+            GZ[a * N + p] = gv;
+        }
+        bool fl = !any || sqrt(nn) <= vi.thr;
+        if (from_dual && !fl) {
+            double uu = 0.0;
+            for (int a = 0; a < g.k; ++a) {
+                const double ua = (double)U[a * N + p] / g.wmax;
+                uu += ua * ua;
+            }
+            const double r = AL ? ((double)AL[p] == 0.0 ? 0.0 : vi.gs * (double)AL[p]) : vi.gs;
+            fl = sqrt(uu) < r * (1.0 - g.eta);
+        }
+        F[p] = fl ? (any ? 1 : 3) : 0;  // bit 0: flat; bit 1: no active neighbour
+        P[p] = (int)p;
+        C[p] = 0;
+        A[2 * p] = 0ull;
+        A[2 * p + 1] = 0ull;
+    }
+}
+
+// flat pixels with an active neighbour join it (tv_iso.cpp:601-608)
+__global__ void st_union(VjpGeom g, VjpBuffers bf) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const uint8_t *F = bf.flat + (int64_t)b * N;
+    int *P = bf.root + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        if (F[p] != 1) continue;
+        const Px x = pix_of(g, p);
+        for (int a = 0; a < g.k; ++a) {
+            if (!x.has[a]) continue;
+            int u = (int)p, v = (int)(p + g.S[a]);
+            for (int tries = 0;; ++tries) {
+                u = uf_find_h(P, u);
+                v = uf_find_h(P, v);
+                if (u == v) break;
+                const int hi = u > v ? u : v, lo = u > v ? v : u;
+                const int old = atomicCAS(P + hi, hi, lo);
+                if (old == hi) break;
+                u = old;
+                v = lo;
+                if (tries > (1 << 24)) {
+                    atomicExch(bf.err, 2);
+                    break;
+                }
+            }
+        }
+    }
+}
+
+// every pixel to its root (each thread writes its own entry); region sizes
+__global__ void st_roots(VjpGeom g, VjpBuffers bf) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    int *P = bf.root + (int64_t)b * N;
+    int *C = bf.cnt + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const int r = uf_root_r(P, (int)p);
+        P[p] = r;
+        atomicAdd(C + r, 1);
+    }
+}
+
+// ---- region sums of pixel values: max pass, atomic pass, read-out ----------------
+
+// pass 1 over the per-pixel values v_p (kind: 0 the cotangent g, 1 the product
+// y = pix + G^T H G pix of the conjugate gradients, 2 the Jacobi terms): the
+// per-image maximum |v| sets the fixed-point exponent.
+template <class T>
+__device__ __forceinline__ double apply_y(const VjpGeom &g, const VjpBuffers &bf, int b, int64_t p) {
+    // y_p = c[root p] - sum_a w_a (h_a[p] - h_a[p - e_a]) (tv_iso.cpp:870-884)
+    const int64_t N = g.N;
+    const int *R = bf.root + (int64_t)b * N;
+    const double *PV = bf.pv + (int64_t)b * N;
+    const double *Hh = bf.h + (int64_t)b * g.k * N;
+    double y = PV[R[p]];
+    for (int a = 0; a < g.k; ++a) {
+        if (g.wa[a] == 0.0) continue;
+        const int64_t co = (p / g.S[a]) % g.L[a];
+        const double prev = co > 0 ? Hh[a * N + p - g.S[a]] : 0.0;
+        y -= g.wa[a] * (Hh[a * N + p] - prev);
+    }
+    return y;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kT) rs_max(VjpGeom g, VjpBuffers bf, int kind, const T *__restrict__ gin) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    if (kind == 1 && bf.cg[b].status != kCgLive) return;
+    const int64_t N = g.N;
+    double m = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        double v;
+        if (kind == 0) v = (double)gin[(int64_t)b * N + p];
+        else v = apply_y<T>(g, bf, b, p);
+        if (kind == 1) bf.y[(int64_t)b * N + p] = v;
+        m = fmax(m, fabs(v));
+    }
+    double mx, unused;
+    if (!img_reduce(bf, b, blockIdx.x, gridDim.x, m, 0.0, sh, &flag, mx, unused, true)) return;
+    bf.cg[b].fx = fixed_exp(mx, N);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kT) rs_add(VjpGeom g, VjpBuffers bf, int kind, const T *__restrict__ gin) {
+    const int b = blockIdx.y;
+    if (kind == 1 && bf.cg[b].status != kCgLive) return;
+    const int64_t N = g.N;
+    const int s = bf.cg[b].fx;
+    const int *R = bf.root + (int64_t)b * N;
+    unsigned long long *A = bf.acc + (int64_t)b * 2 * N;
+    const int64_t n_pad = ((N + 31) / 32) * 32;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_pad; p += (int64_t)gridDim.x * blockDim.x) {
+        const bool act = p < N;
+        double v = 0.0;
+        int slot = 0;
+        if (act) {
+            v = kind == 0 ? (double)gin[(int64_t)b * N + p] : bf.y[(int64_t)b * N + p];
+            slot = R[p];
+        }
+        racc(A, slot, v, s, act);
+    }
+}
+
+// read-out at the roots: out[C] = the sum, accumulators cleared
+__global__ void rs_read(VjpGeom g, VjpBuffers bf, int kind, double *outv) {
+    const int b = blockIdx.y;
+    if (kind == 1 && bf.cg[b].status != kCgLive) return;
+    const int64_t N = g.N;
+    const int s = bf.cg[b].fx;
+    const int *R = bf.root + (int64_t)b * N;
+    unsigned long long *A = bf.acc + (int64_t)b * 2 * N;
+    double *O = outv + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        if (R[p] != p) continue;
+        O[p] = from_fixed(A[2 * p], (long long)A[2 * p + 1], s);
+        A[2 * p] = 0ull;
+        A[2 * p + 1] = 0ull;
+    }
+}
+
+// ---- Jacobi diagonal ---------------------------------------------------------
+
+template <class T>
+__device__ __forceinline__ int jterms(const VjpGeom &g, const VjpBuffers &bf, int b, int64_t p, int *slot,
+                                      double *val) {
+    const int64_t N = g.N;
+    if (bf.flat[(int64_t)b * N + p] & 1) return 0;
+    const int *R = bf.root + (int64_t)b * N;
+    const double *GZ = bf.gz + (int64_t)b * g.k * N;
+    const VjpImage &vi = bf.vimg[b];
+    const Px x = pix_of(g, p);
+    double nn = 0.0;
+    for (int a = 0; a < g.k; ++a) nn += GZ[a * N + p] * GZ[a * N + p];
+    const double nr = sqrt(nn);
+    double rp = vi.gs;
+    if (bf.alpha) {
+        const double al = (double)static_cast<const T *>(bf.alpha)[(int64_t)b * bf.alpha_stride + p];
+        rp = al == 0.0 ? 0.0 : vi.gs * al;
+    }
+    const double hs = rp / fmax(nr, vi.mu);
+    int lab[4];
+    lab[0] = R[p];
+    for (int a = 0; a < g.k; ++a) lab[a + 1] = x.has[a] ? R[p + g.S[a]] : -1;
+    int n = 0;
+    for (int c = 0; c <= g.k; ++c) {
+        const int C = lab[c];
+        if (C < 0) continue;
+        bool seen = false;
+        for (int e = 0; e < c; ++e) seen = seen || lab[e] == C;
+        if (seen) continue;
+        double hh = 0.0, nh = 0.0;
+        for (int a = 0; a < g.k; ++a) {
+            if (!x.has[a]) continue;
+            const double h = g.wa[a] * ((lab[a + 1] == C ? 1.0 : 0.0) - (lab[0] == C ? 1.0 : 0.0));
+            hh += h * h;
+            nh += h * GZ[a * N + p] / nr;
+        }
+        slot[n] = C;
+        val[n] = hs * (hh - nh * nh);
+        ++n;
+    }
+    return n;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kT) jac_max(VjpGeom g, VjpBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    double m = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        int slot[4];
+        double val[4];
+        const int n = jterms<T>(g, bf, b, p, slot, val);
+        for (int i = 0; i < n; ++i) m = fmax(m, fabs(val[i]));
+        if (bf.root[(int64_t)b * N + p] == p) m = fmax(m, (double)bf.cnt[(int64_t)b * N + p]);
+    }
+    double mx, unused;
+    if (!img_reduce(bf, b, blockIdx.x, gridDim.x, m, 0.0, sh, &flag, mx, unused, true)) return;
+    bf.cg[b].fx = fixed_exp(mx * 8.0, N);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kT) jac_add(VjpGeom g, VjpBuffers bf) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const int s = bf.cg[b].fx;
+    unsigned long long *A = bf.acc + (int64_t)b * 2 * N;
+    const int64_t n_pad = ((N + 31) / 32) * 32;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_pad; p += (int64_t)gridDim.x * blockDim.x) {
+        int slot[4] = {0, 0, 0, 0};
+        double val[4] = {0.0, 0.0, 0.0, 0.0};
+        int n = 0;
+        if (p < N) {
+            n = jterms<T>(g, bf, b, p, slot, val);
+            if (bf.root[(int64_t)b * N + p] == p) {  // |C| at the root
+                slot[n] = (int)p;
+                val[n] = (double)bf.cnt[(int64_t)b * N + p];
+                ++n;
+            }
+        }
+        for (int i = 0; i < 5; ++i) {
+            const bool act = i < n;
+            racc(A, act ? slot[i] : 0, act ? val[i] : 0.0, s, act);
+        }
+    }
+}
+
+// ---- conjugate gradients (tv_iso.cpp:891-934) --------------------------------
+
+// initial state: dinv = 1 / diag, bn = sum b^2 / |C|, x = 0, r = b, pv = r dinv, rz
+__global__ void __launch_bounds__(kT) cg_init(VjpGeom g, VjpBuffers bf, double tol, int max_iter) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const int *R = bf.root + (int64_t)b * N;
+    const int *C = bf.cnt + (int64_t)b * N;
+    double *X = bf.x + (int64_t)b * N, *Rr = bf.r + (int64_t)b * N, *PV = bf.pv + (int64_t)b * N;
+    double *DI = bf.dinv + (int64_t)b * N;
+    const double *Bv = bf.b + (int64_t)b * N;
+    double bn = 0.0, rz = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        if (R[p] != p) continue;
+        const double di = 1.0 / DI[p];
+        DI[p] = di;
+        const double bv = Bv[p];
+        X[p] = 0.0;
+        Rr[p] = bv;
+        PV[p] = bv * di;
+        bn += bv * bv / (double)C[p];
+        rz += bv * bv * di;
+    }
+    double tbn, trz;
+    if (!img_reduce(bf, b, blockIdx.x, gridDim.x, bn, rz, sh, &flag, tbn, trz, false)) return;
+    CgState &cs = bf.cg[b];
+    cs.bn = tbn;
+    cs.rz = trz;
+    cs.res = 1.0;
+    cs.it = 0;
+    const double t = tol > 0.0 ? tol : fmax(1e-10, bf.vimg[b].rel);
+    cs.tol = t;
+    cs.status = (tbn == 0.0 || bf.img[b].mode == kModeNan) ? kCgDone : kCgLive;
+    if (tbn == 0.0) cs.res = 0.0;
+    if (cs.status == kCgLive) atomicAdd(bf.live, 1);
+    cs.max_iter = max_iter;
+}
+
+// h = H G pix with pix = pv[root] (tv_iso.cpp:870-877, 809-827)
+template <class T>
+__global__ void __launch_bounds__(kT) cg_hg(VjpGeom g, VjpBuffers bf) {
+    const int b = blockIdx.y;
+    if (bf.cg[b].status != kCgLive) return;
+    const int64_t N = g.N;
+    const int *R = bf.root + (int64_t)b * N;
+    const double *PV = bf.pv + (int64_t)b * N;
+    const double *GZ = bf.gz + (int64_t)b * g.k * N;
+    const uint8_t *F = bf.flat + (int64_t)b * N;
+    double *Hh = bf.h + (int64_t)b * g.k * N;
+    const VjpImage &vi = bf.vimg[b];
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const Px x = pix_of(g, p);
+        if (F[p] & 1) {
+            for (int a = 0; a < g.k; ++a) Hh[a * N + p] = 0.0;
+            continue;
+        }
+        const double c0 = PV[R[p]];
+        double y[3] = {0.0, 0.0, 0.0}, nn = 0.0, dot = 0.0;
+        for (int a = 0; a < g.k; ++a) {
+            y[a] = x.has[a] ? g.wa[a] * (PV[R[p + g.S[a]]] - c0) : 0.0;
+            nn += GZ[a * N + p] * GZ[a * N + p];
+        }
+        const double nr = sqrt(nn);
+        for (int a = 0; a < g.k; ++a) dot += GZ[a * N + p] * y[a];
+        double rp = vi.gs;
+        if (bf.alpha) {
+            const double al = (double)static_cast<const T *>(bf.alpha)[(int64_t)b * bf.alpha_stride + p];
+            rp = al == 0.0 ? 0.0 : vi.gs * al;
+        }
+        const double h = rp / fmax(nr, vi.mu);
+        for (int a = 0; a < g.k; ++a) {
+            const double na = GZ[a * N + p] / nr;
+            Hh[a * N + p] = h * (y[a] - na * dot / nr);
+        }
+    }
+}
+
+// after qv = A pv: alpha = rz / <pv, qv>
+__global__ void __launch_bounds__(kT) cg_alpha(VjpGeom g, VjpBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    if (bf.cg[b].status != kCgLive) return;
+    const int64_t N = g.N;
+    const int *R = bf.root + (int64_t)b * N;
+    const double *PV = bf.pv + (int64_t)b * N, *QV = bf.qv + (int64_t)b * N;
+    double pq = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x)
+        if (R[p] == p) pq += PV[p] * QV[p];
+    double t, unused;
+    if (!img_reduce(bf, b, blockIdx.x, gridDim.x, pq, 0.0, sh, &flag, t, unused, false)) return;
+    CgState &cs = bf.cg[b];
+    if (!(t > 0.0)) {
+        cs.status = kCgDone;
+        atomicSub(bf.live, 1);
+        return;
+    }
+    cs.alpha = cs.rz / t;
+}
+
+// x += alpha pv, r -= alpha qv; beta, the residual and the stopping test
+__global__ void __launch_bounds__(kT) cg_step(VjpGeom g, VjpBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    if (bf.cg[b].status != kCgLive) return;
+    const int64_t N = g.N;
+    const double al = bf.cg[b].alpha;
+    const int *R = bf.root + (int64_t)b * N;
+    const int *C = bf.cnt + (int64_t)b * N;
+    double *X = bf.x + (int64_t)b * N, *Rr = bf.r + (int64_t)b * N;
+    const double *PV = bf.pv + (int64_t)b * N, *QV = bf.qv + (int64_t)b * N, *DI = bf.dinv + (int64_t)b * N;
+    double rzn = 0.0, rn = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        if (R[p] != p) continue;
+        X[p] += al * PV[p];
+        const double r = Rr[p] - al * QV[p];
+        Rr[p] = r;
+        rzn += r * r * DI[p];
+        rn += r * r / (double)C[p];
+    }
+    double t0, t1;
+    if (!img_reduce(bf, b, blockIdx.x, gridDim.x, rzn, rn, sh, &flag, t0, t1, false)) return;
+    CgState &cs = bf.cg[b];
+    cs.beta = t0 / cs.rz;
+    cs.rz = t0;
+    cs.it += 1;
+    cs.res = sqrt(t1 / cs.bn);
+    if (!(cs.res > cs.tol) || cs.it >= cs.max_iter) {
+        cs.status = kCgDone;
+        atomicSub(bf.live, 1);
+    }
+}
+
+__global__ void cg_pv(VjpGeom g, VjpBuffers bf) {
+    const int b = blockIdx.y;
+    if (bf.cg[b].status != kCgLive) return;
+    const int64_t N = g.N;
+    const double be = bf.cg[b].beta;
+    const int *R = bf.root + (int64_t)b * N;
+    double *PV = bf.pv + (int64_t)b * N;
+    const double *Rr = bf.r + (int64_t)b * N, *DI = bf.dinv + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x)
+        if (R[p] == p) PV[p] = Rr[p] * DI[p] + be * PV[p];
+}
+
+// ---- outputs (tv_iso.cpp:1014-1057) --------------------------------------------
+
+// gx = M x; per image the step's gradient -sum_A alpha_p <(G v)_p, n_p>
+template <class T>
+__global__ void __launch_bounds__(kT) vjp_out(VjpGeom g, VjpBuffers bf, const T *__restrict__ gin, T *__restrict__ gx,
+                                              int conj) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const int *R = bf.root + (int64_t)b * N;
+    const double *X = bf.x + (int64_t)b * N;
+    const double *GZ = bf.gz + (int64_t)b * g.k * N;
+    const uint8_t *F = bf.flat + (int64_t)b * N;
+    const bool nan = bf.img[b].mode == kModeNan;
+    const bool empty = bf.cg[b].bn == 0.0;
+    double gg = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const double v = empty ? 0.0 : X[R[p]];
+        const double gi = (double)gin[(int64_t)b * N + p];
+        double outv = nan ? (double)CUDART_NAN : v;
+        if (conj) outv = gi - outv;
+        gx[(int64_t)b * N + p] = (T)outv;
+        if (nan || (F[p] & 1)) continue;
+        const Px x = pix_of(g, p);
+        double nn = 0.0, t = 0.0;
+        for (int a = 0; a < g.k; ++a) nn += GZ[a * N + p] * GZ[a * N + p];
+        const double nr = sqrt(nn);
+        for (int a = 0; a < g.k; ++a) {
+            const double gv = x.has[a] && !empty ? g.wa[a] * (X[R[p + g.S[a]]] - v) : 0.0;
+            t += gv * GZ[a * N + p] / nr;
+        }
+        double al = 1.0;
+        if (bf.alpha)
+            al = (double)static_cast<const T *>(bf.alpha)[(int64_t)b * bf.alpha_stride + p];
+        gg += al * t;
+    }
+    double tg, unused;
+    if (!img_reduce(bf, b, blockIdx.x, gridDim.x, gg, 0.0, sh, &flag, tg, unused, false)) return;
+    bf.ggam[b] = nan ? (double)CUDART_NAN : (conj ? 0.0 : -tg);
+}
+
+int pblocks(const VjpGeom &g) {
+    int64_t nb = (g.N + kT * 4 - 1) / (kT * 4);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(nb, 512));
+}
+
+template <class T>
+cudaError_t structure_t(const VjpGeom &g, const VjpBuffers &bf, cudaStream_t s) {
+    const dim3 grid(pblocks(g), (unsigned)g.B);
+    st_flat<T><<<grid, kT, 0, s>>>(g, bf);
+    st_union<<<grid, kT, 0, s>>>(g, bf);
+    st_roots<<<grid, kT, 0, s>>>(g, bf);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t vjp_t(const VjpGeom &g, const VjpBuffers &bf, const void *gin, void *gx, double tol, int max_iter, int conj,
+                  cudaStream_t s, int *h_live, cudaEvent_t ev, int64_t *launches) {
+    const dim3 grid(pblocks(g), (unsigned)g.B);
+    const T *gi = static_cast<const T *>(gin);
+    int64_t nl = 0;
+    // right-hand side b = M^T g and the Jacobi diagonal
+    rs_max<T><<<grid, kT, 0, s>>>(g, bf, 0, gi);
+    rs_add<T><<<grid, kT, 0, s>>>(g, bf, 0, gi);
+    rs_read<<<grid, kT, 0, s>>>(g, bf, 0, bf.b);
+    jac_max<T><<<grid, kT, 0, s>>>(g, bf);
+    jac_add<T><<<grid, kT, 0, s>>>(g, bf);
+    rs_read<<<grid, kT, 0, s>>>(g, bf, 0, bf.dinv);
+    cudaMemsetAsync(bf.live, 0, sizeof(int), s);
+    cg_init<<<grid, kT, 0, s>>>(g, bf, tol, max_iter);
+    nl += 7;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int chunk = 8;
+    for (int it = 0; it < max_iter + chunk; it += chunk) {
+        for (int j = 0; j < chunk; ++j) {
+            cg_hg<T><<<grid, kT, 0, s>>>(g, bf);
+            rs_max<T><<<grid, kT, 0, s>>>(g, bf, 1, gi);
+            rs_add<T><<<grid, kT, 0, s>>>(g, bf, 1, gi);
+            rs_read<<<grid, kT, 0, s>>>(g, bf, 1, bf.qv);
+            cg_alpha<<<grid, kT, 0, s>>>(g, bf);
+            cg_step<<<grid, kT, 0, s>>>(g, bf);
+            cg_pv<<<grid, kT, 0, s>>>(g, bf);
+            nl += 7;
+        }
+        e = cudaMemcpyAsync(h_live, bf.live, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaEventRecord(ev, s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev);
+        if (e != cudaSuccess) return e;
+        if (*h_live == 0) break;
+    }
+    vjp_out<T><<<grid, kT, 0, s>>>(g, bf, gi, static_cast<T *>(gx), conj);
+    ++nl;
+    if (launches) *launches = nl;
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t vjp_structure(int dtype, const VjpGeom &g, const VjpBuffers &bf, cudaStream_t s) {
+    return dtype == 1 ? structure_t<float>(g, bf, s) : structure_t<double>(g, bf, s);
+}
+
+cudaError_t vjp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *gin, void *gx, double tol,
+                      int max_iter, int conj, cudaStream_t s, int *h_live, cudaEvent_t ev, int64_t *launches) {
+    return dtype == 1 ? vjp_t<float>(g, bf, gin, gx, tol, max_iter, conj, s, h_live, ev, launches)
+                      : vjp_t<double>(g, bf, gin, gx, tol, max_iter, conj, s, h_live, ev, launches);
+}
+
+}  // namespace fpb

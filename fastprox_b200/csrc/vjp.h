@@ -1,0 +1,66 @@
+// Host-visible structures of the isotropic TV derivative (tv_vjp.cu).
+#pragma once
+
+#include <cuda_runtime_api.h>
+
+#include <cstdint>
+
+#include "engine.h"
+
+namespace fpb {
+
+enum CgStatus : int { kCgLive = 0, kCgDone = 1 };
+
+struct VjpGeom {
+    int k;
+    int64_t L[3], S[3];
+    int64_t N, B;
+    double wa[3];  // active axis weights (0 elsewhere)
+    double wh[3];  // wa / wmax, as the forward used them
+    double wmax;
+    double eta;    // relative margin below the radius that counts as inside
+};
+
+// Per image, from the kept forward (tv_iso.cpp:559-570): the step at the
+// solved scale, the curvature cap, the certified relative error of z (the
+// default tolerance of the conjugate gradients) and the flat threshold.
+struct VjpImage {
+    double gs, mu, rel, thr;
+};
+
+struct CgState {
+    double rz, bn, alpha, beta, res, tol;
+    int it, status, max_iter, fx;
+};
+
+struct VjpBuffers {
+    // the forward's point
+    const void *d = nullptr;
+    const void *U[2] = {nullptr, nullptr};
+    const IsoImage *img = nullptr;
+    const IsoState *st = nullptr;
+    const void *alpha = nullptr;
+    int64_t alpha_stride = 0;
+    int dtype = 1;
+    // structure
+    uint8_t *flat = nullptr;
+    int *root = nullptr, *cnt = nullptr;
+    double *gz = nullptr;  // k x B x N
+    unsigned long long *acc = nullptr;  // 2 x B x N, 128-bit region accumulators
+    // conjugate gradients (region vectors at the roots' slots) and scratch
+    double *b = nullptr, *x = nullptr, *r = nullptr, *pv = nullptr, *qv = nullptr, *dinv = nullptr, *y = nullptr;
+    double *h = nullptr;  // k x B x N
+    VjpImage *vimg = nullptr;
+    CgState *cg = nullptr;
+    double *ggam = nullptr;  // per-image step gradient
+    double *part = nullptr;
+    unsigned *ticket = nullptr;
+    int *live = nullptr, *err = nullptr;
+    int max_part = 0;
+};
+
+cudaError_t vjp_structure(int dtype, const VjpGeom &g, const VjpBuffers &bf, cudaStream_t s);
+cudaError_t vjp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *gin, void *gx, double tol,
+                      int max_iter, int conj, cudaStream_t s, int *h_live, cudaEvent_t ev, int64_t *launches);
+
+}  // namespace fpb

@@ -10,6 +10,7 @@
 #include "engine.h"
 #include "aniso.h"
 #include "launch.h"
+#include "vjp.h"
 
 namespace fpb {
 enum OpKind : int { kIso = 1, kAniso = 2 };
@@ -56,6 +57,18 @@ struct fp_workspace {
     int *live = nullptr;
     int *err = nullptr;
     int max_part = 0;
+    // derivative (keep_structure workspaces): structure and conjugate gradients
+    uint8_t *v_flat = nullptr;
+    int *v_root = nullptr, *v_cnt = nullptr;
+    double *v_gz = nullptr, *v_h = nullptr, *v_vec = nullptr, *v_ggam = nullptr;
+    unsigned long long *v_acc = nullptr;
+    fpb::VjpImage *v_img = nullptr;
+    fpb::CgState *v_cg = nullptr;
+    fpb::VjpImage *h_vimg = nullptr;
+    fpb::CgState *h_cg = nullptr;
+    double *h_ggam = nullptr;
+    bool struct_valid = false;
+    bool conj = false;
     // pinned host memory
     int *h_live = nullptr;
     fpb::IsoImage *h_img = nullptr;
