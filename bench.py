@@ -44,6 +44,14 @@ BYTES_PER_PIXEL_ITER = 40  # d 4 + u 8 + v 8 in, u 8 + v 8 out, alpha 4 (fp32)
 WORKLOAD = "tv_iso 2D, 64 x 512^2 fp32 phantom+noise(0.1), pixel weights U[0.5,1.5], gamma {0.05,0.1,0.2}, gap<=1e-6"
 
 
+def reduce_max_time(t, dist, device):
+    """The slowest rank's device time: the whole job's time (replicas)."""
+    import torch
+    tt = torch.tensor([t], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
 def make_inputs(seed=0):
     from fastprox_b200 import synth
     x = synth.phantom(B, H, W, seed=seed, sigma=0.1)
@@ -155,6 +163,22 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
+def profile_case():
+    """The benchmark batch (64 x 512^2, pixel weights, three steps) solved for
+    exactly 8 iterations: launch 0 is the cold start, launches 4 and 8 carry
+    gap checks, the rest are plain iterations."""
+    import torch
+
+    from fastprox_b200 import TVIso
+    x, alpha, steps = make_inputs()
+    xt = torch.as_tensor(x, device="cuda")
+    st = torch.as_tensor(steps, device="cuda")
+    op = TVIso(2, pixel_weights=alpha)
+    z, info = op.solve(xt, st, tol=0.0, max_iter=8, with_dual=False)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": True, "iters": int(info.iters)}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -162,7 +186,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="one solve of the benchmark batch with 8 iterations (tol 0): the case for ncu captures")
+    ap.add_argument("--workload", default="iso512", choices=["iso512", "aniso512", "uneven", "vjp", "serve"],
+                    help="iso512 (default, the headline line); the others report the other workloads")
+    ap.add_argument("--serve-seconds", type=float, default=20.0)
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case()
+        return
+    if args.workload != "iso512" and args.impl == "ours":
+        from fastprox_b200 import workloads
+        print(json.dumps(getattr(workloads, args.workload)(args)))
+        return
     if args.impl == "reference":
         run_reference_arm(args)
         return
@@ -216,10 +252,8 @@ def main():
         torch.cuda.synchronize(dev)
     t = ev0.elapsed_time(ev1) / 1e3
     if world > 1:
-        tt = torch.tensor([t], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = reduce_max_time(t, dist, dev)
         dist.barrier()
-        t = float(tt.item())
     value = world * B * args.steps / t
     ms_per_step = t / args.steps * 1e3
     assert info.converged, "benchmark solve did not converge"
@@ -239,9 +273,7 @@ def main():
     torch.cuda.synchronize(dev)
     te = time.perf_counter() - t0
     if world > 1:
-        tt = torch.tensor([te], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
+        te = reduce_max_time(te, dist, dev)
     e2e = world * B * e2e_steps / te
 
     peak, peak_kind = peaks()

@@ -83,4 +83,22 @@ struct IsoCall {
     double w_act;          // its weight
 };
 
+// One image of a ragged batch: its shape, its place in the arena (pixel
+// offset; the dual pairs sit at twice it), its tiles and its stopping limit.
+struct RagSlot {
+    int H, W;
+    int64_t off;
+    int nblk;       // tiles (blocks) of the image
+    int max_iter;
+    int rows;       // rows per tile
+    int vec;        // pixels per thread along a row
+    double wh0, wh1, tau;
+};
+
+// One tile of the work list: the image's slot, the tile's index within the
+// image (its partial-sum slot), its first row and first column.
+struct RagItem {
+    int slot, blk, r0, cs;
+};
+
 }  // namespace fpb

@@ -56,6 +56,11 @@ inline int iso_variant(int64_t k, int max_iter, bool warm) {
 cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, void *out,
                          cudaStream_t s);
 
+// One step of a ragged batch: the three kernel variants over the work list
+// of `vec` (items[0 .. *n_items), grid >= *n_items blocks).
+cudaError_t iso_ragged_step(int dtype, int vec, const RagItem *items, const int *n_items, int grid,
+                            const RagSlot *slots, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s);
+
 // Fills gammas[i] = v for i < n.
 cudaError_t fill_double(double *dst, double v, int64_t n, cudaStream_t s);
 // Gathers a strided array of n_dims dims into a contiguous one (element

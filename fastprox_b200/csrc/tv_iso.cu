@@ -728,6 +728,65 @@ __global__ void __launch_bounds__(128) iso2d_lean_kernel(StepArgs A, IsoCall c, 
 }
 
 // ---------------------------------------------------------------------------
+// The ragged step: images of any size in one arena, a device-resident work
+// list of (image, tile) items, each image at its own iteration with its own
+// buffer parity (its state's fin_par). Three variants (cold start, gap
+// check, plain) are launched per step; an item's block runs only in the
+// variant its image's state asks for.
+// ---------------------------------------------------------------------------
+
+template <class T, int VEC, bool GAP, bool ZIN>
+__global__ void __launch_bounds__(128) iso2d_ragged_kernel(const RagItem *__restrict__ items,
+                                                           const int *__restrict__ n_items,
+                                                           const RagSlot *__restrict__ slots, IsoCall c, IsoBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    if ((int)blockIdx.x >= *n_items) return;
+    const RagItem item = items[blockIdx.x];
+    const int b = item.slot;
+    const RagSlot sl = slots[b];
+    const IsoState st = bf.st[b];
+    if (st.status != kLive) return;
+    const int it = st.it;
+    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == sl.max_iter)) || (it == 0 && st.warm);
+    const bool zin = st.zero_in != 0;
+    if (do_gap != GAP || zin != ZIN) return;
+    const IsoImage im = bf.img[b];
+    const int H = sl.H, W = sl.W;
+    const int64_t N = (int64_t)H * W;
+    const bool do_upd = it < sl.max_iter;
+    const bool test = do_upd && (it & 3) == 0;
+    const int pin = st.fin_par, pout = pin ^ 1;
+    const T *D = static_cast<const T *>(bf.d) + sl.off;
+    const T *U0 = static_cast<const T *>(bf.U[pin]) + 2 * sl.off;
+    const T *V0 = st.vsel ? U0 : static_cast<const T *>(bf.V[pin]) + 2 * sl.off;
+    T *UO0 = static_cast<T *>(bf.U[pout]) + 2 * sl.off;
+    T *VO0 = static_cast<T *>(bf.V[pout]) + 2 * sl.off;
+    const int cb = item.cs + (int)threadIdx.x * VEC;
+    const int r0 = item.r0;
+    const int r1 = min(H, r0 + sl.rows);
+    double gap_acc = 0.0, dot_acc = 0.0;
+    lean_rows<T, VEC, false, GAP, ZIN>(D, U0, U0 + N, V0, V0 + N, UO0, UO0 + N, VO0, VO0 + N, nullptr, H, W, cb, r0, r1,
+                                       (T)sl.wh0, (T)sl.wh1, (T)sl.tau, (T)st.beta, (T)im.radius, (T)im.bound, test,
+                                       do_upd, gap_acc, dot_acc);
+    const double gsum = GAP ? block_sum(gap_acc, sh) : 0.0;
+    const double dsum = test ? block_sum(dot_acc, sh) : 0.0;
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[item.blk * 2 + 0] = gsum;
+        part[item.blk * 2 + 1] = dsum;
+    }
+    if (!arrive_last(bf.ticket + b, sl.nblk, &flag)) return;
+    const double gap = GAP ? sum_partials(part, sl.nblk, 2, 0, sh) : 0.0;
+    const double dot = test ? sum_partials(part, sl.nblk, 2, 1, sh) : 0.0;
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2 = st;
+    control(s2, im, sl.max_iter, GAP, test, gap, dot, pin, bf.live);
+    bf.st[b] = s2;
+}
+
+// ---------------------------------------------------------------------------
 // The 2D step with a TMA row pipeline (sm_100a): one elected thread streams
 // whole row segments of d, v, u (and the pixel weights) from HBM into a ring
 // of shared-memory slots with bulk asynchronous copies (cp.async.bulk,
@@ -1360,7 +1419,29 @@ cudaError_t finalize_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf
     return cudaGetLastError();
 }
 
+template <class T, int VEC>
+void launch_ragged_t(const RagItem *items, const int *n_items, int grid, const RagSlot *slots, const IsoCall &c,
+                     const IsoBuffers &bf, cudaStream_t s) {
+    const int bx = 128;
+    iso2d_ragged_kernel<T, VEC, false, true><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf);
+    iso2d_ragged_kernel<T, VEC, true, false><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf);
+    iso2d_ragged_kernel<T, VEC, false, false><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf);
+}
+
 }  // namespace
+
+cudaError_t iso_ragged_step(int dtype, int vec, const RagItem *items, const int *n_items, int grid,
+                            const RagSlot *slots, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
+    if (grid <= 0) return cudaSuccess;
+    if (dtype == 1) {
+        if (vec == 4) launch_ragged_t<float, 4>(items, n_items, grid, slots, c, bf, s);
+        else launch_ragged_t<float, 1>(items, n_items, grid, slots, c, bf, s);
+    } else {
+        if (vec == 2) launch_ragged_t<double, 2>(items, n_items, grid, slots, c, bf, s);
+        else launch_ragged_t<double, 1>(items, n_items, grid, slots, c, bf, s);
+    }
+    return cudaGetLastError();
+}
 
 int iso_setup_blocks(const Geometry &g) {
     int64_t nb = (g.N + kScanThreads * 8 - 1) / (kScanThreads * 8);

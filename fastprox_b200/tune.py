@@ -1,0 +1,77 @@
+"""The autotuner of the ragged-batch engine: tile height (rows per block) and
+iterations per captured graph chunk, chosen by timing short solves of the
+actual batch and cached per shape class (in-process, and in
+~/.cache/fastprox_b200/tune.json when that directory is writable).
+
+A tuning solve runs 16 iterations (tol 0) of every image with each
+candidate; the choice changes how work is tiled and how often the host
+polls, never the iterations of an image (the same tiling is then used for
+every image of that class, so results stay reproducible).
+"""
+
+from __future__ import annotations
+
+import json
+import math
+import os
+import pathlib
+import time
+
+ROWS = (8, 16, 32)
+STEPS = (4, 8, 16)
+_CACHE: dict = {}
+_PATH = pathlib.Path(os.environ.get("FASTPROX_B200_TUNE", str(pathlib.Path.home() / ".cache" / "fastprox_b200"
+                                                                / "tune.json")))
+
+
+def shape_class(shapes):
+    """The class of a batch: log2 of its median image size and of its count."""
+    import numpy as np
+    px = sorted(int(h) * int(w) for h, w in shapes)
+    med = px[len(px) // 2]
+    return f"m{int(math.log2(max(med, 1)))}_n{int(math.log2(max(len(px), 1)))}"
+
+
+def _load():
+    if not _CACHE and _PATH.exists():
+        try:
+            _CACHE.update(json.loads(_PATH.read_text()))
+        except (OSError, ValueError):
+            pass
+
+
+def _save():
+    try:
+        _PATH.parent.mkdir(parents=True, exist_ok=True)
+        _PATH.write_text(json.dumps(_CACHE, indent=1))
+    except OSError:
+        pass
+
+
+def tune(images, max_pixels, retune=False):
+    """images: [(x (H, W) CUDA tensor, gamma, tol)]. Returns {'rows', 'steps'}."""
+    import torch
+
+    from .batch import RaggedBatch
+    _load()
+    key = shape_class([tuple(x.shape[-2:]) for x, _, _ in images])
+    if key in _CACHE and not retune:
+        return _CACHE[key]
+    best, best_t = None, math.inf
+    for rows in ROWS:
+        for steps in STEPS:
+            b = RaggedBatch(len(images), max_pixels, rows=rows)
+            for x, g, _ in images:
+                b.admit(x, g, 0.0, max_iter=16)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            while b.pending:
+                b.run(steps=steps)
+            torch.cuda.synchronize()
+            t = time.perf_counter() - t0
+            if t < best_t:
+                best, best_t = {"rows": rows, "steps": steps}, t
+            del b
+    _CACHE[key] = best
+    _save()
+    return best

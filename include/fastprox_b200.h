@@ -182,6 +182,41 @@ FP_API int         fp_default_threads(void);
 FP_API fp_status fp_b200_workspace_stats(const fp_workspace *ws, int64_t *kernel_launches,
                                          int64_t *step_launches);
 
+/* Ragged batches and continuous batching (no counterpart in the reference,
+ * whose calls take one array shape each). An fp_b200_batch solves isotropic
+ * 2D TV (an operator from fp_op_tv_iso, unit or axis weights, no pixel
+ * weights) on images of any sizes at once: admitted images share one set of
+ * kernel launches, each image stops on its own gap, and images can be
+ * admitted between calls to fp_b200_batch_run while others iterate.
+ * Results are the same bits whatever else is in the batch.
+ *
+ * create: capacity for max_images images and max_pixels pixels in all, every
+ * byte of device memory allocated here, on the current device; dtype FP_F32
+ * or FP_F64 (the images' dtype). admit: x and z are device pointers to
+ * contiguous (height, width) arrays (z may be x), copied in now, solved by
+ * later runs; tol and max_iter as in fp_prox, per image; FP_ENOMEM when no
+ * slot or not enough contiguous pixels are free (admit again after a run has
+ * finished others). run: repeats `steps` iterations of every live image (as a
+ * captured CUDA graph) until at least one image has finished or none is live;
+ * writes the finished images' z, and their slots, gaps and iterations (a
+ * negative count: stopped at max_iter) into arrays of max_images entries;
+ * *nlive, the images still iterating. All calls on one batch run on its
+ * stream (set_stream; NULL by default) and must not overlap. */
+typedef struct fp_b200_batch fp_b200_batch;
+FP_API fp_status fp_b200_batch_create(const fp_op *op, int64_t max_images, int64_t max_pixels, int dtype,
+                                      fp_b200_batch **out);
+FP_API void      fp_b200_batch_free(fp_b200_batch *bt);
+FP_API fp_status fp_b200_batch_set_stream(fp_b200_batch *bt, void *stream);
+/* Rows per tile of images admitted from now on (0: chosen from the image
+ * height); the tuner sets it. */
+FP_API fp_status fp_b200_batch_set_rows(fp_b200_batch *bt, int rows);
+FP_API fp_status fp_b200_batch_admit(fp_b200_batch *bt, const void *x, int64_t height, int64_t width, double gamma,
+                                     double tol, int max_iter, void *z, int *slot);
+FP_API fp_status fp_b200_batch_run(fp_b200_batch *bt, int steps, int *finished, double *gaps, int *iters,
+                                   int *nfinished, int *nlive);
+FP_API fp_status fp_b200_batch_stats(const fp_b200_batch *bt, int64_t *kernel_launches, int64_t *steps,
+                                     int64_t *free_pixels);
+
 /* Isotropic 2D TV prox of a small float32 batch without allocating any
  * memory. No counterpart in the reference ABI.
  *
