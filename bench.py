@@ -163,13 +163,24 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
-def profile_case():
-    """The benchmark batch (64 x 512^2, pixel weights, three steps) solved for
-    exactly 8 iterations: launch 0 is the cold start, launches 4 and 8 carry
-    gap checks, the rest are plain iterations."""
+def profile_case(kind="iso"):
+    """iso: the benchmark batch (64 x 512^2, pixel weights, three steps)
+    solved for exactly 8 iterations: launch 0 is the cold start, launches 4
+    and 8 carry gap checks, the rest are plain iterations. aniso: 16 of its
+    images, anisotropic with edge weights, solved to gap 1e-6 (every kernel of
+    the method, polish included)."""
     import torch
 
-    from fastprox_b200 import TVIso
+    from fastprox_b200 import TVAniso, TVIso, synth
+    if kind == "aniso":
+        B = 16
+        x = torch.as_tensor(synth.phantom(B, 512, 512, seed=0), device="cuda")
+        beta = synth.pixel_weights((2, 512, 512), seed=1)
+        st = torch.as_tensor([(0.05, 0.1, 0.2)[i % 3] for i in range(B)], device="cuda", dtype=torch.float64)
+        z, info = TVAniso(2, edge_weights=beta).solve(x, st, tol=1e-6, max_iter=2000, with_dual=False)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": "aniso", "iters": int(info.iters)}))
+        return
     x, alpha, steps = make_inputs()
     xt = torch.as_tensor(x, device="cuda")
     st = torch.as_tensor(steps, device="cuda")
@@ -186,14 +197,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--profile-case", action="store_true",
-                    help="one solve of the benchmark batch with 8 iterations (tol 0): the case for ncu captures")
+    ap.add_argument("--profile-case", nargs="?", const="iso", default=None, choices=["iso", "aniso"],
+                    help="iso: one solve of the benchmark batch with 8 iterations (tol 0); aniso: 16 images "
+                         "anisotropic to gap 1e-6; the cases for ncu captures")
     ap.add_argument("--workload", default="iso512", choices=["iso512", "aniso512", "uneven", "vjp", "serve"],
                     help="iso512 (default, the headline line); the others report the other workloads")
     ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-workers", type=int, default=4, help="worker streams for anisotropic and 3D requests")
     args = ap.parse_args()
     if args.profile_case:
-        profile_case()
+        profile_case(args.profile_case)
         return
     if args.workload != "iso512" and args.impl == "ours":
         from fastprox_b200 import workloads

@@ -18,7 +18,7 @@ from .image_tv import TVIso
 
 
 class RaggedBatch:
-    def __init__(self, max_images, max_pixels, dtype="float32", weights=None, rows=0, stream=None):
+    def __init__(self, max_images, max_pixels, dtype="float32", weights=None, rows=0, stream=None, graphs=True):
         import torch
         self.op = TVIso(2, weights)
         self.max_images = int(max_images)
@@ -30,6 +30,8 @@ class RaggedBatch:
         capi.check(capi.lib().fp_b200_batch_set_stream(self._h, C.c_void_p(s)), "batch_stream")
         if rows:
             capi.check(capi.lib().fp_b200_batch_set_rows(self._h, int(rows)), "batch_rows")
+        if not graphs:
+            capi.check(capi.lib().fp_b200_batch_set_graphs(self._h, 0), "batch_graphs")
         self.pending = 0
         self._keep = {}
         self._fin = np.zeros(self.max_images, np.int32)
@@ -60,10 +62,13 @@ class RaggedBatch:
         self.pending += 1
         return slot.value
 
-    def run(self, steps=8):
-        """Iterates until some images finish; returns [(slot, z, gap, iters, converged)]."""
+    def run(self, steps=8, max_chunks=0):
+        """Iterates until some images finish (or, with max_chunks > 0, at most
+        that many chunks of `steps` iterations); returns
+        [(slot, z, gap, iters, converged)]."""
         nf, nl = C.c_int(0), C.c_int(0)
-        capi.check(capi.lib().fp_b200_batch_run(self._h, int(steps), self._fin.ctypes.data_as(C.POINTER(C.c_int)),
+        capi.check(capi.lib().fp_b200_batch_run(self._h, int(steps), int(max_chunks),
+                                                self._fin.ctypes.data_as(C.POINTER(C.c_int)),
                                                 self._gaps.ctypes.data_as(C.POINTER(C.c_double)),
                                                 self._its.ctypes.data_as(C.POINTER(C.c_int)), C.byref(nf),
                                                 C.byref(nl)), "batch_run")

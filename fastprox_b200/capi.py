@@ -83,13 +83,15 @@ SIGNATURES = {
     "fp_version_string": (C.c_char_p, []),
     "fp_default_threads": (C.c_int, []),
     "fp_b200_workspace_stats": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "fp_b200_release_cached": (None, []),
     "fp_b200_batch_create": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int, C.POINTER(_P)]),
     "fp_b200_batch_free": (None, [_P]),
     "fp_b200_batch_set_stream": (C.c_int, [_P, _P]),
     "fp_b200_batch_set_rows": (C.c_int, [_P, C.c_int]),
+    "fp_b200_batch_set_graphs": (C.c_int, [_P, C.c_int]),
     "fp_b200_batch_admit": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int, _P,
                                       C.POINTER(C.c_int)]),
-    "fp_b200_batch_run": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int),
+    "fp_b200_batch_run": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int),
                                     C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "fp_b200_batch_stats": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "fp_b200_tv_iso_noalloc": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int,

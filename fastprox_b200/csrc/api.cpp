@@ -18,6 +18,7 @@
 #include "../../include/fastprox_b200.h"
 #include "engine.h"
 #include "launch.h"
+#include "pool.h"
 #include "workspace.h"
 
 using namespace fpb;
@@ -403,36 +404,29 @@ namespace {
 
 void free_ws_memory(fp_workspace *ws) {
     DeviceScope ds(ws->device);
-    for (void *p : ws->dev_allocs) cudaFree(p);
-    ws->dev_allocs.clear();
-    for (void *p : ws->host_allocs) cudaFreeHost(p);
-    ws->host_allocs.clear();
+    pool_free(ws->device, ws->dev_block);
+    ws->dev_block = nullptr;
+    pinned_give(ws->host_block, ws->host_bytes);
+    ws->host_block = nullptr;
     for (int i = 0; i < 2; ++i)
         if (ws->ev[i]) cudaEventDestroy(ws->ev[i]);
     ws->ev[0] = ws->ev[1] = nullptr;
 }
 
-fp_status dev_alloc(fp_workspace *ws, void **p, size_t bytes) {
-    *p = nullptr;
-    if (bytes == 0) bytes = 16;
-    if (cudaMalloc(p, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        return FP_ENOMEM;
+// The buffers of a workspace, laid out in one block (256-byte aligned
+// pieces) before the block exists; place() points them into it.
+struct Layout {
+    std::vector<std::pair<void **, size_t>> parts;
+    size_t total = 0;
+    void add(void **p, size_t bytes) {
+        *p = nullptr;
+        parts.emplace_back(p, total);
+        total += (std::max<size_t>(bytes, 16) + 255) / 256 * 256;
     }
-    ws->dev_allocs.push_back(*p);
-    return FP_OK;
-}
-
-fp_status host_alloc(fp_workspace *ws, void **p, size_t bytes) {
-    *p = nullptr;
-    if (bytes == 0) bytes = 16;
-    if (cudaHostAlloc(p, bytes, cudaHostAllocDefault) != cudaSuccess) {
-        cudaGetLastError();
-        return FP_ENOMEM;
+    void place(void *base) const {
+        for (const auto &pr : parts) *pr.first = static_cast<char *>(base) + pr.second;
     }
-    ws->host_allocs.push_back(*p);
-    return FP_OK;
-}
+};
 
 // The image plan of x: leading axes are the batch, the last k the image.
 fp_status image_geometry(const fp_op &op, const Arr &x, Geometry &g) {
@@ -487,9 +481,8 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     const size_t img = (size_t)B * (size_t)N * T;
     const size_t dualb = img * (size_t)g.k;
     fp_status s = FP_OK;
-    auto A = [&](void **p, size_t bytes) {
-        if (s == FP_OK) s = dev_alloc(ws.get(), p, bytes);
-    };
+    Layout dev, host;
+    auto A = [&](void **p, size_t bytes) { dev.add(p, bytes); };
     A(&ws->d, img);
     A(&ws->stage, img);  // strided or conjugate inputs, strided outputs
     for (int i = 0; i < 2; ++i) {
@@ -497,15 +490,13 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
         A(&ws->V[i], dualb);
     }
     A(&ws->dual, dualb);
+    std::vector<char> spatial_h;
     if (!op->spatial.empty()) {
         A(&ws->spatial, op->spatial.size() * T);
-        if (s == FP_OK) {
-            std::vector<char> tmp(op->spatial.size() * T);
-            for (size_t i = 0; i < op->spatial.size(); ++i) {
-                if (T == 4) reinterpret_cast<float *>(tmp.data())[i] = (float)op->spatial[i];
-                else reinterpret_cast<double *>(tmp.data())[i] = op->spatial[i];
-            }
-            if (cudaMemcpy(ws->spatial, tmp.data(), tmp.size(), cudaMemcpyHostToDevice) != cudaSuccess) s = FP_EDEVICE;
+        spatial_h.resize(op->spatial.size() * T);
+        for (size_t i = 0; i < op->spatial.size(); ++i) {
+            if (T == 4) reinterpret_cast<float *>(spatial_h.data())[i] = (float)op->spatial[i];
+            else reinterpret_cast<double *>(spatial_h.data())[i] = op->spatial[i];
         }
     }
     // per-image state, partials and tickets; launch shape (tuning hints from
@@ -547,6 +538,7 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
         A((void **)&ws->v_img, (size_t)B * sizeof(VjpImage));
         A((void **)&ws->v_cg, (size_t)B * sizeof(CgState));
         A((void **)&ws->v_ggam, (size_t)B * sizeof(double));
+        A((void **)&ws->v_gw, (size_t)B * 3 * sizeof(double));
     }
     A((void **)&ws->img, (size_t)B * sizeof(IsoImage));
     A((void **)&ws->st, (size_t)B * sizeof(IsoState));
@@ -555,9 +547,7 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     A((void **)&ws->ticket, (size_t)B * sizeof(unsigned));
     A((void **)&ws->live, 16);
     A((void **)&ws->err, 16);
-    auto H = [&](void **p, size_t bytes) {
-        if (s == FP_OK) s = host_alloc(ws.get(), p, bytes);
-    };
+    auto H = [&](void **p, size_t bytes) { host.add(p, bytes); };
     H((void **)&ws->h_live, 4 * sizeof(int));
     H((void **)&ws->h_img, (size_t)B * sizeof(IsoImage));
     H((void **)&ws->h_st, (size_t)B * sizeof(IsoState));
@@ -566,17 +556,35 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
         H((void **)&ws->h_vimg, (size_t)B * sizeof(VjpImage));
         H((void **)&ws->h_cg, (size_t)B * sizeof(CgState));
         H((void **)&ws->h_ggam, (size_t)B * sizeof(double));
+        H((void **)&ws->h_gw, (size_t)B * 3 * sizeof(double));
     }
     if (op->kind == kAniso) {
         H((void **)&ws->h_an_img, (size_t)B * sizeof(AnImage));
         H((void **)&ws->h_an_st, (size_t)B * sizeof(AnState));
     }
     if (ws->host_mode) H(&ws->h_stage, img);
-    if (s == FP_OK && cudaMemset(ws->ticket, 0, (size_t)B * sizeof(unsigned)) != cudaSuccess) s = FP_EDEVICE;
-    if (s == FP_OK && cudaMemset(ws->err, 0, 16) != cudaSuccess) s = FP_EDEVICE;
+    // one pinned block and one device block from the pools (no device-wide
+    // synchronisation); tickets and the error flag start at zero
+    ws->host_bytes = host.total;
+    ws->host_block = pinned_take(host.total);
+    if (!ws->host_block) s = FP_ENOMEM;
+    if (s == FP_OK) {
+        host.place(ws->host_block);
+        std::memset(ws->host_block, 0, host.total);
+        void *base = nullptr;
+        const cudaError_t e = pool_alloc(device, dev.total, &base, [&](cudaStream_t ps) {
+            dev.place(base);
+            cudaError_t r = cudaMemsetAsync(ws->ticket, 0, (size_t)B * sizeof(unsigned), ps);
+            if (r == cudaSuccess) r = cudaMemsetAsync(ws->err, 0, 16, ps);
+            if (r == cudaSuccess && !spatial_h.empty())
+                r = cudaMemcpyAsync(ws->spatial, spatial_h.data(), spatial_h.size(), cudaMemcpyHostToDevice, ps);
+            return r;
+        });
+        ws->dev_block = base;
+        if (e != cudaSuccess) s = e == cudaErrorMemoryAllocation ? FP_ENOMEM : FP_EDEVICE;
+    }
     for (int i = 0; i < 2 && s == FP_OK; ++i)
         if (cudaEventCreateWithFlags(&ws->ev[i], cudaEventDisableTiming) != cudaSuccess) s = FP_EDEVICE;
-    if (s == FP_OK && cudaDeviceSynchronize() != cudaSuccess) s = FP_EDEVICE;
     if (s != FP_OK) {
         cudaGetLastError();
         free_ws_memory(ws.get());
@@ -749,7 +757,9 @@ fp_status dual_io(fp_workspace *ws, const fp_array *arr, bool set) {
                 }
             }
             if (bad) return FP_EINVAL;
-            if (cudaMemcpy(ws->dual, h.data(), h.size(), cudaMemcpyHostToDevice) != cudaSuccess) return FP_EDEVICE;
+            if (cudaMemcpyAsync(ws->dual, h.data(), h.size(), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return FP_EDEVICE;
             ws->seeded = true;
             ws->dual_valid = true;
             return FP_OK;
@@ -778,14 +788,16 @@ fp_status dual_io(fp_workspace *ws, const fp_array *arr, bool set) {
             }
         }
         if (bad) return FP_EINVAL;
-        if (cudaStreamSynchronize(st) != cudaSuccess) return FP_EDEVICE;
-        if (cudaMemcpy(ws->dual, h.data(), h.size(), cudaMemcpyHostToDevice) != cudaSuccess) return FP_EDEVICE;
+        if (cudaMemcpyAsync(ws->dual, h.data(), h.size(), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return FP_EDEVICE;
         ws->seeded = true;
         ws->dual_valid = true;
         return FP_OK;
     }
-    if (cudaStreamSynchronize(st) != cudaSuccess) return FP_EDEVICE;
-    if (cudaMemcpy(h.data(), ws->dual, h.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return FP_EDEVICE;
+    if (cudaMemcpyAsync(h.data(), ws->dual, h.size(), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return FP_EDEVICE;
     std::vector<int64_t> idx((size_t)a.ndim, 0);
     for (int64_t i = 0; i < n; ++i) {
         int64_t off = 0;
@@ -1012,6 +1024,8 @@ fp_status run_aniso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *z
     return cuda_status(e);
 }
 
+fp_status copy_or_fill(fp_workspace *ws, const Arr *src, const Arr &dst, double fill, void *scratch);
+
 fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *oa, const fp_options *opt,
                     fp_workspace *ws, fp_info *info, bool conj, const fp_array *sa) {
     if (!op || !xa || !oa) return FP_EINVAL;
@@ -1089,6 +1103,7 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
         ws->valid = false;
         ws->info_valid = false;
         ws->struct_valid = false;
+        ws->identity = false;
         ws->conj = conj;
     }
     if (x.numel() == 0) {
@@ -1123,6 +1138,23 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
     DeviceScope dsc(ws->device);
     if (x.device == FP_DEVICE_CUDA) {
         if (pointer_device(x.data) != ws->device || pointer_device(out.data) != ws->device) return FP_EINVAL;
+    }
+    if (identity) {
+        // sigma = 0 in the conjugate: y itself, and with keep the identity's
+        // derivatives (api.cpp:529-534)
+        if (fp_status st = copy_or_fill(ws, &x, out, 0.0, nullptr)) return st;
+        std::fill(ws->gaps.begin(), ws->gaps.end(), 0.0);
+        std::fill(ws->zerrs.begin(), ws->zerrs.end(), 0.0);
+        std::fill(ws->iters.begin(), ws->iters.end(), 0);
+        ws->seeded = false;
+        if (keep) {
+            ws->valid = true;
+            ws->identity = true;
+        }
+        ws->info = fp_info{0.0, 0, 0};
+        ws->info_status = FP_OK;
+        ws->info_valid = true;
+        return FP_OK;
     }
     if (device_steps) {
         // the steps into the workspace (as doubles), read back and checked
@@ -1265,10 +1297,14 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e);
     {
-        int herr = 0;
-        if (cudaMemcpy(&herr, ws->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return FP_EDEVICE;
-        if (herr) {
-            cudaMemset(ws->err, 0, sizeof(int));
+        // the device error flag (an internal consistency check), read on the stream
+        e = cudaMemcpyAsync(ws->h_live + 3, ws->err, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e);
+        if (ws->h_live[3]) {
+            ws->h_live[3] = 0;
+            cudaMemsetAsync(ws->err, 0, sizeof(int), s);
+            cudaStreamSynchronize(s);
             return FP_EDEVICE;
         }
     }
@@ -1335,40 +1371,77 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
 
 namespace {
 
-// The derivative at the kept point (the reference's vjp_impl,
-// src/api/api.cpp:693-738, and image_vjp_driver, src/core/driver.hpp:1505-1560):
-// gx = J^T g and the step's gradient summed over the batch. Isotropic TV.
-fp_status vjp_impl(const fp_op *op, fp_workspace *ws, const fp_array *ga, fp_array *gxa, double *ggamma,
-                   fp_array *ggdev, fp_array *gpa) {
-    if (!op || !ws || !ga || !gxa) return FP_EINVAL;
-    if (ws->op != op || !ws->valid) return FP_EINVAL;
-    if (op->kind != kIso) return FP_EINVAL;  // anisotropic derivatives: not on the device yet
-    if (gpa) return FP_EINVAL;               // parameter gradients: not on the device yet
-    Arr g, gx;
-    if (fp_status s = to_arr(ga, g)) return s;
-    if (fp_status s = to_arr(gxa, gx)) return s;
-    if (g.dtype != ws->dtype || gx.dtype != ws->dtype) return FP_EDTYPE;
-    if (g.ndim != ws->ndim || gx.ndim != ws->ndim) return FP_ESHAPE;
-    for (int d = 0; d < ws->ndim; ++d)
-        if (g.shape[d] != ws->shape[d] || gx.shape[d] != ws->shape[d]) return FP_ESHAPE;
-    if (fp_status s = check_output(&g, gx)) return s;
-    if (g.device != gx.device || ws->host_mode != (g.device == FP_DEVICE_CPU)) return FP_EINVAL;
-    Arr gg;
-    if (ggdev) {
-        if (fp_status s = to_arr(ggdev, gg)) return s;
-        if (gg.device != FP_DEVICE_CUDA || gg.numel() != 1) return FP_EINVAL;
+// Elementwise copy between two host arrays of one dtype and shape (any
+// strides; dst may be src exactly), or a fill of dst when src is null.
+void host_copy(const Arr *src, const Arr &dst, double fill) {
+    const int64_t n = dst.numel();
+    const size_t T = dst.itemsize();
+    std::vector<int64_t> idx((size_t)dst.ndim, 0);
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t od = 0, os = 0;
+        for (int d = 0; d < dst.ndim; ++d) {
+            od += idx[(size_t)d] * dst.strides[d];
+            if (src) os += idx[(size_t)d] * src->strides[d];
+        }
+        char *q = dst.data + od * (int64_t)T;
+        if (src) std::memmove(q, src->data + os * (int64_t)T, T);
+        else if (dst.dtype == FP_F32) *reinterpret_cast<float *>(q) = (float)fill;
+        else *reinterpret_cast<double *>(q) = fill;
+        for (int d = dst.ndim - 1; d >= 0; --d) {
+            if (++idx[(size_t)d] < dst.shape[d]) break;
+            idx[(size_t)d] = 0;
+        }
     }
-    const Geometry &g0 = ws->g;
-    if (g0.B * g0.N == 0) {
-        if (ggamma) *ggamma = 0.0;
+}
+
+// dst = src (or the fill) for arrays on the workspace's side: host loops, or
+// device copies through `scratch` (dst's size) on the stream.
+fp_status copy_or_fill(fp_workspace *ws, const Arr *src, const Arr &dst, double fill, void *scratch) {
+    if (dst.numel() == 0) return FP_OK;
+    if (ws->host_mode) {
+        host_copy(src, dst, fill);
         return FP_OK;
     }
-    DeviceScope dsc(ws->device);
     cudaStream_t s = ws->stream;
-    const size_t T = ws->dtype == FP_F32 ? 4 : 8;
+    cudaError_t e = cudaSuccess;
+    if (src) {
+        e = strided_copy(src->data, src->dtype, src->shape, src->strides, dst.ndim, dst.data, dst.dtype, dst.strides, s);
+    } else {
+        const int64_t n = dst.numel();
+        const size_t T = dst.itemsize();
+        std::vector<char> h((size_t)n * T);
+        for (int64_t i = 0; i < n; ++i) {
+            if (T == 4) reinterpret_cast<float *>(h.data())[i] = (float)fill;
+            else reinterpret_cast<double *>(h.data())[i] = fill;
+        }
+        int64_t cst[FP_MAX_NDIM];
+        int64_t sz = 1;
+        for (int d = dst.ndim - 1; d >= 0; --d) {
+            cst[d] = sz;
+            sz *= dst.shape[d];
+        }
+        e = cudaMemcpyAsync(scratch, h.data(), h.size(), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = strided_copy(scratch, dst.dtype, dst.shape, cst, dst.ndim, dst.data, dst.dtype, dst.strides, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return cuda_status(e);
+}
+
+// A parameter vector of m entries (ndim <= 1) on the host or the device.
+fp_status param_array(const fp_array *a, int64_t m, Arr &t) {
+    if (fp_status s = to_arr(a, t)) return s;
+    if (a->ndim > 1 || t.shape[0] != m) return FP_ESHAPE;
+    return FP_OK;
+}
+
+// The kept point's geometry and device buffers for the derivatives, and its
+// structure, built once per kept call (the reference's TVIso::save,
+// src/ops/tv_iso.cpp:551-631, done lazily).
+fp_status deriv_prepare(const fp_op *op, fp_workspace *ws, VjpGeom &vg, VjpBuffers &bf) {
+    const Geometry &g0 = ws->g;
+    cudaStream_t s = ws->stream;
     const int64_t total = g0.B * g0.N;
-    // geometry and the forward's weights
-    VjpGeom vg{};
+    vg = VjpGeom{};
     vg.k = g0.k;
     for (int a = 0; a < 3; ++a) vg.L[a] = g0.L[a];
     vg.S[g0.k - 1] = 1;
@@ -1380,18 +1453,25 @@ fp_status vjp_impl(const fp_op *op, fp_workspace *ws, const fp_array *ga, fp_arr
     for (int a = 0; a < g0.k; ++a)
         if (g0.L[a] > 1) wmax_all = std::max(wmax_all, op->w[a]);
     double wmax = 0.0;
+    int nact = 0;
+    vg.act1 = -1;
     for (int a = 0; a < 3; ++a) {
         const bool act = a < g0.k && op->w[a] > 0.0 && g0.L[a] > 1 && op->w[a] >= 1e-100 * wmax_all;
         vg.wa[a] = act ? op->w[a] : 0.0;
         wmax = std::max(wmax, vg.wa[a]);
+        if (act) {
+            ++nact;
+            vg.act1 = a;
+        }
     }
+    if (nact != 1) vg.act1 = -1;
     vg.wmax = wmax > 0.0 ? wmax : 1.0;
     for (int a = 0; a < 3; ++a) vg.wh[a] = vg.wa[a] / vg.wmax;
     const double eps = ws->dtype == FP_F32 ? (double)std::numeric_limits<float>::epsilon() : 2.2e-16;
     // the flat margin below the radius: the reference's 1e-9, or 64 eps where
     // the iterates are float32 (its device path's dual_eta)
     vg.eta = ws->dtype == FP_F32 ? 64.0 * eps : 1e-9;
-    VjpBuffers bf;
+    bf = VjpBuffers{};
     bf.d = ws->d;
     bf.U[0] = ws->U[0];
     bf.U[1] = ws->U[1];
@@ -1417,119 +1497,323 @@ fp_status vjp_impl(const fp_op *op, fp_workspace *ws, const fp_array *ga, fp_arr
     bf.vimg = ws->v_img;
     bf.cg = ws->v_cg;
     bf.ggam = ws->v_ggam;
+    bf.gw = ws->v_gw;
     bf.part = ws->part;
     bf.ticket = ws->ticket;
     bf.live = ws->live;
     bf.err = ws->err;
     bf.max_part = ws->max_part;
     if (!bf.flat) return FP_EINVAL;
+    if (ws->struct_valid) return FP_OK;
+    // per image, from the forward (tv_iso.cpp:559-570), at the solved scale
+    for (int64_t b = 0; b < g0.B; ++b) {
+        const IsoImage &im = ws->h_img[b];
+        const IsoState &st = ws->h_st[b];
+        VjpImage &vi = ws->h_vimg[b];
+        const bool from_dual = im.mode == kModeFdpg;
+        const double gap_s = im.mode == kModeFdpg ? std::max(st.gp, 0.0) : 0.0;
+        vi.gs = std::ldexp(im.gamma_in, -im.e);
+        vi.rel = im.dd > 0.0 ? std::sqrt(2.0 * gap_s / im.dd) : 0.0;
+        vi.mu = from_dual ? 0.1 * vg.wmax * std::sqrt(2.0 * gap_s / (double)g0.N) : 0.0;
+        vi.thr = from_dual ? vg.wmax * 64.0 * eps * std::ldexp(im.maxabs, -im.e) : 0.0;
+    }
+    cudaError_t e = cudaMemcpyAsync(ws->v_img, ws->h_vimg, (size_t)g0.B * sizeof(VjpImage), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = vjp_structure(ws->dtype, vg, bf, s);
+    if (e != cudaSuccess) return cuda_status(e);
+    ws->struct_valid = true;
+    return FP_OK;
+}
+
+// An input image batch (cotangent or tangent) as a contiguous device array:
+// itself, or a copy in `stage`.
+fp_status stage_input(fp_workspace *ws, const Arr &a, void *stage, const void **dev) {
+    cudaStream_t s = ws->stream;
+    const int64_t total = a.numel();
+    const size_t T = a.itemsize();
     cudaError_t e = cudaSuccess;
-    if (!ws->struct_valid) {
-        // per image, from the forward (tv_iso.cpp:559-570), at the solved scale
-        for (int64_t b = 0; b < g0.B; ++b) {
-            const IsoImage &im = ws->h_img[b];
-            const IsoState &st = ws->h_st[b];
-            VjpImage &vi = ws->h_vimg[b];
-            const bool from_dual = im.mode == kModeFdpg;
-            const double gap_s = im.mode == kModeFdpg ? std::max(st.gp, 0.0) : 0.0;
-            vi.gs = std::ldexp(im.gamma_in, -im.e);
-            vi.rel = im.dd > 0.0 ? std::sqrt(2.0 * gap_s / im.dd) : 0.0;
-            vi.mu = from_dual ? 0.1 * vg.wmax * std::sqrt(2.0 * gap_s / (double)g0.N) : 0.0;
-            vi.thr = from_dual ? vg.wmax * 64.0 * eps * std::ldexp(im.maxabs, -im.e) : 0.0;
-        }
-        e = cudaMemcpyAsync(ws->v_img, ws->h_vimg, (size_t)g0.B * sizeof(VjpImage), cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = vjp_structure(ws->dtype, vg, bf, s);
-        if (e != cudaSuccess) return cuda_status(e);
-        ws->struct_valid = true;
-    }
-    // the cotangent and the output, contiguous on the device (V buffers are
-    // free after the solve)
-    const void *gsrc = nullptr;
-    int64_t cst[FP_MAX_NDIM];
-    {
-        int64_t sz = 1;
-        for (int d = g.ndim - 1; d >= 0; --d) {
-            cst[d] = sz;
-            sz *= g.shape[d];
-        }
-    }
     if (ws->host_mode) {
         std::vector<char> tmp((size_t)total * T);
-        std::vector<int64_t> idx((size_t)g.ndim, 0);
-        for (int64_t i = 0; i < total; ++i) {
-            int64_t off = 0;
-            for (int d = 0; d < g.ndim; ++d) off += idx[(size_t)d] * g.strides[d];
-            std::memcpy(tmp.data() + i * (int64_t)T, g.data + off * (int64_t)T, T);
-            for (int d = g.ndim - 1; d >= 0; --d) {
-                if (++idx[(size_t)d] < g.shape[d]) break;
-                idx[(size_t)d] = 0;
-            }
+        Arr c = a;
+        int64_t cst[FP_MAX_NDIM];
+        int64_t sz = 1;
+        for (int d = a.ndim - 1; d >= 0; --d) {
+            cst[d] = sz;
+            sz *= a.shape[d];
         }
-        e = cudaMemcpyAsync(ws->V[0], tmp.data(), tmp.size(), cudaMemcpyHostToDevice, s);
+        c.data = tmp.data();
+        for (int d = 0; d < a.ndim; ++d) c.strides[d] = cst[d];
+        host_copy(&a, c, 0.0);
+        e = cudaMemcpyAsync(stage, tmp.data(), tmp.size(), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        gsrc = ws->V[0];
-    } else if (g.contiguous()) {
-        if (pointer_device(g.data) != ws->device) return FP_EINVAL;
-        gsrc = g.data;
+        *dev = stage;
+    } else if (a.contiguous()) {
+        if (pointer_device(a.data) != ws->device) return FP_EINVAL;
+        *dev = a.data;
     } else {
-        e = strided_copy(g.data, g.dtype, g.shape, g.strides, g.ndim, ws->V[0], g.dtype, cst, s);
-        gsrc = ws->V[0];
-    }
-    if (e != cudaSuccess) return cuda_status(e);
-    const bool direct = !ws->host_mode && gx.contiguous();
-    void *gdst = direct ? gx.data : ws->V[1];
-    if (direct && pointer_device(gx.data) != ws->device) return FP_EINVAL;
-    int64_t nl = 0;
-    e = vjp_solve(ws->dtype, vg, bf, gsrc, gdst, ws->deriv_tol, ws->deriv_max_iter, ws->conj ? 1 : 0, s, ws->h_live,
-                  ws->ev[0], &nl);
-    if (e != cudaSuccess) return cuda_status(e);
-    if (!direct) {
-        if (ws->host_mode) {
-            std::vector<char> tmp((size_t)total * T);
-            e = cudaMemcpyAsync(tmp.data(), gdst, tmp.size(), cudaMemcpyDeviceToHost, s);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-            if (e != cudaSuccess) return cuda_status(e);
-            std::vector<int64_t> idx((size_t)gx.ndim, 0);
-            for (int64_t i = 0; i < total; ++i) {
-                int64_t off = 0;
-                for (int d = 0; d < gx.ndim; ++d) off += idx[(size_t)d] * gx.strides[d];
-                std::memcpy(gx.data + off * (int64_t)T, tmp.data() + i * (int64_t)T, T);
-                for (int d = gx.ndim - 1; d >= 0; --d) {
-                    if (++idx[(size_t)d] < gx.shape[d]) break;
-                    idx[(size_t)d] = 0;
-                }
-            }
-        } else {
-            e = strided_copy(gdst, gx.dtype, gx.shape, cst, gx.ndim, gx.data, gx.dtype, gx.strides, s);
-            if (e != cudaSuccess) return cuda_status(e);
+        if (pointer_device(a.data) != ws->device) return FP_EINVAL;
+        int64_t cst[FP_MAX_NDIM];
+        int64_t sz = 1;
+        for (int d = a.ndim - 1; d >= 0; --d) {
+            cst[d] = sz;
+            sz *= a.shape[d];
         }
+        e = strided_copy(a.data, a.dtype, a.shape, a.strides, a.ndim, stage, a.dtype, cst, s);
+        *dev = stage;
     }
-    e = cudaMemcpyAsync(ws->h_ggam, ws->v_ggam, (size_t)g0.B * sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(ws->h_cg, ws->v_cg, (size_t)g0.B * sizeof(CgState), cudaMemcpyDeviceToHost, s);
+    return cuda_status(e);
+}
+
+// The result image batch from the contiguous device buffer `res` into out
+// (nothing to do when res is out itself).
+fp_status unstage_output(fp_workspace *ws, const void *res, const Arr &out) {
+    if (res == out.data) return FP_OK;
+    cudaStream_t s = ws->stream;
+    const int64_t total = out.numel();
+    const size_t T = out.itemsize();
+    int64_t cst[FP_MAX_NDIM];
+    int64_t sz = 1;
+    for (int d = out.ndim - 1; d >= 0; --d) {
+        cst[d] = sz;
+        sz *= out.shape[d];
+    }
+    cudaError_t e;
+    if (ws->host_mode) {
+        std::vector<char> tmp((size_t)total * T);
+        e = cudaMemcpyAsync(tmp.data(), res, tmp.size(), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e);
+        Arr c = out;
+        c.data = tmp.data();
+        for (int d = 0; d < out.ndim; ++d) c.strides[d] = cst[d];
+        host_copy(&c, out, 0.0);
+        return FP_OK;
+    }
+    e = strided_copy(res, out.dtype, out.shape, cst, out.ndim, out.data, out.dtype, out.strides, s);
+    return cuda_status(e);
+}
+
+// The derivative's residual and iterations over the images.
+fp_status read_cg(fp_workspace *ws, int64_t nl) {
+    cudaStream_t s = ws->stream;
+    const int64_t B = ws->g.B;
+    cudaError_t e = cudaMemcpyAsync(ws->h_cg, ws->v_cg, (size_t)B * sizeof(CgState), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e);
-    double tot = 0.0, res = 0.0;
+    double res = 0.0;
     int its = 0;
-    for (int64_t b = 0; b < g0.B; ++b) {
-        tot += ws->h_ggam[b];
+    for (int64_t b = 0; b < B; ++b) {
         res = std::max(res, ws->h_cg[b].res);
         its = std::max(its, ws->h_cg[b].it);
     }
     ws->deriv_residual = res;
     ws->deriv_iters = its;
     ws->kernel_launches = nl;
-    if (ggamma) *ggamma = tot;
-    if (ggdev) {
-        if (gg.dtype == FP_F32) {
-            const float v = (float)tot;
-            e = cudaMemcpy(gg.data, &v, sizeof v, cudaMemcpyHostToDevice);
-        } else {
-            e = cudaMemcpy(gg.data, &tot, sizeof tot, cudaMemcpyHostToDevice);
-        }
-        if (e != cudaSuccess) return cuda_status(e);
-    }
     return FP_OK;
+}
+
+// The derivative at the kept point (the reference's vjp_impl,
+// src/api/api.cpp:693-738, and image_vjp_driver, src/core/driver.hpp:1505-1560):
+// gx = J^T g, the step's gradient and the parameters' (axis weights, then
+// pixel weights), each summed over the batch. Isotropic TV.
+fp_status vjp_impl(const fp_op *op, fp_workspace *ws, const fp_array *ga, fp_array *gxa, double *ggamma,
+                   fp_array *ggdev, fp_array *gpa) {
+    if (!op || !ws || !ga || !gxa) return FP_EINVAL;
+    if (ws->op != op || !ws->valid) return FP_EINVAL;
+    if (op->kind != kIso) return FP_EINVAL;  // anisotropic derivatives: not on the device yet
+    Arr g, gx;
+    if (fp_status s = to_arr(ga, g)) return s;
+    if (fp_status s = to_arr(gxa, gx)) return s;
+    if (g.dtype != ws->dtype || gx.dtype != ws->dtype) return FP_EDTYPE;
+    if (g.ndim != ws->ndim || gx.ndim != ws->ndim) return FP_ESHAPE;
+    for (int d = 0; d < ws->ndim; ++d)
+        if (g.shape[d] != ws->shape[d] || gx.shape[d] != ws->shape[d]) return FP_ESHAPE;
+    if (fp_status s = check_output(&g, gx)) return s;
+    if (g.device != gx.device || ws->host_mode != (g.device == FP_DEVICE_CPU)) return FP_EINVAL;
+    const int64_t P = fp_op_nparams(op);
+    Arr gp;
+    if (gpa)  // validated before any work
+        if (fp_status s = param_array(gpa, P, gp)) return s;
+    Arr gg;
+    if (ggdev) {
+        if (fp_status s = to_arr(ggdev, gg)) return s;
+        if (gg.device != FP_DEVICE_CUDA || gg.numel() != 1) return FP_EINVAL;
+    }
+    const Geometry &g0 = ws->g;
+    DeviceScope dsc(ws->device);
+    cudaStream_t s = ws->stream;
+    std::vector<double> tot((size_t)P, 0.0);
+    double gsum = 0.0;
+    auto finish = [&]() -> fp_status {
+        // the step's and the parameters' gradients to the caller
+        if (ggamma) *ggamma = gsum;
+        cudaError_t e = cudaSuccess;
+        if (ggdev) {
+            if (gg.dtype == FP_F32) {
+                const float v = (float)gsum;
+                e = cudaMemcpyAsync(gg.data, &v, sizeof v, cudaMemcpyHostToDevice, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            } else {
+                e = cudaMemcpyAsync(gg.data, &gsum, sizeof gsum, cudaMemcpyHostToDevice, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            }
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+        if (!gpa || P == 0) return FP_OK;
+        if (gp.device == FP_DEVICE_CPU) {
+            for (int64_t i = 0; i < P; ++i) {
+                char *q = gp.data + i * gp.strides[0] * (int64_t)gp.itemsize();
+                if (gp.dtype == FP_F32) *reinterpret_cast<float *>(q) = (float)tot[(size_t)i];
+                else *reinterpret_cast<double *>(q) = tot[(size_t)i];
+            }
+            return FP_OK;
+        }
+        if (pointer_device(gp.data) != ws->device) return FP_EINVAL;
+        // through the derivative scratch (7 B N >= k + N doubles)
+        double *scr = ws->v_vec;
+        if (!scr) return FP_EINVAL;
+        const int64_t one = 1, shp = P;
+        e = cudaMemcpyAsync(scr, tot.data(), (size_t)P * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = strided_copy(scr, FP_F64, &shp, &one, 1, gp.data, gp.dtype, gp.strides, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        return cuda_status(e);
+    };
+    if (ws->identity) {  // gx = g; no parameter gradient; the sigma-derivative NaN (api.cpp:711-716)
+        if (fp_status st = copy_or_fill(ws, &g, gx, 0.0, nullptr)) return st;
+        gsum = std::numeric_limits<double>::quiet_NaN();
+        return finish();
+    }
+    if (g0.B * g0.N == 0) return finish();
+    VjpGeom vg;
+    VjpBuffers bf;
+    if (fp_status st = deriv_prepare(op, ws, vg, bf)) return st;
+    // the cotangent and the output, contiguous on the device (the V buffers
+    // are free after the solve)
+    const void *gsrc = nullptr;
+    if (fp_status st = stage_input(ws, g, ws->V[0], &gsrc)) return st;
+    const bool direct = !ws->host_mode && gx.contiguous();
+    void *gdst = direct ? gx.data : ws->V[1];
+    if (direct && pointer_device(gx.data) != ws->device) return FP_EINVAL;
+    const bool params = gpa && P > 0;
+    int64_t nl = 0;
+    cudaError_t e = vjp_solve(ws->dtype, vg, bf, gsrc, gdst, ws->deriv_tol, ws->deriv_max_iter, ws->conj ? 1 : 0,
+                              params, s, ws->h_live, ws->ev[0], &nl);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (fp_status st = unstage_output(ws, gdst, gx)) return st;
+    e = cudaMemcpyAsync(ws->h_ggam, ws->v_ggam, (size_t)g0.B * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && params)
+        e = cudaMemcpyAsync(ws->h_gw, ws->v_gw, (size_t)g0.B * 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    std::vector<double> ga_host;
+    const int64_t na = P - op->k;  // pixel weights
+    if (e == cudaSuccess && params && na > 0) {
+        ga_host.resize((size_t)na);
+        e = cudaMemcpyAsync(ga_host.data(), bf.qv, (size_t)na * sizeof(double), cudaMemcpyDeviceToHost, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e);
+    for (int64_t b = 0; b < g0.B; ++b) gsum += ws->h_ggam[b];
+    if (params) {
+        for (int a = 0; a < op->k; ++a)
+            for (int64_t b = 0; b < g0.B; ++b) tot[(size_t)a] += ws->h_gw[3 * b + a];
+        for (int64_t i = 0; i < na; ++i) tot[(size_t)(op->k + i)] = ga_host[(size_t)i];
+        // the conjugate y - prox(y): -sigma times the parameters' gradients,
+        // sigma = 1 for TV (api.cpp:726-730)
+        if (ws->conj)
+            for (double &v : tot) v = -v;
+    }
+    if (fp_status st = read_cg(ws, nl)) return st;
+    return finish();
+}
+
+// dout = J_x dx + (dz/dgamma) dgamma + (dz/dtheta) dtheta at the kept point
+// (the reference's jvp_impl, src/api/api.cpp:583-616, image_jvp_driver,
+// src/core/driver.hpp:1448-1503, and TVIso::jvp_img, src/ops/tv_iso.cpp:953-997).
+// Isotropic TV.
+fp_status jvp_impl(const fp_op *op, fp_workspace *ws, const fp_array *dxa, double dgamma, const fp_array *dpa,
+                   fp_array *oa) {
+    if (!op || !ws || !oa) return FP_EINVAL;
+    if (ws->op != op || !ws->valid) return FP_EINVAL;
+    if (!std::isfinite(dgamma)) return FP_EPARAM;
+    Arr dx, out;
+    if (fp_status s = to_arr(oa, out)) return s;
+    auto like_ws = [&](const Arr &a) {
+        if (a.dtype != ws->dtype) return FP_EDTYPE;
+        if (a.ndim != ws->ndim) return FP_ESHAPE;
+        for (int d = 0; d < a.ndim; ++d)
+            if (a.shape[d] != ws->shape[d]) return FP_ESHAPE;
+        return FP_OK;
+    };
+    if (fp_status s = like_ws(out)) return s;
+    if (dxa) {
+        if (fp_status s = to_arr(dxa, dx)) return s;
+        if (fp_status s = like_ws(dx)) return s;
+    }
+    if (fp_status s = check_output(dxa ? &dx : nullptr, out)) return s;
+    const int64_t P = fp_op_nparams(op);
+    Arr dp;
+    const bool has_dp = dpa && P > 0;
+    if (has_dp)
+        if (fp_status s = param_array(dpa, P, dp)) return s;
+    if (ws->host_mode != (out.device == FP_DEVICE_CPU)) return FP_EINVAL;
+    if (dxa && dx.device != out.device) return FP_EINVAL;
+    if (op->kind != kIso) return FP_EINVAL;  // anisotropic derivatives: not on the device yet
+    DeviceScope dsc(ws->device);
+    if (ws->identity)  // J = I; the sigma-derivative NaN (api.cpp:603-607)
+        return copy_or_fill(ws, dgamma != 0.0 ? nullptr : (dxa ? &dx : nullptr), out,
+                            dgamma != 0.0 ? std::numeric_limits<double>::quiet_NaN() : 0.0, ws->V[1]);
+    const Geometry &g0 = ws->g;
+    if (g0.B * g0.N == 0) return FP_OK;
+    if (ws->conj) dgamma = 0.0;  // y - prox(y) is constant in sigma for TV (api.cpp:610)
+    cudaStream_t s = ws->stream;
+    VjpGeom vg;
+    VjpBuffers bf;
+    if (fp_status st = deriv_prepare(op, ws, vg, bf)) return st;
+    // the parameter direction: the axis weights on the host, the pixel
+    // weights as doubles in qv (free until the solve)
+    JvpDir dir{{0.0, 0.0, 0.0}};
+    const double *dalpha = nullptr;
+    const int64_t na = P - op->k;
+    cudaError_t e = cudaSuccess;
+    if (has_dp) {
+        if (dp.device == FP_DEVICE_CPU) {
+            std::vector<double> v((size_t)P);
+            for (int64_t i = 0; i < P; ++i) {
+                const char *q = dp.data + i * dp.strides[0] * (int64_t)dp.itemsize();
+                v[(size_t)i] = dp.dtype == FP_F32 ? (double)*reinterpret_cast<const float *>(q)
+                                                  : *reinterpret_cast<const double *>(q);
+            }
+            for (int a = 0; a < op->k; ++a) dir.dw[a] = v[(size_t)a];
+            if (na > 0) e = cudaMemcpyAsync(bf.qv, v.data() + op->k, (size_t)na * sizeof(double),
+                                            cudaMemcpyHostToDevice, s);
+        } else {
+            if (pointer_device(dp.data) != ws->device) return FP_EINVAL;
+            const int64_t one = 1, kk = op->k;
+            double hw[3] = {0.0, 0.0, 0.0};
+            e = strided_copy(dp.data, dp.dtype, &kk, dp.strides, 1, bf.b, FP_F64, &one, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(hw, bf.b, (size_t)kk * sizeof(double), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess && na > 0)
+                e = strided_copy(dp.data + kk * dp.strides[0] * (int64_t)dp.itemsize(), dp.dtype, &na, dp.strides, 1,
+                                 bf.qv, FP_F64, &one, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            for (int a = 0; a < op->k; ++a) dir.dw[a] = hw[a];
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e);
+        for (int a = 0; a < op->k; ++a)
+            if (!std::isfinite(dir.dw[a])) return FP_EPARAM;
+        if (na > 0) dalpha = bf.qv;
+    }
+    const void *dsrc = nullptr;
+    if (dxa)
+        if (fp_status st = stage_input(ws, dx, ws->V[0], &dsrc)) return st;
+    const bool direct = !ws->host_mode && out.contiguous();
+    void *ddst = direct ? out.data : ws->V[1];
+    if (direct && pointer_device(out.data) != ws->device) return FP_EINVAL;
+    int64_t nl = 0;
+    e = jvp_solve(ws->dtype, vg, bf, dsrc, ddst, dgamma, dir, dalpha, ws->deriv_tol, ws->deriv_max_iter,
+                  ws->conj ? 1 : 0, s, ws->h_live, ws->ev[0], &nl);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (fp_status st = unstage_output(ws, ddst, out)) return st;
+    return read_cg(ws, nl);
 }
 
 }  // namespace
@@ -1554,6 +1838,8 @@ FP_API fp_status fp_prox_conj(const fp_op *op, double sigma, const fp_array *y, 
     return guard([&] { return prox_impl(op, sigma, y, out, opt, ws, info, true, nullptr); });
 }
 
+FP_API void fp_b200_release_cached(void) { pool_release_cached(); }
+
 FP_API fp_status fp_b200_workspace_stats(const fp_workspace *ws, int64_t *kernel_launches, int64_t *step_launches) {
     if (!ws || !ws->info_valid) return FP_EINVAL;
     if (kernel_launches) *kernel_launches = ws->kernel_launches;
@@ -1563,12 +1849,7 @@ FP_API fp_status fp_b200_workspace_stats(const fp_workspace *ws, int64_t *kernel
 
 FP_API fp_status fp_jvp(const fp_op *op, const fp_workspace *ws, const fp_array *dx, double dgamma,
                         const fp_array *dparams, fp_array *dout) {
-    (void)dx;
-    (void)dgamma;
-    (void)dparams;
-    (void)dout;
-    if (!op || !ws || !ws->valid) return FP_EINVAL;
-    return FP_EINVAL;
+    return guard([&] { return jvp_impl(op, const_cast<fp_workspace *>(ws), dx, dgamma, dparams, dout); });
 }
 
 FP_API fp_status fp_vjp(const fp_op *op, const fp_workspace *ws, const fp_array *g, fp_array *gx, double *ggamma,

@@ -15,6 +15,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -87,6 +89,7 @@ struct fp_b200_batch {
     // graphs of `chunk` steps, keyed by (grid0, grid1, chunk)
     std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
     int rows_hint = 0;
+    bool use_graphs = true;
     int64_t steps_run = 0, kernel_launches = 0;
     double wh[2] = {1.0, 1.0}, tau = 0.125;
 };
@@ -273,7 +276,13 @@ cudaError_t launch_steps(fp_b200_batch *bt, int steps) {
     return cudaSuccess;
 }
 
+void trace(const char *what, cudaError_t e) {
+    if (e != cudaSuccess && std::getenv("FASTPROX_B200_DEBUG"))
+        std::fprintf(stderr, "fastprox_b200 batch: %s: %s\n", what, cudaGetErrorString(e));
+}
+
 cudaError_t run_chunk(fp_b200_batch *bt, int steps) {
+    if (!bt->use_graphs) return launch_steps(bt, steps);
     const auto key = std::make_tuple(bt->grid[0], bt->grid[1], steps);
     auto it = bt->graphs.find(key);
     if (it == bt->graphs.end()) {
@@ -291,13 +300,23 @@ cudaError_t run_chunk(fp_b200_batch *bt, int steps) {
         bt->stream = keep;
         cudaStreamDestroy(cap);
         if (e != cudaSuccess) {
+            // a capture can fail while other threads use the device; run the
+            // chunk as plain launches instead, and stop capturing
+            trace("graph capture", e);
+            cudaGetLastError();
             if (graph) cudaGraphDestroy(graph);
-            return e;
+            bt->use_graphs = false;
+            return launch_steps(bt, steps);
         }
         cudaGraphExec_t exec = nullptr;
         e = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return e;
+        if (e != cudaSuccess) {
+            trace("graph instantiate", e);
+            cudaGetLastError();
+            bt->use_graphs = false;
+            return launch_steps(bt, steps);
+        }
         it = bt->graphs.emplace(key, exec).first;
     }
     return cudaGraphLaunch(it->second, bt->stream);
@@ -403,6 +422,12 @@ FP_API fp_status fp_b200_batch_set_stream(fp_b200_batch *bt, void *stream) {
     return FP_OK;
 }
 
+FP_API fp_status fp_b200_batch_set_graphs(fp_b200_batch *bt, int on) {
+    if (!bt) return FP_EINVAL;
+    bt->use_graphs = on != 0;
+    return FP_OK;
+}
+
 FP_API fp_status fp_b200_batch_set_rows(fp_b200_batch *bt, int rows) {
     if (!bt || rows < 0 || rows > 1024) return FP_EINVAL;
     bt->rows_hint = rows;
@@ -483,11 +508,12 @@ FP_API fp_status fp_b200_batch_admit(fp_b200_batch *bt, const void *x, int64_t h
 }
 
 // Runs chunks of `steps` iterations until at least one admitted image has
-// finished (or none is live), finalises the finished ones into their z,
-// frees their slots, and reports them (slots, gaps, iterations; each array
-// max_images long). *nfinished = 0 with *nlive = 0: nothing was admitted.
-FP_API fp_status fp_b200_batch_run(fp_b200_batch *bt, int steps, int *finished, double *gaps, int *iters,
-                                   int *nfinished, int *nlive) {
+// finished, none is live or max_chunks (> 0) chunks ran, finalises the
+// finished ones into their z, frees their slots, and reports them (slots,
+// gaps, iterations; each array max_images long). *nfinished = 0 with
+// *nlive = 0: nothing was admitted.
+FP_API fp_status fp_b200_batch_run(fp_b200_batch *bt, int steps, int max_chunks, int *finished, double *gaps,
+                                   int *iters, int *nfinished, int *nlive) {
     return guard_b([&] {
         if (!bt || steps < 1 || !nfinished) return FP_EINVAL;
         *nfinished = 0;
@@ -498,14 +524,17 @@ FP_API fp_status fp_b200_batch_run(fp_b200_batch *bt, int steps, int *finished, 
         }
         const size_t S = (size_t)bt->max_slots;
         std::vector<int> done;
-        for (int guard_iter = 0; guard_iter < (1 << 20); ++guard_iter) {
+        const int chunks = max_chunks > 0 ? max_chunks : (1 << 20);
+        for (int chunk = 0; chunk < chunks; ++chunk) {
             cudaError_t e = run_chunk(bt, steps);
+            trace("run", e);
             if (e != cudaSuccess) return FP_EDEVICE;
             bt->steps_run += steps;
             bt->kernel_launches += (int64_t)steps * 6;
             e = cudaMemcpyAsync(bt->h_st, bt->st, S * sizeof(IsoState), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaMemcpyAsync(bt->h_live, bt->live, sizeof(int), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            trace("poll", e);
             if (e != cudaSuccess) return FP_EDEVICE;
             for (size_t i = 0; i < S; ++i)
                 if (bt->sh[i].used && bt->h_st[i].status != kLive) done.push_back((int)i);

@@ -193,6 +193,9 @@ __global__ void __launch_bounds__(kT) st_flat(VjpGeom g, VjpBuffers bf) {
     int *P = bf.root + (int64_t)b * N;
     int *C = bf.cnt + (int64_t)b * N;
     unsigned long long *A = bf.acc + (int64_t)b * 2 * N;
+    // an image with no active axis (gamma 0) has none here either: every
+    // pixel flat and alone, G z = 0 (tv_iso.cpp:938-939)
+    const bool ident = mode == kModeIdentity;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
         const Px x = pix_of(g, p);
         const double z0 = z_at<T>(g, bf, b, p);
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(kT) st_flat(VjpGeom g, VjpBuffers bf) {
         bool any = false;
         for (int a = 0; a < g.k; ++a) {
             double gv = 0.0;
-            if (x.has[a]) {
+            if (x.has[a] && !ident) {
                 gv = g.wa[a] * (z_at<T>(g, bf, b, p + g.S[a]) - z0);
                 nn += gv * gv;
                 any = true;
@@ -271,8 +274,8 @@ __global__ void st_roots(VjpGeom g, VjpBuffers bf) {
 // ---- region sums of pixel values: max pass, atomic pass, read-out ----------------
 
 // pass 1 over the per-pixel values v_p (kind: 0 the cotangent g, 1 the product
-// y = pix + G^T H G pix of the conjugate gradients, 2 the Jacobi terms): the
-// per-image maximum |v| sets the fixed-point exponent.
+// y = pix + G^T H G pix of the conjugate gradients, 3 a right-hand side
+// already in y): the per-image maximum |v| sets the fixed-point exponent.
 template <class T>
 __device__ __forceinline__ double apply_y(const VjpGeom &g, const VjpBuffers &bf, int b, int64_t p) {
     // y_p = c[root p] - sum_a w_a (h_a[p] - h_a[p - e_a]) (tv_iso.cpp:870-884)
@@ -301,6 +304,7 @@ __global__ void __launch_bounds__(kT) rs_max(VjpGeom g, VjpBuffers bf, int kind,
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
         double v;
         if (kind == 0) v = (double)gin[(int64_t)b * N + p];
+        else if (kind == 3) v = bf.y[(int64_t)b * N + p];
         else v = apply_y<T>(g, bf, b, p);
         if (kind == 1) bf.y[(int64_t)b * N + p] = v;
         m = fmax(m, fabs(v));
@@ -627,6 +631,221 @@ __global__ void __launch_bounds__(kT) vjp_out(VjpGeom g, VjpBuffers bf, const T 
     bf.ggam[b] = nan ? (double)CUDART_NAN : (conj ? 0.0 : -tg);
 }
 
+// ---- parameter gradients and the forward derivative (tv_iso.cpp:953-1057) -------
+
+// The dual of an image solved as one 1D TV per fiber along its active axis
+// (tv_iso.cpp:386-397): u[p] = -(1/w) sum_{i <= p} (d - z) along the fiber,
+// 0 at its end; into out (B x N), for those images only.
+template <class T>
+__global__ void tv1d_dual(VjpGeom g, VjpBuffers bf, double *out) {
+    const int b = blockIdx.y;
+    if (bf.img[b].mode != kModeTv1d || g.act1 < 0) return;
+    const int a = g.act1;
+    const int64_t N = g.N, L = g.L[a], S = g.S[a];
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *Z = static_cast<const T *>(bf.U[0]) + (int64_t)b * g.k * N;
+    double *O = out + (int64_t)b * N;
+    const double w = g.wa[a];
+    for (int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; f < N / L; f += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t st = (f / S) * L * S + f % S;  // the fiber's first pixel
+        double cs = 0.0;
+        for (int64_t i = 0; i < L; ++i) {
+            const int64_t o = st + i * S;
+            cs += (double)D[o] - (double)Z[o];
+            O[o] = i + 1 < L ? -cs / w : 0.0;
+        }
+    }
+}
+
+// u_a[q] of image b at the solved scale in the reference's form (z = d - G^T u)
+template <class T>
+__device__ __forceinline__ double u_at(const VjpGeom &g, const VjpBuffers &bf, int b, int a, int64_t q,
+                                       const double *u1d) {
+    const int mode = bf.img[b].mode;
+    if (mode == kModeFdpg)
+        return (double)static_cast<const T *>(bf.U[bf.st[b].fin_par])[((int64_t)b * g.k + a) * g.N + q] / g.wmax;
+    if (mode == kModeTv1d && a == g.act1) return u1d[(int64_t)b * g.N + q];
+    return 0.0;
+}
+
+// the radius gamma alpha_p at the solved scale
+template <class T>
+__device__ __forceinline__ double radius_at(const VjpBuffers &bf, int b, int64_t p) {
+    const double gs = bf.vimg[b].gs;
+    if (!bf.alpha) return gs;
+    const double al = (double)static_cast<const T *>(bf.alpha)[(int64_t)b * bf.alpha_stride + p];
+    return al == 0.0 ? 0.0 : gs * al;
+}
+
+// v = J^T g at a pixel: its region's value (NaN for a NaN image)
+__device__ __forceinline__ double v_at(const VjpGeom &g, const VjpBuffers &bf, int b, int64_t q) {
+    if (bf.img[b].mode == kModeNan) return (double)CUDART_NAN;
+    if (bf.cg[b].bn == 0.0) return 0.0;
+    return bf.x[(int64_t)b * g.N + bf.root[(int64_t)b * g.N + q]];
+}
+
+// Per pixel, the terms of the parameter gradients from v = J^T g
+// (tv_iso.cpp:1020-1057), each times -2^e:
+//   h_a[p] = (v[p + e_a] - v[p]) u_a[p] + [p non-flat] (H G v)_{a,p} (G z)_{a,p} / w_a
+//   y[p]   = gamma alpha_p <(G v)_p, n_p> on non-flat pixels (alpha's gradient)
+template <class T>
+__global__ void __launch_bounds__(kT) vjp_params(VjpGeom g, VjpBuffers bf, const double *u1d) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const int mode = bf.img[b].mode;
+    const double sc = ldexp(1.0, bf.img[b].e);
+    const double *GZ = bf.gz + (int64_t)b * g.k * N;
+    const uint8_t *F = bf.flat + (int64_t)b * N;
+    double *Hh = bf.h + (int64_t)b * g.k * N;
+    double *Y = bf.y + (int64_t)b * N;
+    const VjpImage &vi = bf.vimg[b];
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        double hv[3] = {0.0, 0.0, 0.0}, ay = 0.0;
+        if (mode != kModeIdentity) {
+            const Px x = pix_of(g, p);
+            const double v0 = v_at(g, bf, b, p);
+            double gv[3] = {0.0, 0.0, 0.0};
+            for (int a = 0; a < g.k; ++a) {
+                const bool next = g.L[a] > 1 && x.co[a] + 1 < g.L[a];
+                const double vn = next ? v_at(g, bf, b, p + g.S[a]) : 0.0;
+                if (next) hv[a] = (vn - v0) * u_at<T>(g, bf, b, a, p, u1d);
+                if (x.has[a]) gv[a] = g.wa[a] * (vn - v0);
+            }
+            if (!(F[p] & 1)) {
+                double nn = 0.0, dot = 0.0;
+                for (int a = 0; a < g.k; ++a) {
+                    nn += GZ[a * N + p] * GZ[a * N + p];
+                    dot += GZ[a * N + p] * gv[a];
+                }
+                const double nr = sqrt(nn);
+                const double h = radius_at<T>(bf, b, p) / fmax(nr, vi.mu);
+                double t = 0.0;
+                for (int a = 0; a < g.k; ++a) {
+                    const double na = GZ[a * N + p] / nr;
+                    const double hg = h * (gv[a] - na * dot / nr);
+                    if (g.wa[a] != 0.0) hv[a] += hg * GZ[a * N + p] / g.wa[a];
+                    t += gv[a] * na;
+                }
+                if (bf.alpha) ay = -(sc * vi.gs) * t;
+            }
+        }
+        for (int a = 0; a < g.k; ++a) Hh[a * N + p] = -sc * hv[a];
+        Y[p] = ay;
+    }
+}
+
+// per image, the sums of h_a0 and h_a1 (a1 < 0: none) into gw[3 b + a]
+__global__ void __launch_bounds__(kT) param_sums(VjpGeom g, VjpBuffers bf, int a0, int a1) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const double *H0 = bf.h + ((int64_t)b * g.k + a0) * N;
+    const double *H1 = a1 >= 0 ? bf.h + ((int64_t)b * g.k + a1) * N : nullptr;
+    double s0 = 0.0, s1 = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        s0 += H0[p];
+        if (H1) s1 += H1[p];
+    }
+    double t0, t1;
+    if (!img_reduce(bf, b, blockIdx.x, gridDim.x, s0, s1, sh, &flag, t0, t1, false)) return;
+    bf.gw[3 * b + a0] = t0;
+    if (a1 >= 0) bf.gw[3 * b + a1] = t1;
+}
+
+// alpha's gradient: out[p] = sum over the images, in order, of y[b][p]
+__global__ void alpha_sum(VjpGeom g, VjpBuffers bf, double *out) {
+    const int64_t N = g.N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        double t = 0.0;
+        for (int64_t b = 0; b < g.B; ++b) t += bf.y[b * N + p];
+        out[p] = t;
+    }
+}
+
+// The forward derivative's right-hand side before G^T (tv_iso.cpp:958-985):
+//   y[p] = dx[p] + sum_a 2^e dw_a (u_a[p] - u_a[p - e_a]),
+//   c_p  = H_p (2^e dW D z)_p + dr_p n_p on non-flat pixels (0 on flat ones),
+//   dr_p = dgamma alpha_p + gamma 2^e dalpha_p  (dgamma without pixel weights),
+// c into h.
+template <class T>
+__global__ void __launch_bounds__(kT) jvp_terms(VjpGeom g, VjpBuffers bf, const T *__restrict__ dx, double dgamma,
+                                                JvpDir dir, const double *__restrict__ dalpha, const double *u1d) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const int mode = bf.img[b].mode;
+    const double sc = ldexp(1.0, bf.img[b].e);
+    const double *GZ = bf.gz + (int64_t)b * g.k * N;
+    const uint8_t *F = bf.flat + (int64_t)b * N;
+    double *Hh = bf.h + (int64_t)b * g.k * N;
+    double *Y = bf.y + (int64_t)b * N;
+    const VjpImage &vi = bf.vimg[b];
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const Px x = pix_of(g, p);
+        double rhs = dx ? (double)dx[(int64_t)b * N + p] : 0.0;
+        double c[3] = {0.0, 0.0, 0.0};
+        if (mode != kModeIdentity) {
+            for (int a = 0; a < g.k; ++a) {
+                if (dir.dw[a] == 0.0 || g.L[a] <= 1) continue;
+                const double prev = x.co[a] > 0 ? u_at<T>(g, bf, b, a, p - g.S[a], u1d) : 0.0;
+                rhs += sc * dir.dw[a] * (u_at<T>(g, bf, b, a, p, u1d) - prev);
+            }
+            if (!(F[p] & 1)) {
+                double nn = 0.0, dot = 0.0;
+                for (int a = 0; a < g.k; ++a) {
+                    c[a] = g.wa[a] != 0.0 ? sc * dir.dw[a] * GZ[a * N + p] / g.wa[a] : 0.0;
+                    nn += GZ[a * N + p] * GZ[a * N + p];
+                    dot += GZ[a * N + p] * c[a];
+                }
+                const double nr = sqrt(nn);
+                const double h = radius_at<T>(bf, b, p) / fmax(nr, vi.mu);
+                double dr = dgamma;
+                if (bf.alpha) {
+                    const double al = (double)static_cast<const T *>(bf.alpha)[(int64_t)b * bf.alpha_stride + p];
+                    dr = dgamma * al + (dalpha ? vi.gs * (sc * dalpha[p]) : 0.0);
+                }
+                for (int a = 0; a < g.k; ++a) {
+                    const double na = GZ[a * N + p] / nr;
+                    c[a] = h * (c[a] - na * dot / nr) + dr * na;
+                }
+            }
+        }
+        Y[p] = rhs;
+        for (int a = 0; a < g.k; ++a) Hh[a * N + p] = c[a];
+    }
+}
+
+// y -= G^T c, i.e. y[p] += sum_a w_a (c_a[p] - c_a[p - e_a]) (tv_iso.cpp:986)
+__global__ void __launch_bounds__(kT) jvp_rhs(VjpGeom g, VjpBuffers bf) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const double *Hh = bf.h + (int64_t)b * g.k * N;
+    double *Y = bf.y + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        double t = Y[p];
+        for (int a = 0; a < g.k; ++a) {
+            if (g.wa[a] == 0.0) continue;
+            const int64_t co = (p / g.S[a]) % g.L[a];
+            const double prev = co > 0 ? Hh[a * N + p - g.S[a]] : 0.0;
+            t += g.wa[a] * (Hh[a * N + p] - prev);
+        }
+        Y[p] = t;
+    }
+}
+
+// dz = M x (every pixel its region's value); the conjugate's dx - dz
+template <class T>
+__global__ void __launch_bounds__(kT) jvp_out(VjpGeom g, VjpBuffers bf, const T *__restrict__ dx, T *__restrict__ dz,
+                                              int conj) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        double v = v_at(g, bf, b, p);
+        if (conj) v = (dx ? (double)dx[(int64_t)b * N + p] : 0.0) - v;
+        dz[(int64_t)b * N + p] = (T)v;
+    }
+}
+
 int pblocks(const VjpGeom &g) {
     int64_t nb = (g.N + kT * 4 - 1) / (kT * 4);
     return (int)std::max<int64_t>(1, std::min<int64_t>(nb, 512));
@@ -641,16 +860,16 @@ cudaError_t structure_t(const VjpGeom &g, const VjpBuffers &bf, cudaStream_t s) 
     return cudaGetLastError();
 }
 
+// The system on the regions for a right-hand side (kind 0: the pixel vector
+// gin; 3: the one in y): region sums, the Jacobi diagonal, and conjugate
+// gradients in chunks of 8 iterations until every image has stopped.
 template <class T>
-cudaError_t vjp_t(const VjpGeom &g, const VjpBuffers &bf, const void *gin, void *gx, double tol, int max_iter, int conj,
-                  cudaStream_t s, int *h_live, cudaEvent_t ev, int64_t *launches) {
+cudaError_t solve_system(const VjpGeom &g, const VjpBuffers &bf, int kind, const T *gin, double tol, int max_iter,
+                         cudaStream_t s, int *h_live, cudaEvent_t ev, int64_t &nl) {
     const dim3 grid(pblocks(g), (unsigned)g.B);
-    const T *gi = static_cast<const T *>(gin);
-    int64_t nl = 0;
-    // right-hand side b = M^T g and the Jacobi diagonal
-    rs_max<T><<<grid, kT, 0, s>>>(g, bf, 0, gi);
-    rs_add<T><<<grid, kT, 0, s>>>(g, bf, 0, gi);
-    rs_read<<<grid, kT, 0, s>>>(g, bf, 0, bf.b);
+    rs_max<T><<<grid, kT, 0, s>>>(g, bf, kind, gin);
+    rs_add<T><<<grid, kT, 0, s>>>(g, bf, kind, gin);
+    rs_read<<<grid, kT, 0, s>>>(g, bf, kind, bf.b);
     jac_max<T><<<grid, kT, 0, s>>>(g, bf);
     jac_add<T><<<grid, kT, 0, s>>>(g, bf);
     rs_read<<<grid, kT, 0, s>>>(g, bf, 0, bf.dinv);
@@ -663,8 +882,8 @@ cudaError_t vjp_t(const VjpGeom &g, const VjpBuffers &bf, const void *gin, void 
     for (int it = 0; it < max_iter + chunk; it += chunk) {
         for (int j = 0; j < chunk; ++j) {
             cg_hg<T><<<grid, kT, 0, s>>>(g, bf);
-            rs_max<T><<<grid, kT, 0, s>>>(g, bf, 1, gi);
-            rs_add<T><<<grid, kT, 0, s>>>(g, bf, 1, gi);
+            rs_max<T><<<grid, kT, 0, s>>>(g, bf, 1, gin);
+            rs_add<T><<<grid, kT, 0, s>>>(g, bf, 1, gin);
             rs_read<<<grid, kT, 0, s>>>(g, bf, 1, bf.qv);
             cg_alpha<<<grid, kT, 0, s>>>(g, bf);
             cg_step<<<grid, kT, 0, s>>>(g, bf);
@@ -677,7 +896,55 @@ cudaError_t vjp_t(const VjpGeom &g, const VjpBuffers &bf, const void *gin, void 
         if (e != cudaSuccess) return e;
         if (*h_live == 0) break;
     }
+    return cudaSuccess;
+}
+
+template <class T>
+cudaError_t vjp_t(const VjpGeom &g, const VjpBuffers &bf, const void *gin, void *gx, double tol, int max_iter, int conj,
+                  bool params, cudaStream_t s, int *h_live, cudaEvent_t ev, int64_t *launches) {
+    const dim3 grid(pblocks(g), (unsigned)g.B);
+    const T *gi = static_cast<const T *>(gin);
+    int64_t nl = 0;
+    cudaError_t e = solve_system<T>(g, bf, 0, gi, tol, max_iter, s, h_live, ev, nl);
+    if (e != cudaSuccess) return e;
     vjp_out<T><<<grid, kT, 0, s>>>(g, bf, gi, static_cast<T *>(gx), conj);
+    ++nl;
+    if (params) {
+        // r, y, h and qv are free once the gradients are solved
+        tv1d_dual<T><<<grid, kT, 0, s>>>(g, bf, bf.r);
+        vjp_params<T><<<grid, kT, 0, s>>>(g, bf, bf.r);
+        param_sums<<<grid, kT, 0, s>>>(g, bf, 0, g.k > 1 ? 1 : -1);
+        nl += 3;
+        if (g.k > 2) {
+            param_sums<<<grid, kT, 0, s>>>(g, bf, 2, -1);
+            ++nl;
+        }
+        if (bf.alpha) {
+            alpha_sum<<<pblocks(g), kT, 0, s>>>(g, bf, bf.qv);
+            ++nl;
+        }
+    }
+    if (launches) *launches = nl;
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t jvp_t(const VjpGeom &g, const VjpBuffers &bf, const void *dx, void *dz, double dgamma, const JvpDir &dir,
+                  const double *dalpha, double tol, int max_iter, int conj, cudaStream_t s, int *h_live,
+                  cudaEvent_t ev, int64_t *launches) {
+    const dim3 grid(pblocks(g), (unsigned)g.B);
+    const T *dxi = static_cast<const T *>(dx);
+    int64_t nl = 0;
+    // the single-axis duals into r, which the solve then overwrites
+    tv1d_dual<T><<<grid, kT, 0, s>>>(g, bf, bf.r);
+    jvp_terms<T><<<grid, kT, 0, s>>>(g, bf, dxi, dgamma, dir, dalpha, bf.r);
+    jvp_rhs<<<grid, kT, 0, s>>>(g, bf);
+    nl += 3;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = solve_system<T>(g, bf, 3, static_cast<const T *>(nullptr), tol, max_iter, s, h_live, ev, nl);
+    if (e != cudaSuccess) return e;
+    jvp_out<T><<<grid, kT, 0, s>>>(g, bf, dxi, static_cast<T *>(dz), conj);
     ++nl;
     if (launches) *launches = nl;
     return cudaGetLastError();
@@ -690,9 +957,18 @@ cudaError_t vjp_structure(int dtype, const VjpGeom &g, const VjpBuffers &bf, cud
 }
 
 cudaError_t vjp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *gin, void *gx, double tol,
-                      int max_iter, int conj, cudaStream_t s, int *h_live, cudaEvent_t ev, int64_t *launches) {
-    return dtype == 1 ? vjp_t<float>(g, bf, gin, gx, tol, max_iter, conj, s, h_live, ev, launches)
-                      : vjp_t<double>(g, bf, gin, gx, tol, max_iter, conj, s, h_live, ev, launches);
+                      int max_iter, int conj, bool params, cudaStream_t s, int *h_live, cudaEvent_t ev,
+                      int64_t *launches) {
+    return dtype == 1 ? vjp_t<float>(g, bf, gin, gx, tol, max_iter, conj, params, s, h_live, ev, launches)
+                      : vjp_t<double>(g, bf, gin, gx, tol, max_iter, conj, params, s, h_live, ev, launches);
+}
+
+cudaError_t jvp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *dx, void *dz, double dgamma,
+                      const JvpDir &dir, const double *dalpha, double tol, int max_iter, int conj, cudaStream_t s,
+                      int *h_live, cudaEvent_t ev, int64_t *launches) {
+    return dtype == 1 ? jvp_t<float>(g, bf, dx, dz, dgamma, dir, dalpha, tol, max_iter, conj, s, h_live, ev, launches)
+                      : jvp_t<double>(g, bf, dx, dz, dgamma, dir, dalpha, tol, max_iter, conj, s, h_live, ev,
+                                      launches);
 }
 
 }  // namespace fpb

@@ -19,6 +19,12 @@ struct VjpGeom {
     double wh[3];  // wa / wmax, as the forward used them
     double wmax;
     double eta;    // relative margin below the radius that counts as inside
+    int act1;      // the active axis when there is exactly one, else -1
+};
+
+// A direction in the axis weights for the forward derivative.
+struct JvpDir {
+    double dw[3];
 };
 
 // Per image, from the kept forward (tv_iso.cpp:559-570): the step at the
@@ -53,6 +59,7 @@ struct VjpBuffers {
     VjpImage *vimg = nullptr;
     CgState *cg = nullptr;
     double *ggam = nullptr;  // per-image step gradient
+    double *gw = nullptr;    // per-image axis-weight gradients, 3 per image
     double *part = nullptr;
     unsigned *ticket = nullptr;
     int *live = nullptr, *err = nullptr;
@@ -60,7 +67,16 @@ struct VjpBuffers {
 };
 
 cudaError_t vjp_structure(int dtype, const VjpGeom &g, const VjpBuffers &bf, cudaStream_t s);
+// gx = J^T gin per image, the step's gradient into ggam and, with params,
+// the axis weights' into gw and the pixel weights' (summed over the images)
+// into qv[0, N).
 cudaError_t vjp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *gin, void *gx, double tol,
-                      int max_iter, int conj, cudaStream_t s, int *h_live, cudaEvent_t ev, int64_t *launches);
+                      int max_iter, int conj, bool params, cudaStream_t s, int *h_live, cudaEvent_t ev,
+                      int64_t *launches);
+// dz = J_x dx + (dz/dgamma) dgamma + (dz/dw) dw + (dz/dalpha) dalpha per image;
+// dx and dalpha (N doubles on the device, outside x, r, y and h) may be null.
+cudaError_t jvp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *dx, void *dz, double dgamma,
+                      const JvpDir &dir, const double *dalpha, double tol, int max_iter, int conj, cudaStream_t s,
+                      int *h_live, cudaEvent_t ev, int64_t *launches);
 
 }  // namespace fpb

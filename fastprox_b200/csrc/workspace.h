@@ -60,14 +60,15 @@ struct fp_workspace {
     // derivative (keep_structure workspaces): structure and conjugate gradients
     uint8_t *v_flat = nullptr;
     int *v_root = nullptr, *v_cnt = nullptr;
-    double *v_gz = nullptr, *v_h = nullptr, *v_vec = nullptr, *v_ggam = nullptr;
+    double *v_gz = nullptr, *v_h = nullptr, *v_vec = nullptr, *v_ggam = nullptr, *v_gw = nullptr;
     unsigned long long *v_acc = nullptr;
     fpb::VjpImage *v_img = nullptr;
     fpb::CgState *v_cg = nullptr;
     fpb::VjpImage *h_vimg = nullptr;
     fpb::CgState *h_cg = nullptr;
-    double *h_ggam = nullptr;
+    double *h_ggam = nullptr, *h_gw = nullptr;
     bool struct_valid = false;
+    bool identity = false;  // the kept call was a conjugate at sigma = 0: J = I
     bool conj = false;
     // pinned host memory
     int *h_live = nullptr;
@@ -78,7 +79,8 @@ struct fp_workspace {
     double *h_gam = nullptr;
     void *h_stage = nullptr;
     cudaEvent_t ev[2] = {nullptr, nullptr};
-    std::vector<void *> dev_allocs, host_allocs;
+    void *dev_block = nullptr, *host_block = nullptr;  // every buffer above lies in one of these
+    size_t host_bytes = 0;
     // launch shape and polling
     fpb::StepShape shape_{};
     int chunk = 8;

@@ -16,6 +16,9 @@ Serving (``serve_stream``):
   streams, so their kernels overlap with the batch's.
 * admission is capped by an HBM budget: a request waits while the memory its
   solve needs (its workspace, or its share of the batch arena) would exceed it.
+* the batch runs a bounded number of iterations per loop pass, so arrivals
+  join it within a few iterations; workspaces come from the library's memory
+  pool, so per-request set-up never synchronises the device.
 The baseline (``one_at_a_time``) solves the same requests in arrival order,
 one fp_prox call at a time on one stream.
 Latency is measured on the host from a request's arrival to its result being
@@ -96,13 +99,15 @@ def _ws_bytes(r):
     return n * 4 * (3 + 5 * k) + n * 24
 
 
-def serve_stream(reqs, src, budget_bytes=120e9, workers=4, steps=4):
+def serve_stream(reqs, src, budget_bytes=120e9, workers=4, steps=8):
     """Continuous batching. Returns per-request latencies (s) and the span."""
     import torch
 
     from .batch import RaggedBatch
     arena_px = 64 * 1024 * 1024
-    batch = RaggedBatch(max_images=512, max_pixels=arena_px)
+    main = torch.cuda.Stream()
+    # worker threads use the device while the batch runs: plain launches
+    batch = RaggedBatch(max_images=512, max_pixels=arena_px, graphs=False, stream=main.cuda_stream)
     arena_bytes = arena_px * 44
     used = arena_bytes
     lock = threading.Lock()
@@ -110,9 +115,10 @@ def serve_stream(reqs, src, budget_bytes=120e9, workers=4, steps=4):
     tls = threading.local()
     counter = iter(range(1 << 30))
 
-    def work(r):
+    def work(r, ready):
         if not hasattr(tls, "s"):
             tls.s = streams[next(counter) % workers]
+        tls.s.wait_event(ready)
         with torch.cuda.stream(tls.s):
             z, info = _solve_one(r)
             tls.s.synchronize()
@@ -130,7 +136,8 @@ def serve_stream(reqs, src, budget_bytes=120e9, workers=4, steps=4):
         now = time.perf_counter() - t0
         while nxt < len(reqs) and reqs[nxt].t <= now:
             r = reqs[nxt]
-            r.x = src.image(r)
+            with torch.cuda.stream(main):
+                r.x = src.image(r)
             r.bytes = _ws_bytes(r)
             waiting.append(r)
             nxt += 1
@@ -148,12 +155,14 @@ def serve_stream(reqs, src, budget_bytes=120e9, workers=4, steps=4):
                     if ok:
                         used += r.bytes
                 if ok:
-                    futures[pool.submit(work, r)] = r
+                    ready = torch.cuda.Event()
+                    ready.record(main)
+                    futures[pool.submit(work, r, ready)] = r
                 else:
                     still.append(r)
         waiting = still
         if batch.pending:
-            for slot, z, gap, it, conv in batch.run(steps=steps):
+            for slot, z, gap, it, conv in batch.run(steps=steps, max_chunks=1):
                 r = inflight.pop(slot)
                 lat[r.i] = time.perf_counter() - t0 - r.t
                 done += 1
@@ -172,7 +181,8 @@ def serve_stream(reqs, src, budget_bytes=120e9, workers=4, steps=4):
     return lat, span
 
 
-def one_at_a_time(reqs, src):
+def one_at_a_time(reqs, src, service=None):
+    """The plain path; `service` (a dict) collects the GPU seconds per kind."""
     import torch
     lat = np.zeros(len(reqs))
     t0 = time.perf_counter()
@@ -181,26 +191,33 @@ def one_at_a_time(reqs, src):
         if r.t > now:
             time.sleep(r.t - now)
         r.x = src.image(r)
+        torch.cuda.synchronize()
+        ts = time.perf_counter()
         _solve_one(r)
         torch.cuda.synchronize()
-        lat[r.i] = time.perf_counter() - t0 - r.t
+        te = time.perf_counter()
+        if service is not None:
+            service[r.kind] = service.get(r.kind, 0.0) + (te - ts)
+        lat[r.i] = te - t0 - r.t
     return lat, time.perf_counter() - t0
 
 
-def run(seconds=20.0, rate=200.0, seed=0):
+def run(seconds=20.0, rate=200.0, seed=0, workers=4):
     import torch
     src = ImageSource(seed)
     warm = make_requests(0.2, rate, seed + 1)
-    serve_stream(warm, src)
+    serve_stream(warm, src, workers=workers)
     reqs = make_requests(seconds, rate, seed)
-    lat, span = serve_stream(reqs, src)
+    lat, span = serve_stream(reqs, src, workers=workers)
     reqs_b = make_requests(seconds, rate, seed)
-    lat_b, span_b = one_at_a_time(reqs_b, src)
+    service = {}
+    lat_b, span_b = one_at_a_time(reqs_b, src, service)
     torch.cuda.synchronize()
     kinds = {k: sum(r.kind == k for r in reqs) for k in ("iso2d", "aniso2d", "iso3d")}
     return {"workload": "serve", "metric": "serve p50/p99 latency (ms) and images/s, Poisson arrivals",
-            "rate_per_s": rate, "seconds": seconds, "requests": len(reqs), "kinds": kinds,
+            "rate_per_s": rate, "seconds": seconds, "requests": len(reqs), "kinds": kinds, "workers": workers,
             "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
             "images_per_s": len(reqs) / span,
             "plain_p50_ms": float(np.percentile(lat_b, 50) * 1e3), "plain_p99_ms": float(np.percentile(lat_b, 99) * 1e3),
-            "plain_images_per_s": len(reqs_b) / span_b}
+            "plain_images_per_s": len(reqs_b) / span_b,
+            "plain_service_s": {k: round(v, 3) for k, v in service.items()}}

@@ -36,7 +36,8 @@ def aniso512(args):
     B, H, W = 64, 512, 512
     x = torch.as_tensor(synth.phantom(B, H, W, seed=0), device="cuda")
     steps = torch.as_tensor([(0.05, 0.1, 0.2)[i % 3] for i in range(B)], device="cuda", dtype=torch.float64)
-    op = TVAniso(2)
+    # per-edge weights U[0.5, 1.5], one (2, H, W) map for the batch
+    op = TVAniso(2, edge_weights=synth.pixel_weights((2, H, W), seed=1))
     out = torch.empty_like(x)
     for _ in range(max(args.warmup, 1)):
         z, info = op.solve(x, steps, tol=1e-6, max_iter=2000, out=out, with_dual=False)
@@ -47,7 +48,7 @@ def aniso512(args):
     e1.record()
     torch.cuda.synchronize()
     t = e0.elapsed_time(e1) / 1e3 / args.steps
-    return {"workload": "aniso512", "metric": "TV-prox images/s at gap<=1e-6 (512^2 fp32, anisotropic)",
+    return {"workload": "aniso512", "metric": "TV-prox images/s at gap<=1e-6 (512^2 fp32, anisotropic, edge weights)",
             "value": B / t, "unit": "images/s", "ms_per_step": t * 1e3, "converged": bool(info.converged),
             "iters": {"min": int(info.image_iters.min()), "median": float(np.median(info.image_iters)),
                       "max": int(info.image_iters.max())}}
@@ -163,7 +164,7 @@ def vjp(args):
     return {"workload": "vjp", "metric": "forward+backward seconds, (16,3,256,256) fp32, implicit VJP",
             "value": t_ours, "unit": "s", "peak_torch_bytes": int(peak_ours),
             "unrolled400_seconds": t_unrolled, "unrolled400_peak_bytes": int(peak_unrolled),
-            "loss": float(loss), "loss_unrolled400": float(loss_u), "ggamma": float(gg)}
+            "loss": float(loss.detach()), "loss_unrolled400": float(loss_u.detach()), "ggamma": float(gg)}
 
 
 def _unrolled_fista(x, gamma, iters):
@@ -197,4 +198,4 @@ def _unrolled_fista(x, gamma, iters):
 
 def serve(args):
     from . import serve as srv
-    return srv.run(seconds=args.serve_seconds)
+    return srv.run(seconds=args.serve_seconds, workers=getattr(args, "serve_workers", 4))

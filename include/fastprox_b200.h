@@ -143,7 +143,10 @@ FP_API fp_status fp_prox_conj(const fp_op *op, double sigma, const fp_array *y,
                               fp_workspace *ws, fp_info *info);
 
 /* Replace include/fastprox.h:646-654 and :779-780: derivatives at the point
- * kept by the last prox call with keep_structure. */
+ * kept by the last prox call with keep_structure (isotropic TV; an
+ * anisotropic point gives FP_EINVAL). theta = the k axis weights, then the
+ * pixel weights in C order (fp_op_nparams entries); gparams and dparams may be
+ * host or device arrays, float32 or float64, ndim <= 1. */
 FP_API fp_status fp_jvp(const fp_op *op, const fp_workspace *ws,
                         const fp_array *dx, double dgamma,
                         const fp_array *dparams, fp_array *dout);
@@ -182,6 +185,13 @@ FP_API int         fp_default_threads(void);
 FP_API fp_status fp_b200_workspace_stats(const fp_workspace *ws, int64_t *kernel_launches,
                                          int64_t *step_launches);
 
+/* Workspaces take their device memory from a stream-ordered pool per device
+ * and their pinned host memory from a cache, so creating and freeing one
+ * (once per call when fp_prox gets ws = NULL) never synchronises the whole
+ * device. Freed memory stays cached for the next workspace; this returns it
+ * all to the driver. */
+FP_API void fp_b200_release_cached(void);
+
 /* Ragged batches and continuous batching (no counterpart in the reference,
  * whose calls take one array shape each). An fp_b200_batch solves isotropic
  * 2D TV (an operator from fp_op_tv_iso, unit or axis weights, no pixel
@@ -200,20 +210,27 @@ FP_API fp_status fp_b200_workspace_stats(const fp_workspace *ws, int64_t *kernel
  * captured CUDA graph) until at least one image has finished or none is live;
  * writes the finished images' z, and their slots, gaps and iterations (a
  * negative count: stopped at max_iter) into arrays of max_images entries;
- * *nlive, the images still iterating. All calls on one batch run on its
- * stream (set_stream; NULL by default) and must not overlap. */
+ * *nlive, the images still iterating. max_chunks > 0 bounds the chunks of
+ * `steps` iterations one run may take (it may then return with none
+ * finished, so that a serving loop can admit new images in between). All
+ * calls on one batch run on its stream (set_stream; NULL by default) and
+ * must not overlap. */
 typedef struct fp_b200_batch fp_b200_batch;
 FP_API fp_status fp_b200_batch_create(const fp_op *op, int64_t max_images, int64_t max_pixels, int dtype,
                                       fp_b200_batch **out);
 FP_API void      fp_b200_batch_free(fp_b200_batch *bt);
 FP_API fp_status fp_b200_batch_set_stream(fp_b200_batch *bt, void *stream);
+/* Whether runs replay captured CUDA graphs (the default) or launch their
+ * kernels one by one; a capture that fails (other threads using the device)
+ * falls back to launches by itself. */
+FP_API fp_status fp_b200_batch_set_graphs(fp_b200_batch *bt, int on);
 /* Rows per tile of images admitted from now on (0: chosen from the image
  * height); the tuner sets it. */
 FP_API fp_status fp_b200_batch_set_rows(fp_b200_batch *bt, int rows);
 FP_API fp_status fp_b200_batch_admit(fp_b200_batch *bt, const void *x, int64_t height, int64_t width, double gamma,
                                      double tol, int max_iter, void *z, int *slot);
-FP_API fp_status fp_b200_batch_run(fp_b200_batch *bt, int steps, int *finished, double *gaps, int *iters,
-                                   int *nfinished, int *nlive);
+FP_API fp_status fp_b200_batch_run(fp_b200_batch *bt, int steps, int max_chunks, int *finished, double *gaps,
+                                   int *iters, int *nfinished, int *nlive);
 FP_API fp_status fp_b200_batch_stats(const fp_b200_batch *bt, int64_t *kernel_launches, int64_t *steps,
                                      int64_t *free_pixels);
 

@@ -186,6 +186,18 @@ def vjp(res: Result, g, nparams: int):
     return gx, gg.value, gp
 
 
+def jvp(res: Result, dx, dgamma: float, dparams=None):
+    """fp_jvp at a kept Result: dz for the direction (dx, dgamma, dparams);
+    dx or dparams None reads as zero."""
+    L = lib()
+    dz = np.empty_like(res.z)
+    dxa = None if dx is None else _Arr(np.ascontiguousarray(dx, res.z.dtype))
+    dpa = None if dparams is None else _Arr(np.ascontiguousarray(dparams, np.float64))
+    _check(L.fp_jvp(res._op, res._ws, None if dxa is None else dxa.ref(), float(dgamma),
+                    None if dpa is None else dpa.ref(), _Arr(dz).ref()), "fp_jvp")
+    return dz
+
+
 def release(res: Result):
     L = lib()
     if getattr(res, "_ws", None) is not None:

@@ -75,3 +75,26 @@ def test_alone_equals_in_the_mix_and_continuous_admission(cuda):
     for k in range(len(imgs)):
         z, gap, it, conv = res[k]
         assert torch.equal(z, alone[k][0]) and it == alone[k][2] and gap == alone[k][1], SHAPES[k]
+
+
+def test_bounded_runs_give_the_same_results(cuda):
+    """max_chunks = 1: each run takes one chunk and may finish nothing; the
+    images' results are the same bits as with unbounded runs."""
+    import torch
+    from fastprox_b200.batch import RaggedBatch
+    imgs = _images(cuda)
+    b = RaggedBatch(max_images=16, max_pixels=200_000)
+    slots = [b.admit(x, g, t, max_iter=5000) for x, g, t in imgs]
+    ref = _run_all(b)
+    ref = [ref[s] for s in slots]
+    b = RaggedBatch(max_images=16, max_pixels=200_000)
+    owner = {b.admit(x, g, t, max_iter=5000): k for k, (x, g, t) in enumerate(imgs)}
+    res, empty_runs = {}, 0
+    while b.pending:
+        out = b.run(steps=8, max_chunks=1)
+        empty_runs += not out
+        for slot, z, gap, it, conv in out:
+            res[owner.pop(slot)] = (z, gap, it, conv)
+    assert empty_runs > 0
+    for k in range(len(imgs)):
+        assert torch.equal(res[k][0], ref[k][0]) and res[k][1:] == ref[k][1:], SHAPES[k]
