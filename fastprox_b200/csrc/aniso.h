@@ -84,6 +84,8 @@ __device__ __forceinline__ void check_done(AnState &s, double gp, double target)
 int an_pixel_blocks(const AnGeom &g);
 cudaError_t aniso_setup(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, const void *x,
                         cudaStream_t s);
+// Kernel attributes the rounds need, set before the first capture or launch.
+void aniso_prepare(int dtype);
 cudaError_t aniso_round(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s,
                         int64_t *launches);
 cudaError_t aniso_output(int dtype, const AnGeom &g, const AnBuffers &bf, void *out, cudaStream_t s);

@@ -518,6 +518,13 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     ws->max_part = std::max(iso_setup_blocks(g), ws->shape_.gx * ws->shape_.gy);
     ws->max_part = std::max(ws->max_part, 4096);
     if (op->kind == kAniso) {
+        // the untiled fibre passes: a block of 128 fibres per partial, three
+        // axes in one launch for FDPG-3
+        int64_t nfmax = 0;
+        for (int a = 0; a < g.k; ++a) nfmax = std::max<int64_t>(nfmax, g.N / std::max<int64_t>(g.L[a], 1));
+        ws->max_part = (int)std::max<int64_t>(ws->max_part, 3 * ((nfmax + 127) / 128));
+    }
+    if (op->kind == kAniso) {
         A((void **)&ws->an_img, (size_t)B * sizeof(AnImage));
         A((void **)&ws->an_st, (size_t)B * sizeof(AnState));
         A(&ws->an_scratch, img);
@@ -995,6 +1002,7 @@ fp_status run_aniso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *z
     if (e == cudaSuccess) e = aniso_setup(ws->dtype, g, c, bf, xsrc, s);
     if (e != cudaSuccess) return cuda_status(e);
     int64_t launches = 5;
+    aniso_prepare(ws->dtype);
     // rounds of launches (an iteration each, with its check, polish and
     // retirement), the live count read back behind two rounds in flight
     int slot = 0, inflight = 0;

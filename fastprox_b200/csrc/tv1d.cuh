@@ -12,8 +12,11 @@
 // the worst case (long ramps) is quadratic.
 //
 // The input is read through a functor in(i) (a fiber of a sum of arrays,
-// say) and the output written through out(i, v), so passes can fuse their
-// operands without staging them.
+// say) and the output written through a sink: segment(k0, k1, v) sets entries
+// k0..k1 to v, and finish(n) runs once at the end. EagerSink writes every
+// entry through out(i, v) at once; a sink may also note the segment's end only
+// and fill the entries in finish, so that the threads of a warp do not wait
+// on one another's long write loops at every jump.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -22,21 +25,30 @@
 
 namespace fpb {
 
+template <class Out>
+struct EagerSink {
+    Out out;
+    __device__ __forceinline__ void segment(int k0, int k1, double v) const {
+        for (int i = k0; i <= k1; ++i) out(i, v);
+    }
+    __device__ __forceinline__ void finish(int) const {}
+};
+
 // Condat's scan over a piece of m entries, radius(e) on edge (e, e + 1);
 // radius(m - 1) is read but does not change the result.
-template <class In, class Out, class R>
-__device__ void condat_piece(const In &in, const Out &out, int64_t m, const R &radius) {
+template <class In, class Sink, class R>
+__device__ void condat_piece(const In &in, const Sink &out, int m, const R &radius) {
     if (m == 1) {
-        out(0, in(0));
+        out.segment(0, 0, in(0));
         return;
     }
-    int64_t k = 0, k0 = 0, km = 0, kp = 0;
+    int k = 0, k0 = 0, km = 0, kp = 0;
     double lk = radius(0);
     const double y0 = in(0);
     double vmin = y0 - lk, vmax = y0 + lk;
     double umin = lk, umax = -lk;
     auto jump_down = [&]() {  // closes [k0, km] at vmin; the edge km carries +radius
-        for (int64_t i = k0; i <= km; ++i) out(i, vmin);
+        out.segment(k0, km, vmin);
         const double le = radius(km);
         k = k0 = kp = km = km + 1;
         lk = radius(k);
@@ -47,7 +59,7 @@ __device__ void condat_piece(const In &in, const Out &out, int64_t m, const R &r
         umax = -lk;
     };
     auto jump_up = [&]() {  // closes [k0, kp] at vmax; the edge kp carries -radius
-        for (int64_t i = k0; i <= kp; ++i) out(i, vmax);
+        out.segment(k0, kp, vmax);
         const double le = radius(kp);
         k = k0 = km = kp = kp + 1;
         lk = radius(k);
@@ -88,7 +100,7 @@ __device__ void condat_piece(const In &in, const Out &out, int64_t m, const R &r
             jump_up();
         } else {
             const double v = vmin + umin / (double)(k - k0 + 1);
-            for (int64_t i = k0; i < m; ++i) out(i, v);
+            out.segment(k0, m - 1, v);
             return;
         }
     }
@@ -98,14 +110,14 @@ __device__ void condat_piece(const In &in, const Out &out, int64_t m, const R &r
 template <class F>
 struct Shifted {
     F f;
-    int64_t o;
-    __device__ __forceinline__ auto operator()(int64_t i) const { return f(i + o); }
+    int o;
+    __device__ __forceinline__ auto operator()(int i) const { return f(i + o); }
 };
-template <class F>
-struct ShiftedOut {
-    F f;
-    int64_t o;
-    __device__ __forceinline__ void operator()(int64_t i, double v) const { f(i + o, v); }
+template <class S>
+struct ShiftedSink {
+    S s;
+    int o;
+    __device__ __forceinline__ void segment(int k0, int k1, double v) const { s.segment(k0 + o, k1 + o, v); }
 };
 
 // prox of lam * sum_e w(e) |z_{e+1} - z_e| on one fiber of n entries, w(e)
@@ -114,51 +126,68 @@ struct ShiftedOut {
 // clamped at 2 j range, a bound that an edge can never reach
 // (src/ops/tv1d.cpp:238-246); no edge active past (n / 2) range gives the
 // constant mean.
-template <class In, class Out, class Wt>
-__device__ void tv1d_fiber(const In &in, const Out &out, int64_t n, double lam, bool has_w, const Wt &w) {
+template <class In, class Sink, class Wt>
+__device__ void tv1d_fiber_sink(const In &in, const Sink &out, int n, double lam, bool has_w, const Wt &w) {
     double lo = in(0), hi = lo;
-    for (int64_t i = 1; i < n; ++i) {
+    bool cut = false;  // a zero-weight edge
+    for (int i = 1; i < n; ++i) {
         const double v = in(i);
         lo = v < lo ? v : lo;
         hi = v > hi ? v : hi;
+        if (has_w) cut = cut || w(i - 1) == 0.0;
     }
     const double range = hi - lo;
     if (n == 1 || lam == 0.0 || range == 0.0) {
-        for (int64_t i = 0; i < n; ++i) out(i, in(i));
+        for (int i = 0; i < n; ++i) out.segment(i, i, in(i));
+        out.finish(n);
         return;
     }
     if (!has_w) {
         if (lam >= (double)(n / 2) * range) {
             double s = 0.0;
-            for (int64_t i = 0; i < n; ++i) s += in(i);
-            const double v = s / (double)n;
-            for (int64_t i = 0; i < n; ++i) out(i, v);
+            for (int i = 0; i < n; ++i) s += in(i);
+            out.segment(0, n - 1, s / (double)n);
+            out.finish(n);
             return;
         }
         const double cap = 2.0 * (double)((n / 2) > 0 ? (n / 2) : 1) * range;
         const double l = lam < cap ? lam : cap;
-        condat_piece(in, out, n, [l](int64_t) { return l; });
+        condat_piece(in, out, n, [l](int) { return l; });
+        out.finish(n);
         return;
     }
-    int64_t s = 0;
-    for (int64_t e = 0; e < n; ++e) {
-        if (e == n - 1 || w(e) == 0.0) {
-            const int64_t m = e - s + 1;
-            auto rad = [&](int64_t j) -> double {
-                if (j >= m - 1) return 0.0;
-                const double r = lam * w(s + j);
-                const int64_t jj = (j + 1 < m - 1 - j) ? j + 1 : m - 1 - j;
-                const double cap = 2.0 * (double)(jj > 0 ? jj : 1) * range;
-                return r < cap ? r : cap;
-            };
-            condat_piece(Shifted<In>{in, s}, ShiftedOut<Out>{out, s}, m, rad);
-            s = e + 1;
+    auto piece = [&](int s, int m) {
+        auto rad = [&](int j) -> double {
+            if (j >= m - 1) return 0.0;
+            const double r = lam * w(s + j);
+            const int jj = (j + 1 < m - 1 - j) ? j + 1 : m - 1 - j;
+            const double cap = 2.0 * (double)(jj > 0 ? jj : 1) * range;
+            return r < cap ? r : cap;
+        };
+        condat_piece(Shifted<In>{in, s}, ShiftedSink<Sink>{out, s}, m, rad);
+    };
+    if (!cut) {
+        piece(0, n);
+    } else {
+        int s = 0;
+        for (int e = 0; e < n; ++e) {
+            if (e == n - 1 || w(e) == 0.0) {
+                piece(s, e - s + 1);
+                s = e + 1;
+            }
         }
     }
+    out.finish(n);
+}
+
+// The same with the result written through out(i, v) as it is found.
+template <class In, class Out, class Wt>
+__device__ void tv1d_fiber(const In &in, const Out &out, int n, double lam, bool has_w, const Wt &w) {
+    tv1d_fiber_sink(in, EagerSink<Out>{out}, n, lam, has_w, w);
 }
 
 struct NoWeight {
-    __device__ __forceinline__ double operator()(int64_t) const { return 1.0; }
+    __device__ __forceinline__ double operator()(int) const { return 1.0; }
 };
 
 }  // namespace fpb

@@ -23,8 +23,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 
 #include "aniso.h"
 #include "common.cuh"
@@ -235,9 +237,9 @@ __device__ __forceinline__ void fibre_prox(const AnCall &c, const AnBuffers &bf,
                                            double lam, const In &in, const Out &out) {
     if (c.has_beta) {
         const T *bw = static_cast<const T *>(bf.beta) + (int64_t)a * c.N + base;
-        tv1d_fiber(in, out, fb.L, lam, true, BetaW<T>{bw, fb.s});
+        tv1d_fiber(in, out, (int)fb.L, lam, true, BetaW<T>{bw, fb.s});
     } else {
-        tv1d_fiber(in, out, fb.L, lam, false, NoWeight{});
+        tv1d_fiber(in, out, (int)fb.L, lam, false, NoWeight{});
     }
 }
 
@@ -319,6 +321,295 @@ __global__ void __launch_bounds__(128) an_pass2(AnGeom g, AnCall c, AnBuffers bf
     s2.beta = (t - 1.0) / tn;
     s2.tn = tn;
     if (s2.it == s2.chk_next || s2.it == c.max_iter) s2.stage = kStCheck;
+    bf.st[b] = s2;
+}
+
+// ---------------------------------------------------------------------------
+// Fibre tiles in shared memory
+// ---------------------------------------------------------------------------
+//
+// A thread walking one fibre through global memory waits a memory latency at
+// every step of Condat's scan (each step depends on the last), and a batch has
+// only as many fibres as rows or columns: the passes above run latency-bound
+// at a few percent of the memory bandwidth. The tiled passes copy the inputs of
+// fb fibres (and their edge weights) into shared memory first, with loads
+// that do not depend on one another and are coalesced (along the fibre when
+// fibres are contiguous, across fibres otherwise), run the scans out of shared
+// memory (the result overwrites the input: Condat never reads back an entry it
+// has written), and store the results the same way. A tile is L x (fb + 1)
+// entries (the odd row length keeps both copy directions free of bank
+// conflicts; thread t of the scan always reads bank t + i mod 32). The values
+// and their order of operations are those of the untiled passes.
+
+struct TileCfg {
+    int fb[3];  // fibres per block along each axis (0: the axis does not fit)
+};
+
+template <class T>
+struct TileIn {
+    const T *s;
+    int P, t;
+    __device__ __forceinline__ double operator()(int i) const { return (double)s[i * P + t]; }
+};
+// A segment writes its value at its last entry and marks it (one bit per
+// entry, word i / 32 of the fibre's column); finish fills each segment's
+// other entries from its end, backwards, and clears the marks.
+template <class T>
+struct TileSink {
+    T *s;
+    unsigned *m;
+    int P, t;
+    __device__ __forceinline__ void segment(int, int k1, double v) const {
+        s[k1 * P + t] = (T)v;
+        m[(k1 >> 5) * P + t] |= 1u << (k1 & 31);
+    }
+    __device__ __forceinline__ void finish(int n) const {
+        T v = T(0);
+        for (int w = (n - 1) >> 5; w >= 0; --w) {
+            const unsigned bits = m[w * P + t];
+            m[w * P + t] = 0u;
+            const int top = (w << 5) + 31 < n - 1 ? (w << 5) + 31 : n - 1;
+            for (int i = top; i >= (w << 5); --i) {
+                const int j = i * P + t;
+                if (bits & (1u << (i & 31))) v = s[j];
+                else s[j] = v;
+            }
+        }
+    }
+};
+
+// tile[i][r] = ld(o) for the block's nv fibres, o the entry's offset in the image
+template <class T, class Ld>
+__device__ __forceinline__ void tile_load(T *tile, int P, const Fib &fb, int64_t f0, int nv, const Ld &ld) {
+    const int L = (int)fb.L, n = nv * L;
+    if (fb.s == 1) {
+        for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+            const int r = idx / L, i = idx - r * L;
+            tile[i * P + r] = ld(fb.base(f0 + r) + i);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+            const int i = idx / nv, r = idx - i * nv;
+            tile[i * P + r] = ld(fb.base(f0 + r) + (int64_t)i * fb.s);
+        }
+    }
+}
+
+// st(o, tile[i][r]) for the block's nv fibres, in the order of tile_load
+template <class T, class St>
+__device__ __forceinline__ void tile_store(const T *tile, int P, const Fib &fb, int64_t f0, int nv, const St &st) {
+    const int L = (int)fb.L, n = nv * L;
+    if (fb.s == 1) {
+        for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+            const int r = idx / L, i = idx - r * L;
+            st(fb.base(f0 + r) + i, tile[i * P + r]);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+            const int i = idx / nv, r = idx - i * nv;
+            st(fb.base(f0 + r) + (int64_t)i * fb.s, tile[i * P + r]);
+        }
+    }
+}
+
+// The tiles of a block in shared memory: the fibres' inputs (then results),
+// their edge weights when there are any, and one mark bit per entry.
+template <class T>
+struct Tiles {
+    T *in, *w;
+    unsigned *mk;
+    __device__ __forceinline__ Tiles(unsigned char *smem, const AnCall &c, int L, int P) {
+        in = reinterpret_cast<T *>(smem);
+        w = in + L * P;
+        mk = reinterpret_cast<unsigned *>(in + (c.has_beta ? 2 : 1) * L * P);
+        const int nw = ((L + 31) >> 5) * P;
+        for (int i = threadIdx.x; i < nw; i += blockDim.x) mk[i] = 0u;
+    }
+};
+
+// Shared-memory bytes of a tile of fb fibres of L entries.
+__host__ __device__ __forceinline__ size_t tile_bytes(int L, int fb, int nbuf, size_t tsize) {
+    const size_t P = (size_t)fb + 1;
+    return (size_t)nbuf * tsize * (size_t)L * P + 4 * (((size_t)L + 31) / 32) * P;
+}
+
+// The scans of a loaded tile (edge weights in the second tile when present).
+template <class T>
+__device__ __forceinline__ void tile_scan(const AnCall &c, const Tiles<T> &tl, int P, int nv, int L, double lam) {
+    const int t = threadIdx.x;
+    if (t >= nv) return;
+    const TileIn<T> in{tl.in, P, t};
+    const TileSink<T> out{tl.in, tl.mk, P, t};
+    if (c.has_beta) tv1d_fiber_sink(in, out, L, lam, true, TileIn<T>{tl.w, P, t});
+    else tv1d_fiber_sink(in, out, L, lam, false, NoWeight{});
+}
+
+constexpr int kTileThreads = 32;
+
+// an_pass1 on tiles
+template <class T>
+__global__ void __launch_bounds__(kTileThreads) an_pass1_tile(AnGeom g, AnCall c, AnBuffers bf, TileCfg tc) {
+    extern __shared__ __align__(16) unsigned char an_smem[];
+    const int b = blockIdx.y;
+    const AnState &st = bf.st[b];
+    if (st.status != kLive || st.stage != kStIter) return;
+    const AnImage &im = bf.img[b];
+    if (im.mode != kAnAdbpg) return;
+    const int a = im.a1;
+    const Fib fb = fibers(g, a);
+    const int FB = tc.fb[a];
+    const int64_t f0 = (int64_t)blockIdx.x * FB;
+    if (f0 >= fb.nfib) return;
+    const int nv = (int)(fb.nfib - f0 < FB ? fb.nfib - f0 : FB), P = FB + 1;
+    const Tiles<T> tl(an_smem, c, (int)fb.L, P);
+    const int64_t N = g.N;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *Wv = static_cast<const T *>(bf.wv) + (int64_t)b * g.k * N;
+    tile_load(tl.in, P, fb, f0, nv, [D, Wv](int64_t o) { return (T)(D[o] + Wv[o]); });
+    if (c.has_beta) {
+        const T *bw = static_cast<const T *>(bf.beta) + (int64_t)a * c.N;
+        tile_load(tl.w, P, fb, f0, nv, [bw](int64_t o) { return bw[o]; });
+    }
+    __syncthreads();
+    tile_scan(c, tl, P, nv, (int)fb.L, im.lam[a]);
+    __syncthreads();
+    T *U = static_cast<T *>(bf.u) + (int64_t)b * N;
+    tile_store(tl.in, P, fb, f0, nv, [U](int64_t o, T v) { U[o] = v; });
+}
+
+// an_pass2 on tiles, with the dual update, the extrapolation and the restart
+// logic of an_pass2
+template <class T>
+__global__ void __launch_bounds__(kTileThreads) an_pass2_tile(AnGeom g, AnCall c, AnBuffers bf, TileCfg tc) {
+    extern __shared__ __align__(16) unsigned char an_smem[];
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const AnState st = bf.st[b];
+    if (st.status != kLive || st.stage != kStIter) return;
+    const AnImage &im = bf.img[b];
+    if (im.mode != kAnAdbpg) return;
+    const int a = im.a2;
+    const Fib fb = fibers(g, a);
+    const int FB = tc.fb[a];
+    const int64_t f0 = (int64_t)blockIdx.x * FB;
+    const int64_t N = g.N;
+    const bool test = st.it % kCheck == 0;
+    const T beta = (T)st.beta;
+    double up = 0.0;
+    if (f0 < fb.nfib) {
+        const int nv = (int)(fb.nfib - f0 < FB ? fb.nfib - f0 : FB), P = FB + 1;
+        const Tiles<T> tl(an_smem, c, (int)fb.L, P);
+        const T *U = static_cast<const T *>(bf.u) + (int64_t)b * N;
+        T *Wv = static_cast<T *>(bf.wv) + (int64_t)b * g.k * N;
+        T *Y = static_cast<T *>(bf.y) + (int64_t)b * g.k * N;
+        T *Z = static_cast<T *>(bf.z) + (int64_t)b * N;
+        tile_load(tl.in, P, fb, f0, nv, [U, Wv](int64_t o) { return (T)(U[o] - Wv[o]); });
+        if (c.has_beta) {
+            const T *bw = static_cast<const T *>(bf.beta) + (int64_t)a * c.N;
+            tile_load(tl.w, P, fb, f0, nv, [bw](int64_t o) { return bw[o]; });
+        }
+        __syncthreads();
+        tile_scan(c, tl, P, nv, (int)fb.L, im.lam[a]);
+        __syncthreads();
+        tile_store(tl.in, P, fb, f0, nv, [&](int64_t o, T z) {
+            const T v = U[o] - Wv[o];
+            const T yn = z - v;
+            const T y = Y[o], w = Wv[o];
+            if (test) up += (double)((w - yn) * (yn - y));
+            Wv[o] = yn + beta * (yn - y);
+            Y[o] = yn;
+            Z[o] = z;
+        });
+    }
+    double dot, unused;
+    if (!reduce2(bf, b, blockIdx.x, gridDim.x, test ? up : 0.0, 0.0, sh, &flag, dot, unused)) return;
+    AnState s2 = st;
+    s2.since += 1;
+    double t = s2.tn;
+    if (test && dot > 0.0 && s2.since >= s2.last) {
+        s2.last = s2.since;
+        s2.since = 0;
+        s2.restart = 1;
+        t = 1.0;
+    } else {
+        s2.restart = 0;
+    }
+    s2.it += 1;
+    const double tn = fista_t(t);
+    s2.beta = (t - 1.0) / tn;
+    s2.tn = tn;
+    if (s2.it == s2.chk_next || s2.it == c.max_iter) s2.stage = kStCheck;
+    bf.st[b] = s2;
+}
+
+// an_fdpg3_pass on tiles (blockIdx.y = axis)
+template <class T>
+__global__ void __launch_bounds__(kTileThreads) an_fdpg3_tile(AnGeom g, AnCall c, AnBuffers bf, TileCfg tc) {
+    extern __shared__ __align__(16) unsigned char an_smem[];
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.z;
+    const AnState st = bf.st[b];
+    if (st.status != kLive || st.stage != kStIter) return;
+    const AnImage &im = bf.img[b];
+    if (im.mode != kAnFdpg3) return;
+    const int64_t N = g.N;
+    const bool test = st.it % kCheck == 0;
+    const T beta = (T)st.beta;
+    double up = 0.0;
+    const int a = blockIdx.y;
+    const Fib fb = fibers(g, a);
+    const int FB = tc.fb[a];
+    const int64_t f0 = (int64_t)blockIdx.x * FB;
+    if (f0 < fb.nfib) {
+        const int nv = (int)(fb.nfib - f0 < FB ? fb.nfib - f0 : FB), P = FB + 1;
+        const Tiles<T> tl(an_smem, c, (int)fb.L, P);
+        const T *U = static_cast<const T *>(bf.u) + (int64_t)b * N;
+        T *Wa = static_cast<T *>(bf.wv) + ((int64_t)b * 3 + a) * N;
+        T *Ya = static_cast<T *>(bf.y) + ((int64_t)b * 3 + a) * N;
+        // the three axes write disjoint scratch: zp (a = 0), z (a = 1), dual slot (a = 2)
+        T *Za = static_cast<T *>(bf.zp) + (int64_t)b * N;
+        if (a == 1) Za = static_cast<T *>(bf.z) + (int64_t)b * N;
+        if (a == 2) Za = static_cast<T *>(bf.scratch) + (int64_t)b * N;
+        tile_load(tl.in, P, fb, f0, nv, [U, Wa](int64_t o) { return (T)(U[o] - T(3) * Wa[o]); });
+        if (c.has_beta) {
+            const T *bw = static_cast<const T *>(bf.beta) + (int64_t)a * c.N;
+            tile_load(tl.w, P, fb, f0, nv, [bw](int64_t o) { return bw[o]; });
+        }
+        __syncthreads();
+        tile_scan(c, tl, P, nv, (int)fb.L, 3.0 * im.lam[a]);
+        __syncthreads();
+        tile_store(tl.in, P, fb, f0, nv, [&](int64_t o, T z) {
+            const T v = U[o] - T(3) * Wa[o];
+            const T yn = (z - v) / T(3);
+            const T y = Ya[o], w = Wa[o];
+            if (test) up += (double)((w - yn) * (yn - y));
+            Wa[o] = yn + beta * (yn - y);
+            Ya[o] = yn;
+            Za[o] = z;
+        });
+    }
+    double dot, unused;
+    const unsigned nblk = gridDim.x * gridDim.y;
+    const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
+    if (!reduce2(bf, b, blk, nblk, test ? up : 0.0, 0.0, sh, &flag, dot, unused)) return;
+    AnState s2 = st;
+    s2.since += 1;
+    double t = s2.tn;
+    if (test && dot > 0.0 && s2.since >= s2.last) {
+        s2.last = s2.since;
+        s2.since = 0;
+        s2.restart = 1;
+        t = 1.0;
+    } else {
+        s2.restart = 0;
+    }
+    s2.it += 1;
+    const double tn = fista_t(t);
+    s2.beta = (t - 1.0) / tn;
+    s2.tn = tn;
+    if (s2.it % kCheck == 0 || s2.it == c.max_iter) s2.stage = kStCheck;
     bf.st[b] = s2;
 }
 
@@ -853,6 +1144,56 @@ cudaError_t setup_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, const
     return cudaGetLastError();
 }
 
+// Fibres per tile along each axis: the most (1, 2, 4, ...) up to a cap whose
+// tile fits a budget (several blocks to an SM: at this latency-bound scan,
+// more warps beat fuller ones), else one fibre in up to 200 KB; 0 when even
+// that does not fit (the untiled pass then runs).
+constexpr int kTileSmemMax = 200 * 1024;
+
+// The tiled kernels may take up to kTileSmemMax of dynamic shared memory. Set
+// once per kernel, before any launch: the attribute is per function, and
+// threads launching with different sizes must not lower it under one another.
+template <class T>
+void tile_attributes() {
+    static std::atomic<unsigned long long> done{0};  // one bit per device
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    const unsigned long long bit = 1ull << dev;
+    if (done.load() & bit) return;
+    cudaFuncSetAttribute(an_pass1_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemMax);
+    cudaFuncSetAttribute(an_pass2_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemMax);
+    cudaFuncSetAttribute(an_fdpg3_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemMax);
+    done.fetch_or(bit);
+}
+template <class T>
+TileCfg tile_cfg(const AnGeom &g, const AnCall &c, size_t &smem) {
+    // fibres per block: at most fb_max, and tiles of at most budget bytes
+    // (tuning hints FASTPROX_B200_TILE_FB and FASTPROX_B200_TILE_KB)
+    static const int fb_max = [] {
+        const char *v = std::getenv("FASTPROX_B200_TILE_FB");
+        const int f = v ? std::atoi(v) : 0;
+        return (f >= 1 && f <= 32) ? f : 4;
+    }();
+    static const size_t budget = [] {
+        const char *v = std::getenv("FASTPROX_B200_TILE_KB");
+        const int k = v ? std::atoi(v) : 0;
+        return (size_t)((k >= 8 && k <= 200) ? k : 48) * 1024;
+    }();
+    TileCfg tc{{0, 0, 0}};
+    smem = 0;
+    const int nbuf = c.has_beta ? 2 : 1;
+    for (int a = 0; a < g.k; ++a) {
+        const int L = (int)g.L[a];
+        auto bytes = [&](int fb) { return tile_bytes(L, fb, nbuf, sizeof(T)); };
+        int fb = 1;
+        while (fb * 2 <= fb_max && bytes(fb * 2) <= budget) fb *= 2;
+        if (bytes(fb) > (size_t)kTileSmemMax) fb = 0;
+        tc.fb[a] = fb;
+        if (fb) smem = std::max(smem, bytes(fb));
+    }
+    return tc;
+}
+
 template <class T>
 cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s, int64_t *launches) {
     const unsigned B = (unsigned)g.B;
@@ -866,13 +1207,40 @@ cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaS
     for (int a = 0; a < g.k; ++a) nfmax = std::max(nfmax, nf[a]);
     const unsigned fbk = (unsigned)((nfmax + 127) / 128);
     if (c.has_adbpg) {
-        an_pass1<T><<<dim3(fbk, B), 128, 0, s>>>(g, c, bf);
-        an_pass2<T><<<dim3(fbk, B), 128, 0, s>>>(g, c, bf);
+        size_t smem = 0;
+        const TileCfg tc = tile_cfg<T>(g, c, smem);
+        bool tiled = true;
+        int64_t tblk = 0;
+        for (int a = 0; a < g.k; ++a) {
+            if (g.L[a] > 1 && tc.fb[a] == 0) tiled = false;
+            if (tc.fb[a]) tblk = std::max<int64_t>(tblk, (nf[a] + tc.fb[a] - 1) / tc.fb[a]);
+        }
+        if (tiled && tblk > 0 && tblk <= bf.max_part) {
+            tile_attributes<T>();
+            an_pass1_tile<T><<<dim3((unsigned)tblk, B), kTileThreads, smem, s>>>(g, c, bf, tc);
+            an_pass2_tile<T><<<dim3((unsigned)tblk, B), kTileThreads, smem, s>>>(g, c, bf, tc);
+        } else {
+            an_pass1<T><<<dim3(fbk, B), 128, 0, s>>>(g, c, bf);
+            an_pass2<T><<<dim3(fbk, B), 128, 0, s>>>(g, c, bf);
+        }
         nl += 2;
     }
     if (c.has_fdpg3) {
         an_fdpg3_u<T><<<pg, kThreads, 0, s>>>(g, bf);
-        an_fdpg3_pass<T><<<dim3(fbk, 3, B), 128, 0, s>>>(g, c, bf);
+        size_t smem = 0;
+        const TileCfg tc = tile_cfg<T>(g, c, smem);
+        int64_t tblk = 0;
+        bool tiled = g.k == 3;
+        for (int a = 0; a < g.k; ++a) {
+            if (tc.fb[a] == 0) tiled = false;
+            else tblk = std::max<int64_t>(tblk, (nf[a] + tc.fb[a] - 1) / tc.fb[a]);
+        }
+        if (tiled && tblk > 0 && 3 * tblk <= bf.max_part) {
+            tile_attributes<T>();
+            an_fdpg3_tile<T><<<dim3((unsigned)tblk, 3, B), kTileThreads, smem, s>>>(g, c, bf, tc);
+        } else {
+            an_fdpg3_pass<T><<<dim3(fbk, 3, B), 128, 0, s>>>(g, c, bf);
+        }
         nl += 2;
     }
     an_restart_copy<T><<<pg, kThreads, 0, s>>>(g, bf);
@@ -918,6 +1286,11 @@ int an_pixel_blocks(const AnGeom &g) {
 cudaError_t aniso_setup(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, const void *x,
                         cudaStream_t s) {
     return dtype == 1 ? setup_t<float>(g, c, bf, x, s) : setup_t<double>(g, c, bf, x, s);
+}
+
+void aniso_prepare(int dtype) {
+    if (dtype == 1) tile_attributes<float>();
+    else tile_attributes<double>();
 }
 
 cudaError_t aniso_round(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s,
