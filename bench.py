@@ -168,10 +168,16 @@ def profile_case(kind="iso"):
     solved for exactly 8 iterations: launch 0 is the cold start, launches 4
     and 8 carry gap checks, the rest are plain iterations. aniso: 16 of its
     images, anisotropic with edge weights, solved to gap 1e-6 (every kernel of
-    the method, polish included)."""
+    the method, polish included). iso3d: 8 volumes of 128^3 for 8 iterations."""
     import torch
 
     from fastprox_b200 import TVAniso, TVIso, synth
+    if kind == "iso3d":
+        x = torch.as_tensor(synth.phantom3d(8, 128, 128, 128, seed=0), device="cuda")
+        z, info = TVIso(3).solve(x, 0.1, tol=0.0, max_iter=8, with_dual=False)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": "iso3d", "iters": int(info.iters)}))
+        return
     if kind == "aniso":
         B = 16
         x = torch.as_tensor(synth.phantom(B, 512, 512, seed=0), device="cuda")
@@ -197,10 +203,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--profile-case", nargs="?", const="iso", default=None, choices=["iso", "aniso"],
+    ap.add_argument("--profile-case", nargs="?", const="iso", default=None, choices=["iso", "aniso", "iso3d"],
                     help="iso: one solve of the benchmark batch with 8 iterations (tol 0); aniso: 16 images "
-                         "anisotropic to gap 1e-6; the cases for ncu captures")
-    ap.add_argument("--workload", default="iso512", choices=["iso512", "aniso512", "uneven", "vjp", "serve"],
+                         "anisotropic to gap 1e-6; iso3d: 8 x 128^3 with 8 iterations; the cases for ncu captures")
+    ap.add_argument("--workload", default="iso512", choices=["iso512", "aniso512", "iso3d", "uneven", "vjp", "serve"],
                     help="iso512 (default, the headline line); the others report the other workloads")
     ap.add_argument("--serve-seconds", type=float, default=20.0)
     ap.add_argument("--serve-workers", type=int, default=4, help="worker streams for anisotropic and 3D requests")

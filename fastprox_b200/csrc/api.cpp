@@ -552,6 +552,8 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     A((void **)&ws->gammas, (size_t)B * sizeof(double));
     A((void **)&ws->part, (size_t)B * (size_t)ws->max_part * 2 * sizeof(double));
     A((void **)&ws->ticket, (size_t)B * sizeof(unsigned));
+    A((void **)&ws->lmap, (size_t)B * sizeof(int));
+    A((void **)&ws->lcnt, sizeof(int));
     A((void **)&ws->live, 16);
     A((void **)&ws->err, 16);
     auto H = [&](void **p, size_t bytes) { host.add(p, bytes); };
@@ -916,14 +918,18 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     if (e != cudaSuccess) return cuda_status(e);
     // The iteration: chunks of launches, each followed by a read of the live
     // count; two chunks in flight so the device never waits for the host.
+    // Once fewer images are live than the launches cover, the launches cover
+    // a list of the live ones (images only retire, so a list built after the
+    // count was read holds every image still live): the tail of a batch, where
+    // a few slow images remain, launches only their blocks.
     const int chunk = ws->chunk > 0 ? ws->chunk : 8;
     int par = 0, slot = 0, inflight = 0;
-    int64_t launched = 0;
+    int64_t launched = 0, lists = 0, nimg = g.B;
     const int64_t cap = (int64_t)max_iter + 1 + 2 * chunk;
     bool done = false;
     while (!done) {
         for (int j = 0; j < chunk; ++j) {
-            e = iso_step(ws->dtype, g, c, bf, ws->shape_, par, iso_variant(launched, max_iter, warm), s);
+            e = iso_step(ws->dtype, g, c, bf, ws->shape_, par, iso_variant(launched, max_iter, warm), nimg, s);
             if (e != cudaSuccess) return cuda_status(e);
             par ^= 1;
             ++launched;
@@ -937,12 +943,22 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
             e = cudaEventSynchronize(ws->ev[slot]);
             if (e != cudaSuccess) return cuda_status(e);
             --inflight;
-            if (ws->h_live[slot] == 0) done = true;
+            const int live = ws->h_live[slot];
+            if (live == 0) {
+                done = true;
+            } else if (live < nimg) {
+                e = iso_live_list(ws->st, g.B, ws->lmap, ws->lcnt, s);
+                if (e != cudaSuccess) return cuda_status(e);
+                bf.lmap = ws->lmap;
+                bf.lcnt = ws->lcnt;
+                nimg = live;
+                ++lists;
+            }
         }
         if (launched >= cap) done = true;
     }
     ws->launches = launched;
-    ws->kernel_launches += launched + 3 + (warm ? 1 : 0) + 1 + ((c.na == 1 && !c.has_alpha) ? 1 : 0);
+    ws->kernel_launches += launched + lists + 3 + (warm ? 1 : 0) + 1 + ((c.na == 1 && !c.has_alpha) ? 1 : 0);
     e = iso_finalize(ws->dtype, g, c, bf, zdst, s);
     return cuda_status(e);
 }

@@ -23,11 +23,17 @@ struct IsoBuffers {
     int *live = nullptr;        // images still iterating
     int *err = nullptr;         // set by a kernel whose copies never completed
     int max_part = 0;
+    // The step's images: with lmap, launch slot z runs image lmap[z] for
+    // z < *lcnt (the images still live when the list was built, in order);
+    // without, slot z runs image z.
+    const int *lmap = nullptr;
+    const int *lcnt = nullptr;
 };
 
 // Launch shape of the step kernel, picked per geometry (and by the tuner).
 struct StepShape {
-    int kind = 0;   // 0: 2D row-marching, 1: generic (one thread per pixel), 2: 2D TMA row pipeline
+    int kind = 0;   // 0: 2D row-marching, 1: generic (one thread per pixel), 2: 2D TMA row pipeline,
+                    // 4: 2D lean row-marching, 5: 3D slice-marching tiles
     int vec = 1;    // pixels per thread along the contiguous axis (march)
     int bx = 128;   // threads per block
     int rows = 16;  // rows per block (march)
@@ -41,12 +47,15 @@ int iso_setup_blocks(const Geometry &g);
 // initialisation, and the warm-start projection of the stored dual.
 cudaError_t iso_setup(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const void *x,
                       int warm, int par, cudaStream_t s);
+// The list of live images (by their states), for bf.lmap / bf.lcnt.
+cudaError_t iso_live_list(const IsoState *st, int64_t B, int *lmap, int *lcnt, cudaStream_t s);
 // One dual-FISTA iteration (and the gap / restart tests it carries) for
-// every live image, reading buffers par and writing par ^ 1.
-// variant (the lean kernel, chosen from the launch index k of a call):
+// every live image, reading buffers par and writing par ^ 1, over nimg launch
+// slots (g.B, or at least the count of bf's live list).
+// variant (the lean and 3D kernels, chosen from the launch index k of a call):
 // 1 the cold first iteration (u = v = 0), 2 a launch carrying a gap check, 0 otherwise.
 cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh,
-                     int par, int variant, cudaStream_t s);
+                     int par, int variant, int64_t nimg, cudaStream_t s);
 inline int iso_variant(int64_t k, int max_iter, bool warm) {
     if (k == 0) return warm ? 2 : 1;
     return (k % 4 == 0 || k == max_iter) ? 2 : 0;

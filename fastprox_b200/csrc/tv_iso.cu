@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 
@@ -307,11 +308,53 @@ __device__ void control(IsoState &st, const IsoImage &im, int max_iter, bool do_
     st.fin_par = par_in ^ 1;
 }
 
+// The image of launch slot z (-1: none, the live list is shorter).
+__device__ __forceinline__ int step_image(const IsoBuffers &bf, unsigned z) {
+    if (!bf.lmap) return (int)z;
+    return (int)z < *bf.lcnt ? bf.lmap[z] : -1;
+}
+
+// The live images in order: one block scans the states in chunks.
+__global__ void __launch_bounds__(1024) live_list_kernel(const IsoState *st, int64_t B, int *lmap, int *lcnt) {
+    __shared__ int wsum[32];
+    __shared__ int base;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int64_t c0 = 0; c0 < B; c0 += blockDim.x) {
+        const int64_t i = c0 + threadIdx.x;
+        const int f = (i < B && st[i].status == kLive) ? 1 : 0;
+        int x = f;  // inclusive scan in the warp
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int w = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            wsum[lane] = w;  // inclusive over warps
+        }
+        __syncthreads();
+        const int before = base + (wid > 0 ? wsum[wid - 1] : 0) + x - f;
+        if (f) lmap[before] = (int)i;
+        __syncthreads();
+        if (threadIdx.x == 0) base += wsum[(blockDim.x >> 5) - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *lcnt = base;
+}
+
 struct StepArgs {
     Geometry g;
     int max_iter;
     int par;
     int rows;
+    int64_t nimg;  // launch slots (host side: the grid's image extent)
 };
 
 // ---------------------------------------------------------------------------
@@ -332,7 +375,8 @@ template <class T, int VEC, bool ALPHA>
 __global__ void __launch_bounds__(256) iso2d_march_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     __shared__ double sh[32];
     __shared__ int flag;
-    const int b = blockIdx.z;
+    const int b = step_image(bf, blockIdx.z);
+    if (b < 0) return;
     const IsoState st = bf.st[b];
     if (st.status != kLive) return;
     const IsoImage im = bf.img[b];
@@ -679,7 +723,8 @@ template <class T, int VEC, bool ALPHA, bool GAP, bool ZIN>
 __global__ void __launch_bounds__(128) iso2d_lean_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     __shared__ double sh[32];
     __shared__ int flag;
-    const int b = blockIdx.z;
+    const int b = step_image(bf, blockIdx.z);
+    if (b < 0) return;
     const IsoState st = bf.st[b];
     if (st.status != kLive) return;
     const int it = st.it;
@@ -849,7 +894,8 @@ __global__ void __launch_bounds__(128) iso2d_tma_kernel(StepArgs A, IsoCall c, I
     __shared__ uint64_t bars[kSlots];
     __shared__ double sh[32];
     __shared__ int flag;
-    const int b = blockIdx.z;
+    const int b = step_image(bf, blockIdx.z);
+    if (b < 0) return;
     const IsoState st = bf.st[b];
     if (st.status != kLive) return;
     const IsoImage im = bf.img[b];
@@ -1073,7 +1119,8 @@ template <class T, int K, bool ALPHA>
 __global__ void __launch_bounds__(256) iso_generic_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     __shared__ double sh[32];
     __shared__ int flag;
-    const int b = blockIdx.y;
+    const int b = step_image(bf, blockIdx.y);
+    if (b < 0) return;
     const IsoState st = bf.st[b];
     if (st.status != kLive) return;
     const IsoImage im = bf.img[b];
@@ -1176,6 +1223,207 @@ __global__ void __launch_bounds__(256) iso_generic_kernel(StepArgs A, IsoCall c,
     bf.ticket[b] = 0;
     IsoState s2 = st;
     control(s2, im, A.max_iter, do_gap, test, gap, dot, pin, bf.live);
+    bf.st[b] = s2;
+}
+
+// ---------------------------------------------------------------------------
+// The 3D step: a block owns a kTY x kTX tile of the (axis 1, axis 2) plane and
+// marches along axis 0 through a chunk of A.rows slices. For each slice it
+// stages d and the dual of the next slice over the tile and a one-entry halo
+// in shared memory (three slices in rotation), forms z of the next slice over
+// the tile and its forward halo (two slices of z in rotation), and updates the
+// tile at the current slice from z of this slice and of the next. Every array
+// is read from HBM once per iteration; the halo entries are neighbouring
+// tiles' and come from the caches. The per-pixel arithmetic is the generic
+// step's (tv_iso.cpp:251-288, 499-524), the projection by rsqrt as in 2D.
+// ---------------------------------------------------------------------------
+
+constexpr int k3TX = 32, k3TY = 8;
+constexpr int k3RX = k3TX + 2, k3RY = k3TY + 2, k3R = k3RX * k3RY;  // staged region: tile plus halo
+constexpr int k3ZX = k3TX + 1, k3Z = (k3TY + 1) * k3ZX;              // z: tile plus forward halo
+
+template <class T, bool ALPHA, bool GAP, bool ZIN>
+__global__ void __launch_bounds__(k3TX * k3TY) iso3d_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+    constexpr int NA = GAP ? 7 : 4;  // staged arrays: d, v0..v2 (and u0..u2 for the gap)
+    extern __shared__ __align__(16) unsigned char i3_smem[];
+    T(*reg)[NA][k3R] = reinterpret_cast<T(*)[NA][k3R]>(i3_smem);
+    T(*zs)[GAP ? 2 : 1][k3Z] = reinterpret_cast<T(*)[GAP ? 2 : 1][k3Z]>(i3_smem + 3 * NA * k3R * sizeof(T));
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = step_image(bf, blockIdx.z);
+    if (b < 0) return;
+    const IsoState st = bf.st[b];
+    if (st.status != kLive) return;
+    const int it = st.it;
+    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == A.max_iter)) || (it == 0 && st.warm);
+    const bool zin = st.zero_in != 0;
+    if (do_gap != GAP || zin != ZIN) {
+        if (threadIdx.x == 0) atomicExch(bf.err, 3);
+        return;
+    }
+    const IsoImage im = bf.img[b];
+    const int D0 = (int)A.g.L[0], D1 = (int)A.g.L[1], D2 = (int)A.g.L[2];
+    const int64_t N = A.g.N;
+    const int64_t S0 = (int64_t)D1 * D2;
+    const bool do_upd = it < A.max_iter;
+    const bool test = do_upd && (it & 3) == 0;
+    const int pin = A.par, pout = A.par ^ 1;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *U = static_cast<const T *>(bf.U[pin]) + (int64_t)b * 3 * N;
+    const T *V = st.vsel ? U : static_cast<const T *>(bf.V[pin]) + (int64_t)b * 3 * N;
+    T *UO = static_cast<T *>(bf.U[pout]) + (int64_t)b * 3 * N;
+    T *VO = static_cast<T *>(bf.V[pout]) + (int64_t)b * 3 * N;
+    const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
+    const T wh0 = (T)c.wh[0], wh1 = (T)c.wh[1], wh2 = (T)c.wh[2];
+    const T tau = (T)c.tau, beta = (T)st.beta, rad = (T)im.radius, bnd = (T)im.bound;
+    const int tid = threadIdx.x, ty = tid / k3TX, tx = tid % k3TX;
+    const int x0 = blockIdx.x * k3TX;
+    const int nyt = (D1 + k3TY - 1) / k3TY;
+    const int y0 = (blockIdx.y % nyt) * k3TY;
+    const int s0 = (blockIdx.y / nyt) * A.rows;
+    const int s1 = min(D0, s0 + A.rows);
+    auto q3 = [](int sl) { return (sl + 3) % 3; };
+    // The region entries this thread stages (tid and tid + 256): their
+    // offsets in a slice and whether they lie in the image.
+    constexpr int kE = (k3R + k3TX * k3TY - 1) / (k3TX * k3TY);
+    int64_t poff[kE];
+    bool inimg[kE];
+#pragma unroll
+    for (int e = 0; e < kE; ++e) {
+        const int i = tid + e * k3TX * k3TY;
+        const int gy = y0 - 1 + i / k3RX, gx = x0 - 1 + i % k3RX;
+        inimg[e] = i < k3R && gy >= 0 && gy < D1 && gx >= 0 && gx < D2;
+        poff[e] = inimg[e] ? (int64_t)gy * D2 + gx : 0;
+    }
+    // Slices go through registers: the loads of slice sl + 2 are issued
+    // before the work on slice sl and land in shared memory one step later.
+    T pf[kE][NA];
+    auto fetch = [&](int sl) {
+#pragma unroll
+        for (int e = 0; e < kE; ++e) {
+            const bool in = inimg[e] && sl >= 0 && sl < D0;
+            const int64_t o = in ? (int64_t)sl * S0 + poff[e] : 0;
+            pf[e][0] = in ? D[o] : T(0);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) pf[e][1 + a] = (in && !ZIN) ? V[a * N + o] : T(0);
+            if (GAP)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) pf[e][(GAP ? 4 : 1) + a] = (in && !ZIN) ? U[a * N + o] : T(0);
+        }
+    };
+    auto put = [&](int sl) {
+        T(*r)[k3R] = reg[q3(sl)];
+#pragma unroll
+        for (int e = 0; e < kE; ++e) {
+            const int i = tid + e * k3TX * k3TY;
+            if (i < k3R)
+#pragma unroll
+                for (int a = 0; a < NA; ++a) r[a][i] = pf[e][a];
+        }
+    };
+    // z of slice sl (of v, and of u for the gap) over the tile and its forward halo
+    auto zslice = [&](int sl) {
+        const T(*r)[k3R] = reg[q3(sl)];
+        const T(*rp)[k3R] = reg[q3(sl - 1)];
+        T(*z)[k3Z] = zs[sl & 1];
+        for (int i = tid; i < k3Z; i += k3TX * k3TY) {
+            const int zy = i / k3ZX, zx = i % k3ZX;
+            const int j = (zy + 1) * k3RX + zx + 1;
+            z[0][i] = r[0][j] + wh0 * (r[1][j] - rp[1][j]) + wh1 * (r[2][j] - r[2][j - k3RX]) +
+                      wh2 * (r[3][j] - r[3][j - 1]);
+            if (GAP)
+                z[GAP ? 1 : 0][i] = r[0][j] + wh0 * (r[4][j] - rp[4][j]) + wh1 * (r[5][j] - r[5][j - k3RX]) +
+                                    wh2 * (r[6][j] - r[6][j - 1]);
+        }
+    };
+    const int gy = y0 + ty, gx = x0 + tx;
+    const bool own = gy < D1 && gx < D2;
+    const int64_t ooff = own ? (int64_t)gy * D2 + gx : 0;
+    // u at this thread's entry of a slice (the gap variant stages it)
+    T pu[3] = {T(0), T(0), T(0)};
+    auto fetch_u = [&](int sl) {
+        if (GAP || ZIN || !own || sl >= s1) return;
+        const int64_t o = (int64_t)sl * S0 + ooff;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) pu[a] = U[a * N + o];
+    };
+    double gap_acc = 0.0, dot_acc = 0.0;
+    fetch(s0 - 1);
+    put(s0 - 1);
+    fetch(s0);
+    put(s0);
+    fetch(s0 + 1);
+    fetch_u(s0);
+    __syncthreads();
+    zslice(s0);
+    for (int sl = s0; sl < s1; ++sl) {
+        put(sl + 1);
+        T uc[3] = {pu[0], pu[1], pu[2]};
+        if (sl + 1 < s1) {
+            fetch(sl + 2);
+            fetch_u(sl + 1);
+        }
+        __syncthreads();
+        zslice(sl + 1);
+        __syncthreads();
+        if (own) {
+            const T(*r)[k3R] = reg[q3(sl)];
+            const T(*zc)[k3Z] = zs[sl & 1];
+            const T(*zn)[k3Z] = zs[(sl + 1) & 1];
+            const int i = ty * k3ZX + tx, j = (ty + 1) * k3RX + tx + 1;
+            const int64_t o = (int64_t)sl * S0 + ooff;
+            const bool h0 = sl + 1 < D0, h1 = gy + 1 < D1, h2 = gx + 1 < D2;
+            const T z0 = zc[0][i];
+            const T g0 = h0 ? wh0 * (zn[0][i] - z0) : T(0);
+            const T g1 = h1 ? wh1 * (zc[0][i + k3ZX] - z0) : T(0);
+            const T g2 = h2 ? wh2 * (zc[0][i + 1] - z0) : T(0);
+            T vc[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                vc[a] = r[1 + a][j];
+                if (GAP) uc[a] = r[(GAP ? 4 : 1) + a][j];
+            }
+            const T cv0 = wh0 != T(0) ? vc[0] + tau * g0 : T(0);
+            const T cv1 = wh1 != T(0) ? vc[1] + tau * g1 : T(0);
+            const T cv2 = wh2 != T(0) ? vc[2] + tau * g2 : T(0);
+            const T nn = cv0 * cv0 + cv1 * cv1 + cv2 * cv2;
+            const T rp = pixel_radius<T, ALPHA>(rad, bnd, AL, (int64_t)o);
+            const T sc = nn > rp * rp ? rp * rsqrt_t(nn) : T(1);
+            const T un[3] = {cv0 * sc, cv1 * sc, cv2 * sc};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (test) dot_acc += (double)((vc[a] - un[a]) * (un[a] - uc[a]));
+                if (do_upd) {
+                    VO[a * N + o] = un[a] + beta * (un[a] - uc[a]);
+                    UO[a * N + o] = un[a];
+                }
+            }
+            if (GAP) {
+                const T zu = zc[GAP ? 1 : 0][i];
+                const T gu0 = h0 ? wh0 * (zn[GAP ? 1 : 0][i] - zu) : T(0);
+                const T gu1 = h1 ? wh1 * (zc[GAP ? 1 : 0][i + k3ZX] - zu) : T(0);
+                const T gu2 = h2 ? wh2 * (zc[GAP ? 1 : 0][i + 1] - zu) : T(0);
+                gap_acc += (double)(rp * sqrt_t(gu0 * gu0 + gu1 * gu1 + gu2 * gu2) -
+                                    (gu0 * uc[0] + gu1 * uc[1] + gu2 * uc[2]));
+            }
+        }
+    }
+    const unsigned nblk = gridDim.x * gridDim.y;
+    const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
+    const double gsum = GAP ? block_sum(gap_acc, sh) : 0.0;
+    const double dsum = test ? block_sum(dot_acc, sh) : 0.0;
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[blk * 2 + 0] = gsum;
+        part[blk * 2 + 1] = dsum;
+    }
+    if (!arrive_last(bf.ticket + b, nblk, &flag)) return;
+    const double gap = GAP ? sum_partials(part, nblk, 2, 0, sh) : 0.0;
+    const double dot = test ? sum_partials(part, nblk, 2, 1, sh) : 0.0;
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2 = st;
+    control(s2, im, A.max_iter, GAP, test, gap, dot, pin, bf.live);
     bf.st[b] = s2;
 }
 
@@ -1340,7 +1588,7 @@ cudaError_t setup_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, c
 template <class T, int VEC, bool ALPHA>
 void launch_lean_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s,
                    int variant) {
-    const dim3 grid(sh.gx, sh.gy, (unsigned)A.g.B);
+    const dim3 grid(sh.gx, sh.gy, (unsigned)A.nimg);
     if (variant == 1) iso2d_lean_kernel<T, VEC, ALPHA, false, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
     else if (variant == 2) iso2d_lean_kernel<T, VEC, ALPHA, true, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
     else iso2d_lean_kernel<T, VEC, ALPHA, false, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
@@ -1353,9 +1601,42 @@ void launch_lean(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuf
     else launch_lean_a<T, VEC, false>(sh, A, c, bf, s, variant);
 }
 
+// Dynamic shared memory of the 3D step: three staged slices and two of z.
+template <class T, bool GAP>
+constexpr size_t iso3d_smem() {
+    return (size_t)3 * (GAP ? 7 : 4) * k3R * sizeof(T) + (size_t)2 * (GAP ? 2 : 1) * k3Z * sizeof(T);
+}
+
+// The attribute is per function and device: set once, to the kernel's size.
+template <class T, bool ALPHA, bool GAP, bool ZIN>
+void iso3d_attr() {
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    const unsigned long long bit = 1ull << dev;
+    if (done.load() & bit) return;
+    cudaFuncSetAttribute(iso3d_kernel<T, ALPHA, GAP, ZIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)iso3d_smem<T, GAP>());
+    done.fetch_or(bit);
+}
+
+template <class T, bool ALPHA, bool GAP, bool ZIN>
+void launch_3d_v(const dim3 &grid, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
+    iso3d_attr<T, ALPHA, GAP, ZIN>();
+    iso3d_kernel<T, ALPHA, GAP, ZIN><<<grid, k3TX * k3TY, iso3d_smem<T, GAP>(), s>>>(A, c, bf);
+}
+
+template <class T, bool ALPHA>
+void launch_3d_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s, int variant) {
+    const dim3 grid(sh.gx, sh.gy, (unsigned)A.nimg);
+    if (variant == 1) launch_3d_v<T, ALPHA, false, true>(grid, A, c, bf, s);
+    else if (variant == 2) launch_3d_v<T, ALPHA, true, false>(grid, A, c, bf, s);
+    else launch_3d_v<T, ALPHA, false, false>(grid, A, c, bf, s);
+}
+
 template <class T, int VEC>
 void launch_march(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
-    const dim3 grid(sh.gx, sh.gy, (unsigned)A.g.B);
+    const dim3 grid(sh.gx, sh.gy, (unsigned)A.nimg);
     if (c.has_alpha) iso2d_march_kernel<T, VEC, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
     else iso2d_march_kernel<T, VEC, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
 }
@@ -1370,19 +1651,24 @@ void launch_tma(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuff
         cudaFuncSetAttribute(iso2d_tma_kernel<T, VEC, ALPHA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         configured = smem;
     }
-    const dim3 grid(sh.gx, sh.gy, (unsigned)A.g.B);
+    const dim3 grid(sh.gx, sh.gy, (unsigned)A.nimg);
     iso2d_tma_kernel<T, VEC, ALPHA><<<grid, sh.bx, smem, s>>>(A, c, bf);
 }
 
 template <class T>
 cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh, int par,
-                   int variant, cudaStream_t s) {
+                   int variant, int64_t nimg, cudaStream_t s) {
     StepArgs A;
     A.g = g;
     A.max_iter = c.max_iter;
     A.par = par;
     A.rows = sh.rows;
-    if (sh.kind == 4) {
+    A.nimg = nimg;
+    if (nimg <= 0) return cudaSuccess;
+    if (sh.kind == 5) {
+        if (c.has_alpha) launch_3d_a<T, true>(sh, A, c, bf, s, variant);
+        else launch_3d_a<T, false>(sh, A, c, bf, s, variant);
+    } else if (sh.kind == 4) {
         if (sh.vec == 4) launch_lean<T, 4>(sh, A, c, bf, s, variant);
         else if (sh.vec == 2) launch_lean<T, 2>(sh, A, c, bf, s, variant);
         else launch_lean<T, 1>(sh, A, c, bf, s, variant);
@@ -1395,7 +1681,7 @@ cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, co
         else if (sh.vec == 2) launch_march<T, 2>(sh, A, c, bf, s);
         else launch_march<T, 1>(sh, A, c, bf, s);
     } else {
-        const dim3 grid(sh.gx, (unsigned)g.B);
+        const dim3 grid(sh.gx, (unsigned)nimg);
         if (g.k == 2) {
             if (c.has_alpha) iso_generic_kernel<T, 2, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
             else iso_generic_kernel<T, 2, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
@@ -1481,6 +1767,18 @@ StepShape iso_pick_shape(int dtype, const Geometry &g, int rows_hint, int bx_hin
         if (rows <= 0) rows = (int)std::max<int64_t>(4, std::min<int64_t>(16, H / 32));
         sh.rows = rows;
         sh.gy = (int)((H + rows - 1) / rows);
+    } else if (g.k == 3 && kind_hint != 1 && g.L[0] * g.L[1] * g.L[2] < 2147483647LL) {
+        // 3D: tiles of the (axis 1, axis 2) plane marching through chunks of
+        // slices; chunks short enough for a few blocks per SM, at most 4096
+        // blocks per image (the partial sums)
+        sh.kind = 5;
+        sh.bx = k3TX * k3TY;
+        const int64_t xt = (g.L[2] + k3TX - 1) / k3TX, yt = (g.L[1] + k3TY - 1) / k3TY;
+        int64_t rows = rows_hint > 0 ? rows_hint : 8;
+        while (xt * yt * ((g.L[0] + rows - 1) / rows) > 4096) rows *= 2;
+        sh.rows = (int)rows;
+        sh.gx = (int)xt;
+        sh.gy = (int)(yt * ((g.L[0] + rows - 1) / rows));
     } else {
         sh.kind = 1;
         sh.vec = 1;
@@ -1499,8 +1797,14 @@ cudaError_t iso_setup(int dtype, const Geometry &g, const IsoCall &c, const IsoB
 }
 
 cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh,
-                     int par, int variant, cudaStream_t s) {
-    return dtype == 1 ? step_t<float>(g, c, bf, sh, par, variant, s) : step_t<double>(g, c, bf, sh, par, variant, s);
+                     int par, int variant, int64_t nimg, cudaStream_t s) {
+    return dtype == 1 ? step_t<float>(g, c, bf, sh, par, variant, nimg, s)
+                      : step_t<double>(g, c, bf, sh, par, variant, nimg, s);
+}
+
+cudaError_t iso_live_list(const IsoState *st, int64_t B, int *lmap, int *lcnt, cudaStream_t s) {
+    live_list_kernel<<<1, 1024, 0, s>>>(st, B, lmap, lcnt);
+    return cudaGetLastError();
 }
 
 cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, void *out,
@@ -1720,7 +2024,7 @@ extern "C" FP_API fp_status fp_b200_tv_iso_noalloc(const float *x, float *z, int
     const int chunk = 8;
     for (;;) {
         for (int j = 0; j < chunk; ++j) {
-            e = iso_step(FP_F32, g, c, bf, sh, par, iso_variant(launched, max_iter, false), s);
+            e = iso_step(FP_F32, g, c, bf, sh, par, iso_variant(launched, max_iter, false), g.B, s);
             if (e != cudaSuccess) return FP_EDEVICE;
             par ^= 1;
             ++launched;

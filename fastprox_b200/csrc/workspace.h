@@ -54,6 +54,7 @@ struct fp_workspace {
     double *gammas = nullptr;
     double *part = nullptr;
     unsigned *ticket = nullptr;
+    int *lmap = nullptr, *lcnt = nullptr;  // the live images of a call, B + 1 ints
     int *live = nullptr;
     int *err = nullptr;
     int max_part = 0;

@@ -227,3 +227,25 @@ def test_steps_per_image_on_device(cuda):
     z, info = _solve(c, torch.as_tensor(c["x"], device=cuda))
     assert _nrel(z.cpu().numpy(), c["z"]) <= TOL32
     assert info.image_iters[0] == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_3d_multi_tile_against_reference(cuda, dtype):
+    """A volume spanning several tiles of the slice-marching 3D step in every
+    axis (two x tiles, nine y tiles, five chunks of slices), with pixel
+    weights, against the reference library on the same input."""
+    torch = _torch()
+    from fastprox_b200 import TVIso, synth
+    from oracle import ref_capi
+    if not ref_capi.available():
+        pytest.skip("reference library not built")
+    x = synth.phantom3d(1, 40, 70, 50, seed=21).astype(dtype)
+    al = synth.pixel_weights((40, 70, 50), seed=22)
+    tol = 1e-6 if dtype == np.float32 else 1e-10
+    r = ref_capi.solve(x, 0.08, iso=True, k=3, spatial=al, tol=tol, max_iter=100000)
+    z, info = TVIso(3, pixel_weights=al).solve(torch.as_tensor(x, device=cuda), 0.08, tol=tol, max_iter=100000)
+    zz = z.cpu().numpy()
+    assert _nrel(zz, r.z) <= (TOL32 if dtype == np.float32 else TOL64), _nrel(zz, r.z)
+    it = int(info.image_iters[0])
+    itr = int(r.iters[0])
+    assert abs(it - itr) <= (max(4, 0.2 * itr) if dtype == np.float32 else 0), (it, itr)
