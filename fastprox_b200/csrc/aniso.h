@@ -60,6 +60,9 @@ struct AnBuffers {
     int *live = nullptr;
     int *err = nullptr;
     int max_part = 0;
+    // a round's images: with lmap, launch slot z runs image lmap[z] for z < *lcnt
+    const int *lmap = nullptr;
+    const int *lcnt = nullptr;
 };
 
 // CheckSchedule::done (src/ops/tv_aniso.cpp:400-413): after the first two
@@ -86,8 +89,11 @@ cudaError_t aniso_setup(int dtype, const AnGeom &g, const AnCall &c, const AnBuf
                         cudaStream_t s);
 // Kernel attributes the rounds need, set before the first capture or launch.
 void aniso_prepare(int dtype);
-cudaError_t aniso_round(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s,
-                        int64_t *launches);
+// One round over nimg launch slots (g.B, or at least the count of bf's live list).
+cudaError_t aniso_round(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, int64_t nimg,
+                        cudaStream_t s, int64_t *launches);
+// The list of live images (by their states), for bf.lmap / bf.lcnt.
+cudaError_t aniso_live_list(const AnState *st, int64_t B, int *lmap, int *lcnt, cudaStream_t s);
 cudaError_t aniso_output(int dtype, const AnGeom &g, const AnBuffers &bf, void *out, cudaStream_t s);
 
 }  // namespace fpb

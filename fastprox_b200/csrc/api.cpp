@@ -1021,12 +1021,13 @@ fp_status run_aniso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *z
     aniso_prepare(ws->dtype);
     // rounds of launches (an iteration each, with its check, polish and
     // retirement), the live count read back behind two rounds in flight
+    // (over a list of the live images once fewer are live, as in run_iso)
     int slot = 0, inflight = 0;
-    int64_t rounds = 0;
+    int64_t rounds = 0, nimg = g.B;
     const int64_t cap = (int64_t)max_iter + 4;
     bool done = false;
     while (!done) {
-        e = aniso_round(ws->dtype, g, c, bf, s, &launches);
+        e = aniso_round(ws->dtype, g, c, bf, nimg, s, &launches);
         if (e != cudaSuccess) return cuda_status(e);
         ++rounds;
         e = cudaMemcpyAsync(ws->h_live + slot, ws->live, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -1038,7 +1039,17 @@ fp_status run_aniso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *z
             e = cudaEventSynchronize(ws->ev[slot]);
             if (e != cudaSuccess) return cuda_status(e);
             --inflight;
-            if (ws->h_live[slot] == 0) done = true;
+            const int live = ws->h_live[slot];
+            if (live == 0) {
+                done = true;
+            } else if (live < nimg) {
+                e = aniso_live_list(ws->an_st, g.B, ws->lmap, ws->lcnt, s);
+                if (e != cudaSuccess) return cuda_status(e);
+                bf.lmap = ws->lmap;
+                bf.lcnt = ws->lcnt;
+                nimg = live;
+                ++launches;
+            }
         }
         if (rounds >= cap) done = true;
     }

@@ -68,6 +68,47 @@ __device__ __forceinline__ Fib fibers(const AnGeom &g, int a) {
     return f;
 }
 
+// The image of launch slot z in a round (-1: none, the live list is shorter).
+__device__ __forceinline__ int round_image(const AnBuffers &bf, unsigned z) {
+    if (!bf.lmap) return (int)z;
+    return (int)z < *bf.lcnt ? bf.lmap[z] : -1;
+}
+
+// The live images in order (one block).
+__global__ void __launch_bounds__(1024) an_live_list(const AnState *st, int64_t B, int *lmap, int *lcnt) {
+    __shared__ int wsum[32];
+    __shared__ int base;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int64_t c0 = 0; c0 < B; c0 += blockDim.x) {
+        const int64_t i = c0 + threadIdx.x;
+        const int f = (i < B && st[i].status == kLive) ? 1 : 0;
+        int x = f;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int w = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        const int before = base + (wid > 0 ? wsum[wid - 1] : 0) + x - f;
+        if (f) lmap[before] = (int)i;
+        __syncthreads();
+        if (threadIdx.x == 0) base += wsum[(blockDim.x >> 5) - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *lcnt = base;
+}
+
 __device__ __forceinline__ double *img_part(const AnBuffers &bf, int b) { return bf.part + (int64_t)b * bf.max_part * 2; }
 
 // Ends a per-image reduction: block partial (two sums) to part, and in the
@@ -246,7 +287,8 @@ __device__ __forceinline__ void fibre_prox(const AnCall &c, const AnBuffers &bf,
 // ADBPG first block step: u = prox_{g1}(d + w) along a1 (tv_aniso.cpp:459-460).
 template <class T>
 __global__ void __launch_bounds__(128) an_pass1(AnGeom g, AnCall c, AnBuffers bf) {
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState &st = bf.st[b];
     if (st.status != kLive || st.stage != kStIter) return;
     const AnImage &im = bf.img[b];
@@ -271,7 +313,8 @@ template <class T>
 __global__ void __launch_bounds__(128) an_pass2(AnGeom g, AnCall c, AnBuffers bf) {
     __shared__ double sh[32];
     __shared__ int flag;
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState st = bf.st[b];
     if (st.status != kLive || st.stage != kStIter) return;
     const AnImage &im = bf.img[b];
@@ -450,7 +493,8 @@ constexpr int kTileThreads = 32;
 template <class T>
 __global__ void __launch_bounds__(kTileThreads) an_pass1_tile(AnGeom g, AnCall c, AnBuffers bf, TileCfg tc) {
     extern __shared__ __align__(16) unsigned char an_smem[];
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState &st = bf.st[b];
     if (st.status != kLive || st.stage != kStIter) return;
     const AnImage &im = bf.img[b];
@@ -484,7 +528,8 @@ __global__ void __launch_bounds__(kTileThreads) an_pass2_tile(AnGeom g, AnCall c
     extern __shared__ __align__(16) unsigned char an_smem[];
     __shared__ double sh[32];
     __shared__ int flag;
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState st = bf.st[b];
     if (st.status != kLive || st.stage != kStIter) return;
     const AnImage &im = bf.img[b];
@@ -549,7 +594,8 @@ __global__ void __launch_bounds__(kTileThreads) an_fdpg3_tile(AnGeom g, AnCall c
     extern __shared__ __align__(16) unsigned char an_smem[];
     __shared__ double sh[32];
     __shared__ int flag;
-    const int b = blockIdx.z;
+    const int b = round_image(bf, blockIdx.z);
+    if (b < 0) return;
     const AnState st = bf.st[b];
     if (st.status != kLive || st.stage != kStIter) return;
     const AnImage &im = bf.img[b];
@@ -616,7 +662,8 @@ __global__ void __launch_bounds__(kTileThreads) an_fdpg3_tile(AnGeom g, AnCall c
 // After a restart the extrapolated dual restarts from y (tv_aniso.cpp:474-477).
 template <class T>
 __global__ void an_restart_copy(AnGeom g, AnBuffers bf) {
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState &st = bf.st[b];
     if (st.status != kLive || !st.restart) return;
     const int64_t n = (int64_t)g.k * g.N;
@@ -630,7 +677,8 @@ __global__ void an_restart_copy(AnGeom g, AnBuffers bf) {
 // y_a+ = (prox_{3 g_a}(u - 3 w_a) - (u - 3 w_a)) / 3 and the extrapolation.
 template <class T>
 __global__ void an_fdpg3_u(AnGeom g, AnBuffers bf) {
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState &st = bf.st[b];
     if (st.status != kLive || st.stage != kStIter || bf.img[b].mode != kAnFdpg3) return;
     const int64_t N = g.N;
@@ -645,7 +693,8 @@ template <class T>
 __global__ void __launch_bounds__(128) an_fdpg3_pass(AnGeom g, AnCall c, AnBuffers bf) {
     __shared__ double sh[32];
     __shared__ int flag;
-    const int b = blockIdx.z;
+    const int b = round_image(bf, blockIdx.z);
+    if (b < 0) return;
     const AnState st = bf.st[b];
     if (st.status != kLive || st.stage != kStIter) return;
     const AnImage &im = bf.img[b];
@@ -708,7 +757,8 @@ __global__ void __launch_bounds__(128) an_fdpg3_pass(AnGeom g, AnCall c, AnBuffe
 // contiguous axis c = 2 (tv_aniso.cpp:118-123).
 template <class T>
 __global__ void __launch_bounds__(128) an_fdpg3_primal(AnGeom g, AnCall c, AnBuffers bf, int stage) {
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState &st = bf.st[b];
     if (st.status != kLive || st.stage != stage) return;
     const AnImage &im = bf.img[b];
@@ -751,7 +801,8 @@ template <class T>
 __global__ void __launch_bounds__(kThreads) an_gap(AnGeom g, AnCall c, AnBuffers bf, int stage) {
     __shared__ double sh[32];
     __shared__ int flag;
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState st = bf.st[b];
     if (st.status != kLive || st.stage != stage) return;
     if (stage == kStFinal && (st.polished || st.it == 0 || bf.img[b].mode != kAnAdbpg)) return;
@@ -804,7 +855,8 @@ __global__ void __launch_bounds__(kThreads) an_gap(AnGeom g, AnCall c, AnBuffers
 // stage kStPolish: for a polish; kStFinal: the final rebuild zp = d - q1 - q2.
 template <class T>
 __global__ void an_dual(AnGeom g, AnBuffers bf, int stage) {
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState &st = bf.st[b];
     if (st.status != kLive || st.stage != stage) return;
     if (stage == kStFinal && (st.polished || st.it == 0)) return;
@@ -851,7 +903,8 @@ __global__ void an_dual(AnGeom g, AnBuffers bf, int stage) {
 // bound is flat (bit a), the others move lam_e sign(p_e) from j to i in zp.
 template <class T>
 __global__ void __launch_bounds__(128) an_mark(AnGeom g, AnCall c, AnBuffers bf, int a) {
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState &st = bf.st[b];
     if (st.status != kLive || st.stage != kStPolish) return;
     const AnImage &im = bf.img[b];
@@ -899,7 +952,8 @@ __device__ __forceinline__ int uf_find(int *P, int i) {
 // their ends, the larger root hooked under the smaller by compare-and-swap,
 // so each root is the smallest index of its component.
 __global__ void an_union(AnGeom g, AnBuffers bf) {
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState &st = bf.st[b];
     if (st.status != kLive || st.stage != kStPolish) return;
     const int64_t N = g.N;
@@ -946,7 +1000,8 @@ __device__ __forceinline__ int uf_root(const int *P, int i) {
 // every entry to its root; the region sums of zp (64-bit fixed point) and sizes
 template <class T>
 __global__ void an_region_sum(AnGeom g, AnBuffers bf) {
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState &st = bf.st[b];
     if (st.status != kLive || st.stage != kStPolish) return;
     const int64_t N = g.N;
@@ -970,7 +1025,8 @@ template <class T>
 __global__ void __launch_bounds__(kThreads) an_polish_gap(AnGeom g, AnCall c, AnBuffers bf) {
     __shared__ double sh[32];
     __shared__ int flag;
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState st = bf.st[b];
     if (st.status != kLive || st.stage != kStPolish) return;
     const AnImage im = bf.img[b];
@@ -1035,7 +1091,8 @@ __global__ void __launch_bounds__(kThreads) an_polish_gap(AnGeom g, AnCall c, An
 // the accepted candidate: zp = region means
 template <class T>
 __global__ void an_polish_write(AnGeom g, AnBuffers bf) {
-    const int b = blockIdx.y;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
     const AnState &st = bf.st[b];
     if (st.status != kLive || !st.pol_accept) return;
     const int64_t N = g.N;
@@ -1195,8 +1252,10 @@ TileCfg tile_cfg(const AnGeom &g, const AnCall &c, size_t &smem) {
 }
 
 template <class T>
-cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s, int64_t *launches) {
-    const unsigned B = (unsigned)g.B;
+cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, int64_t nimg, cudaStream_t s,
+                   int64_t *launches) {
+    if (nimg <= 0) return cudaSuccess;
+    const unsigned B = (unsigned)nimg;
     int64_t nl = 0;
     const int pb = an_pixel_blocks(g);
     const dim3 pg(pb, B);
@@ -1260,11 +1319,12 @@ cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaS
     an_polish_gap<T><<<pg, kThreads, 0, s>>>(g, c, bf);
     an_polish_write<T><<<pg, kThreads, 0, s>>>(g, bf);
     nl += 5 + g.k;
-    // final rebuild, then retirement
-    an_final_skip<<<(B + 127) / 128, 128, 0, s>>>(g, bf);
+    // final rebuild, then retirement (over every image)
+    const unsigned BA = (unsigned)g.B;
+    an_final_skip<<<(BA + 127) / 128, 128, 0, s>>>(g, bf);
     an_dual<T><<<pg, kThreads, 0, s>>>(g, bf, kStFinal);
     an_gap<T><<<pg, kThreads, 0, s>>>(g, c, bf, kStFinal);
-    an_retire<<<(B + 127) / 128, 128, 0, s>>>(g, bf);
+    an_retire<<<(BA + 127) / 128, 128, 0, s>>>(g, bf);
     nl += 4;
     if (launches) *launches += nl;
     return cudaGetLastError();
@@ -1293,9 +1353,14 @@ void aniso_prepare(int dtype) {
     else tile_attributes<double>();
 }
 
-cudaError_t aniso_round(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s,
-                        int64_t *launches) {
-    return dtype == 1 ? round_t<float>(g, c, bf, s, launches) : round_t<double>(g, c, bf, s, launches);
+cudaError_t aniso_round(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, int64_t nimg,
+                        cudaStream_t s, int64_t *launches) {
+    return dtype == 1 ? round_t<float>(g, c, bf, nimg, s, launches) : round_t<double>(g, c, bf, nimg, s, launches);
+}
+
+cudaError_t aniso_live_list(const AnState *st, int64_t B, int *lmap, int *lcnt, cudaStream_t s) {
+    an_live_list<<<1, 1024, 0, s>>>(st, B, lmap, lcnt);
+    return cudaGetLastError();
 }
 
 cudaError_t aniso_output(int dtype, const AnGeom &g, const AnBuffers &bf, void *out, cudaStream_t s) {
