@@ -209,7 +209,7 @@ def main():
     ap.add_argument("--workload", default="iso512", choices=["iso512", "aniso512", "iso3d", "uneven", "vjp", "serve"],
                     help="iso512 (default, the headline line); the others report the other workloads")
     ap.add_argument("--serve-seconds", type=float, default=20.0)
-    ap.add_argument("--serve-workers", type=int, default=4, help="worker streams for anisotropic and 3D requests")
+    ap.add_argument("--serve-workers", type=int, default=16, help="worker streams for anisotropic and 3D requests")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)

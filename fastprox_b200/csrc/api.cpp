@@ -533,15 +533,17 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
         A((void **)&ws->an_cnt, (size_t)B * (size_t)N * sizeof(int));
         A((void **)&ws->an_sum, (size_t)B * (size_t)N * sizeof(unsigned long long));
     }
-    if (ws->keep && op->kind == kIso) {
+    if (ws->keep) {
         const size_t bn = (size_t)B * (size_t)N, kk = (size_t)g.k;
         A((void **)&ws->v_flat, bn);
+        if (op->kind == kAniso) A((void **)&ws->v_code, bn);
         A((void **)&ws->v_root, bn * sizeof(int));
         A((void **)&ws->v_cnt, bn * sizeof(int));
         A((void **)&ws->v_gz, kk * bn * sizeof(double));
         A((void **)&ws->v_h, kk * bn * sizeof(double));
         A((void **)&ws->v_vec, 7 * bn * sizeof(double));
         A((void **)&ws->v_acc, 2 * bn * sizeof(unsigned long long));
+        static_assert(sizeof(VjpImage) == sizeof(AnVjpImage), "one per-image record of the kept point");
         A((void **)&ws->v_img, (size_t)B * sizeof(VjpImage));
         A((void **)&ws->v_cg, (size_t)B * sizeof(CgState));
         A((void **)&ws->v_ggam, (size_t)B * sizeof(double));
@@ -561,7 +563,7 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     H((void **)&ws->h_img, (size_t)B * sizeof(IsoImage));
     H((void **)&ws->h_st, (size_t)B * sizeof(IsoState));
     H((void **)&ws->h_gam, (size_t)B * sizeof(double));
-    if (ws->keep && op->kind == kIso) {
+    if (ws->keep) {
         H((void **)&ws->h_vimg, (size_t)B * sizeof(VjpImage));
         H((void **)&ws->h_cg, (size_t)B * sizeof(CgState));
         H((void **)&ws->h_ggam, (size_t)B * sizeof(double));
@@ -1539,6 +1541,43 @@ fp_status deriv_prepare(const fp_op *op, fp_workspace *ws, VjpGeom &vg, VjpBuffe
     bf.err = ws->err;
     bf.max_part = ws->max_part;
     if (!bf.flat) return FP_EINVAL;
+    if (op->kind == kAniso) {
+        // the anisotropic kept point (tv_aniso.cpp:1012-1180): every axis of
+        // extent > 1 carries edges, their weights op->w
+        for (int a = 0; a < 3; ++a) {
+            vg.w[a] = a < g0.k ? op->w[a] : 0.0;
+            vg.bmax[a] = 1.0;
+        }
+        if (!op->spatial.empty())
+            for (int a = 0; a < g0.k; ++a) {
+                double m = 0.0;
+                for (int64_t i = 0; i < g0.N; ++i) m = std::max(m, op->spatial[(size_t)(a * g0.N + i)]);
+                vg.bmax[a] = m;
+            }
+        vg.eps_t = eps;
+        bf.zp = static_cast<const char *>(ws->U[1]) + (size_t)total * (ws->dtype == FP_F32 ? 4 : 8);
+        bf.qd = ws->dual;
+        bf.beta = ws->spatial;
+        bf.aimg = ws->an_img;
+        bf.ast = ws->an_st;
+        bf.avimg = reinterpret_cast<AnVjpImage *>(ws->v_img);
+        bf.code = ws->v_code;
+        if (ws->struct_valid) return FP_OK;
+        auto *hv = reinterpret_cast<AnVjpImage *>(ws->h_vimg);
+        for (int64_t b = 0; b < g0.B; ++b) {
+            const AnImage &im = ws->h_an_img[b];
+            const AnState &st = ws->h_an_st[b];
+            AnVjpImage &vi = hv[b];
+            vi.gamma = im.gamma_in;
+            vi.gap = (im.mode == kAnAdbpg || im.mode == kAnFdpg3) ? std::max(st.gp, 0.0) : 0.0;
+            vi.tau = vi.tau0 = 0.0;
+        }
+        cudaError_t e = cudaMemcpyAsync(ws->v_img, hv, (size_t)g0.B * sizeof(AnVjpImage), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = an_vjp_structure(ws->dtype, vg, bf, s);
+        if (e != cudaSuccess) return cuda_status(e);
+        ws->struct_valid = true;
+        return FP_OK;
+    }
     if (ws->struct_valid) return FP_OK;
     // per image, from the forward (tv_iso.cpp:559-570), at the solved scale
     for (int64_t b = 0; b < g0.B; ++b) {
@@ -1654,7 +1693,6 @@ fp_status vjp_impl(const fp_op *op, fp_workspace *ws, const fp_array *ga, fp_arr
                    fp_array *ggdev, fp_array *gpa) {
     if (!op || !ws || !ga || !gxa) return FP_EINVAL;
     if (ws->op != op || !ws->valid) return FP_EINVAL;
-    if (op->kind != kIso) return FP_EINVAL;  // anisotropic derivatives: not on the device yet
     Arr g, gx;
     if (fp_status s = to_arr(ga, g)) return s;
     if (fp_status s = to_arr(gxa, gx)) return s;
@@ -1730,6 +1768,35 @@ fp_status vjp_impl(const fp_op *op, fp_workspace *ws, const fp_array *ga, fp_arr
     if (direct && pointer_device(gx.data) != ws->device) return FP_EINVAL;
     const bool params = gpa && P > 0;
     int64_t nl = 0;
+    if (op->kind == kAniso) {
+        // component averages, no linear solve (tv_aniso.cpp:1398-1440)
+        const int64_t nb = P - op->k;  // edge weights
+        std::vector<double> gb((size_t)std::max<int64_t>(nb, 0));
+        cudaError_t e = an_vjp_solve(ws->dtype, vg, bf, gsrc, gdst, ws->conj ? 1 : 0, true,
+                                     (params && nb > 0) ? gb.data() : nullptr, s, &nl);
+        if (e != cudaSuccess) return cuda_status(e);
+        if (fp_status st = unstage_output(ws, gdst, gx)) return st;
+        e = cudaMemcpyAsync(ws->h_gw, ws->v_gw, (size_t)g0.B * 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e);
+        // d/dw_a = -gamma sum_C S_{C,a} g_C; d/dgamma = -sum_a w_a sum_C S_{C,a} g_C
+        const auto *hv = reinterpret_cast<const AnVjpImage *>(ws->h_vimg);
+        for (int64_t b = 0; b < g0.B; ++b)
+            for (int a = 0; a < op->k; ++a) {
+                tot[(size_t)a] -= hv[b].gamma * ws->h_gw[3 * b + a];
+                gsum -= op->w[a] * ws->h_gw[3 * b + a];
+            }
+        if (params) {
+            for (int64_t i = 0; i < nb; ++i) tot[(size_t)(op->k + i)] = gb[(size_t)i];
+            if (ws->conj)
+                for (double &v : tot) v = -v;
+        }
+        if (ws->conj) gsum = 0.0;  // y - prox(y) is constant in sigma
+        ws->deriv_residual = 0.0;
+        ws->deriv_iters = 0;
+        ws->kernel_launches = nl;
+        return finish();
+    }
     cudaError_t e = vjp_solve(ws->dtype, vg, bf, gsrc, gdst, ws->deriv_tol, ws->deriv_max_iter, ws->conj ? 1 : 0,
                               params, s, ws->h_live, ws->ev[0], &nl);
     if (e != cudaSuccess) return cuda_status(e);
@@ -1790,7 +1857,6 @@ fp_status jvp_impl(const fp_op *op, fp_workspace *ws, const fp_array *dxa, doubl
         if (fp_status s = param_array(dpa, P, dp)) return s;
     if (ws->host_mode != (out.device == FP_DEVICE_CPU)) return FP_EINVAL;
     if (dxa && dx.device != out.device) return FP_EINVAL;
-    if (op->kind != kIso) return FP_EINVAL;  // anisotropic derivatives: not on the device yet
     DeviceScope dsc(ws->device);
     if (ws->identity)  // J = I; the sigma-derivative NaN (api.cpp:603-607)
         return copy_or_fill(ws, dgamma != 0.0 ? nullptr : (dxa ? &dx : nullptr), out,
@@ -1802,11 +1868,13 @@ fp_status jvp_impl(const fp_op *op, fp_workspace *ws, const fp_array *dxa, doubl
     VjpGeom vg;
     VjpBuffers bf;
     if (fp_status st = deriv_prepare(op, ws, vg, bf)) return st;
-    // the parameter direction: the axis weights on the host, the pixel
-    // weights as doubles in qv (free until the solve)
+    // the parameter direction: the axis weights on the host, the pixel (or
+    // edge) weights as doubles on the device, in qv (N) for isotropic TV and
+    // h (k N) for anisotropic TV (both free until the solve)
     JvpDir dir{{0.0, 0.0, 0.0}};
     const double *dalpha = nullptr;
     const int64_t na = P - op->k;
+    double *dtail = op->kind == kAniso ? bf.h : bf.qv;
     cudaError_t e = cudaSuccess;
     if (has_dp) {
         if (dp.device == FP_DEVICE_CPU) {
@@ -1817,7 +1885,7 @@ fp_status jvp_impl(const fp_op *op, fp_workspace *ws, const fp_array *dxa, doubl
                                                   : *reinterpret_cast<const double *>(q);
             }
             for (int a = 0; a < op->k; ++a) dir.dw[a] = v[(size_t)a];
-            if (na > 0) e = cudaMemcpyAsync(bf.qv, v.data() + op->k, (size_t)na * sizeof(double),
+            if (na > 0) e = cudaMemcpyAsync(dtail, v.data() + op->k, (size_t)na * sizeof(double),
                                             cudaMemcpyHostToDevice, s);
         } else {
             if (pointer_device(dp.data) != ws->device) return FP_EINVAL;
@@ -1827,7 +1895,7 @@ fp_status jvp_impl(const fp_op *op, fp_workspace *ws, const fp_array *dxa, doubl
             if (e == cudaSuccess) e = cudaMemcpyAsync(hw, bf.b, (size_t)kk * sizeof(double), cudaMemcpyDeviceToHost, s);
             if (e == cudaSuccess && na > 0)
                 e = strided_copy(dp.data + kk * dp.strides[0] * (int64_t)dp.itemsize(), dp.dtype, &na, dp.strides, 1,
-                                 bf.qv, FP_F64, &one, s);
+                                 dtail, FP_F64, &one, s);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
             for (int a = 0; a < op->k; ++a) dir.dw[a] = hw[a];
         }
@@ -1835,7 +1903,7 @@ fp_status jvp_impl(const fp_op *op, fp_workspace *ws, const fp_array *dxa, doubl
         if (e != cudaSuccess) return cuda_status(e);
         for (int a = 0; a < op->k; ++a)
             if (!std::isfinite(dir.dw[a])) return FP_EPARAM;
-        if (na > 0) dalpha = bf.qv;
+        if (na > 0) dalpha = dtail;
     }
     const void *dsrc = nullptr;
     if (dxa)
@@ -1844,6 +1912,16 @@ fp_status jvp_impl(const fp_op *op, fp_workspace *ws, const fp_array *dxa, doubl
     void *ddst = direct ? out.data : ws->V[1];
     if (direct && pointer_device(out.data) != ws->device) return FP_EINVAL;
     int64_t nl = 0;
+    if (op->kind == kAniso) {
+        e = an_jvp_solve(ws->dtype, vg, bf, dsrc, ddst, dgamma, dir, dalpha, ws->conj ? 1 : 0, s, &nl);
+        if (e != cudaSuccess) return cuda_status(e);
+        if (fp_status st = unstage_output(ws, ddst, out)) return st;
+        e = cudaStreamSynchronize(s);
+        ws->deriv_residual = 0.0;
+        ws->deriv_iters = 0;
+        ws->kernel_launches = nl;
+        return cuda_status(e);
+    }
     e = jvp_solve(ws->dtype, vg, bf, dsrc, ddst, dgamma, dir, dalpha, ws->deriv_tol, ws->deriv_max_iter,
                   ws->conj ? 1 : 0, s, ws->h_live, ws->ev[0], &nl);
     if (e != cudaSuccess) return cuda_status(e);

@@ -1206,6 +1206,7 @@ cudaError_t setup_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, const
 // more warps beat fuller ones), else one fibre in up to 200 KB; 0 when even
 // that does not fit (the untiled pass then runs).
 constexpr int kTileSmemMax = 200 * 1024;
+constexpr int64_t kSpreadBlocks = 148 * 8;  // blocks a launch should have before its tiles grow
 
 // The tiled kernels may take up to kTileSmemMax of dynamic shared memory. Set
 // once per kernel, before any launch: the attribute is per function, and
@@ -1223,7 +1224,7 @@ void tile_attributes() {
     done.fetch_or(bit);
 }
 template <class T>
-TileCfg tile_cfg(const AnGeom &g, const AnCall &c, size_t &smem) {
+TileCfg tile_cfg(const AnGeom &g, const AnCall &c, int64_t nimg, size_t &smem) {
     // fibres per block: at most fb_max, and tiles of at most budget bytes
     // (tuning hints FASTPROX_B200_TILE_FB and FASTPROX_B200_TILE_KB)
     static const int fb_max = [] {
@@ -1242,8 +1243,11 @@ TileCfg tile_cfg(const AnGeom &g, const AnCall &c, size_t &smem) {
     for (int a = 0; a < g.k; ++a) {
         const int L = (int)g.L[a];
         auto bytes = [&](int fb) { return tile_bytes(L, fb, nbuf, sizeof(T)); };
+        // fewer fibres per block when the launch has few fibres in all (one
+        // large image), so that its blocks spread over every SM
+        const int64_t fibres = nimg * (g.N / std::max<int64_t>(g.L[a], 1));
         int fb = 1;
-        while (fb * 2 <= fb_max && bytes(fb * 2) <= budget) fb *= 2;
+        while (fb * 2 <= fb_max && bytes(fb * 2) <= budget && fibres / (fb * 2) >= kSpreadBlocks) fb *= 2;
         if (bytes(fb) > (size_t)kTileSmemMax) fb = 0;
         tc.fb[a] = fb;
         if (fb) smem = std::max(smem, bytes(fb));
@@ -1267,7 +1271,7 @@ cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, int64
     const unsigned fbk = (unsigned)((nfmax + 127) / 128);
     if (c.has_adbpg) {
         size_t smem = 0;
-        const TileCfg tc = tile_cfg<T>(g, c, smem);
+        const TileCfg tc = tile_cfg<T>(g, c, nimg, smem);
         bool tiled = true;
         int64_t tblk = 0;
         for (int a = 0; a < g.k; ++a) {
@@ -1287,7 +1291,7 @@ cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, int64
     if (c.has_fdpg3) {
         an_fdpg3_u<T><<<pg, kThreads, 0, s>>>(g, bf);
         size_t smem = 0;
-        const TileCfg tc = tile_cfg<T>(g, c, smem);
+        const TileCfg tc = tile_cfg<T>(g, c, nimg, smem);
         int64_t tblk = 0;
         bool tiled = g.k == 3;
         for (int a = 0; a < g.k; ++a) {

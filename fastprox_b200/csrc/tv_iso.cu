@@ -720,7 +720,7 @@ __device__ __forceinline__ void lean_rows(const T *__restrict__ D, const T *__re
 // of a call is at the same iteration); an image at another iteration (which
 // a single call never has) is flagged as an error rather than solved wrongly.
 template <class T, int VEC, bool ALPHA, bool GAP, bool ZIN>
-__global__ void __launch_bounds__(128) iso2d_lean_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+__global__ void __launch_bounds__(128, (GAP ? 5 : 1)) iso2d_lean_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     __shared__ double sh[32];
     __shared__ int flag;
     const int b = step_image(bf, blockIdx.z);

@@ -846,6 +846,325 @@ __global__ void __launch_bounds__(kT) jvp_out(VjpGeom g, VjpBuffers bf, const T 
     }
 }
 
+// ---- anisotropic TV: structure and derivatives (tv_aniso.cpp:1012-1440) ----------
+
+// z of image b at the solved scale: the input for an image without an active
+// axis, NaN for a NaN image, else the solver's z (or its polished zp)
+template <class T>
+__device__ __forceinline__ double an_z(const VjpGeom &g, const VjpBuffers &bf, int b, int64_t q) {
+    const int mode = bf.aimg[b].mode;
+    const int64_t N = g.N;
+    if (mode == kAnNan) return (double)CUDART_NAN;
+    if (mode == kAnIdentity) return (double)static_cast<const T *>(bf.d)[(int64_t)b * N + q];
+    const T *Z = static_cast<const T *>(bf.ast[b].zsel ? bf.zp : bf.U[1]) + (int64_t)b * N;
+    return (double)Z[q];
+}
+
+// q_a of image b at the solved scale (the dual is kept at the input's scale)
+template <class T>
+__device__ __forceinline__ double an_q(const VjpGeom &g, const VjpBuffers &bf, int b, int a, int64_t q) {
+    const AnImage &im = bf.aimg[b];
+    const double v = (double)static_cast<const T *>(bf.qd)[((int64_t)a * g.B + b) * g.N + q];
+    return im.e ? ldexp(v, -im.e) : v;
+}
+
+// lam_a of image b at the solved scale; a NaN image takes none (its
+// components are single entries, tv_aniso.cpp:284-290)
+__device__ __forceinline__ double an_lam(const VjpBuffers &bf, int b, int a) {
+    const AnImage &im = bf.aimg[b];
+    return im.mode == kAnNan ? 0.0 : im.lam[a];
+}
+
+template <class T>
+__device__ __forceinline__ double an_beta(const VjpGeom &g, const VjpBuffers &bf, int a, int64_t i) {
+    return bf.beta ? (double)static_cast<const T *>(bf.beta)[(int64_t)a * g.N + i] : 1.0;
+}
+
+// jump_bound (tv_aniso.cpp:1257-1300) per image: A = TV(z) + sum |z| |d - z|,
+// the range of z and max |d|, summed and maxed in fixed trees, then tau and
+// tau0; the structure's arrays are reset on the way.
+template <class T>
+__global__ void __launch_bounds__(kT) ad_bound(VjpGeom g, VjpBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    uint8_t *F = bf.flat + (int64_t)b * N, *Cd = bf.code + (int64_t)b * N;
+    int *R = bf.root + (int64_t)b * N, *Cn = bf.cnt + (int64_t)b * N;
+    unsigned long long *Ac = bf.acc + (int64_t)b * 2 * N;
+    double lam[3];
+    for (int a = 0; a < 3; ++a) lam[a] = a < g.k ? an_lam(bf, b, a) : 0.0;
+    double A = 0.0, dm = 0.0, zhi = -DBL_MAX, nlo = -DBL_MAX;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const Px x = pix_of(g, p);
+        const double z = an_z<T>(g, bf, b, p), d = (double)D[p];
+        double tv = 0.0;
+        for (int a = 0; a < g.k; ++a)
+            if (lam[a] != 0.0 && x.co[a] + 1 < g.L[a])
+                tv += lam[a] * an_beta<T>(g, bf, a, p) * fabs(an_z<T>(g, bf, b, p + g.S[a]) - z);
+        A += tv + fabs(z) * fabs(d - z);
+        dm = fmax(dm, fabs(d));
+        zhi = fmax(zhi, z);
+        nlo = fmax(nlo, -z);
+        F[p] = 0;
+        Cd[p] = 0;
+        R[p] = (int)p;
+        Cn[p] = 0;
+        Ac[2 * p] = 0ull;
+        Ac[2 * p + 1] = 0ull;
+    }
+    // four values per block: A (sum), max |d|, max z, max -z
+    const double sA = block_sum(A, sh);
+    const double sD = block_max(dm, sh);
+    const double sZ = block_max(zhi, sh);
+    const double sN = block_max(nlo, sh);
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 4 + 0] = sA;
+        part[blockIdx.x * 4 + 1] = sD;
+        part[blockIdx.x * 4 + 2] = sZ;
+        part[blockIdx.x * 4 + 3] = sN;
+    }
+    if (!arrive_last(bf.ticket + b, gridDim.x, &flag)) return;
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    double tA = 0.0, tD = 0.0, tZ = -DBL_MAX, tN = -DBL_MAX;
+    for (unsigned i = 0; i < gridDim.x; ++i) {
+        tA += part[i * 4 + 0];
+        tD = fmax(tD, part[i * 4 + 1]);
+        tZ = fmax(tZ, part[i * 4 + 2]);
+        tN = fmax(tN, part[i * 4 + 3]);
+    }
+    double lmax = 0.0;
+    for (int a = 0; a < g.k; ++a)
+        if (lam[a] != 0.0 && g.L[a] > 1) lmax += lam[a] * g.bmax[a];
+    AnVjpImage &vi = bf.avimg[b];
+    const double none = (double)CUDART_NAN;
+    if (!(lmax > 0.0)) {
+        vi.tau = vi.tau0 = none;
+        return;
+    }
+    const double range = tZ + tN;
+    const double tau0 = 64.0 * g.eps_t * (tD + 2.0 * lmax);
+    vi.tau0 = tau0;
+    const double gap = fmax(vi.gap, 0.0);
+    if (!(2.0 * sqrt(2.0 * gap) < range)) {
+        vi.tau = none;
+        return;
+    }
+    const double M = (double)((g.k + 1) * N);
+    const double gp = gap + (M + 4.0) * DBL_EPSILON * tA;
+    const double tau = 2.0 * sqrt(2.0 * gp) + tau0;
+    vi.tau = tau < range ? tau : none;
+}
+
+__device__ __forceinline__ uint8_t an_sgn(double v, int sh) {
+    return (uint8_t)((((unsigned)(v > 0.0)) | ((unsigned)(v < 0.0) << 1)) << sh);
+}
+
+// edge_codes / code_chunk (tv_aniso.cpp:1095-1160) along axis a, one thread
+// per fibre: the 1D dual p_e from the running sum of q_a; an edge with a bound
+// is flat when its dual is strictly inside it (and its jump not certified) or
+// its jump is within the rounding allowance; the others carry a sign, from the
+// dual or, certified or without weight, from z's jump.
+template <class T>
+__global__ void __launch_bounds__(128) ad_codes(VjpGeom g, VjpBuffers bf, int a) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N, L = g.L[a], s = g.S[a];
+    if (L <= 1) return;
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= N / L) return;
+    const int64_t base = (f / s) * L * s + f % s;
+    uint8_t *F = bf.flat + (int64_t)b * N, *Cd = bf.code + (int64_t)b * N;
+    const double lam = an_lam(bf, b, a);
+    const AnVjpImage vi = bf.avimg[b];
+    const bool cert = vi.tau == vi.tau;
+    const int sh = 2 * a;
+    const uint8_t bit = (uint8_t)(1u << a);
+    double acc = 0.0;
+    double zi = an_z<T>(g, bf, b, base);
+    for (int64_t l = 0; l + 1 < L; ++l) {
+        const int64_t i = base + l * s;
+        const double zn = an_z<T>(g, bf, b, i + s);
+        const uint8_t zc = an_sgn(zi - zn, sh);
+        if (!(lam > 0.0)) {
+            Cd[i] |= zc;
+        } else {
+            acc += an_q<T>(g, bf, b, a, i);
+            const double pe = -acc;
+            const double w = an_beta<T>(g, bf, a, i);
+            const double le = lam * w;
+            const double jump = fabs(zn - zi);
+            const bool certified = cert && le > 0.0 && jump > vi.tau;
+            const bool flat = (fabs(pe) < le * (1.0 - g.eta) && !certified) || (le > 0.0 && jump <= vi.tau0);
+            const bool from_z = certified || (bf.beta && w == 0.0);
+            const uint8_t c = from_z ? zc : an_sgn(-pe, sh);
+            if (flat) F[i] |= bit;
+            else Cd[i] |= c;
+        }
+        zi = zn;
+    }
+}
+
+// flat edges join their ends (union-find, roots at the smallest index)
+__global__ void ad_union(VjpGeom g, VjpBuffers bf) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const uint8_t *F = bf.flat + (int64_t)b * N;
+    int *P = bf.root + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const uint8_t fl = F[p];
+        if (!fl) continue;
+        for (int a = 0; a < g.k; ++a) {
+            if (!((fl >> a) & 1)) continue;
+            int u = (int)p, v = (int)(p + g.S[a]);
+            for (int tries = 0;; ++tries) {
+                u = uf_find_h(P, u);
+                v = uf_find_h(P, v);
+                if (u == v) break;
+                const int hi = u > v ? u : v, lo = u > v ? v : u;
+                const int old = atomicCAS(P + hi, hi, lo);
+                if (old == hi) break;
+                u = old;
+                v = lo;
+                if (tries > (1 << 24)) {
+                    atomicExch(bf.err, 2);
+                    break;
+                }
+            }
+        }
+    }
+}
+
+// The sign of the edge (i, i + S[a]) between two components (1, -1), else 0.
+__device__ __forceinline__ int an_edge_sign(const VjpGeom &g, const VjpBuffers &bf, int b, int a, int64_t i) {
+    const int64_t N = g.N;
+    const int cf = (bf.code[(int64_t)b * N + i] >> (2 * a)) & 3;
+    if (cf == 0) return 0;
+    const int *R = bf.root + (int64_t)b * N;
+    if (R[i + g.S[a]] == R[i]) return 0;
+    return cf == 1 ? 1 : -1;
+}
+
+// y = the term of entry i in S_{C(i),a}: its edge (i, i + e_a) to another
+// component minus the edge (i - e_a, i) from one, each sign_e beta_e
+// (tv_aniso.cpp:1187-1255)
+template <class T>
+__global__ void __launch_bounds__(kT) ad_term(VjpGeom g, VjpBuffers bf, int a) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    double *Y = bf.y + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        double e = 0.0;
+        if (g.L[a] > 1) {
+            const int64_t co = (p / g.S[a]) % g.L[a];
+            if (co + 1 < g.L[a]) {
+                const int sf = an_edge_sign(g, bf, b, a, p);
+                if (sf) e += sf * an_beta<T>(g, bf, a, p);
+            }
+            if (co > 0) {
+                const int sb = an_edge_sign(g, bf, b, a, p - g.S[a]);
+                if (sb) e -= sb * an_beta<T>(g, bf, a, p - g.S[a]);
+            }
+        }
+        Y[p] = e;
+    }
+}
+
+// the component averages of the cotangent G_C = sum_C g / |C| at the roots
+// (from the region sums in b); gx = G_C(i) (the conjugate's g - G); per root
+// the products S_{C,a} G_C into h for the parameter sums
+template <class T>
+__global__ void __launch_bounds__(kT) ad_vjp_out(VjpGeom g, VjpBuffers bf, const T *__restrict__ gin,
+                                                  T *__restrict__ gx, int conj) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const int *R = bf.root + (int64_t)b * N, *Cn = bf.cnt + (int64_t)b * N;
+    const double *Bv = bf.b + (int64_t)b * N;
+    double *X = bf.x + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const int r = R[p];
+        const double G = Bv[r] / (double)Cn[r];
+        double o = G;
+        if (conj) o = (double)gin[(int64_t)b * N + p] - G;
+        gx[(int64_t)b * N + p] = (T)o;
+        if (r == p) X[p] = G;
+        for (int a = 0; a < g.k; ++a)
+            bf.h[((int64_t)b * g.k + a) * N + p] = r == p ? bf.gz[((int64_t)b * g.k + a) * N + p] * G : 0.0;
+    }
+}
+
+// the edge weights' gradient along axis a, per image:
+// -gamma w_a sign_e (G_C(i) - G_C(i + e_a)) at the edge's first entry
+template <class T>
+__global__ void __launch_bounds__(kT) ad_vjp_beta(VjpGeom g, VjpBuffers bf, int a) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const int *R = bf.root + (int64_t)b * N;
+    const double *X = bf.x + (int64_t)b * N;
+    const double gam = bf.avimg[b].gamma;
+    double *Y = bf.y + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        double v = 0.0;
+        if (g.L[a] > 1 && (p / g.S[a]) % g.L[a] + 1 < g.L[a]) {
+            const int sg = an_edge_sign(g, bf, b, a, p);
+            if (sg) v = -gam * g.w[a] * sg * (X[R[p]] - X[R[p + g.S[a]]]);
+        }
+        Y[p] = v;
+    }
+}
+
+// The forward derivative's per-entry terms (tv_aniso.cpp:1362-1395):
+// dx_i, minus gamma w_a dbeta_e sign_e for the edge leaving i, plus it for the
+// edge entering i, summed per component afterwards.
+template <class T>
+__global__ void __launch_bounds__(kT) ad_jvp_terms(VjpGeom g, VjpBuffers bf, const T *__restrict__ dx,
+                                                    const double *__restrict__ dbeta) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const double gam = bf.avimg[b].gamma;
+    double *Y = bf.y + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        double t = dx ? (double)dx[(int64_t)b * N + p] : 0.0;
+        if (dbeta)
+            for (int a = 0; a < g.k; ++a) {
+                if (g.L[a] <= 1) continue;
+                const int64_t co = (p / g.S[a]) % g.L[a];
+                if (co + 1 < g.L[a]) {
+                    const int sf = an_edge_sign(g, bf, b, a, p);
+                    if (sf) t -= gam * g.w[a] * dbeta[(int64_t)a * N + p] * sf;
+                }
+                if (co > 0) {
+                    const int sb = an_edge_sign(g, bf, b, a, p - g.S[a]);
+                    if (sb) t += gam * g.w[a] * dbeta[(int64_t)a * N + p - g.S[a]] * sb;
+                }
+            }
+        Y[p] = t;
+    }
+}
+
+// dz_C = (sum_C t - sum_a (dgamma w_a + gamma dw_a) S_{C,a}) / |C|, every
+// entry its component's; the conjugate's dx - dz
+template <class T>
+__global__ void __launch_bounds__(kT) ad_jvp_out(VjpGeom g, VjpBuffers bf, const T *__restrict__ dx,
+                                                  T *__restrict__ dz, double dgamma, JvpDir dir, int conj) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const int *R = bf.root + (int64_t)b * N, *Cn = bf.cnt + (int64_t)b * N;
+    const double *Bv = bf.b + (int64_t)b * N;
+    const double gam = bf.avimg[b].gamma;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const int r = R[p];
+        double t = Bv[r];
+        for (int a = 0; a < g.k; ++a)
+            t -= (dgamma * g.w[a] + gam * dir.dw[a]) * bf.gz[((int64_t)b * g.k + a) * N + r];
+        double v = t / (double)Cn[r];
+        if (conj) v = (dx ? (double)dx[(int64_t)b * N + p] : 0.0) - v;
+        dz[(int64_t)b * N + p] = (T)v;
+    }
+}
+
 int pblocks(const VjpGeom &g) {
     int64_t nb = (g.N + kT * 4 - 1) / (kT * 4);
     return (int)std::max<int64_t>(1, std::min<int64_t>(nb, 512));
@@ -950,6 +1269,78 @@ cudaError_t jvp_t(const VjpGeom &g, const VjpBuffers &bf, const void *dx, void *
     return cudaGetLastError();
 }
 
+template <class T>
+cudaError_t an_structure_t(const VjpGeom &g, const VjpBuffers &bf, cudaStream_t s) {
+    const dim3 grid(pblocks(g), (unsigned)g.B);
+    ad_bound<T><<<grid, kT, 0, s>>>(g, bf);
+    for (int a = 0; a < g.k; ++a) {
+        const int64_t nf = g.N / g.L[a];
+        ad_codes<T><<<dim3((unsigned)((nf + 127) / 128), (unsigned)g.B), 128, 0, s>>>(g, bf, a);
+    }
+    ad_union<<<grid, kT, 0, s>>>(g, bf);
+    st_roots<<<grid, kT, 0, s>>>(g, bf);
+    // S_{C,a}: exact region sums of the edge terms, into gz at the roots
+    for (int a = 0; a < g.k; ++a) {
+        ad_term<T><<<grid, kT, 0, s>>>(g, bf, a);
+        rs_max<T><<<grid, kT, 0, s>>>(g, bf, 3, static_cast<const T *>(nullptr));
+        rs_add<T><<<grid, kT, 0, s>>>(g, bf, 3, static_cast<const T *>(nullptr));
+        // read-out into a B x N slice, then to image-major k x N
+        rs_read<<<grid, kT, 0, s>>>(g, bf, 3, bf.r);
+        cudaError_t e = cudaMemcpy2DAsync(bf.gz + (int64_t)a * g.N, (size_t)g.k * g.N * sizeof(double), bf.r,
+                                          (size_t)g.N * sizeof(double), (size_t)g.N * sizeof(double), (size_t)g.B,
+                                          cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t an_vjp_t(const VjpGeom &g, const VjpBuffers &bf, const void *gin, void *gx, int conj, bool params,
+                     double *gb, cudaStream_t s, int64_t *launches) {
+    const dim3 grid(pblocks(g), (unsigned)g.B);
+    const T *gi = static_cast<const T *>(gin);
+    int64_t nl = 0;
+    rs_max<T><<<grid, kT, 0, s>>>(g, bf, 0, gi);
+    rs_add<T><<<grid, kT, 0, s>>>(g, bf, 0, gi);
+    rs_read<<<grid, kT, 0, s>>>(g, bf, 0, bf.b);
+    ad_vjp_out<T><<<grid, kT, 0, s>>>(g, bf, gi, static_cast<T *>(gx), conj);
+    nl += 4;
+    if (params) {
+        param_sums<<<grid, kT, 0, s>>>(g, bf, 0, g.k > 1 ? 1 : -1);
+        ++nl;
+        if (g.k > 2) {
+            param_sums<<<grid, kT, 0, s>>>(g, bf, 2, -1);
+            ++nl;
+        }
+        if (bf.beta && gb) {
+            for (int a = 0; a < g.k; ++a) {
+                ad_vjp_beta<T><<<grid, kT, 0, s>>>(g, bf, a);
+                alpha_sum<<<pblocks(g), kT, 0, s>>>(g, bf, bf.qv);
+                nl += 2;
+                cudaError_t e = cudaMemcpyAsync(gb + (int64_t)a * g.N, bf.qv, (size_t)g.N * sizeof(double),
+                                                cudaMemcpyDeviceToHost, s);
+                if (e != cudaSuccess) return e;
+            }
+        }
+    }
+    if (launches) *launches = nl;
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t an_jvp_t(const VjpGeom &g, const VjpBuffers &bf, const void *dx, void *dz, double dgamma,
+                     const JvpDir &dir, const double *dbeta, int conj, cudaStream_t s, int64_t *launches) {
+    const dim3 grid(pblocks(g), (unsigned)g.B);
+    const T *dxi = static_cast<const T *>(dx);
+    ad_jvp_terms<T><<<grid, kT, 0, s>>>(g, bf, dxi, dbeta);
+    rs_max<T><<<grid, kT, 0, s>>>(g, bf, 3, static_cast<const T *>(nullptr));
+    rs_add<T><<<grid, kT, 0, s>>>(g, bf, 3, static_cast<const T *>(nullptr));
+    rs_read<<<grid, kT, 0, s>>>(g, bf, 3, bf.b);
+    ad_jvp_out<T><<<grid, kT, 0, s>>>(g, bf, dxi, static_cast<T *>(dz), dgamma, dir, conj);
+    if (launches) *launches = 5;
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 cudaError_t vjp_structure(int dtype, const VjpGeom &g, const VjpBuffers &bf, cudaStream_t s) {
@@ -969,6 +1360,26 @@ cudaError_t jvp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const v
     return dtype == 1 ? jvp_t<float>(g, bf, dx, dz, dgamma, dir, dalpha, tol, max_iter, conj, s, h_live, ev, launches)
                       : jvp_t<double>(g, bf, dx, dz, dgamma, dir, dalpha, tol, max_iter, conj, s, h_live, ev,
                                       launches);
+}
+
+}  // namespace fpb
+
+namespace fpb {
+
+cudaError_t an_vjp_structure(int dtype, const VjpGeom &g, const VjpBuffers &bf, cudaStream_t s) {
+    return dtype == 1 ? an_structure_t<float>(g, bf, s) : an_structure_t<double>(g, bf, s);
+}
+
+cudaError_t an_vjp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *gin, void *gx, int conj,
+                         bool params, double *gb, cudaStream_t s, int64_t *launches) {
+    return dtype == 1 ? an_vjp_t<float>(g, bf, gin, gx, conj, params, gb, s, launches)
+                      : an_vjp_t<double>(g, bf, gin, gx, conj, params, gb, s, launches);
+}
+
+cudaError_t an_jvp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *dx, void *dz, double dgamma,
+                         const JvpDir &dir, const double *dbeta, int conj, cudaStream_t s, int64_t *launches) {
+    return dtype == 1 ? an_jvp_t<float>(g, bf, dx, dz, dgamma, dir, dbeta, conj, s, launches)
+                      : an_jvp_t<double>(g, bf, dx, dz, dgamma, dir, dbeta, conj, s, launches);
 }
 
 }  // namespace fpb

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 
+#include "aniso.h"
 #include "engine.h"
 
 namespace fpb {
@@ -20,6 +21,11 @@ struct VjpGeom {
     double wmax;
     double eta;    // relative margin below the radius that counts as inside
     int act1;      // the active axis when there is exactly one, else -1
+    // anisotropic structure: the largest edge weight along each axis (1
+    // without edge weights), the axis weights, and the rounding allowance
+    double bmax[3];
+    double w[3];
+    double eps_t;  // the epsilon of the iterates' dtype
 };
 
 // A direction in the axis weights for the forward derivative.
@@ -32,6 +38,13 @@ struct JvpDir {
 // default tolerance of the conjugate gradients) and the flat threshold.
 struct VjpImage {
     double gs, mu, rel, thr;
+};
+
+// Per image of an anisotropic kept point: its step (at the input's scale),
+// its gap at the solved scale, and the jump thresholds of the structure
+// (tv_aniso.cpp:1257-1300; tau NaN: no jump certified).
+struct AnVjpImage {
+    double gamma, gap, tau, tau0;
 };
 
 struct CgState {
@@ -60,6 +73,17 @@ struct VjpBuffers {
     CgState *cg = nullptr;
     double *ggam = nullptr;  // per-image step gradient
     double *gw = nullptr;    // per-image axis-weight gradients, 3 per image
+    // anisotropic kept point: the solved z (z or zp per image), the dual at
+    // the input's scale, edge weights, per-image solver records and the
+    // structure's edge codes (2 bits per axis: 1 for +, 2 for -); S_{C,a}
+    // at the roots' slots in gz
+    const void *zp = nullptr;
+    const void *qd = nullptr;
+    const void *beta = nullptr;
+    const AnImage *aimg = nullptr;
+    const AnState *ast = nullptr;
+    AnVjpImage *avimg = nullptr;
+    uint8_t *code = nullptr;
     double *part = nullptr;
     unsigned *ticket = nullptr;
     int *live = nullptr, *err = nullptr;
@@ -67,6 +91,16 @@ struct VjpBuffers {
 };
 
 cudaError_t vjp_structure(int dtype, const VjpGeom &g, const VjpBuffers &bf, cudaStream_t s);
+// Anisotropic TV (tv_aniso.cpp:1012-1180, 1367-1440): the structure of the
+// kept point (flat edges, components, boundary sums S_{C,a}); the VJP (gx,
+// the step's gradient per image into ggam, the axis weights' into gw and,
+// with edge weights, the edge weights' summed over the images into gb, k N
+// doubles on the host); the JVP (dbeta: k N doubles on the device, or null).
+cudaError_t an_vjp_structure(int dtype, const VjpGeom &g, const VjpBuffers &bf, cudaStream_t s);
+cudaError_t an_vjp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *gin, void *gx, int conj,
+                         bool params, double *gb, cudaStream_t s, int64_t *launches);
+cudaError_t an_jvp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *dx, void *dz, double dgamma,
+                         const JvpDir &dir, const double *dbeta, int conj, cudaStream_t s, int64_t *launches);
 // gx = J^T gin per image, the step's gradient into ggam and, with params,
 // the axis weights' into gw and the pixel weights' (summed over the images)
 // into qv[0, N).

@@ -59,7 +59,7 @@ struct fp_workspace {
     int *err = nullptr;
     int max_part = 0;
     // derivative (keep_structure workspaces): structure and conjugate gradients
-    uint8_t *v_flat = nullptr;
+    uint8_t *v_flat = nullptr, *v_code = nullptr;
     int *v_root = nullptr, *v_cnt = nullptr;
     double *v_gz = nullptr, *v_h = nullptr, *v_vec = nullptr, *v_ggam = nullptr, *v_gw = nullptr;
     unsigned long long *v_acc = nullptr;

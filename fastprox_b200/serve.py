@@ -99,7 +99,7 @@ def _ws_bytes(r):
     return n * 4 * (3 + 5 * k) + n * 24
 
 
-def serve_stream(reqs, src, budget_bytes=120e9, workers=4, steps=8):
+def serve_stream(reqs, src, budget_bytes=120e9, workers=16, steps=8):
     """Continuous batching. Returns per-request latencies (s) and the span."""
     import torch
 
@@ -202,7 +202,7 @@ def one_at_a_time(reqs, src, service=None):
     return lat, time.perf_counter() - t0
 
 
-def run(seconds=20.0, rate=200.0, seed=0, workers=4):
+def run(seconds=20.0, rate=200.0, seed=0, workers=16):
     import torch
     src = ImageSource(seed)
     warm = make_requests(0.2, rate, seed + 1)

@@ -9,7 +9,8 @@ of the last ``ndim`` axes of ``x`` and is differentiable in ``x`` and
 ``gamma`` (a number or a tensor broadcasting to the batch shape): the
 backward pass is the implicit-differentiation VJP on the device (``fp_vjp``),
 one linear solve on the solution's flat regions, with memory independent of
-the iteration count. ``tv_aniso`` solves anisotropic TV (forward only).
+the iteration count. ``tv_aniso`` solves anisotropic TV, differentiable the
+same way (its VJP averages over the solution's constant components).
 """
 
 from __future__ import annotations
@@ -101,10 +102,16 @@ def tv_iso(x, gamma=1.0, *, ndim=2, weights=None, pixel_weights=None, tol=1e-6, 
 
 
 def tv_aniso(x, gamma=1.0, *, ndim=2, weights=None, edge_weights=None, tol=1e-6, max_iter=1000, return_info=False):
-    """Anisotropic TV prox of the last ``ndim`` axes of ``x`` (forward only)."""
+    """Anisotropic TV prox of the last ``ndim`` axes of ``x`` (differentiable
+    in ``x`` and a scalar ``gamma``: the backward pass averages the cotangent
+    over the solution's constant components, tv_aniso.cpp:1398-1440)."""
+    if not isinstance(x, torch.Tensor):
+        raise TypeError("x must be a torch.Tensor")
+    if ndim not in (2, 3) or x.dim() < ndim:
+        raise ValueError("ndim must be 2 or 3 and x must have at least ndim dimensions")
     op = TVAniso(ndim, weights, None if edge_weights is None else np.asarray(
         edge_weights.detach().cpu() if isinstance(edge_weights, torch.Tensor) else edge_weights, np.float64))
-    with torch.no_grad():
-        z, info = op.solve(x.detach(), float(gamma) if not isinstance(gamma, torch.Tensor) or gamma.numel() == 1
-                           else gamma.detach(), tol=tol, max_iter=max_iter, with_dual=False)
-    return (z, info) if return_info else z
+    g, _ = _gamma_per_image(gamma, x, ndim)
+    cfg = {"tol": float(tol), "max_iter": int(max_iter)}
+    z = _DeviceTV.apply(op, cfg, x, g)
+    return (z, cfg["info"]) if return_info else z

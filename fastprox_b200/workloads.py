@@ -227,4 +227,4 @@ def _unrolled_fista(x, gamma, iters):
 
 def serve(args):
     from . import serve as srv
-    return srv.run(seconds=args.serve_seconds, workers=getattr(args, "serve_workers", 4))
+    return srv.run(seconds=args.serve_seconds, workers=getattr(args, "serve_workers", 16))

@@ -143,10 +143,11 @@ FP_API fp_status fp_prox_conj(const fp_op *op, double sigma, const fp_array *y,
                               fp_workspace *ws, fp_info *info);
 
 /* Replace include/fastprox.h:646-654 and :779-780: derivatives at the point
- * kept by the last prox call with keep_structure (isotropic TV; an
- * anisotropic point gives FP_EINVAL). theta = the k axis weights, then the
- * pixel weights in C order (fp_op_nparams entries); gparams and dparams may be
- * host or device arrays, float32 or float64, ndim <= 1. */
+ * kept by the last prox call with keep_structure, isotropic or anisotropic
+ * TV. theta = the k axis weights, then the pixel weights (isotropic) or edge
+ * weights (anisotropic, k x shape) in C order (fp_op_nparams entries);
+ * gparams and dparams may be host or device arrays, float32 or float64,
+ * ndim <= 1. */
 FP_API fp_status fp_jvp(const fp_op *op, const fp_workspace *ws,
                         const fp_array *dx, double dgamma,
                         const fp_array *dparams, fp_array *dout);
