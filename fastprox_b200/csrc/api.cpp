@@ -517,6 +517,8 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     if (const int ch = env_int("FASTPROX_B200_CHUNK")) ws->chunk = ch;
     ws->max_part = std::max(iso_setup_blocks(g), ws->shape_.gx * ws->shape_.gy);
     ws->max_part = std::max(ws->max_part, 4096);
+    if (ws->shape_.kind == 4)  // per-row partial sums of the lean 2D step
+        ws->max_part = (int)std::max<int64_t>(ws->max_part, (int64_t)ws->shape_.gx * g.L[0]);
     if (op->kind == kAniso) {
         // the untiled fibre passes: a block of 128 fibres per partial, three
         // axes in one launch for FDPG-3

@@ -355,7 +355,11 @@ struct StepArgs {
     int par;
     int rows;
     int64_t nimg;  // launch slots (host side: the grid's image extent)
+    int row_part;  // lean 2D step: per-row partial sums (H x column blocks slots)
 };
+
+constexpr int kLeanRowsMax = 32;  // rows per block of the lean 2D step
+constexpr int64_t kTailBlocks = 148 * 4;  // blocks a lean launch should have before its blocks grow
 
 // ---------------------------------------------------------------------------
 // The 2D row-marching step: a warp spans 32 * VEC consecutive columns, a
@@ -565,7 +569,7 @@ __device__ __forceinline__ void lean_rows(const T *__restrict__ D, const T *__re
                                           T *__restrict__ UO1, T *__restrict__ VO0, T *__restrict__ VO1,
                                           const T *__restrict__ AL, int H, int W, int cb, int r0, int r1, T wh0, T wh1,
                                           T tau, T beta, T rad, T bnd, bool test, bool store, double &gap_acc,
-                                          double &dot_acc) {
+                                          double &dot_acc, double *rowp = nullptr) {
     const int lane = threadIdx.x & 31;
     const bool colok = cb < W;
     const bool ext = lane == 31 && cb + VEC < W;  // the next warp's first column
@@ -713,6 +717,20 @@ __device__ __forceinline__ void lean_rows(const T *__restrict__ D, const T *__re
         x_z = nx_z;
         x_zu = nx_zu;
         off = offn;
+        if (rowp && (GAP || test)) {
+            // this row's sums over the warp (a fixed tree), per warp in shared
+            // memory: rowp[(row - r0) * 8 + 2 * warp + (0: gap, 1: dot)]
+            double gv = gap_acc, dv = dot_acc;
+            for (int o = 16; o > 0; o >>= 1) {
+                gv += __shfl_down_sync(0xffffffffu, gv, o);
+                dv += __shfl_down_sync(0xffffffffu, dv, o);
+            }
+            if (lane == 0) {
+                rowp[(i - r0) * 8 + 2 * (threadIdx.x >> 5) + 0] = gv;
+                rowp[(i - r0) * 8 + 2 * (threadIdx.x >> 5) + 1] = dv;
+            }
+            gap_acc = dot_acc = 0.0;
+        }
     }
 }
 
@@ -720,7 +738,7 @@ __device__ __forceinline__ void lean_rows(const T *__restrict__ D, const T *__re
 // of a call is at the same iteration); an image at another iteration (which
 // a single call never has) is flagged as an error rather than solved wrongly.
 template <class T, int VEC, bool ALPHA, bool GAP, bool ZIN>
-__global__ void __launch_bounds__(128, (GAP ? 5 : 1)) iso2d_lean_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+__global__ void __launch_bounds__(128, 5) iso2d_lean_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     __shared__ double sh[32];
     __shared__ int flag;
     const int b = step_image(bf, blockIdx.z);
@@ -750,21 +768,41 @@ __global__ void __launch_bounds__(128, (GAP ? 5 : 1)) iso2d_lean_kernel(StepArgs
     const int r0 = blockIdx.y * A.rows;
     const int r1 = min(H, r0 + A.rows);
     double gap_acc = 0.0, dot_acc = 0.0;
+    __shared__ double rowp[kLeanRowsMax * 8];
     lean_rows<T, VEC, ALPHA, GAP, ZIN>(D, U0, U0 + N, V0, V0 + N, UO0, UO0 + N, VO0, VO0 + N, AL, H, W, cb, r0, r1,
                                        (T)c.wh[0], (T)c.wh[1], (T)c.tau, (T)st.beta, (T)im.radius, (T)im.bound, test,
-                                       do_upd, gap_acc, dot_acc);
+                                       do_upd, gap_acc, dot_acc, A.row_part ? rowp : nullptr);
     const unsigned nblk = gridDim.x * gridDim.y;
     const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
-    const double gsum = GAP ? block_sum(gap_acc, sh) : 0.0;
-    const double dsum = test ? block_sum(dot_acc, sh) : 0.0;
     double *part = bf.part + (int64_t)b * bf.max_part * 2;
-    if (threadIdx.x == 0) {
-        part[blk * 2 + 0] = gsum;
-        part[blk * 2 + 1] = dsum;
+    unsigned nslot = nblk;
+    if (A.row_part) {
+        // one slot per (row, column block), each the sum of its warps in
+        // order: the same sums however many rows a block takes
+        __syncthreads();
+        const int nw = (int)(blockDim.x >> 5);
+        if ((GAP || test) && (int)threadIdx.x < r1 - r0) {
+            double gv = 0.0, dv = 0.0;
+            for (int w = 0; w < nw; ++w) {
+                gv += rowp[threadIdx.x * 8 + 2 * w];
+                dv += rowp[threadIdx.x * 8 + 2 * w + 1];
+            }
+            const int64_t slot = (int64_t)(r0 + threadIdx.x) * gridDim.x + blockIdx.x;
+            part[slot * 2 + 0] = gv;
+            part[slot * 2 + 1] = dv;
+        }
+        nslot = (unsigned)H * gridDim.x;
+    } else {
+        const double gsum = GAP ? block_sum(gap_acc, sh) : 0.0;
+        const double dsum = test ? block_sum(dot_acc, sh) : 0.0;
+        if (threadIdx.x == 0) {
+            part[blk * 2 + 0] = gsum;
+            part[blk * 2 + 1] = dsum;
+        }
     }
     if (!arrive_last(bf.ticket + b, nblk, &flag)) return;
-    const double gap = GAP ? sum_partials(part, nblk, 2, 0, sh) : 0.0;
-    const double dot = test ? sum_partials(part, nblk, 2, 1, sh) : 0.0;
+    const double gap = GAP ? sum_partials(part, nslot, 2, 0, sh) : 0.0;
+    const double dot = test ? sum_partials(part, nslot, 2, 1, sh) : 0.0;
     if (threadIdx.x != 0) return;
     bf.ticket[b] = 0;
     IsoState s2 = st;
@@ -1664,14 +1702,28 @@ cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, co
     A.par = par;
     A.rows = sh.rows;
     A.nimg = nimg;
+    A.row_part = 0;
     if (nimg <= 0) return cudaSuccess;
+    StepShape sh2 = sh;
+    if (sh.kind == 4 && (int64_t)sh.gx * g.L[0] <= bf.max_part && sh.rows <= kLeanRowsMax) {
+        // per-row partial sums make the sums independent of the rows per
+        // block, so a launch over few live images (the tail of a batch) takes
+        // shorter blocks, more of them, to spread over the SMs
+        A.row_part = 1;
+        const int64_t H = g.L[0];
+        int rows = sh.rows;
+        while (rows > 2 && nimg * sh.gx * ((H + rows - 1) / rows) < kTailBlocks) rows /= 2;
+        sh2.rows = rows;
+        sh2.gy = (int)((H + rows - 1) / rows);
+        A.rows = rows;
+    }
     if (sh.kind == 5) {
         if (c.has_alpha) launch_3d_a<T, true>(sh, A, c, bf, s, variant);
         else launch_3d_a<T, false>(sh, A, c, bf, s, variant);
     } else if (sh.kind == 4) {
-        if (sh.vec == 4) launch_lean<T, 4>(sh, A, c, bf, s, variant);
-        else if (sh.vec == 2) launch_lean<T, 2>(sh, A, c, bf, s, variant);
-        else launch_lean<T, 1>(sh, A, c, bf, s, variant);
+        if (sh.vec == 4) launch_lean<T, 4>(sh2, A, c, bf, s, variant);
+        else if (sh.vec == 2) launch_lean<T, 2>(sh2, A, c, bf, s, variant);
+        else launch_lean<T, 1>(sh2, A, c, bf, s, variant);
     } else if (sh.kind == 2) {
         constexpr int V = 16 / sizeof(T);
         if (c.has_alpha) launch_tma<T, V, true>(sh, A, c, bf, s);
