@@ -8,7 +8,9 @@
 namespace fpb {
 
 enum AnMode : int { kAnAdbpg = 0, kAnFdpg3 = 1, kAnSingle = 2, kAnIdentity = 3, kAnNan = 4, kAnInf = 5 };
-enum AnStage : int { kStIter = 0, kStCheck = 1, kStPolish = 2, kStFinal = 3, kStDone = 4 };
+// kStWarm: a warm start's pass z = prox_{g1}(d + y) and its dual before the
+// second check (tv_aniso.cpp:467-486)
+enum AnStage : int { kStIter = 0, kStCheck = 1, kStPolish = 2, kStFinal = 3, kStDone = 4, kStWarm = 5 };
 
 struct AnGeom {
     int k;
@@ -26,6 +28,7 @@ struct AnCall {
     double beta_max;
     int64_t N;
     int has_adbpg, has_fdpg3;
+    int warm;  // the call starts from the dual in bf.dual
 };
 
 struct AnImage {
@@ -41,6 +44,7 @@ struct AnImage {
 struct AnState {
     int status, stage, it, since, last, restart, warm, polished, zsel, pol_accept;
     int chk_next, chk_prev_it;
+    int wphase, pad;  // a warm start: 1 before its first check's outcome, 2 before its second's, else 0
     double tn, beta, gp, gz, accept, chk_prev, pol_next;
 };
 
@@ -87,6 +91,11 @@ __device__ __forceinline__ void check_done(AnState &s, double gp, double target)
 int an_pixel_blocks(const AnGeom &g);
 cudaError_t aniso_setup(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, const void *x,
                         cudaStream_t s);
+// A warm start (tv_aniso.cpp:316-320, 436-486, 539-543, 630-684): the dual
+// in bf.dual (the input's scale) made feasible fibre by fibre at the solved
+// scale, y and the extrapolation from it, and z = d - sum_a q_a for a first
+// check at iteration 0.
+cudaError_t aniso_warm(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s);
 // Kernel attributes the rounds need, set before the first capture or launch.
 void aniso_prepare(int dtype);
 // One round over nimg launch slots (g.B, or at least the count of bf's live list).

@@ -967,7 +967,8 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     return cuda_status(e);
 }
 
-fp_status run_aniso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zdst, double tol, int max_iter) {
+fp_status run_aniso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zdst, double tol, int max_iter,
+                    bool warm) {
     const Geometry &g0 = ws->g;
     cudaStream_t s = ws->stream;
     const size_t T = ws->dtype == FP_F32 ? 4 : 8;
@@ -1020,6 +1021,8 @@ fp_status run_aniso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *z
     if (e == cudaSuccess) e = cudaMemsetAsync(ws->U[0], 0, (size_t)g.k * bn * T, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(ws->V[0], 0, (size_t)g.k * bn * T, s);
     if (e == cudaSuccess) e = aniso_setup(ws->dtype, g, c, bf, xsrc, s);
+    c.warm = warm && (c.has_adbpg || c.has_fdpg3) ? 1 : 0;
+    if (e == cudaSuccess && c.warm) e = aniso_warm(ws->dtype, g, c, bf, s);
     if (e != cudaSuccess) return cuda_status(e);
     int64_t launches = 5;
     aniso_prepare(ws->dtype);
@@ -1288,8 +1291,7 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
     if (op->kind == kIso) {
         if (fp_status st2 = run_iso(ws, op, xsrc, zdst, o.tol, o.max_iter, warm)) return st2;
     } else {
-        // anisotropic warm starts restart cold (the dual seed is not read)
-        if (fp_status st2 = run_aniso(ws, op, xsrc, zdst, o.tol, o.max_iter)) return st2;
+        if (fp_status st2 = run_aniso(ws, op, xsrc, zdst, o.tol, o.max_iter, warm)) return st2;
     }
     if (conj) {
         e = conj_finish(ws->dtype, ysave, zdst, total, s);

@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(128) an_pass1(AnGeom g, AnCall c, AnBuffers bf
     const int b = round_image(bf, blockIdx.y);
     if (b < 0) return;
     const AnState &st = bf.st[b];
-    if (st.status != kLive || st.stage != kStIter) return;
+    if (st.status != kLive || (st.stage != kStIter && st.stage != kStWarm)) return;
     const AnImage &im = bf.img[b];
     if (im.mode != kAnAdbpg) return;
     const int a = im.a1;
@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(kTileThreads) an_pass1_tile(AnGeom g, AnCall c
     const int b = round_image(bf, blockIdx.y);
     if (b < 0) return;
     const AnState &st = bf.st[b];
-    if (st.status != kLive || st.stage != kStIter) return;
+    if (st.status != kLive || (st.stage != kStIter && st.stage != kStWarm)) return;
     const AnImage &im = bf.img[b];
     if (im.mode != kAnAdbpg) return;
     const int a = im.a1;
@@ -659,6 +659,120 @@ __global__ void __launch_bounds__(kTileThreads) an_fdpg3_tile(AnGeom g, AnCall c
     bf.st[b] = s2;
 }
 
+// ---------------------------------------------------------------------------
+// Warm starts (tv_aniso.cpp:316-320, 436-486, 539-543, 630-684)
+// ---------------------------------------------------------------------------
+
+// feasible_dual along axis a, one thread per fibre: q_a at the solved scale
+// (zero on an inactive axis); a fibre whose running sums -p_e stay within
+// their bounds and end at 0 up to rounding is kept, any other rebuilt from
+// its running sums clipped to [-lam_e, lam_e] (non-finite ones 0).
+template <class T>
+__global__ void __launch_bounds__(128) an_warm_feasible(AnGeom g, AnCall c, AnBuffers bf, int a) {
+    const int b = blockIdx.y;
+    const AnImage &im = bf.img[b];
+    if (bf.st[b].status != kLive || (im.mode != kAnAdbpg && im.mode != kAnFdpg3)) return;
+    const Fib fb = fibers(g, a);
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= fb.nfib) return;
+    const int64_t N = g.N, B = g.B, base = fb.base(f), s = fb.s, L = fb.L;
+    T *Q = static_cast<T *>(bf.dual) + ((int64_t)a * B + b) * N + base;
+    const double lam = im.lam[a];
+    const T *bw = c.has_beta ? static_cast<const T *>(bf.beta) + (int64_t)a * c.N + base : nullptr;
+    if (!(lam > 0.0)) {
+        for (int64_t l = 0; l < L; ++l) Q[l * s] = T(0);
+        return;
+    }
+    double acc = 0.0, mass = 0.0, peak = -lam;
+    for (int64_t l = 0; l < L; ++l) {
+        const double q = im.e ? ldexp((double)Q[l * s], -im.e) : (double)Q[l * s];
+        Q[l * s] = (T)q;
+        acc += q;
+        mass += fabs(q);
+        const double e = l + 1 < L ? fabs(acc) - (bw ? lam * (double)bw[l * s] : lam) : -lam;
+        peak = (e > peak || e != e) ? e : peak;
+    }
+    const double eps = sizeof(T) == 4 ? 1.1920928955078125e-07 : DBL_EPSILON;
+    const double tol = 1e-10 * lam + 16.0 * eps * mass;
+    if (isfinite(mass) && peak <= tol && fabs(acc) <= tol) return;
+    double run = 0.0, prev = 0.0;
+    for (int64_t l = 0; l < L; ++l) {
+        const double qi = (double)Q[l * s];
+        run += qi;
+        double pe = 0.0;
+        const double lb = (l + 1 < L && bw) ? lam * (double)bw[l * s] : lam;
+        if (l + 1 < L && isfinite(run)) pe = fmin(fmax(-run, -lb), lb);
+        Q[l * s] = (T)(prev - pe);
+        prev = pe;
+    }
+}
+
+// y = -q2 and z = d - q1 - q2 (ADBPG), y_a = -q_a (FDPG-3); w = y
+template <class T>
+__global__ void an_warm_init(AnGeom g, AnBuffers bf) {
+    const int b = blockIdx.y;
+    const AnImage &im = bf.img[b];
+    if (bf.st[b].status != kLive || (im.mode != kAnAdbpg && im.mode != kAnFdpg3)) return;
+    const int64_t N = g.N, B = g.B;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *Q = static_cast<const T *>(bf.dual);
+    T *Y = static_cast<T *>(bf.y) + (int64_t)b * g.k * N;
+    T *Wv = static_cast<T *>(bf.wv) + (int64_t)b * g.k * N;
+    T *Z = static_cast<T *>(bf.z) + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        if (im.mode == kAnAdbpg) {
+            const T q1 = Q[((int64_t)im.a1 * B + b) * N + p], q2 = Q[((int64_t)im.a2 * B + b) * N + p];
+            Y[p] = -q2;
+            Wv[p] = -q2;
+            Z[p] = D[p] - q1 - q2;
+        } else {
+            for (int a = 0; a < 3; ++a) {
+                const T q = Q[((int64_t)a * B + b) * N + p];
+                Y[(int64_t)a * N + p] = -q;
+                Wv[(int64_t)a * N + p] = -q;
+            }
+        }
+    }
+}
+
+// the first check at iteration 0
+__global__ void an_warm_state(AnGeom g, AnBuffers bf) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= g.B) return;
+    AnState &st = bf.st[b];
+    const int mode = bf.img[b].mode;
+    if (st.status != kLive || (mode != kAnAdbpg && mode != kAnFdpg3)) return;
+    st.warm = 1;
+    st.stage = kStCheck;
+    st.wphase = mode == kAnAdbpg ? 1 : 0;
+}
+
+// The warm pass's dual (tv_aniso.cpp:443-449): q1 = d + y - u, q2 = -y and
+// z = d - q1 - q2, for the second check.
+template <class T>
+__global__ void an_warm_z(AnGeom g, AnBuffers bf) {
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
+    const AnState &st = bf.st[b];
+    if (st.status != kLive || st.stage != kStWarm) return;
+    const int64_t N = g.N;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *Y = static_cast<const T *>(bf.y) + (int64_t)b * g.k * N;
+    const T *U = static_cast<const T *>(bf.u) + (int64_t)b * N;
+    T *Z = static_cast<T *>(bf.z) + (int64_t)b * N;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const T q1 = D[p] + Y[p] - U[p], q2 = -Y[p];
+        Z[p] = D[p] - q1 - q2;
+    }
+}
+
+__global__ void an_warm_next(AnGeom g, AnBuffers bf) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= g.B) return;
+    AnState &st = bf.st[b];
+    if (st.status == kLive && st.stage == kStWarm) st.stage = kStCheck;
+}
+
 // After a restart the extrapolated dual restarts from y (tv_aniso.cpp:474-477).
 template <class T>
 __global__ void an_restart_copy(AnGeom g, AnBuffers bf) {
@@ -796,6 +910,25 @@ __device__ __forceinline__ double tv_at(const AnGeom &g, const AnCall &c, const 
     return s;
 }
 
+// The stage after a check (and its polish, if any) that left the image
+// unconverged. In the loop: CheckSchedule::done for ADBPG, then iterate (or
+// finish at max_iter). A warm start's first check is followed by its pass
+// (ADBPG) and second check, which take no part in the schedule
+// (tv_aniso.cpp:473-486).
+__device__ __forceinline__ void after_check(AnState &s2, const AnImage &im, bool last) {
+    if (s2.wphase == 1 && im.mode == kAnAdbpg) {
+        s2.wphase = 2;
+        s2.stage = kStWarm;
+        return;
+    }
+    if (s2.wphase != 0) {
+        s2.wphase = 0;
+    } else if (im.mode == kAnAdbpg) {
+        check_done(s2, s2.gp, im.target);
+    }
+    s2.stage = last ? kStFinal : kStIter;
+}
+
 // stage kStCheck: the gap of z; kStFinal: the gap of zp (the final rebuild).
 template <class T>
 __global__ void __launch_bounds__(kThreads) an_gap(AnGeom g, AnCall c, AnBuffers bf, int stage) {
@@ -840,8 +973,7 @@ __global__ void __launch_bounds__(kThreads) an_gap(AnGeom g, AnCall c, AnBuffers
         s2.stage = kStPolish;
     } else {
         s2.gp = gz;
-        if (im.mode == kAnAdbpg) check_done(s2, gz, im.target);
-        s2.stage = last ? kStFinal : kStIter;
+        after_check(s2, im, last);
     }
     bf.st[b] = s2;
 }
@@ -1083,8 +1215,8 @@ __global__ void __launch_bounds__(kThreads) an_polish_gap(AnGeom g, AnCall c, An
         s2.gp = gz;
         s2.pol_accept = 0;
     }
-    if (im.mode == kAnAdbpg) check_done(s2, s2.gp, im.target);
-    s2.stage = (s2.gp <= im.target || last) ? kStFinal : kStIter;
+    if (s2.gp <= im.target) s2.stage = kStFinal;
+    else after_check(s2, im, last);
     bf.st[b] = s2;
 }
 
@@ -1308,6 +1440,12 @@ cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, int64
     }
     an_restart_copy<T><<<pg, kThreads, 0, s>>>(g, bf);
     ++nl;
+    if (c.warm && c.has_adbpg) {
+        // a warm start's pass (run by the first pass above) and its dual
+        an_warm_z<T><<<pg, kThreads, 0, s>>>(g, bf);
+        an_warm_next<<<((unsigned)g.B + 127) / 128, 128, 0, s>>>(g, bf);
+        nl += 2;
+    }
     // gap check (FDPG-3 forms its primal first)
     if (c.has_fdpg3) {
         an_fdpg3_primal<T><<<dim3((unsigned)((nf[2] + 127) / 128), B), 128, 0, s>>>(g, c, bf, kStCheck);
@@ -1335,6 +1473,17 @@ cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, int64
 }
 
 template <class T>
+cudaError_t warm_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s) {
+    for (int a = 0; a < g.k; ++a) {
+        const int64_t nf = g.N / g.L[a];
+        an_warm_feasible<T><<<dim3((unsigned)((nf + 127) / 128), (unsigned)g.B), 128, 0, s>>>(g, c, bf, a);
+    }
+    an_warm_init<T><<<dim3(an_pixel_blocks(g), (unsigned)g.B), kThreads, 0, s>>>(g, bf);
+    an_warm_state<<<((unsigned)g.B + 127) / 128, 128, 0, s>>>(g, bf);
+    return cudaGetLastError();
+}
+
+template <class T>
 cudaError_t output_t(const AnGeom &g, const AnBuffers &bf, void *out, cudaStream_t s) {
     an_output<T><<<dim3(an_pixel_blocks(g), (unsigned)g.B), kThreads, 0, s>>>(g, bf, static_cast<T *>(out));
     return cudaGetLastError();
@@ -1350,6 +1499,10 @@ int an_pixel_blocks(const AnGeom &g) {
 cudaError_t aniso_setup(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, const void *x,
                         cudaStream_t s) {
     return dtype == 1 ? setup_t<float>(g, c, bf, x, s) : setup_t<double>(g, c, bf, x, s);
+}
+
+cudaError_t aniso_warm(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, cudaStream_t s) {
+    return dtype == 1 ? warm_t<float>(g, c, bf, s) : warm_t<double>(g, c, bf, s);
 }
 
 void aniso_prepare(int dtype) {

@@ -20,6 +20,7 @@
 #include <atomic>
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "launch.h"
@@ -359,7 +360,16 @@ struct StepArgs {
 };
 
 constexpr int kLeanRowsMax = 32;  // rows per block of the lean 2D step
-constexpr int64_t kTailBlocks = 148 * 4;  // blocks a lean launch should have before its blocks grow
+// blocks a lean launch should have before its blocks grow (tuning hint
+// FASTPROX_B200_TAIL_BLOCKS)
+int64_t tail_blocks() {
+    static const int64_t v = [] {
+        const char *e = std::getenv("FASTPROX_B200_TAIL_BLOCKS");
+        const long long n = e ? std::atoll(e) : 0;
+        return (int64_t)(n > 0 ? n : 148 * 4);
+    }();
+    return v;
+}
 
 // ---------------------------------------------------------------------------
 // The 2D row-marching step: a warp spans 32 * VEC consecutive columns, a
@@ -1712,7 +1722,7 @@ cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, co
         A.row_part = 1;
         const int64_t H = g.L[0];
         int rows = sh.rows;
-        while (rows > 2 && nimg * sh.gx * ((H + rows - 1) / rows) < kTailBlocks) rows /= 2;
+        while (rows > 2 && nimg * sh.gx * ((H + rows - 1) / rows) < tail_blocks()) rows /= 2;
         sh2.rows = rows;
         sh2.gy = (int)((H + rows - 1) / rows);
         A.rows = rows;

@@ -100,3 +100,46 @@ def test_single_active_axis_is_exact_1d_tv(cuda):
     for b in range(2):
         ref = tv_np.tv1d(x[b, 0], 0.4)
         assert np.abs(z.cpu().numpy()[b, 0] - ref).max() <= 1e-12
+
+
+def test_warm_start_from_converged_dual_takes_no_iterations(cuda):
+    """The dual of a solve restarts it at its first check (iteration 0), in
+    float32 and float64; a warm start at a tighter tolerance continues."""
+    import torch
+    from fastprox_b200 import TVAniso, synth
+    for dt in (torch.float32, torch.float64):
+        x = torch.as_tensor(synth.phantom(2, 40, 48, seed=41), device=cuda).to(dt)
+        op = TVAniso(2)
+        z, info = op.solve(x, 0.1, tol=1e-6, max_iter=5000)
+        z2, info2 = op.solve(x, 0.1, tol=1e-6, max_iter=5000, dual=info.dual)
+        assert info2.iters == 0 and info2.converged
+        assert torch.allclose(z2, z, atol=1e-5)
+        tight = 1e-8 if dt == torch.float32 else 1e-11
+        z3, info3 = op.solve(x, 0.1, tol=tight, max_iter=20000, warm=True)
+        assert info3.converged
+
+
+@pytest.mark.parametrize("k,edge", [(2, False), (2, True), (3, False)])
+def test_warm_start_matches_reference(cuda, k, edge):
+    """A warm start of a nearby problem from the reference's dual of the
+    first (the reference's warm-start path: feasible dual, first check, the
+    warm pass for two axes), against the reference library doing the same, in
+    float64: z to 1e-9 and the same iteration counts."""
+    import torch
+    from fastprox_b200 import TVAniso, synth
+    from oracle import ref_capi
+    if not ref_capi.available():
+        pytest.skip("reference library not built")
+    shape = (2, 24, 30) if k == 2 else (1, 8, 9, 10)
+    x = (synth.phantom(shape[0], shape[1], shape[2], seed=42) if k == 2
+         else synth.phantom3d(shape[0], *shape[1:], seed=42)).astype(np.float64).reshape(shape)
+    x2 = x + 0.01 * np.random.default_rng(43).normal(size=x.shape)
+    beta = synth.pixel_weights((k,) + shape[-k:], seed=44) if edge else None
+    r1 = ref_capi.solve(x, 0.1, iso=False, k=k, spatial=beta, tol=1e-10, max_iter=100000)
+    r2 = ref_capi.solve(x2, 0.1, iso=False, k=k, spatial=beta, tol=1e-10, max_iter=100000, warm_dual=r1.dual)
+    op = TVAniso(k, edge_weights=beta)
+    xt = torch.as_tensor(x2, device=cuda)
+    z, info = op.solve(xt, 0.1, tol=1e-10, max_iter=100000, dual=torch.as_tensor(r1.dual, device=cuda))
+    zz = z.cpu().numpy()
+    assert np.linalg.norm(zz - r2.z) <= 1e-9 * np.linalg.norm(r2.z), np.linalg.norm(zz - r2.z) / np.linalg.norm(r2.z)
+    assert np.array_equal(info.image_iters, r2.iters), (info.image_iters, r2.iters)
