@@ -15,7 +15,7 @@ import numpy as np
 HERE = pathlib.Path(__file__).resolve().parent
 LIB_PATH = HERE / "libfastprox_b200.so"
 
-FP_F32, FP_F64 = 1, 2
+FP_F32, FP_F64, FP_I8, FP_I32, FP_I64 = 1, 2, 3, 4, 5
 FP_DEVICE_CPU, FP_DEVICE_CUDA = 0, 2
 STATUS = ["FP_OK", "FP_EINVAL", "FP_EDTYPE", "FP_ESHAPE", "FP_ENOMEM", "FP_ENOTCONV", "FP_EPARAM",
           "FP_EINTERNAL", "FP_EDEVICE"]
@@ -71,6 +71,15 @@ SIGNATURES = {
     "fp_jvp": (C.c_int, [_P, _P, _A, C.c_double, _A, _A]),
     "fp_vjp": (C.c_int, [_P, _P, _A, _A, C.POINTER(C.c_double), _A]),
     "fp_vjp_device": (C.c_int, [_P, _P, _A, _A, _A, _A]),
+    "fp_workspace_kinks": (C.c_int, [_P, C.c_double, _A, C.POINTER(C.c_int64)]),
+    "fp_workspace_set_branch": (C.c_int, [_P, _A, C.c_double]),
+    "fp_op_struct_kind": (C.c_int, [_P, C.POINTER(C.c_int)]),
+    "fp_workspace_units": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "fp_workspace_states": (C.c_int, [_P, _A, C.POINTER(C.c_int64)]),
+    "fp_workspace_regions": (C.c_int, [_P, _A, _A, C.POINTER(C.c_int64), C.c_int64]),
+    "fp_workspace_constraint": (C.c_int, [_P, _A, C.POINTER(C.c_int8), C.c_int64]),
+    "fp_workspace_deriv_exact": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "fp_workspace_refine": (C.c_int, [_P, _P, C.c_double, C.c_int, _A, C.POINTER(FpInfo)]),
     "fp_device_available": (C.c_int, [C.c_int]),
     "fp_op_device_check": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "fp_workspace_set_stream": (C.c_int, [_P, _P]),
@@ -126,12 +135,14 @@ class ArrayRef:
 
     def __init__(self, a):
         if isinstance(a, np.ndarray):
-            dt = {np.dtype(np.float32): FP_F32, np.dtype(np.float64): FP_F64}[a.dtype]
+            dt = {np.dtype(np.float32): FP_F32, np.dtype(np.float64): FP_F64, np.dtype(np.int8): FP_I8,
+                  np.dtype(np.int32): FP_I32, np.dtype(np.int64): FP_I64}[a.dtype]
             shape, strides = a.shape, tuple(s // a.itemsize for s in a.strides)
             ptr, dev = a.ctypes.data, FP_DEVICE_CPU
         else:  # torch.Tensor
             import torch
-            dt = {torch.float32: FP_F32, torch.float64: FP_F64}[a.dtype]
+            dt = {torch.float32: FP_F32, torch.float64: FP_F64, torch.int8: FP_I8, torch.int32: FP_I32,
+                  torch.int64: FP_I64}[a.dtype]
             shape, strides = tuple(a.shape), tuple(a.stride())
             ptr = a.data_ptr()
             dev = FP_DEVICE_CUDA if a.is_cuda else FP_DEVICE_CPU

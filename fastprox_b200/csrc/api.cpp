@@ -53,7 +53,7 @@ struct Arr {
         for (int d = 0; d < ndim; ++d) n *= shape[d];
         return n;
     }
-    size_t itemsize() const { return dtype == FP_F32 ? 4 : 8; }
+    size_t itemsize() const { return dtype == FP_F32 || dtype == FP_I32 ? 4 : (dtype == FP_I8 ? 1 : 8); }
     bool contiguous() const {
         int64_t s = 1;
         for (int d = ndim - 1; d >= 0; --d) {
@@ -77,14 +77,20 @@ int enum_bits_device(const fp_array *a) {
 
 constexpr int64_t kMaxElems = (int64_t(1) << 60) - 1;
 
-// src/api/api.cpp:57-110: dtype f32/f64, 0 <= ndim <= 32, extents >= 0,
-// the entry count and offset span below 2^60.
-fp_status to_arr(const fp_array *a, Arr &out) {
+// The dtypes an array may have (src/api/api.cpp:54-56): float32 and float64
+// (data), int8 (masks, states, signs, sides), int32 and int64 (labels).
+enum class Dt { Float, Int8, Label };
+
+// src/api/api.cpp:57-110: the dtype of its class, 0 <= ndim <= 32, extents
+// >= 0, the entry count and offset span below 2^60.
+fp_status to_arr(const fp_array *a, Arr &out, Dt kind = Dt::Float) {
     if (!a) return FP_EINVAL;
     const int dev = enum_bits_device(a);
     if (dev != FP_DEVICE_CPU && dev != FP_DEVICE_CUDA) return FP_EINVAL;
     const int dt = enum_bits_dtype(a);
-    if (dt != FP_F32 && dt != FP_F64) return FP_EDTYPE;
+    if (kind == Dt::Float && dt != FP_F32 && dt != FP_F64) return FP_EDTYPE;
+    if (kind == Dt::Int8 && dt != FP_I8) return FP_EDTYPE;
+    if (kind == Dt::Label && dt != FP_I32 && dt != FP_I64) return FP_EDTYPE;
     if (a->ndim < 0 || a->ndim > FP_MAX_NDIM) return FP_ESHAPE;
     out.data = static_cast<char *>(a->data);
     out.dtype = dt;
@@ -538,7 +544,10 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     if (ws->keep) {
         const size_t bn = (size_t)B * (size_t)N, kk = (size_t)g.k;
         A((void **)&ws->v_flat, bn);
-        if (op->kind == kAniso) A((void **)&ws->v_code, bn);
+        if (op->kind == kAniso) {
+            A((void **)&ws->v_code, bn);
+            A((void **)&ws->v_side, bn);
+        }
         A((void **)&ws->v_root, bn * sizeof(int));
         A((void **)&ws->v_cnt, bn * sizeof(int));
         A((void **)&ws->v_gz, kk * bn * sizeof(double));
@@ -1146,6 +1155,7 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
         ws->info_valid = false;
         ws->struct_valid = false;
         ws->identity = false;
+        ws->branch_on = false;  // an override belongs to the point it was set for
         ws->conj = conj;
     }
     if (x.numel() == 0) {
@@ -1566,6 +1576,8 @@ fp_status deriv_prepare(const fp_op *op, fp_workspace *ws, VjpGeom &vg, VjpBuffe
         bf.ast = ws->an_st;
         bf.avimg = reinterpret_cast<AnVjpImage *>(ws->v_img);
         bf.code = ws->v_code;
+        bf.side = ws->branch_on ? ws->v_side : nullptr;
+        vg.stol = ws->branch_tol;
         if (ws->struct_valid) return FP_OK;
         auto *hv = reinterpret_cast<AnVjpImage *>(ws->h_vimg);
         for (int64_t b = 0; b < g0.B; ++b) {
@@ -1933,6 +1945,391 @@ fp_status jvp_impl(const fp_op *op, fp_workspace *ws, const fp_array *dxa, doubl
     return read_cg(ws, nl);
 }
 
+// fp_workspace_refine (the reference's refine_impl, api.cpp:1182-1216): the
+// kept call solved again from its saved input (d at the input's scale) and,
+// warm, from its dual, to tol; the derivatives, the dual and the call's
+// results then describe the refined point. The input is rebuilt in V[1] and
+// a result nobody asked for goes to V[0]: neither is read by the solve after
+// its set-up, nor by the derivatives after it.
+fp_status refine_impl(const fp_op *op, fp_workspace *ws, double tol, int max_iter, fp_array *oa, fp_info *info) {
+    if (!op || !ws || ws->op != op || !ws->valid || !ws->keep) return FP_EINVAL;
+    if (!(tol >= 0.0) || !std::isfinite(tol) || max_iter < 1) return FP_EPARAM;
+    Arr out;
+    if (oa) {
+        if (fp_status s = to_arr(oa, out)) return s;
+        if (out.dtype != ws->dtype) return FP_EDTYPE;
+        if (out.ndim != ws->ndim) return FP_ESHAPE;
+        for (int d = 0; d < out.ndim; ++d)
+            if (out.shape[d] != ws->shape[d]) return FP_ESHAPE;
+        if (fp_status s = check_output(nullptr, out)) return s;
+    }
+    if (ws->identity) return oa ? FP_EINVAL : FP_OK;  // sigma = 0 saved no input to refine
+    const Geometry &g0 = ws->g;
+    const int64_t total = g0.B * g0.N;
+    if (total == 0) return FP_OK;
+    DeviceScope dsc(ws->device);
+    cudaStream_t s = ws->stream;
+    const bool aniso = op->kind == kAniso;
+    const bool conj = ws->conj;
+    // the saved input: d 2^e per image, into V[1]
+    std::vector<int> ex((size_t)g0.B);
+    std::vector<double> steps((size_t)g0.B);
+    for (int64_t b = 0; b < g0.B; ++b) {
+        ex[(size_t)b] = aniso ? ws->h_an_img[b].e : ws->h_img[b].e;
+        steps[(size_t)b] = aniso ? ws->h_an_img[b].gamma_in : ws->h_img[b].gamma_in;
+    }
+    cudaError_t e = cudaMemcpyAsync(ws->lmap, ex.data(), ex.size() * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = unscale_images(ws->dtype, ws->d, ws->lmap, g0.N, g0.B, ws->V[1], s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e);
+    const size_t T = ws->dtype == FP_F32 ? 4 : 8;
+    std::vector<char> hx, hz;
+    fp_array xa{}, za{}, sa{};
+    xa.dtype = (fp_dtype)ws->dtype;
+    xa.ndim = ws->ndim;
+    xa.shape = ws->shape;
+    xa.strides = nullptr;
+    za = xa;
+    if (ws->host_mode) {
+        hx.resize((size_t)total * T);
+        e = cudaMemcpyAsync(hx.data(), ws->V[1], hx.size(), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e);
+        xa.data = hx.data();
+        xa.device = FP_DEVICE_CPU;
+        if (!oa) hz.resize(hx.size());
+        za.data = hz.data();
+        za.device = FP_DEVICE_CPU;
+    } else {
+        xa.data = ws->V[1];
+        xa.device = FP_DEVICE_CUDA;
+        za.data = ws->V[0];
+        za.device = FP_DEVICE_CUDA;
+    }
+    fp_options o{};
+    fp_options_init(&o);
+    o.tol = tol;
+    o.max_iter = max_iter;
+    o.keep_structure = 1;
+    const int64_t one = (int64_t)g0.B;
+    const int64_t bshape[1] = {one};
+    sa.data = steps.data();
+    sa.dtype = FP_F64;
+    sa.ndim = 1;
+    sa.shape = bshape;
+    sa.strides = nullptr;
+    sa.device = FP_DEVICE_CPU;
+    // the steps per image over the batch shape
+    std::vector<int64_t> bsh((size_t)std::max(1, ws->ndim - g0.k));
+    const bool batched = ws->ndim > g0.k;
+    if (batched) {
+        for (int d = 0; d < ws->ndim - g0.k; ++d) bsh[(size_t)d] = ws->shape[d];
+        sa.ndim = ws->ndim - g0.k;
+        sa.shape = bsh.data();
+    }
+    const bool was_warm = ws->warm;
+    ws->warm = true;
+    fp_info local{0.0, 0, 0};
+    fp_status st;
+    fp_array *outp = oa ? oa : &za;
+    if (conj) st = prox_impl(op, 1.0, &xa, outp, &o, ws, info ? info : &local, true, nullptr);
+    else if (batched) st = prox_impl(op, 0.0, &xa, outp, &o, ws, info ? info : &local, false, &sa);
+    else st = prox_impl(op, steps[0], &xa, outp, &o, ws, info ? info : &local, false, nullptr);
+    ws->warm = was_warm;
+    return st;
+}
+
+// ---- structure of the derivative (the reference's api.cpp:1032-1180; its
+// queries refuse device workspaces, which this library answers) ----
+
+fp_status struct_ws(const fp_workspace *ws) {
+    if (!ws || !ws->op || !ws->keep || !ws->valid) return FP_EINVAL;
+    return FP_OK;
+}
+
+int64_t struct_units(const fp_workspace &ws) { return ws.g.B * ws.g.N == 0 ? 0 : ws.g.B; }
+
+// An output array of the queries: x's shape, of its dtype class (Float: x's dtype).
+fp_status struct_out(const fp_workspace &ws, const fp_array *a, Arr &out, Dt kind) {
+    if (fp_status s = to_arr(a, out, kind)) return s;
+    if (kind == Dt::Float && out.dtype != ws.dtype) return FP_EDTYPE;
+    if (out.ndim != ws.ndim) return FP_ESHAPE;
+    for (int d = 0; d < out.ndim; ++d)
+        if (out.shape[d] != ws.shape[d]) return FP_ESHAPE;
+    if (out.numel() > 0 && out.device == FP_DEVICE_CUDA && pointer_device(out.data) != ws.device) return FP_EINVAL;
+    return FP_OK;
+}
+
+// Writes host values (C order, out's element size) into out, on the host or
+// the device (through the workspace's V[0] and a scatter).
+fp_status put_array(fp_workspace *ws, const Arr &out, const std::vector<char> &h) {
+    const int64_t n = out.numel();
+    if (n == 0) return FP_OK;
+    const size_t es = out.itemsize();
+    if (out.device == FP_DEVICE_CPU) {
+        std::vector<int64_t> idx((size_t)out.ndim, 0);
+        for (int64_t i = 0; i < n; ++i) {
+            int64_t o = 0;
+            for (int d = 0; d < out.ndim; ++d) o += idx[(size_t)d] * out.strides[d];
+            std::memcpy(out.data + o * (int64_t)es, h.data() + i * (int64_t)es, es);
+            for (int d = out.ndim - 1; d >= 0; --d) {
+                if (++idx[(size_t)d] < out.shape[d]) break;
+                idx[(size_t)d] = 0;
+            }
+        }
+        return FP_OK;
+    }
+    cudaStream_t s = ws->stream;
+    cudaError_t e;
+    if (out.contiguous()) {
+        e = cudaMemcpyAsync(out.data, h.data(), h.size(), cudaMemcpyHostToDevice, s);
+    } else {
+        e = cudaMemcpyAsync(ws->V[0], h.data(), h.size(), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = scatter_elements(ws->V[0], es, out.ndim, out.shape, out.strides, out.data, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return cuda_status(e);
+}
+
+template <class V>
+std::vector<char> filled(int64_t n, V v) {
+    std::vector<char> h((size_t)n * sizeof(V));
+    for (int64_t i = 0; i < n; ++i) std::memcpy(h.data() + i * (int64_t)sizeof(V), &v, sizeof(V));
+    return h;
+}
+
+// The kept point's structure on the device, and its geometry (for an
+// isotropic point also the weights and the dual, which the kink test reads).
+fp_status struct_prepare(fp_workspace *ws, VjpGeom &vg, VjpBuffers &bf) {
+    const fp_op *op = ws->op;
+    if (fp_status st = deriv_prepare(op, ws, vg, bf)) return st;
+    for (int a = 0; a < 3; ++a) vg.w[a] = a < ws->g.k ? op->w[a] : 0.0;
+    bf.qd = ws->dual;
+    return FP_OK;
+}
+
+fp_status units_impl(const fp_workspace *ws, int64_t *count, int64_t *size) {
+    if (fp_status s = struct_ws(ws)) return s;
+    if (count) *count = struct_units(*ws);
+    if (size) *size = ws->g.N;
+    return FP_OK;
+}
+
+fp_status states_impl(fp_workspace *ws, fp_array *sa, int64_t *nfixed) {
+    if (fp_status s = struct_ws(ws)) return s;
+    Arr st;
+    if (sa)
+        if (fp_status s = struct_out(*ws, sa, st, Dt::Int8)) return s;
+    // every entry of a TV solution moves with its region; after the
+    // conjugate at sigma = 0 the inner prox's Jacobian I - J is 0
+    const int64_t total = ws->g.B * ws->g.N;
+    const int8_t v = ws->identity ? (int8_t)FP_ENTRY_ZERO : (int8_t)FP_ENTRY_FREE;
+    if (sa)
+        if (fp_status s = put_array(ws, st, filled<int8_t>(total, v))) return s;
+    if (nfixed) *nfixed = ws->identity ? total : 0;
+    return FP_OK;
+}
+
+fp_status regions_impl(fp_workspace *ws, fp_array *la, fp_array *ga, int64_t *nregions, int64_t count) {
+    if (fp_status s = struct_ws(ws)) return s;
+    const int64_t units = struct_units(*ws);
+    if (nregions && count != units) return FP_ESHAPE;
+    Arr lab, sg;
+    if (la) {
+        if (fp_status s = struct_out(*ws, la, lab, Dt::Label)) return s;
+        if (lab.dtype == FP_I32 && ws->g.N > std::numeric_limits<int32_t>::max()) return FP_ESHAPE;
+    }
+    if (ga)
+        if (fp_status s = struct_out(*ws, ga, sg, Dt::Int8)) return s;
+    const Geometry &g0 = ws->g;
+    const int64_t total = g0.B * g0.N;
+    if (total == 0) return FP_OK;
+    DeviceScope dsc(ws->device);
+    std::vector<int32_t> hl((size_t)total, -1);
+    std::vector<double> hn((size_t)g0.B, 0.0);
+    if (!ws->identity) {
+        VjpGeom vg;
+        VjpBuffers bf;
+        if (fp_status st = struct_prepare(ws, vg, bf)) return st;
+        cudaStream_t s = ws->stream;
+        int32_t *dl = static_cast<int32_t *>(ws->V[1]);
+        double *dn = ws->v_ggam;
+        cudaError_t e = query_labels(ws->op->kind == kAniso, vg, bf, dl, dn, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hl.data(), dl, (size_t)total * 4, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hn.data(), dn, (size_t)g0.B * 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    if (nregions)
+        for (int64_t b = 0; b < g0.B; ++b) nregions[b] = (int64_t)hn[(size_t)b];
+    if (la) {
+        std::vector<char> h((size_t)total * lab.itemsize());
+        for (int64_t i = 0; i < total; ++i) {
+            if (lab.dtype == FP_I32) std::memcpy(h.data() + i * 4, &hl[(size_t)i], 4);
+            else {
+                const int64_t v = hl[(size_t)i];
+                std::memcpy(h.data() + i * 8, &v, 8);
+            }
+        }
+        if (fp_status st = put_array(ws, lab, h)) return st;
+    }
+    if (ga) {
+        std::vector<char> h((size_t)total);
+        for (int64_t i = 0; i < total; ++i) h[(size_t)i] = (char)(hl[(size_t)i] >= 0 ? 1 : 0);
+        if (fp_status st = put_array(ws, sg, h)) return st;
+    }
+    return FP_OK;
+}
+
+fp_status constraint_impl(fp_workspace *ws, fp_array *ca, int8_t *active, int64_t count) {
+    if (fp_status s = struct_ws(ws)) return s;
+    if (active && count != struct_units(*ws)) return FP_ESHAPE;
+    Arr c;
+    if (ca)
+        if (fp_status s = struct_out(*ws, ca, c, Dt::Float)) return s;
+    // TV has no linear constraint
+    if (active) std::fill(active, active + count, int8_t{0});
+    if (ca) {
+        const int64_t total = ws->g.B * ws->g.N;
+        if (ws->dtype == FP_F32) return put_array(ws, c, filled<float>(total, 0.0f));
+        return put_array(ws, c, filled<double>(total, 0.0));
+    }
+    return FP_OK;
+}
+
+// Every image's derivative exact, and the largest curvature cap of the
+// isotropic derivative in the units of x (the reference's api.cpp:1219-1232).
+fp_status deriv_exact_impl(const fp_workspace *ws, int *exact, double *smoothing) {
+    if (!ws || !ws->valid || !ws->keep) return FP_EINVAL;
+    int all = 1;
+    double mu = 0.0;
+    const Geometry &g0 = ws->g;
+    if (!ws->identity && g0.B * g0.N != 0) {
+        if (ws->op->kind == kAniso) {
+            for (int64_t b = 0; b < g0.B; ++b) {
+                const AnImage &im = ws->h_an_img[b];
+                if ((im.mode == kAnAdbpg || im.mode == kAnFdpg3) && !ws->h_an_st[b].polished) all = 0;
+            }
+        } else {
+            // mu = 0.1 wmax sqrt(2 gap / N) at the solved scale (tv_iso.cpp:566-568)
+            double wmax = 0.0;
+            for (int a = 0; a < g0.k; ++a)
+                if (ws->op->w[a] > 0.0 && g0.L[a] > 1) wmax = std::max(wmax, ws->op->w[a]);
+            for (int64_t b = 0; b < g0.B; ++b) {
+                const IsoImage &im = ws->h_img[b];
+                if (im.mode != kModeFdpg) continue;
+                const double m = 0.1 * wmax * std::sqrt(2.0 * std::max(ws->h_st[b].gp, 0.0) / (double)g0.N);
+                if (m > 0.0) all = 0;
+                mu = std::max(mu, std::ldexp(m, im.e));
+            }
+        }
+    }
+    if (exact) *exact = all;
+    if (smoothing) *smoothing = mu;
+    return FP_OK;
+}
+
+// The kept point's kink mask (FP_I8, x's shape) and the number of entries at
+// a kink (the reference's kinks_impl, api.cpp:857-875).
+fp_status kinks_impl(fp_workspace *ws, double tol, fp_array *ma, int64_t *count) {
+    if (!(tol >= 0.0) || !std::isfinite(tol)) return FP_EPARAM;
+    if (!ws || !ws->op || !ws->keep || !ws->valid) return FP_EINVAL;
+    Arr m;
+    if (ma)
+        if (fp_status s = struct_out(*ws, ma, m, Dt::Int8)) return s;
+    const Geometry &g0 = ws->g;
+    const int64_t total = g0.B * g0.N;
+    std::vector<char> h((size_t)total, 0);
+    int64_t c = 0;
+    if (!ws->identity && total != 0) {
+        DeviceScope dsc(ws->device);
+        VjpGeom vg;
+        VjpBuffers bf;
+        if (fp_status st = struct_prepare(ws, vg, bf)) return st;
+        const bool aniso = ws->op->kind == kAniso;
+        std::vector<double> gam((size_t)g0.B);
+        for (int64_t b = 0; b < g0.B; ++b) gam[(size_t)b] = aniso ? ws->h_an_img[b].gamma_in : ws->h_img[b].gamma_in;
+        cudaStream_t s = ws->stream;
+        // the steps into the structure's scratch (b, free between derivative calls)
+        cudaError_t e = cudaMemcpyAsync(bf.b, gam.data(), gam.size() * 8, cudaMemcpyHostToDevice, s);
+        int8_t *dm = static_cast<int8_t *>(ws->V[1]);
+        if (e == cudaSuccess) e = query_kinks(ws->dtype, aniso, vg, bf, bf.b, tol, dm, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), dm, (size_t)total, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e);
+        for (int64_t i = 0; i < total; ++i) c += h[(size_t)i] != 0;
+    }
+    if (ma)
+        if (fp_status st = put_array(ws, m, h)) return st;
+    if (count) *count = c;
+    return FP_OK;
+}
+
+// A branch override for the derivatives of an anisotropic kept point (the
+// reference's set_branch_impl, api.cpp:993-1028): the structure is rebuilt
+// with side applied at the kinks found with tol; NULL clears it.
+fp_status set_branch_impl(fp_workspace *ws, const fp_array *sa, double tol) {
+    if (!sa) {
+        if (!ws || !ws->op) return FP_EINVAL;
+        if (ws->branch_on) ws->struct_valid = false;
+        ws->branch_on = false;
+        return FP_OK;
+    }
+    if (!(tol >= 0.0) || !std::isfinite(tol)) return FP_EPARAM;
+    if (!ws || !ws->op || !ws->keep) return FP_EINVAL;
+    if (ws->op->kind != kAniso) return FP_EINVAL;  // isotropic TV has no branches
+    if (!ws->valid) return FP_EINVAL;
+    Arr a;
+    if (fp_status s = to_arr(sa, a, Dt::Int8)) return s;
+    if (a.ndim != ws->ndim) return FP_ESHAPE;
+    for (int d = 0; d < a.ndim; ++d)
+        if (a.shape[d] != ws->shape[d]) return FP_ESHAPE;
+    const int64_t total = ws->g.B * ws->g.N;
+    if (ws->identity || total == 0) return FP_OK;
+    // the sides in C order, checked before the workspace changes
+    std::vector<int8_t> h((size_t)total);
+    DeviceScope dsc(ws->device);
+    cudaStream_t s = ws->stream;
+    {
+        std::vector<int64_t> idx((size_t)a.ndim, 0);
+        const bool dev = a.device == FP_DEVICE_CUDA;
+        std::vector<int8_t> whole;
+        int64_t lo = 0, span = 1;
+        if (dev) {
+            // the array's byte range to the host, then read by its strides
+            for (int d = 0; d < a.ndim; ++d) {
+                if (a.shape[d] < 2) continue;
+                const int64_t e = (a.shape[d] - 1) * a.strides[d];
+                if (e < 0) lo += e;
+                else span += e;
+            }
+            span -= lo;
+            whole.resize((size_t)span);
+            cudaError_t e = cudaMemcpyAsync(whole.data(), a.data + lo, (size_t)span, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+        for (int64_t i = 0; i < total; ++i) {
+            int64_t o = 0;
+            for (int d = 0; d < a.ndim; ++d) o += idx[(size_t)d] * a.strides[d];
+            const int8_t v = dev ? whole[(size_t)(o - lo)] : reinterpret_cast<const int8_t *>(a.data)[o];
+            if (v < -1 || v > 1) return FP_EPARAM;
+            h[(size_t)i] = v;
+            for (int d = a.ndim - 1; d >= 0; --d) {
+                if (++idx[(size_t)d] < a.shape[d]) break;
+                idx[(size_t)d] = 0;
+            }
+        }
+    }
+    cudaError_t e = cudaMemcpyAsync(ws->v_side, h.data(), h.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e);
+    ws->branch_on = true;
+    ws->branch_tol = tol;
+    ws->struct_valid = false;
+    return FP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1977,6 +2374,48 @@ FP_API fp_status fp_vjp(const fp_op *op, const fp_workspace *ws, const fp_array 
 FP_API fp_status fp_vjp_device(const fp_op *op, const fp_workspace *ws, const fp_array *g, fp_array *gx,
                                fp_array *ggamma, fp_array *gparams) {
     return guard([&] { return vjp_impl(op, const_cast<fp_workspace *>(ws), g, gx, nullptr, ggamma, gparams); });
+}
+
+FP_API fp_status fp_op_struct_kind(const fp_op *op, int *kind) {
+    if (!op || !kind) return FP_EINVAL;
+    // isotropic: J = M (M^T (I + G^T H G) M)^-1 M^T, range span M, not a
+    // projector; anisotropic: the average over each component, a projector
+    *kind = op->kind == kIso ? FP_STRUCT_CURVED : FP_STRUCT_PROJECTOR;
+    return FP_OK;
+}
+
+FP_API fp_status fp_workspace_units(const fp_workspace *ws, int64_t *count, int64_t *size) {
+    return guard([&] { return units_impl(ws, count, size); });
+}
+
+FP_API fp_status fp_workspace_states(const fp_workspace *ws, fp_array *state, int64_t *nfixed) {
+    return guard([&] { return states_impl(const_cast<fp_workspace *>(ws), state, nfixed); });
+}
+
+FP_API fp_status fp_workspace_regions(const fp_workspace *ws, fp_array *labels, fp_array *sign, int64_t *nregions,
+                                      int64_t count) {
+    return guard([&] { return regions_impl(const_cast<fp_workspace *>(ws), labels, sign, nregions, count); });
+}
+
+FP_API fp_status fp_workspace_constraint(const fp_workspace *ws, fp_array *coef, int8_t *active, int64_t count) {
+    return guard([&] { return constraint_impl(const_cast<fp_workspace *>(ws), coef, active, count); });
+}
+
+FP_API fp_status fp_workspace_deriv_exact(const fp_workspace *ws, int *exact, double *smoothing) {
+    return guard([&] { return deriv_exact_impl(ws, exact, smoothing); });
+}
+
+FP_API fp_status fp_workspace_kinks(const fp_workspace *ws, double tol, fp_array *mask, int64_t *count) {
+    return guard([&] { return kinks_impl(const_cast<fp_workspace *>(ws), tol, mask, count); });
+}
+
+FP_API fp_status fp_workspace_set_branch(fp_workspace *ws, const fp_array *side, double tol) {
+    return guard([&] { return set_branch_impl(ws, side, tol); });
+}
+
+FP_API fp_status fp_workspace_refine(const fp_op *op, fp_workspace *ws, double tol, int max_iter, fp_array *out,
+                                     fp_info *info) {
+    return guard([&] { return refine_impl(op, ws, tol, max_iter, out, info); });
 }
 
 }  // extern "C"

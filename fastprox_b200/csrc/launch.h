@@ -78,6 +78,8 @@ cudaError_t fill_double(double *dst, double v, int64_t n, cudaStream_t s);
 cudaError_t strided_copy(const void *src, int src_dtype, const int64_t *shape, const int64_t *src_strides,
                          int ndim, void *dst, int dst_dtype, const int64_t *dst_strides, cudaStream_t s);
 // out = y - out (the conjugate's y - prox(y)), contiguous, n entries.
+// x = d 2^e[b] for each image b of N entries (e: B ints on the device).
+cudaError_t unscale_images(int dtype, const void *d, const int *e, int64_t N, int64_t B, void *x, cudaStream_t s);
 cudaError_t conj_finish(int dtype, const void *y, void *out, int64_t n, cudaStream_t s);
 
 }  // namespace fpb

@@ -1583,6 +1583,16 @@ __global__ void conj_kernel(const T *__restrict__ y, T *__restrict__ out, int64_
         out[i] = y[i] - out[i];
 }
 
+// x = d 2^e per image (the staged input back at its own scale)
+template <class T>
+__global__ void unscale_kernel(const T *__restrict__ d, const int *__restrict__ e, int64_t N, int64_t B,
+                               T *__restrict__ x) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < B * N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int ex = e[i / N];
+        x[i] = ex ? ldexp_t(d[i], ex) : d[i];
+    }
+}
+
 __global__ void fill_double_kernel(double *dst, double v, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         dst[i] = v;
@@ -1876,6 +1886,17 @@ cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const I
 
 cudaError_t fill_double(double *dst, double v, int64_t n, cudaStream_t s) {
     fill_double_kernel<<<grid_for(n, 256), 256, 0, s>>>(dst, v, n);
+    return cudaGetLastError();
+}
+
+cudaError_t unscale_images(int dtype, const void *d, const int *e, int64_t N, int64_t B, void *x, cudaStream_t s) {
+    if (N * B == 0) return cudaSuccess;
+    if (dtype == 1)
+        unscale_kernel<float><<<grid_for(N * B, 256), 256, 0, s>>>(static_cast<const float *>(d), e, N, B,
+                                                                   static_cast<float *>(x));
+    else
+        unscale_kernel<double><<<grid_for(N * B, 256), 256, 0, s>>>(static_cast<const double *>(d), e, N, B,
+                                                                    static_cast<double *>(x));
     return cudaGetLastError();
 }
 

@@ -997,7 +997,12 @@ __global__ void __launch_bounds__(128) ad_codes(VjpGeom g, VjpBuffers bf, int a)
             const double le = lam * w;
             const double jump = fabs(zn - zi);
             const bool certified = cert && le > 0.0 && jump > vi.tau;
-            const bool flat = (fabs(pe) < le * (1.0 - g.eta) && !certified) || (le > 0.0 && jump <= vi.tau0);
+            bool flat = (fabs(pe) < le * (1.0 - g.eta) && !certified) || (le > 0.0 && jump <= vi.tau0);
+            if (bf.side) {  // a branch override at a kink (tv_aniso.cpp:1150-1154)
+                const int sd = bf.side[(int64_t)b * N + i];
+                const bool kink = sd != 0 && le > 0.0 && jump <= g.stol && fabs(pe) >= le - g.stol;
+                flat = kink ? sd < 0 : flat;
+            }
             const bool from_z = certified || (bf.beta && w == 0.0);
             const uint8_t c = from_z ? zc : an_sgn(-pe, sh);
             if (flat) F[i] |= bit;
@@ -1162,6 +1167,140 @@ __global__ void __launch_bounds__(kT) ad_jvp_out(VjpGeom g, VjpBuffers bf, const
         double v = t / (double)Cn[r];
         if (conj) v = (dx ? (double)dx[(int64_t)b * N + p] : 0.0) - v;
         dz[(int64_t)b * N + p] = (T)v;
+    }
+}
+
+// ---- structure queries ----------------------------------------------------------
+
+__device__ __forceinline__ bool q_nan(const VjpBuffers &bf, bool aniso, int b) {
+    return aniso ? bf.aimg[b].mode == kAnNan : bf.img[b].mode == kModeNan;
+}
+
+// Labels in order of each region's first entry (its root, the smallest
+// index): one block per image scans the roots in order; every other entry
+// then takes its root's label.
+__global__ void __launch_bounds__(1024) q_label_roots(VjpGeom g, VjpBuffers bf, bool aniso, int32_t *labels,
+                                                      double *nreg) {
+    __shared__ int wsum[32];
+    __shared__ int base;
+    const int b = blockIdx.x;
+    const int64_t N = g.N;
+    const int *R = bf.root + (int64_t)b * N;
+    int32_t *Lb = labels + (int64_t)b * N;
+    if (q_nan(bf, aniso, b)) {
+        if (threadIdx.x == 0) nreg[b] = -1.0;
+        return;
+    }
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int64_t c0 = 0; c0 < N; c0 += blockDim.x) {
+        const int64_t i = c0 + threadIdx.x;
+        const int f = (i < N && R[i] == i) ? 1 : 0;
+        int x = f;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int w = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        if (f) Lb[i] = base + (wid > 0 ? wsum[wid - 1] : 0) + x - 1;
+        __syncthreads();
+        if (threadIdx.x == 0) base += wsum[(blockDim.x >> 5) - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) nreg[b] = (double)base;
+}
+
+__global__ void __launch_bounds__(kT) q_label_rest(VjpGeom g, VjpBuffers bf, bool aniso, int32_t *labels) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N;
+    const int *R = bf.root + (int64_t)b * N;
+    int32_t *Lb = labels + (int64_t)b * N;
+    const bool nan = q_nan(bf, aniso, b);
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        if (nan) Lb[p] = -1;
+        else if (R[p] != p) Lb[p] = Lb[R[p]];
+    }
+}
+
+// kink_image of isotropic TV (tv_iso.cpp:654-678): 1 where |(W D z)_p| <= tol
+// and |u_p| >= gamma alpha_p - tol, for pixels of positive radius
+template <class T>
+__global__ void __launch_bounds__(kT) q_kinks_iso(VjpGeom g, VjpBuffers bf, const double *gam, double tol,
+                                                  int8_t *mask) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N, B = g.B;
+    const int e = bf.img[b].e;
+    const T *Q = static_cast<const T *>(bf.qd);
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const Px x = pix_of(g, p);
+        const double z0 = ldexp(z_at<T>(g, bf, b, p), e);
+        double gg = 0.0, uu = 0.0;
+        for (int a = 0; a < g.k; ++a) {
+            if (g.w[a] > 0.0 && x.co[a] + 1 < g.L[a]) {
+                const double t = g.w[a] * (ldexp(z_at<T>(g, bf, b, p + g.S[a]), e) - z0);
+                gg += t * t;
+            }
+            const double u = (double)Q[((int64_t)a * B + b) * N + p];
+            uu += u * u;
+        }
+        double r = gam[b];
+        if (bf.alpha) r *= (double)static_cast<const T *>(bf.alpha)[(int64_t)b * bf.alpha_stride + p];
+        mask[(int64_t)b * N + p] = (int8_t)(r > 0.0 && sqrt(gg) <= tol && sqrt(uu) >= r - tol);
+    }
+}
+
+// kink_image of anisotropic TV (tv_aniso.cpp:1318-1348) along axis a: bit a
+// at the edge's first entry when its jump is within tol of 0 and its 1D dual
+// within tol of its bound gamma w_a beta_e (edges of zero bound are free)
+template <class T>
+__global__ void __launch_bounds__(128) q_kinks_aniso(VjpGeom g, VjpBuffers bf, const double *gam, double tol, int a,
+                                                     int8_t *mask) {
+    const int b = blockIdx.y;
+    const int64_t N = g.N, B = g.B, L = g.L[a], s = g.S[a];
+    const double lam = gam[b] * g.w[a];
+    if (!(lam > 0.0) || L == 1 || bf.aimg[b].mode == kAnNan) return;
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= N / L) return;
+    const int64_t base = (f / s) * L * s + f % s;
+    const int e = bf.aimg[b].e;
+    const T *Q = static_cast<const T *>(bf.qd) + ((int64_t)a * B + b) * N;
+    double acc = 0.0;
+    double zi = ldexp(an_z<T>(g, bf, b, base), e);
+    for (int64_t l = 0; l + 1 < L; ++l) {
+        const int64_t i = base + l * s;
+        acc += (double)Q[i];
+        const double zn = ldexp(an_z<T>(g, bf, b, i + s), e);
+        const double r = bf.beta ? lam * an_beta<T>(g, bf, a, i) : lam;
+        if (r > 0.0 && fabs(zn - zi) <= tol && fabs(acc) >= r - tol)
+            mask[(int64_t)b * N + i] = (int8_t)(mask[(int64_t)b * N + i] | (1 << a));
+        zi = zn;
+    }
+}
+
+struct ScatterDesc {
+    int ndim;
+    int64_t shape[8], st[8];
+};
+
+__global__ void scatter_kernel(const unsigned char *src, size_t esize, ScatterDesc d, int64_t n, unsigned char *dst) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = i, o = 0;
+        for (int k = d.ndim - 1; k >= 0; --k) {
+            o += (r % d.shape[k]) * d.st[k];
+            r /= d.shape[k];
+        }
+        for (size_t j = 0; j < esize; ++j) dst[o * (int64_t)esize + (int64_t)j] = src[i * (int64_t)esize + (int64_t)j];
     }
 }
 
@@ -1380,6 +1519,54 @@ cudaError_t an_jvp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, cons
                          const JvpDir &dir, const double *dbeta, int conj, cudaStream_t s, int64_t *launches) {
     return dtype == 1 ? an_jvp_t<float>(g, bf, dx, dz, dgamma, dir, dbeta, conj, s, launches)
                       : an_jvp_t<double>(g, bf, dx, dz, dgamma, dir, dbeta, conj, s, launches);
+}
+
+}  // namespace fpb
+
+namespace fpb {
+
+cudaError_t query_labels(bool aniso, const VjpGeom &g, const VjpBuffers &bf, int32_t *labels, double *nreg,
+                         cudaStream_t s) {
+    q_label_roots<<<(unsigned)g.B, 1024, 0, s>>>(g, bf, aniso, labels, nreg);
+    q_label_rest<<<dim3(pblocks(g), (unsigned)g.B), kT, 0, s>>>(g, bf, aniso, labels);
+    return cudaGetLastError();
+}
+
+cudaError_t query_kinks(int dtype, bool aniso, const VjpGeom &g, const VjpBuffers &bf, const double *gam,
+                        double tol, int8_t *mask, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(mask, 0, (size_t)g.B * (size_t)g.N, s);
+    if (e != cudaSuccess) return e;
+    if (!aniso) {
+        const dim3 grid(pblocks(g), (unsigned)g.B);
+        if (dtype == 1) q_kinks_iso<float><<<grid, kT, 0, s>>>(g, bf, gam, tol, mask);
+        else q_kinks_iso<double><<<grid, kT, 0, s>>>(g, bf, gam, tol, mask);
+    } else {
+        for (int a = 0; a < g.k; ++a) {
+            const int64_t nf = g.N / g.L[a];
+            const dim3 grid((unsigned)((nf + 127) / 128), (unsigned)g.B);
+            if (dtype == 1) q_kinks_aniso<float><<<grid, 128, 0, s>>>(g, bf, gam, tol, a, mask);
+            else q_kinks_aniso<double><<<grid, 128, 0, s>>>(g, bf, gam, tol, a, mask);
+        }
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t scatter_elements(const void *src, size_t esize, int ndim, const int64_t *shape, const int64_t *strides,
+                             void *dst, cudaStream_t s) {
+    if (ndim > 8) return cudaErrorInvalidValue;
+    ScatterDesc d{};
+    d.ndim = ndim;
+    int64_t n = 1;
+    for (int k = 0; k < ndim; ++k) {
+        d.shape[k] = shape[k];
+        d.st[k] = strides[k];
+        n *= shape[k];
+    }
+    if (n == 0) return cudaSuccess;
+    const int grid = (int)std::min<int64_t>((n + 255) / 256, 4096);
+    scatter_kernel<<<grid, 256, 0, s>>>(static_cast<const unsigned char *>(src), esize, d, n,
+                                        static_cast<unsigned char *>(dst));
+    return cudaGetLastError();
 }
 
 }  // namespace fpb

@@ -26,6 +26,7 @@ struct VjpGeom {
     double bmax[3];
     double w[3];
     double eps_t;  // the epsilon of the iterates' dtype
+    double stol;   // the tolerance of a branch override (side in VjpBuffers)
 };
 
 // A direction in the axis weights for the forward derivative.
@@ -84,6 +85,7 @@ struct VjpBuffers {
     const AnState *ast = nullptr;
     AnVjpImage *avimg = nullptr;
     uint8_t *code = nullptr;
+    const int8_t *side = nullptr;  // a branch override per entry (-1, 0, +1), or null
     double *part = nullptr;
     unsigned *ticket = nullptr;
     int *live = nullptr, *err = nullptr;
@@ -99,6 +101,20 @@ cudaError_t vjp_structure(int dtype, const VjpGeom &g, const VjpBuffers &bf, cud
 cudaError_t an_vjp_structure(int dtype, const VjpGeom &g, const VjpBuffers &bf, cudaStream_t s);
 cudaError_t an_vjp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *gin, void *gx, int conj,
                          bool params, double *gb, cudaStream_t s, int64_t *launches);
+// Structure queries of a kept point whose structure is built (the reference's
+// fp_workspace_regions and fp_workspace_kinks, api.cpp:1076-1170, 857-875):
+// per image the labels of its regions numbered in order of their first
+// entries into labels (B x N int32), their count into nreg (B doubles; -1 for
+// a NaN image, whose labels are -1); the kink codes at tolerance tol into
+// mask (B x N int8, zeroed here), z and the dual at the input's scale.
+cudaError_t query_labels(bool aniso, const VjpGeom &g, const VjpBuffers &bf, int32_t *labels, double *nreg,
+                         cudaStream_t s);
+cudaError_t query_kinks(int dtype, bool aniso, const VjpGeom &g, const VjpBuffers &bf, const double *gam,
+                        double tol, int8_t *mask, cudaStream_t s);
+// A contiguous device array of n elements of esize bytes into a strided one
+// (ndim <= 8 axes, strides in elements).
+cudaError_t scatter_elements(const void *src, size_t esize, int ndim, const int64_t *shape, const int64_t *strides,
+                             void *dst, cudaStream_t s);
 cudaError_t an_jvp_solve(int dtype, const VjpGeom &g, const VjpBuffers &bf, const void *dx, void *dz, double dgamma,
                          const JvpDir &dir, const double *dbeta, int conj, cudaStream_t s, int64_t *launches);
 // gx = J^T gin per image, the step's gradient into ggam and, with params,

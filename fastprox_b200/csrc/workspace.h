@@ -70,6 +70,9 @@ struct fp_workspace {
     double *h_ggam = nullptr, *h_gw = nullptr;
     bool struct_valid = false;
     bool identity = false;  // the kept call was a conjugate at sigma = 0: J = I
+    int8_t *v_side = nullptr;  // an anisotropic branch override per entry (device)
+    bool branch_on = false;
+    double branch_tol = 0.0;
     bool conj = false;
     // pinned host memory
     int *h_live = nullptr;

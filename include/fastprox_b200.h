@@ -157,6 +157,63 @@ FP_API fp_status fp_vjp(const fp_op *op, const fp_workspace *ws,
 FP_API fp_status fp_vjp_device(const fp_op *op, const fp_workspace *ws, const fp_array *g,
                                fp_array *gx, fp_array *ggamma, fp_array *gparams);
 
+/* Replace include/fastprox.h:510-512: the kink mask of the kept point
+ * (FP_I8, x's shape, any strides, host or device; NULL for the count only)
+ * at tolerance tol and the number of entries at a kink: isotropic TV 1 where
+ * |(W D z)_p| <= tol and |u_p| >= gamma alpha_p - tol, anisotropic TV bit a
+ * at an edge (p, p + e_a) with |z jump| <= tol and |p_e| >= lam_e - tol
+ * (zero bounds are never kinks). set_branch (anisotropic TV; FP_EINVAL for
+ * isotropic TV) picks at each kink the piece the derivatives differentiate:
+ * side -1 joins the edge's two ends, +1 keeps them apart, 0 the default; it
+ * holds until the next prox call or a call with side NULL. */
+FP_API fp_status fp_workspace_kinks(const fp_workspace *ws, double tol, fp_array *mask,
+                                    int64_t *count);
+FP_API fp_status fp_workspace_set_branch(fp_workspace *ws, const fp_array *side, double tol);
+
+/* Replace include/fastprox.h:514-579: the structure of the derivative at the
+ * kept point. Units are the images; every entry of a TV solution is FREE,
+ * with sign +1, in a region (its label, numbered in order of first entries
+ * within its image; -1 and sign 0 in an image holding a NaN, whose region
+ * count is -1); no linear constraint. After fp_prox_conj at sigma = 0 every
+ * entry is ZERO, without regions. The reference answers these on host
+ * workspaces only (FP_EINVAL on a device one); here every workspace is
+ * answered, the outputs host or device arrays. */
+typedef enum {
+    FP_ENTRY_FREE  = 0,
+    FP_ENTRY_ZERO  = 1,
+    FP_ENTRY_LOWER = 2,
+    FP_ENTRY_UPPER = 3
+} fp_entry_state;
+
+typedef enum {
+    FP_STRUCT_NONE      = 0,
+    FP_STRUCT_PROJECTOR = 1, /* anisotropic TV: the average over each region */
+    FP_STRUCT_WEIGHTED  = 2,
+    FP_STRUCT_CURVED    = 3  /* isotropic TV: range span M, not a projector */
+} fp_struct_kind;
+
+FP_API fp_status fp_op_struct_kind(const fp_op *op, int *kind);
+FP_API fp_status fp_workspace_units(const fp_workspace *ws, int64_t *count, int64_t *size);
+FP_API fp_status fp_workspace_states(const fp_workspace *ws, fp_array *state, int64_t *nfixed);
+FP_API fp_status fp_workspace_regions(const fp_workspace *ws, fp_array *labels, fp_array *sign,
+                                      int64_t *nregions, int64_t count);
+FP_API fp_status fp_workspace_constraint(const fp_workspace *ws, fp_array *coef, int8_t *active,
+                                         int64_t count);
+
+/* Replaces include/fastprox.h:769: whether every image's derivative is
+ * exact (anisotropic TV: its polish certified the regions; isotropic TV:
+ * without smoothing) and the largest curvature cap mu of the isotropic
+ * derivative, in the units of x. */
+FP_API fp_status fp_workspace_deriv_exact(const fp_workspace *ws, int *exact, double *smoothing);
+
+/* Replaces include/fastprox.h:770-771: the kept call solved again from its
+ * saved input, warm from its dual, to tol within max_iter; the derivatives,
+ * the dual and the call's results then describe the refined point (the first
+ * call's z is not changed). out (x's shape and dtype, may be NULL) receives
+ * the refined result; FP_ENOTCONV as fp_prox. */
+FP_API fp_status fp_workspace_refine(const fp_op *op, fp_workspace *ws, double tol, int max_iter,
+                                     fp_array *out, fp_info *info);
+
 /* Replace include/fastprox.h:712 and :718. */
 FP_API int       fp_device_available(fp_device dev);
 FP_API fp_status fp_op_device_check(const fp_op *op, fp_device dev, int *row_parallel_only);

@@ -72,6 +72,11 @@ def lib():
                              C.POINTER(FpArray)]
         L.fp_jvp.argtypes = [P, P, C.POINTER(FpArray), C.c_double, C.POINTER(FpArray), C.POINTER(FpArray)]
         L.fp_workspace_set_deriv_tol.argtypes = [P, C.c_double, C.c_int]
+        L.fp_workspace_regions.argtypes = [P, C.POINTER(FpArray), C.POINTER(FpArray), C.POINTER(C.c_int64),
+                                           C.c_int64]
+        L.fp_workspace_kinks.argtypes = [P, C.c_double, C.POINTER(FpArray), C.POINTER(C.c_int64)]
+        L.fp_workspace_set_branch.argtypes = [P, C.POINTER(FpArray), C.c_double]
+        L.fp_workspace_deriv_exact.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.fp_workspace_deriv_info.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_int)]
         L.fp_strerror.restype = C.c_char_p
         _lib = L
@@ -85,7 +90,8 @@ class _Arr:
         self.a = a
         self.shape = (C.c_int64 * max(1, a.ndim))(*a.shape)
         self.strides = (C.c_int64 * max(1, a.ndim))(*[s // a.itemsize for s in a.strides])
-        dt = {np.dtype(np.float32): FP_F32, np.dtype(np.float64): FP_F64}[a.dtype]
+        dt = {np.dtype(np.float32): FP_F32, np.dtype(np.float64): FP_F64, np.dtype(np.int8): 3,
+              np.dtype(np.int32): 4, np.dtype(np.int64): 5}[a.dtype]
         self.s = FpArray(a.ctypes.data, dt, a.ndim, self.shape, self.strides, 0)
 
     def ref(self):
@@ -196,6 +202,37 @@ def jvp(res: Result, dx, dgamma: float, dparams=None):
     _check(L.fp_jvp(res._op, res._ws, None if dxa is None else dxa.ref(), float(dgamma),
                     None if dpa is None else dpa.ref(), _Arr(dz).ref()), "fp_jvp")
     return dz
+
+
+def regions(res: Result, nimages: int):
+    """fp_workspace_regions at a kept Result: (labels int64, nregions)."""
+    L = lib()
+    lab = np.empty(res.z.shape, np.int64)
+    nreg = (C.c_int64 * nimages)()
+    _check(L.fp_workspace_regions(res._ws, _Arr(lab).ref(), None, nreg, nimages), "regions")
+    return lab, np.array(list(nreg), np.int64)
+
+
+def kinks(res: Result, tol: float):
+    """fp_workspace_kinks at a kept Result: (mask int8, count)."""
+    L = lib()
+    m = np.empty(res.z.shape, np.int8)
+    c = C.c_int64()
+    _check(L.fp_workspace_kinks(res._ws, float(tol), _Arr(m).ref(), C.byref(c)), "kinks")
+    return m, c.value
+
+
+def set_branch(res: Result, side, tol: float):
+    L = lib()
+    sa = None if side is None else _Arr(np.ascontiguousarray(side, np.int8))
+    _check(L.fp_workspace_set_branch(res._ws, None if sa is None else sa.ref(), float(tol)), "set_branch")
+
+
+def deriv_exact(res: Result):
+    L = lib()
+    ex, mu = C.c_int(), C.c_double()
+    _check(L.fp_workspace_deriv_exact(res._ws, C.byref(ex), C.byref(mu)), "deriv_exact")
+    return ex.value, mu.value
 
 
 def release(res: Result):
