@@ -278,9 +278,9 @@ __device__ __forceinline__ void fibre_prox(const AnCall &c, const AnBuffers &bf,
                                            double lam, const In &in, const Out &out) {
     if (c.has_beta) {
         const T *bw = static_cast<const T *>(bf.beta) + (int64_t)a * c.N + base;
-        tv1d_fiber(in, out, (int)fb.L, lam, true, BetaW<T>{bw, fb.s});
+        tv1d_fiber<T>(in, out, (int)fb.L, lam, true, BetaW<T>{bw, fb.s}, DivRecip<T>{});
     } else {
-        tv1d_fiber(in, out, (int)fb.L, lam, false, NoWeight{});
+        tv1d_fiber<T>(in, out, (int)fb.L, lam, false, NoWeight{}, DivRecip<T>{});
     }
 }
 
@@ -392,7 +392,7 @@ template <class T>
 struct TileIn {
     const T *s;
     int P, t;
-    __device__ __forceinline__ double operator()(int i) const { return (double)s[i * P + t]; }
+    __device__ __forceinline__ T operator()(int i) const { return s[i * P + t]; }
 };
 // A segment writes its value at its last entry and marks it (one bit per
 // entry, word i / 32 of the fibre's column); finish fills each segment's
@@ -456,38 +456,45 @@ __device__ __forceinline__ void tile_store(const T *tile, int P, const Fib &fb, 
 }
 
 // The tiles of a block in shared memory: the fibres' inputs (then results),
-// their edge weights when there are any, and one mark bit per entry.
+// their edge weights when there are any, one mark bit per entry, and the
+// reciprocals 1/m (m <= L) of the scans.
 template <class T>
 struct Tiles {
-    T *in, *w;
+    T *in, *w, *rc;
     unsigned *mk;
     __device__ __forceinline__ Tiles(unsigned char *smem, const AnCall &c, int L, int P) {
         in = reinterpret_cast<T *>(smem);
         w = in + L * P;
         mk = reinterpret_cast<unsigned *>(in + (c.has_beta ? 2 : 1) * L * P);
         const int nw = ((L + 31) >> 5) * P;
+        rc = reinterpret_cast<T *>(mk + ((nw + 1) & ~1));
         for (int i = threadIdx.x; i < nw; i += blockDim.x) mk[i] = 0u;
+        const DivRecip<T> div;
+        for (int m = threadIdx.x; m <= L; m += blockDim.x) rc[m] = m ? div(m) : T(0);
     }
 };
 
 // Shared-memory bytes of a tile of fb fibres of L entries.
 __host__ __device__ __forceinline__ size_t tile_bytes(int L, int fb, int nbuf, size_t tsize) {
     const size_t P = (size_t)fb + 1;
-    return (size_t)nbuf * tsize * (size_t)L * P + 4 * (((size_t)L + 31) / 32) * P;
+    const size_t nw = (((size_t)L + 31) / 32) * P;
+    return (size_t)nbuf * tsize * (size_t)L * P + 4 * ((nw + 1) & ~(size_t)1) + tsize * ((size_t)L + 1);
 }
 
-// The scans of a loaded tile (edge weights in the second tile when present).
+// The scans of a loaded tile (edge weights in the second tile when present),
+// by the block's first warp, lane t on fibre t, in lockstep (tv1d_warp).
 template <class T>
 __device__ __forceinline__ void tile_scan(const AnCall &c, const Tiles<T> &tl, int P, int nv, int L, double lam) {
     const int t = threadIdx.x;
-    if (t >= nv) return;
+    if (t >= 32) return;
     const TileIn<T> in{tl.in, P, t};
     const TileSink<T> out{tl.in, tl.mk, P, t};
-    if (c.has_beta) tv1d_fiber_sink(in, out, L, lam, true, TileIn<T>{tl.w, P, t});
-    else tv1d_fiber_sink(in, out, L, lam, false, NoWeight{});
+    if (c.has_beta) tv1d_warp<T>(in, out, L, lam, true, TileIn<T>{tl.w, P, t}, TableRecip<T>{tl.rc}, t < nv);
+    else tv1d_warp<T>(in, out, L, lam, false, NoWeight{}, TableRecip<T>{tl.rc}, t < nv);
 }
 
-constexpr int kTileThreads = 32;
+// Threads of a tile block: all copy the tiles in and out, the first warp scans.
+constexpr int kTileThreads = 128;
 
 // an_pass1 on tiles
 template <class T>
@@ -1333,12 +1340,21 @@ cudaError_t setup_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, const
     return cudaGetLastError();
 }
 
-// Fibres per tile along each axis: the most (1, 2, 4, ...) up to a cap whose
-// tile fits a budget (several blocks to an SM: at this latency-bound scan,
-// more warps beat fuller ones), else one fibre in up to 200 KB; 0 when even
-// that does not fit (the untiled pass then runs).
+// Fibres per tile along each axis. A block scans its tile with one warp, so
+// an SM scans as many fibres at once as the tiles of its resident blocks hold
+// (shared memory, registers and threads bound how many blocks it holds): fb
+// makes that number largest, up to 8 fibres (a warp's step takes longer the
+// more lanes it carries, and more warps hide more of its latency: on 64 x
+// 512^2 with edge weights 8 per block ran 3% faster than 16 and 8% faster than
+// 26), among tiles of at most budget bytes (default
+// kTileSmemMax) and while the launch still gives every SM a block; the larger
+// fb on ties, so that fewer warps issue the same steps. fb is 1 or even (the
+// tile's row length fb + 1 odd). 0 when one fibre does not fit: the untiled
+// pass then runs.
 constexpr int kTileSmemMax = 200 * 1024;
-constexpr int64_t kSpreadBlocks = 148 * 8;  // blocks a launch should have before its tiles grow
+constexpr size_t kSmemPerSM = 228 * 1024;  // shared memory of an SM (sm_100)
+constexpr size_t kSmemReserve = 1024 + 512;  // per block: the system's and the kernels' static arrays
+constexpr int kSMs = 148;
 
 // The tiled kernels may take up to kTileSmemMax of dynamic shared memory. Set
 // once per kernel, before any launch: the attribute is per function, and
@@ -1355,34 +1371,66 @@ void tile_attributes() {
     cudaFuncSetAttribute(an_fdpg3_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemMax);
     done.fetch_or(bit);
 }
+
+// Blocks of the tiled kernels an SM holds by registers and threads (their
+// largest register count, allocated per warp in units of 256).
+template <class T>
+int tile_blocks_by_regs() {
+    static const int n = [] {
+        int regs = 0;
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, an_pass1_tile<T>) == cudaSuccess) regs = std::max(regs, fa.numRegs);
+        if (cudaFuncGetAttributes(&fa, an_pass2_tile<T>) == cudaSuccess) regs = std::max(regs, fa.numRegs);
+        if (cudaFuncGetAttributes(&fa, an_fdpg3_tile<T>) == cudaSuccess) regs = std::max(regs, fa.numRegs);
+        const int per_warp = ((std::max(regs, 1) * 32 + 255) / 256) * 256;
+        const int warps = kTileThreads / 32;
+        return std::max(1, std::min(2048 / kTileThreads, 65536 / (per_warp * warps)));
+    }();
+    return n;
+}
+
 template <class T>
 TileCfg tile_cfg(const AnGeom &g, const AnCall &c, int64_t nimg, size_t &smem) {
-    // fibres per block: at most fb_max, and tiles of at most budget bytes
-    // (tuning hints FASTPROX_B200_TILE_FB and FASTPROX_B200_TILE_KB)
+    // tuning hints: FASTPROX_B200_TILE_FB caps fb, FASTPROX_B200_TILE_KB the
+    // tile; FASTPROX_B200_TILES=0 runs the untiled passes (for comparison)
+    static const bool off = [] {
+        const char *v = std::getenv("FASTPROX_B200_TILES");
+        return v && v[0] == '0' && v[1] == 0;
+    }();
     static const int fb_max = [] {
         const char *v = std::getenv("FASTPROX_B200_TILE_FB");
         const int f = v ? std::atoi(v) : 0;
-        return (f >= 1 && f <= 32) ? f : 4;
+        return (f >= 1 && f <= 32) ? f : 8;
     }();
     static const size_t budget = [] {
         const char *v = std::getenv("FASTPROX_B200_TILE_KB");
         const int k = v ? std::atoi(v) : 0;
-        return (size_t)((k >= 8 && k <= 200) ? k : 48) * 1024;
+        return (size_t)((k >= 8 && k <= 200) ? k : 200) * 1024;
     }();
+    const int by_regs = tile_blocks_by_regs<T>();
     TileCfg tc{{0, 0, 0}};
     smem = 0;
     const int nbuf = c.has_beta ? 2 : 1;
-    for (int a = 0; a < g.k; ++a) {
+    for (int a = 0; a < g.k && !off; ++a) {
         const int L = (int)g.L[a];
-        auto bytes = [&](int fb) { return tile_bytes(L, fb, nbuf, sizeof(T)); };
-        // fewer fibres per block when the launch has few fibres in all (one
-        // large image), so that its blocks spread over every SM
         const int64_t fibres = nimg * (g.N / std::max<int64_t>(g.L[a], 1));
-        int fb = 1;
-        while (fb * 2 <= fb_max && bytes(fb * 2) <= budget && fibres / (fb * 2) >= kSpreadBlocks) fb *= 2;
-        if (bytes(fb) > (size_t)kTileSmemMax) fb = 0;
-        tc.fb[a] = fb;
-        if (fb) smem = std::max(smem, bytes(fb));
+        int best = 0;
+        double best_waves = 0.0;
+        for (int fb = 1; fb <= fb_max; fb += (fb == 1 ? 1 : 2)) {
+            const size_t by = tile_bytes(L, fb, nbuf, sizeof(T));
+            if (by > budget || by > (size_t)kTileSmemMax) break;
+            const int per_sm = std::min<int>(by_regs, (int)(kSmemPerSM / (by + kSmemReserve)));
+            if (per_sm < 1) break;
+            const int64_t blocks = (fibres + fb - 1) / fb;
+            if (fb > 1 && blocks < kSMs) break;
+            const double waves = std::max(1.0, (double)blocks / ((double)per_sm * kSMs));
+            if (best == 0 || waves <= best_waves) {
+                best = fb;
+                best_waves = waves;
+            }
+        }
+        tc.fb[a] = best;
+        if (best) smem = std::max(smem, tile_bytes(L, best, nbuf, sizeof(T)));
     }
     return tc;
 }

@@ -1561,7 +1561,7 @@ __global__ void iso_tv1d_kernel(Geometry g, IsoCall c, IsoBuffers bf, T *__restr
     T *Zb = Z + base;
     auto fin = [Db, s](int64_t i) -> double { return (double)Db[i * s]; };
     auto fout = [Zb, s](int64_t i, double v) { Zb[i * s] = (T)v; };
-    tv1d_fiber(fin, fout, L, lam, false, NoWeight{});
+    tv1d_fiber<double>(fin, fout, L, lam, false, NoWeight{}, DivRecip<double>{});
     double cs = 0.0;
     for (int64_t i = 0; i < L; ++i) {
         const int64_t o = base + i * s;
