@@ -751,6 +751,9 @@ template <class T, int VEC, bool ALPHA, bool GAP, bool ZIN>
 __global__ void __launch_bounds__(128, 5) iso2d_lean_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     __shared__ double sh[32];
     __shared__ int flag;
+    // launched as a programmatic dependent of the previous step: nothing of
+    // its output (states, iterates, live list) is read before it completes
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int b = step_image(bf, blockIdx.z);
     if (b < 0) return;
     const IsoState st = bf.st[b];
@@ -782,6 +785,8 @@ __global__ void __launch_bounds__(128, 5) iso2d_lean_kernel(StepArgs A, IsoCall 
     lean_rows<T, VEC, ALPHA, GAP, ZIN>(D, U0, U0 + N, V0, V0 + N, UO0, UO0 + N, VO0, VO0 + N, AL, H, W, cb, r0, r1,
                                        (T)c.wh[0], (T)c.wh[1], (T)c.tau, (T)st.beta, (T)im.radius, (T)im.bound, test,
                                        do_upd, gap_acc, dot_acc, A.row_part ? rowp : nullptr);
+    // the next step's blocks may be scheduled now (they wait for this one)
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const unsigned nblk = gridDim.x * gridDim.y;
     const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
     double *part = bf.part + (int64_t)b * bf.max_part * 2;
@@ -1643,13 +1648,38 @@ cudaError_t setup_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, c
     return cudaGetLastError();
 }
 
+// Launches a step so that it may start while the previous kernel on the
+// stream finishes (programmatic dependent launch): its blocks are scheduled
+// once every block of the previous step has passed its row loop, and wait
+// (griddepcontrol.wait) for that step to complete before reading anything.
+// FASTPROX_B200_PDL=0 launches plainly (for comparison).
+template <class K>
+void launch_step(K kernel, dim3 grid, unsigned bx, cudaStream_t s, const StepArgs &A, const IsoCall &c,
+                 const IsoBuffers &bf) {
+    static const bool pdl = [] {
+        const char *v = std::getenv("FASTPROX_B200_PDL");
+        return !(v && v[0] == '0' && v[1] == 0);
+    }();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(bx);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, A, c, bf);
+}
+
 template <class T, int VEC, bool ALPHA>
 void launch_lean_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s,
                    int variant) {
     const dim3 grid(sh.gx, sh.gy, (unsigned)A.nimg);
-    if (variant == 1) iso2d_lean_kernel<T, VEC, ALPHA, false, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
-    else if (variant == 2) iso2d_lean_kernel<T, VEC, ALPHA, true, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
-    else iso2d_lean_kernel<T, VEC, ALPHA, false, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
+    if (variant == 1) launch_step(iso2d_lean_kernel<T, VEC, ALPHA, false, true>, grid, sh.bx, s, A, c, bf);
+    else if (variant == 2) launch_step(iso2d_lean_kernel<T, VEC, ALPHA, true, false>, grid, sh.bx, s, A, c, bf);
+    else launch_step(iso2d_lean_kernel<T, VEC, ALPHA, false, false>, grid, sh.bx, s, A, c, bf);
 }
 
 template <class T, int VEC>
