@@ -1303,6 +1303,7 @@ __global__ void __launch_bounds__(k3TX * k3TY) iso3d_kernel(StepArgs A, IsoCall 
     T(*zs)[GAP ? 2 : 1][k3Z] = reinterpret_cast<T(*)[GAP ? 2 : 1][k3Z]>(i3_smem + 3 * NA * k3R * sizeof(T));
     __shared__ double sh[32];
     __shared__ int flag;
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // a programmatic dependent of the previous step
     const int b = step_image(bf, blockIdx.z);
     if (b < 0) return;
     const IsoState st = bf.st[b];
@@ -1461,6 +1462,7 @@ __global__ void __launch_bounds__(k3TX * k3TY) iso3d_kernel(StepArgs A, IsoCall 
             }
         }
     }
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const unsigned nblk = gridDim.x * gridDim.y;
     const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
     const double gsum = GAP ? block_sum(gap_acc, sh) : 0.0;
@@ -1650,11 +1652,12 @@ cudaError_t setup_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, c
 
 // Launches a step so that it may start while the previous kernel on the
 // stream finishes (programmatic dependent launch): its blocks are scheduled
-// once every block of the previous step has passed its row loop, and wait
+// once every block of the previous step has finished its pass over the
+// iterates (griddepcontrol.launch_dependents), and wait
 // (griddepcontrol.wait) for that step to complete before reading anything.
 // FASTPROX_B200_PDL=0 launches plainly (for comparison).
 template <class K>
-void launch_step(K kernel, dim3 grid, unsigned bx, cudaStream_t s, const StepArgs &A, const IsoCall &c,
+void launch_step(K kernel, dim3 grid, unsigned bx, size_t smem, cudaStream_t s, const StepArgs &A, const IsoCall &c,
                  const IsoBuffers &bf) {
     static const bool pdl = [] {
         const char *v = std::getenv("FASTPROX_B200_PDL");
@@ -1663,7 +1666,7 @@ void launch_step(K kernel, dim3 grid, unsigned bx, cudaStream_t s, const StepArg
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = dim3(bx);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1677,9 +1680,9 @@ template <class T, int VEC, bool ALPHA>
 void launch_lean_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s,
                    int variant) {
     const dim3 grid(sh.gx, sh.gy, (unsigned)A.nimg);
-    if (variant == 1) launch_step(iso2d_lean_kernel<T, VEC, ALPHA, false, true>, grid, sh.bx, s, A, c, bf);
-    else if (variant == 2) launch_step(iso2d_lean_kernel<T, VEC, ALPHA, true, false>, grid, sh.bx, s, A, c, bf);
-    else launch_step(iso2d_lean_kernel<T, VEC, ALPHA, false, false>, grid, sh.bx, s, A, c, bf);
+    if (variant == 1) launch_step(iso2d_lean_kernel<T, VEC, ALPHA, false, true>, grid, sh.bx, 0, s, A, c, bf);
+    else if (variant == 2) launch_step(iso2d_lean_kernel<T, VEC, ALPHA, true, false>, grid, sh.bx, 0, s, A, c, bf);
+    else launch_step(iso2d_lean_kernel<T, VEC, ALPHA, false, false>, grid, sh.bx, 0, s, A, c, bf);
 }
 
 template <class T, int VEC>
@@ -1711,7 +1714,7 @@ void iso3d_attr() {
 template <class T, bool ALPHA, bool GAP, bool ZIN>
 void launch_3d_v(const dim3 &grid, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
     iso3d_attr<T, ALPHA, GAP, ZIN>();
-    iso3d_kernel<T, ALPHA, GAP, ZIN><<<grid, k3TX * k3TY, iso3d_smem<T, GAP>(), s>>>(A, c, bf);
+    launch_step(iso3d_kernel<T, ALPHA, GAP, ZIN>, grid, k3TX * k3TY, iso3d_smem<T, GAP>(), s, A, c, bf);
 }
 
 template <class T, bool ALPHA>
