@@ -935,17 +935,23 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     // a list of the live ones (images only retire, so a list built after the
     // count was read holds every image still live): the tail of a batch, where
     // a few slow images remain, launches only their blocks.
+    // Iterations 1 and 2 mod 4 (no check in either) run as one launch where
+    // the lean 2D step applies (iso_pair_ok).
     const int chunk = ws->chunk > 0 ? ws->chunk : 8;
+    const bool pairs = iso_pair_ok(g, ws->shape_);
     int par = 0, slot = 0, inflight = 0;
-    int64_t launched = 0, lists = 0, nimg = g.B;
+    int64_t launched = 0, steps = 0, lists = 0, nimg = g.B;
     const int64_t cap = (int64_t)max_iter + 1 + 2 * chunk;
     bool done = false;
     while (!done) {
         for (int j = 0; j < chunk; ++j) {
-            e = iso_step(ws->dtype, g, c, bf, ws->shape_, par, iso_variant(launched, max_iter, warm), nimg, s);
+            const bool pair = pairs && iso_pair_at(launched, max_iter);
+            e = iso_step(ws->dtype, g, c, bf, ws->shape_, par, pair ? kVariantPair : iso_variant(launched, max_iter, warm),
+                         nimg, s);
             if (e != cudaSuccess) return cuda_status(e);
             par ^= 1;
-            ++launched;
+            launched += pair ? 2 : 1;
+            ++steps;
         }
         e = cudaMemcpyAsync(ws->h_live + slot, ws->live, sizeof(int), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaEventRecord(ws->ev[slot], s);
@@ -970,8 +976,8 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
         }
         if (launched >= cap) done = true;
     }
-    ws->launches = launched;
-    ws->kernel_launches += launched + lists + 3 + (warm ? 1 : 0) + 1 + ((c.na == 1 && !c.has_alpha) ? 1 : 0);
+    ws->launches = steps;
+    ws->kernel_launches += steps + lists + 3 + (warm ? 1 : 0) + 1 + ((c.na == 1 && !c.has_alpha) ? 1 : 0);
     e = iso_finalize(ws->dtype, g, c, bf, zdst, s);
     return cuda_status(e);
 }

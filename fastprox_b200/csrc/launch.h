@@ -52,10 +52,16 @@ cudaError_t iso_live_list(const IsoState *st, int64_t B, int *lmap, int *lcnt, c
 // One dual-FISTA iteration (and the gap / restart tests it carries) for
 // every live image, reading buffers par and writing par ^ 1, over nimg launch
 // slots (g.B, or at least the count of bf's live list).
-// variant (the lean and 3D kernels, chosen from the launch index k of a call):
-// 1 the cold first iteration (u = v = 0), 2 a launch carrying a gap check, 0 otherwise.
+// variant (the lean and 3D kernels, chosen from the iteration index k of a call):
+// 1 the cold first iteration (u = v = 0), 2 a launch carrying a gap check, 0 otherwise;
+// kVariantPair two plain iterations (the lean 2D shape only).
 cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh,
                      int par, int variant, int64_t nimg, cudaStream_t s);
+// Variant of iso_step running iterations k and k + 1 in one launch, for k = 1
+// mod 4 and k + 1 < max_iter (neither has a check), where iso_pair_ok.
+constexpr int kVariantPair = 3;
+bool iso_pair_ok(const Geometry &g, const StepShape &sh);
+inline bool iso_pair_at(int64_t k, int max_iter) { return (k & 3) == 1 && k + 1 < max_iter; }
 inline int iso_variant(int64_t k, int max_iter, bool warm) {
     if (k == 0) return warm ? 2 : 1;
     return (k % 4 == 0 || k == max_iter) ? 2 : 0;

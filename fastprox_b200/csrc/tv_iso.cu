@@ -826,6 +826,251 @@ __global__ void __launch_bounds__(128, 5) iso2d_lean_kernel(StepArgs A, IsoCall 
 }
 
 // ---------------------------------------------------------------------------
+// Two plain iterations in one pass over memory (temporal blocking of the
+// lean step).
+//
+// Iterations it and it + 1 carry no gap check and no restart test when
+// neither is 0 mod 4 (nor the last): the second needs nothing of the first
+// but its iterates u' = P(v + tau G z(v)), v' = u' + beta (u' - u), and its
+// beta is the one the per-image control would set, (tn - 1) / fista_t(tn).
+// A block covers whole rows and marches them like the lean step: the first
+// iteration in registers as lean_rows does, on its rows and one more above and
+// below; the second one row behind it, with the first's v' passing between
+// threads through a ring of three rows in shared memory (a thread's left and
+// right neighbours in z(v')). Only u'' and v'' are written. Traffic per pixel
+// and two iterations: d, u, v (and alpha) read once over R + 4 rows for R
+// output rows, u'' and v'' written once: about 50 B against 2 x 40 B for two
+// lean steps. Each iteration's arithmetic is lean_rows' (the same
+// expressions), so the iterates are those of two lean steps.
+// ---------------------------------------------------------------------------
+constexpr int kPairCols = 512;  // columns a block covers: 128 threads x 4
+
+template <class T, bool ALPHA>
+__global__ void __launch_bounds__(128, 4) iso2d_pair_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+    constexpr int VEC = 4;
+    __shared__ __align__(16) T vs[3][2][kPairCols + VEC];  // v' of rows i % 3, both axes
+    __shared__ __align__(16) T ds[2][kPairCols + VEC];     // d of rows i % 2
+    __shared__ int flag;
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // a programmatic dependent of the previous step
+    const int b = step_image(bf, blockIdx.z);
+    if (b < 0) return;
+    const IsoState st = bf.st[b];
+    if (st.status != kLive) return;
+    const int it = st.it;
+    if (it <= 0 || (it & 3) == 0 || ((it + 1) & 3) == 0 || it + 1 >= A.max_iter || st.zero_in) {
+        if (threadIdx.x == 0) atomicExch(bf.err, 3);
+        return;
+    }
+    const IsoImage im = bf.img[b];
+    const int H = (int)A.g.L[0], W = (int)A.g.L[1];
+    const int64_t N = A.g.N;
+    const int pin = A.par, pout = A.par ^ 1;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *U0 = static_cast<const T *>(bf.U[pin]) + (int64_t)b * 2 * N;
+    const T *V0 = st.vsel ? U0 : static_cast<const T *>(bf.V[pin]) + (int64_t)b * 2 * N;
+    const T *U1 = U0 + N, *V1 = V0 + N;
+    T *UO0 = static_cast<T *>(bf.U[pout]) + (int64_t)b * 2 * N;
+    T *VO0 = static_cast<T *>(bf.V[pout]) + (int64_t)b * 2 * N;
+    T *UO1 = UO0 + N, *VO1 = VO0 + N;
+    const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
+    const T wh0 = (T)c.wh[0], wh1 = (T)c.wh[1], tau = (T)c.tau;
+    const T rad = (T)im.radius, bnd = (T)im.bound;
+    const T beta1 = (T)st.beta;
+    const double tn2 = fista_t(st.tn);
+    const T beta2 = (T)((st.tn - 1.0) / tn2);
+
+    const int lane = threadIdx.x & 31;
+    const int cb = (int)threadIdx.x * VEC;
+    const bool colok = cb < W;
+    const bool ext = lane == 31 && cb + VEC < W;  // the next warp's first column (first iteration)
+    const int r0 = blockIdx.y * A.rows;
+    const int r1 = min(H, r0 + A.rows);
+    const int s0 = r0 > 0 ? r0 - 1 : 0;       // rows of the first iteration: s0 .. s1
+    const int s1 = r1 < H ? r1 : H - 1;
+
+    auto ld = [&](const T *P, int off, T(&o)[VEC]) {
+        if (colok) load_pack<T, VEC>(P + off, o);
+        else
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) o[j] = T(0);
+    };
+    auto zrow = [&](const T(&dd)[VEC], const T(&p0)[VEC], const T(&p0p)[VEC], const T(&p1)[VEC], T left, T(&z)[VEC]) {
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            z[j] = dd[j] + wh0 * (p0[j] - p0p[j]) + wh1 * (p1[j] - left);
+            left = p1[j];
+        }
+    };
+    auto radius = [&](const T(&al)[VEC], int j) -> T {
+        if (!ALPHA) return rad;
+        const T r = rad * al[j];
+        return al[j] == T(0) ? T(0) : (r <= bnd ? r : bnd);
+    };
+
+    // first iteration: row s0 and the part of row s0 - 1 it needs (lean_rows)
+    int off = s0 * W + cb;
+    T dc[VEC], v0c[VEC], v1c[VEC], u0c[VEC], u1c[VEC], zc[VEC], v0p[VEC];
+    ld(D, off, dc);
+    ld(V0, off, v0c);
+    ld(V1, off, v1c);
+    ld(U0, off, u0c);
+    ld(U1, off, u1c);
+    if (s0 > 0) ld(V0, off - W, v0p);
+    else
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) v0p[j] = T(0);
+    zrow(dc, v0c, v0p, v1c, (colok && cb > 0) ? V1[off - 1] : T(0), zc);
+    T x_v0 = T(0), x_z = T(0);
+    if (ext) {
+        const T dx = D[off + VEC];
+        x_v0 = V0[off + VEC];
+        const T pv = s0 > 0 ? V0[off + VEC - W] : T(0);
+        x_z = dx + wh0 * (x_v0 - pv) + wh1 * (V1[off + VEC] - v1c[VEC - 1]);
+    }
+    // second iteration's inputs of the row above: v', u', alpha, z(v') (five columns)
+    T pv0[VEC], pv1[VEC], pu0[VEC], pu1[VEC], pal[VEC], zp[VEC + 1];
+#pragma unroll
+    for (int j = 0; j < VEC; ++j) pv0[j] = pv1[j] = pu0[j] = pu1[j] = pal[j] = zp[j] = T(0);
+    zp[VEC] = T(0);
+
+    // the second iteration on row j from z(v') of rows j (zp) and j + 1 (zq)
+    auto second = [&](int j, bool hasn, const T(&zq)[VEC]) {
+        if (!colok) return;
+        T uo0[VEC], uo1[VEC], vo0[VEC], vo1[VEC];
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            const bool hasr = cb + q + 1 < W;
+            const T zright = q + 1 < VEC ? zp[q + 1] : zp[VEC];
+            const T g0 = hasn ? wh0 * (zq[q] - zp[q]) : T(0);
+            const T g1 = hasr ? wh1 * (zright - zp[q]) : T(0);
+            const T cv0 = pv0[q] + tau * g0;
+            const T cv1 = pv1[q] + tau * g1;
+            const T nn = cv0 * cv0 + cv1 * cv1;
+            const T rp = radius(pal, q);
+            const T sc = nn > rp * rp ? rp * rsqrt_t(nn) : T(1);
+            const T un0 = cv0 * sc, un1 = cv1 * sc;
+            vo0[q] = un0 + beta2 * (un0 - pu0[q]);
+            vo1[q] = un1 + beta2 * (un1 - pu1[q]);
+            uo0[q] = un0;
+            uo1[q] = un1;
+        }
+        const int o = j * W + cb;
+        store_pack<T, VEC>(UO0 + o, uo0);
+        store_pack<T, VEC>(UO1 + o, uo1);
+        store_pack<T, VEC>(VO0 + o, vo0);
+        store_pack<T, VEC>(VO1 + o, vo1);
+    };
+
+    for (int i = s0; i <= s1; ++i) {
+        const bool hasn = i + 1 < H;
+        const int offn = off + W;
+        T dn[VEC], v0n[VEC], v1n[VEC], u0n[VEC], u1n[VEC], zn[VEC];
+        T nx_v0 = T(0), nx_z = T(0);
+        if (hasn) {
+            ld(D, offn, dn);
+            ld(V0, offn, v0n);
+            ld(V1, offn, v1n);
+            ld(U0, offn, u0n);
+            ld(U1, offn, u1n);
+            zrow(dn, v0n, v0c, v1n, (colok && cb > 0) ? V1[offn - 1] : T(0), zn);
+            if (ext) {
+                const T dx = D[offn + VEC];
+                nx_v0 = V0[offn + VEC];
+                nx_z = dx + wh0 * (nx_v0 - x_v0) + wh1 * (V1[offn + VEC] - v1n[VEC - 1]);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) zn[j] = u0n[j] = u1n[j] = v0n[j] = v1n[j] = dn[j] = T(0);
+        }
+        T al[VEC];
+        if (ALPHA) {
+            if (colok) load_pack<T, VEC>(AL + off, al);
+            else
+#pragma unroll
+                for (int j = 0; j < VEC; ++j) al[j] = T(0);
+        }
+        T zr = __shfl_down_sync(0xffffffffu, zc[0], 1);
+        if (lane == 31) zr = x_z;
+        // the first iteration on row i
+        T un0[VEC], un1[VEC], vo0[VEC], vo1[VEC];
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            const bool hasr = cb + j + 1 < W;
+            const T zright = j + 1 < VEC ? zc[j + 1] : zr;
+            const T g0 = hasn ? wh0 * (zn[j] - zc[j]) : T(0);
+            const T g1 = hasr ? wh1 * (zright - zc[j]) : T(0);
+            const T cv0 = v0c[j] + tau * g0;
+            const T cv1 = v1c[j] + tau * g1;
+            const T nn = cv0 * cv0 + cv1 * cv1;
+            const T rp = radius(al, j);
+            const T sc = nn > rp * rp ? rp * rsqrt_t(nn) : T(1);
+            un0[j] = cv0 * sc;
+            un1[j] = cv1 * sc;
+            vo0[j] = un0[j] + beta1 * (un0[j] - u0c[j]);
+            vo1[j] = un1[j] + beta1 * (un1[j] - u1c[j]);
+        }
+        if (colok) {
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) {
+                vs[i % 3][0][cb + j] = vo0[j];
+                vs[i % 3][1][cb + j] = vo1[j];
+                ds[i & 1][cb + j] = dc[j];
+            }
+        }
+        __syncthreads();
+        if (i >= r0) {
+            // z(v') on row i: own columns, and the right neighbour's first
+            T zq[VEC + 1];
+            T pr[VEC];
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) pr[j] = i > 0 ? pv0[j] : T(0);
+            zrow(dc, vo0, pr, vo1, (colok && cb > 0) ? vs[i % 3][1][cb - 1] : T(0), reinterpret_cast<T(&)[VEC]>(zq));
+            zq[VEC] = T(0);
+            if (colok && cb + VEC < W) {
+                const T up = i > 0 ? vs[(i + 2) % 3][0][cb + VEC] : T(0);
+                zq[VEC] = ds[i & 1][cb + VEC] + wh0 * (vs[i % 3][0][cb + VEC] - up) +
+                          wh1 * (vs[i % 3][1][cb + VEC] - vo1[VEC - 1]);
+            }
+            if (i - 1 >= r0) second(i - 1, true, reinterpret_cast<const T(&)[VEC]>(zq));
+#pragma unroll
+            for (int j = 0; j <= VEC; ++j) zp[j] = zq[j];
+        }
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            pv0[j] = vo0[j];
+            pv1[j] = vo1[j];
+            pu0[j] = un0[j];
+            pu1[j] = un1[j];
+            if (ALPHA) pal[j] = al[j];
+            dc[j] = dn[j];
+            v0c[j] = v0n[j];
+            v1c[j] = v1n[j];
+            u0c[j] = u0n[j];
+            u1c[j] = u1n[j];
+            zc[j] = zn[j];
+        }
+        x_v0 = nx_v0;
+        x_z = nx_z;
+        off = offn;
+    }
+    // the last row of the image has no row below
+    if (r1 == H && H - 1 >= r0) {
+        T zq[VEC];
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) zq[j] = T(0);
+        second(H - 1, false, zq);
+    }
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (!arrive_last(bf.ticket + b, gridDim.x * gridDim.y, &flag)) return;
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2 = st;
+    control(s2, im, A.max_iter, false, false, 0.0, 0.0, pin, bf.live);
+    control(s2, im, A.max_iter, false, false, 0.0, 0.0, pin, bf.live);
+    bf.st[b] = s2;
+}
+
+// ---------------------------------------------------------------------------
 // The ragged step: images of any size in one arena, a device-resident work
 // list of (image, tile) items, each image at its own iteration with its own
 // buffer parity (its state's fin_par). Three variants (cold start, gap
@@ -1685,6 +1930,20 @@ void launch_lean_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoB
     else launch_step(iso2d_lean_kernel<T, VEC, ALPHA, false, false>, grid, sh.bx, 0, s, A, c, bf);
 }
 
+// Two plain iterations per launch: blocks of whole rows, at least 8 of them
+// (the halo of the first iteration is 4 rows), fewer per block while the
+// launch has too few blocks to spread (the tail of a batch).
+template <class T>
+void launch_pair(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
+    const int64_t H = A.g.L[0];
+    int rows = sh.rows;
+    while (rows > 8 && A.nimg * ((H + rows - 1) / rows) < tail_blocks()) rows /= 2;
+    A.rows = rows;
+    const dim3 grid(1, (unsigned)((H + rows - 1) / rows), (unsigned)A.nimg);
+    if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true>, grid, 128, 0, s, A, c, bf);
+    else launch_step(iso2d_pair_kernel<T, false>, grid, 128, 0, s, A, c, bf);
+}
+
 template <class T, int VEC>
 void launch_lean(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s,
                  int variant) {
@@ -1757,6 +2016,10 @@ cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, co
     A.nimg = nimg;
     A.row_part = 0;
     if (nimg <= 0) return cudaSuccess;
+    if (variant == kVariantPair) {
+        launch_pair<T>(sh, A, c, bf, s);
+        return cudaGetLastError();
+    }
     StepShape sh2 = sh;
     if (sh.kind == 4 && (int64_t)sh.gx * g.L[0] <= bf.max_part && sh.rows <= kLeanRowsMax) {
         // per-row partial sums make the sums independent of the rows per
@@ -1905,6 +2168,15 @@ cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBu
                      int par, int variant, int64_t nimg, cudaStream_t s) {
     return dtype == 1 ? step_t<float>(g, c, bf, sh, par, variant, nimg, s)
                       : step_t<double>(g, c, bf, sh, par, variant, nimg, s);
+}
+
+bool iso_pair_ok(const Geometry &g, const StepShape &sh) {
+    static const bool on = [] {
+        const char *v = std::getenv("FASTPROX_B200_PAIRS");
+        return !(v && v[0] == '0' && v[1] == 0);
+    }();
+    return on && g.k == 2 && sh.kind == 4 && sh.vec == 4 && sh.bx == 128 && sh.gx == 1 && g.L[1] <= kPairCols &&
+           g.L[0] >= 2;
 }
 
 cudaError_t iso_live_list(const IsoState *st, int64_t B, int *lmap, int *lcnt, cudaStream_t s) {

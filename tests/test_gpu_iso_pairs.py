@@ -1,0 +1,70 @@
+"""Two plain isotropic iterations in one launch (iso2d_pair_kernel) against
+the same iterations one launch each: the same arithmetic per iteration, so
+the same iterates, iteration counts and gaps. Covers images with and without
+pixel weights, float32 and float64, heights that leave blocks of one to
+sixteen rows and a last block shorter than the rest, widths below the block's
+512 columns, per-image steps (images that stop at different iterations),
+warm starts, and max_iter values that end inside a pair. The one-launch-each
+run is a child process with FASTPROX_B200_PAIRS=0 (the library reads its
+tuning hints once)."""
+
+import os
+import pathlib
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+
+CASES = [  # (dtype, B, H, W, alpha, tol, max_iter, warm)
+    (np.float32, 3, 512, 512, True, 1e-6, 400, False),
+    (np.float32, 2, 37, 100, False, 1e-7, 500, False),
+    (np.float64, 3, 130, 256, True, 1e-9, 2000, False),
+    (np.float64, 2, 5, 64, False, 0.0, 6, False),
+    (np.float32, 2, 64, 508, True, 0.0, 7, False),
+    (np.float64, 2, 96, 128, False, 1e-8, 3000, True),
+]
+
+
+def _run(i):
+    import torch
+    from fastprox_b200 import TVIso, synth
+    dtype, B, H, W, alpha, tol, max_iter, warm = CASES[i]
+    x = synth.phantom(B, H, W, seed=70 + i).astype(dtype)
+    al = synth.pixel_weights((H, W), seed=80 + i).astype(np.float64) if alpha else None
+    op = TVIso(2, pixel_weights=al)
+    steps = torch.as_tensor(np.linspace(0.05, 0.2, B), device="cuda")
+    xt = torch.as_tensor(x, device="cuda")
+    dual = None
+    if warm:  # a warm start from a loose solve of the same images
+        _, info0 = op.solve(xt, steps, tol=1e-3, max_iter=200)
+        dual = info0.dual
+    z, info = op.solve(xt, steps, tol=tol, max_iter=max_iter, warm=warm, dual=dual)
+    torch.cuda.synchronize()
+    return z.cpu().numpy(), np.asarray(info.image_iters), np.asarray(info.gaps)
+
+
+@pytest.mark.gpu
+def test_pairs_match_single_steps(cuda, tmp_path):
+    env = dict(os.environ, FASTPROX_B200_PAIRS="0")
+    out = tmp_path / "single.npz"
+    r = subprocess.run([sys.executable, str(pathlib.Path(__file__)), str(out)], cwd=ROOT, env=env,
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout + r.stderr
+    ref = np.load(out)
+    for i in range(len(CASES)):
+        z, iters, gaps = _run(i)
+        assert np.array_equal(iters, ref[f"it{i}"]), (i, iters, ref[f"it{i}"])
+        assert np.array_equal(z, ref[f"z{i}"]), (i, np.abs(z - ref[f"z{i}"]).max())
+        assert np.array_equal(gaps, ref[f"g{i}"]), (i, gaps, ref[f"g{i}"])
+
+
+if __name__ == "__main__":  # the single-step run (FASTPROX_B200_PAIRS=0 in the environment)
+    sys.path.insert(0, str(ROOT))
+    res = {}
+    for i in range(len(CASES)):
+        z, iters, gaps = _run(i)
+        res[f"z{i}"], res[f"it{i}"], res[f"g{i}"] = z, iters, gaps
+    np.savez(sys.argv[1], **res)
