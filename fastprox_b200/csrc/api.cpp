@@ -532,6 +532,9 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
         for (int a = 0; a < g.k; ++a) nfmax = std::max<int64_t>(nfmax, g.N / std::max<int64_t>(g.L[a], 1));
         ws->max_part = (int)std::max<int64_t>(ws->max_part, 3 * ((nfmax + 127) / 128));
     }
+    // the first iterate of a pair launch whose second iteration carries the
+    // check (the final u when it passes)
+    if (op->kind != kAniso && x.dtype == FP_F32 && iso_pair_ok(g, ws->shape_, ws->max_part)) A(&ws->U2, dualb);
     if (op->kind == kAniso) {
         A((void **)&ws->an_img, (size_t)B * sizeof(AnImage));
         A((void **)&ws->an_st, (size_t)B * sizeof(AnState));
@@ -935,22 +938,24 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     // a list of the live ones (images only retire, so a list built after the
     // count was read holds every image still live): the tail of a batch, where
     // a few slow images remain, launches only their blocks.
-    // Iterations 1 and 2 mod 4 (no check in either) run as one launch where
-    // the lean 2D step applies (iso_pair_ok).
+    // Iterations 1 and 2 mod 4 (no check in either), and 3 and 4 mod 4 (the
+    // second with the check) run as one launch each where the lean 2D step
+    // applies (iso_pair_ok).
     const int chunk = ws->chunk > 0 ? ws->chunk : 8;
-    const bool pairs = iso_pair_ok(g, ws->shape_);
+    const bool pairs = iso_pair_ok(g, ws->shape_, ws->max_part);
+    bf.U[2] = ws->U2;
     int par = 0, slot = 0, inflight = 0;
     int64_t launched = 0, steps = 0, lists = 0, nimg = g.B;
     const int64_t cap = (int64_t)max_iter + 1 + 2 * chunk;
     bool done = false;
     while (!done) {
         for (int j = 0; j < chunk; ++j) {
-            const bool pair = pairs && iso_pair_at(launched, max_iter);
-            e = iso_step(ws->dtype, g, c, bf, ws->shape_, par, pair ? kVariantPair : iso_variant(launched, max_iter, warm),
+            const int pv = pairs ? iso_pair_at(launched, max_iter, ws->U2 != nullptr) : -1;
+            e = iso_step(ws->dtype, g, c, bf, ws->shape_, par, pv >= 0 ? pv : iso_variant(launched, max_iter, warm),
                          nimg, s);
             if (e != cudaSuccess) return cuda_status(e);
             par ^= 1;
-            launched += pair ? 2 : 1;
+            launched += pv >= 0 ? 2 : 1;
             ++steps;
         }
         e = cudaMemcpyAsync(ws->h_live + slot, ws->live, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -1532,6 +1537,7 @@ fp_status deriv_prepare(const fp_op *op, fp_workspace *ws, VjpGeom &vg, VjpBuffe
     bf.d = ws->d;
     bf.U[0] = ws->U[0];
     bf.U[1] = ws->U[1];
+    bf.U[2] = ws->U2;
     bf.img = ws->img;
     bf.st = ws->st;
     bf.alpha = ws->spatial;

@@ -11,7 +11,7 @@ namespace fpb {
 // Device buffers of an isotropic solve (see engine.h for the layout).
 struct IsoBuffers {
     void *d = nullptr;          // B x N of T
-    void *U[2] = {nullptr, nullptr};
+    void *U[3] = {nullptr, nullptr, nullptr};  // U[2]: the first iterate of a pair launch (optional)
     void *V[2] = {nullptr, nullptr};
     void *dual = nullptr;       // k x B x N of T
     const void *alpha = nullptr;  // pixel weights (T), N or B x N, or null
@@ -57,11 +57,20 @@ cudaError_t iso_live_list(const IsoState *st, int64_t B, int *lmap, int *lcnt, c
 // kVariantPair two plain iterations (the lean 2D shape only).
 cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh,
                      int par, int variant, int64_t nimg, cudaStream_t s);
-// Variant of iso_step running iterations k and k + 1 in one launch, for k = 1
-// mod 4 and k + 1 < max_iter (neither has a check), where iso_pair_ok.
+// Variants of iso_step running iterations k and k + 1 in one launch, where
+// iso_pair_ok (the lean 2D shape over whole rows) and k + 1 < max_iter:
+// kVariantPair for k = 1 mod 4 (neither has a check), kVariantPairGap for
+// k = 3 mod 4 (the second carries the gap check and the restart test; needs
+// the third dual buffer bf.U[2], float32 only).
 constexpr int kVariantPair = 3;
-bool iso_pair_ok(const Geometry &g, const StepShape &sh);
-inline bool iso_pair_at(int64_t k, int max_iter) { return (k & 3) == 1 && k + 1 < max_iter; }
+constexpr int kVariantPairGap = 4;
+bool iso_pair_ok(const Geometry &g, const StepShape &sh, int max_part);
+inline int iso_pair_at(int64_t k, int max_iter, bool gap_pairs) {
+    if (k <= 0 || k + 1 >= max_iter) return -1;
+    if ((k & 3) == 1) return kVariantPair;
+    if ((k & 3) == 3 && gap_pairs) return kVariantPairGap;
+    return -1;
+}
 inline int iso_variant(int64_t k, int max_iter, bool warm) {
     if (k == 0) return warm ? 2 : 1;
     return (k % 4 == 0 || k == max_iter) ? 2 : 0;

@@ -826,30 +826,38 @@ __global__ void __launch_bounds__(128, 5) iso2d_lean_kernel(StepArgs A, IsoCall 
 }
 
 // ---------------------------------------------------------------------------
-// Two plain iterations in one pass over memory (temporal blocking of the
-// lean step).
+// Two iterations in one pass over memory (temporal blocking of the lean step).
 //
-// Iterations it and it + 1 carry no gap check and no restart test when
-// neither is 0 mod 4 (nor the last): the second needs nothing of the first
-// but its iterates u' = P(v + tau G z(v)), v' = u' + beta (u' - u), and its
-// beta is the one the per-image control would set, (tn - 1) / fista_t(tn).
-// A block covers whole rows and marches them like the lean step: the first
-// iteration in registers as lean_rows does, on its rows and one more above and
-// below; the second one row behind it, with the first's v' passing between
-// threads through a ring of three rows in shared memory (a thread's left and
-// right neighbours in z(v')). Only u'' and v'' are written. Traffic per pixel
-// and two iterations: d, u, v (and alpha) read once over R + 4 rows for R
-// output rows, u'' and v'' written once: about 50 B against 2 x 40 B for two
-// lean steps. Each iteration's arithmetic is lean_rows' (the same
-// expressions), so the iterates are those of two lean steps.
+// Iteration it = 1 mod 4 carries no check and no restart test, so the next
+// needs nothing of it but its iterates u' = P(v + tau G z(v)), v' = u' +
+// beta (u' - u); the next beta is the one the per-image control would set,
+// (tn - 1) / fista_t(tn). The pair (it, it + 1) is one launch: a block covers
+// whole rows and marches them like the lean step, the first iteration in
+// registers as lean_rows does, on its rows and one more above and below, the
+// second one row behind it, with the first's v' (and u') passing between
+// threads through rings of three rows in shared memory (a thread's left and
+// right neighbours in z(v'), z(u')). Only the second's u'', v'' are written.
+// Traffic per pixel and two iterations: d, u, v (and alpha) read once over
+// R + 4 rows for R output rows, u'' and v'' written once: about 50 B against
+// 2 x 40 B for two lean steps.
+// GAP2: it = 3 mod 4, the second iteration (0 mod 4) carrying the gap check
+// at u' and the restart test, with lean_rows' per-row partial sums; u' is
+// also written to the third dual buffer (U[2]), the final iterate when the
+// check passes (the state's fin_par is then 2).
+// Each iteration's arithmetic and every sum's order are lean_rows' (the same
+// expressions), so the iterates and the checks are those of two lean steps.
 // ---------------------------------------------------------------------------
 constexpr int kPairCols = 512;  // columns a block covers: 128 threads x 4
 
-template <class T, bool ALPHA>
-__global__ void __launch_bounds__(128, 4) iso2d_pair_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+template <class T, bool ALPHA, bool GAP2>
+__global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     constexpr int VEC = 4;
-    __shared__ __align__(16) T vs[3][2][kPairCols + VEC];  // v' of rows i % 3, both axes
-    __shared__ __align__(16) T ds[2][kPairCols + VEC];     // d of rows i % 2
+    constexpr int NU = GAP2 ? 3 : 1;
+    __shared__ __align__(16) T vs[3][2][kPairCols + VEC];   // v' of rows i % 3, both axes
+    __shared__ __align__(16) T us[NU][2][kPairCols + VEC];  // u' of rows i % 3 (GAP2)
+    __shared__ __align__(16) T ds[2][kPairCols + VEC];      // d of rows i % 2
+    __shared__ double rowp[GAP2 ? kLeanRowsMax * 8 : 1];
+    __shared__ double sh[32];
     __shared__ int flag;
     asm volatile("griddepcontrol.wait;" ::: "memory");  // a programmatic dependent of the previous step
     const int b = step_image(bf, blockIdx.z);
@@ -857,7 +865,7 @@ __global__ void __launch_bounds__(128, 4) iso2d_pair_kernel(StepArgs A, IsoCall 
     const IsoState st = bf.st[b];
     if (st.status != kLive) return;
     const int it = st.it;
-    if (it <= 0 || (it & 3) == 0 || ((it + 1) & 3) == 0 || it + 1 >= A.max_iter || st.zero_in) {
+    if (it <= 0 || (it & 3) != (GAP2 ? 3 : 1) || it + 1 >= A.max_iter || st.zero_in || (GAP2 && !bf.U[2])) {
         if (threadIdx.x == 0) atomicExch(bf.err, 3);
         return;
     }
@@ -872,6 +880,7 @@ __global__ void __launch_bounds__(128, 4) iso2d_pair_kernel(StepArgs A, IsoCall 
     T *UO0 = static_cast<T *>(bf.U[pout]) + (int64_t)b * 2 * N;
     T *VO0 = static_cast<T *>(bf.V[pout]) + (int64_t)b * 2 * N;
     T *UO1 = UO0 + N, *VO1 = VO0 + N;
+    T *UM0 = GAP2 ? static_cast<T *>(bf.U[2]) + (int64_t)b * 2 * N : nullptr;
     const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
     const T wh0 = (T)c.wh[0], wh1 = (T)c.wh[1], tau = (T)c.tau;
     const T rad = (T)im.radius, bnd = (T)im.bound;
@@ -927,38 +936,63 @@ __global__ void __launch_bounds__(128, 4) iso2d_pair_kernel(StepArgs A, IsoCall 
         const T pv = s0 > 0 ? V0[off + VEC - W] : T(0);
         x_z = dx + wh0 * (x_v0 - pv) + wh1 * (V1[off + VEC] - v1c[VEC - 1]);
     }
-    // second iteration's inputs of the row above: v', u', alpha, z(v') (five columns)
-    T pv0[VEC], pv1[VEC], pu0[VEC], pu1[VEC], pal[VEC], zp[VEC + 1];
+    // the second iteration's inputs on the row above: v', u', alpha, and z(v'),
+    // z(u') on five columns (the last the right neighbour's first)
+    T pv0[VEC], pv1[VEC], pu0[VEC], pu1[VEC], pal[VEC], zp[VEC + 1], zup[VEC + 1];
 #pragma unroll
-    for (int j = 0; j < VEC; ++j) pv0[j] = pv1[j] = pu0[j] = pu1[j] = pal[j] = zp[j] = T(0);
-    zp[VEC] = T(0);
+    for (int j = 0; j < VEC; ++j) pv0[j] = pv1[j] = pu0[j] = pu1[j] = pal[j] = T(0);
+#pragma unroll
+    for (int j = 0; j <= VEC; ++j) zp[j] = zup[j] = T(0);
+    double gap_acc = 0.0, dot_acc = 0.0;
 
-    // the second iteration on row j from z(v') of rows j (zp) and j + 1 (zq)
-    auto second = [&](int j, bool hasn, const T(&zq)[VEC]) {
-        if (!colok) return;
-        T uo0[VEC], uo1[VEC], vo0[VEC], vo1[VEC];
+    // the second iteration on row j from z(v') (and z(u')) of rows j and j + 1
+    auto second = [&](int j, bool hasn, const T(&zq)[VEC + 1], const T(&zuq)[VEC + 1]) {
+        if (colok) {
+            T uo0[VEC], uo1[VEC], vo0[VEC], vo1[VEC];
 #pragma unroll
-        for (int q = 0; q < VEC; ++q) {
-            const bool hasr = cb + q + 1 < W;
-            const T zright = q + 1 < VEC ? zp[q + 1] : zp[VEC];
-            const T g0 = hasn ? wh0 * (zq[q] - zp[q]) : T(0);
-            const T g1 = hasr ? wh1 * (zright - zp[q]) : T(0);
-            const T cv0 = pv0[q] + tau * g0;
-            const T cv1 = pv1[q] + tau * g1;
-            const T nn = cv0 * cv0 + cv1 * cv1;
-            const T rp = radius(pal, q);
-            const T sc = nn > rp * rp ? rp * rsqrt_t(nn) : T(1);
-            const T un0 = cv0 * sc, un1 = cv1 * sc;
-            vo0[q] = un0 + beta2 * (un0 - pu0[q]);
-            vo1[q] = un1 + beta2 * (un1 - pu1[q]);
-            uo0[q] = un0;
-            uo1[q] = un1;
+            for (int q = 0; q < VEC; ++q) {
+                const bool hasr = cb + q + 1 < W;
+                const T zright = q + 1 < VEC ? zp[q + 1] : zp[VEC];
+                const T g0 = hasn ? wh0 * (zq[q] - zp[q]) : T(0);
+                const T g1 = hasr ? wh1 * (zright - zp[q]) : T(0);
+                const T cv0 = pv0[q] + tau * g0;
+                const T cv1 = pv1[q] + tau * g1;
+                const T nn = cv0 * cv0 + cv1 * cv1;
+                const T rp = radius(pal, q);
+                const T sc = nn > rp * rp ? rp * rsqrt_t(nn) : T(1);
+                const T un0 = cv0 * sc, un1 = cv1 * sc;
+                if (GAP2) dot_acc += (double)((pv0[q] - un0) * (un0 - pu0[q]) + (pv1[q] - un1) * (un1 - pu1[q]));
+                vo0[q] = un0 + beta2 * (un0 - pu0[q]);
+                vo1[q] = un1 + beta2 * (un1 - pu1[q]);
+                uo0[q] = un0;
+                uo1[q] = un1;
+                if (GAP2) {
+                    const T zuright = q + 1 < VEC ? zup[q + 1] : zup[VEC];
+                    const T gu0 = hasn ? wh0 * (zuq[q] - zup[q]) : T(0);
+                    const T gu1 = hasr ? wh1 * (zuright - zup[q]) : T(0);
+                    gap_acc += (double)(rp * sqrt_t(gu0 * gu0 + gu1 * gu1) - (gu0 * pu0[q] + gu1 * pu1[q]));
+                }
+            }
+            const int o = j * W + cb;
+            store_pack<T, VEC>(UO0 + o, uo0);
+            store_pack<T, VEC>(UO1 + o, uo1);
+            store_pack<T, VEC>(VO0 + o, vo0);
+            store_pack<T, VEC>(VO1 + o, vo1);
         }
-        const int o = j * W + cb;
-        store_pack<T, VEC>(UO0 + o, uo0);
-        store_pack<T, VEC>(UO1 + o, uo1);
-        store_pack<T, VEC>(VO0 + o, vo0);
-        store_pack<T, VEC>(VO1 + o, vo1);
+        if (GAP2) {
+            // this row's sums over the warp (a fixed tree), per warp in shared
+            // memory, as lean_rows: rowp[(row - r0) * 8 + 2 * warp + (0: gap, 1: dot)]
+            double gv = gap_acc, dv = dot_acc;
+            for (int o = 16; o > 0; o >>= 1) {
+                gv += __shfl_down_sync(0xffffffffu, gv, o);
+                dv += __shfl_down_sync(0xffffffffu, dv, o);
+            }
+            if (lane == 0) {
+                rowp[(j - r0) * 8 + 2 * (threadIdx.x >> 5) + 0] = gv;
+                rowp[(j - r0) * 8 + 2 * (threadIdx.x >> 5) + 1] = dv;
+            }
+            gap_acc = dot_acc = 0.0;
+        }
     };
 
     for (int i = s0; i <= s1; ++i) {
@@ -1014,26 +1048,49 @@ __global__ void __launch_bounds__(128, 4) iso2d_pair_kernel(StepArgs A, IsoCall 
             for (int j = 0; j < VEC; ++j) {
                 vs[i % 3][0][cb + j] = vo0[j];
                 vs[i % 3][1][cb + j] = vo1[j];
+                if (GAP2) {
+                    us[i % 3][0][cb + j] = un0[j];
+                    us[i % 3][1][cb + j] = un1[j];
+                }
                 ds[i & 1][cb + j] = dc[j];
+            }
+            if (GAP2 && i >= r0 && i < r1) {
+                store_pack<T, VEC>(UM0 + off, un0);
+                store_pack<T, VEC>(UM0 + N + off, un1);
             }
         }
         __syncthreads();
         if (i >= r0) {
-            // z(v') on row i: own columns, and the right neighbour's first
-            T zq[VEC + 1];
-            T pr[VEC];
+            // z(v') and z(u') on row i: own columns, and the right neighbour's first
+            T zq[VEC + 1], zuq[VEC + 1], pr[VEC];
 #pragma unroll
             for (int j = 0; j < VEC; ++j) pr[j] = i > 0 ? pv0[j] : T(0);
-            zrow(dc, vo0, pr, vo1, (colok && cb > 0) ? vs[i % 3][1][cb - 1] : T(0), reinterpret_cast<T(&)[VEC]>(zq));
+            zrow(dc, vo0, pr, vo1, (colok && cb > 0) ? vs[i % 3][1][cb - 1] : T(0),
+                 reinterpret_cast<T(&)[VEC]>(zq));
             zq[VEC] = T(0);
             if (colok && cb + VEC < W) {
                 const T up = i > 0 ? vs[(i + 2) % 3][0][cb + VEC] : T(0);
                 zq[VEC] = ds[i & 1][cb + VEC] + wh0 * (vs[i % 3][0][cb + VEC] - up) +
                           wh1 * (vs[i % 3][1][cb + VEC] - vo1[VEC - 1]);
             }
-            if (i - 1 >= r0) second(i - 1, true, reinterpret_cast<const T(&)[VEC]>(zq));
+            if (GAP2) {
 #pragma unroll
-            for (int j = 0; j <= VEC; ++j) zp[j] = zq[j];
+                for (int j = 0; j < VEC; ++j) pr[j] = i > 0 ? pu0[j] : T(0);
+                zrow(dc, un0, pr, un1, (colok && cb > 0) ? us[i % 3][1][cb - 1] : T(0),
+                     reinterpret_cast<T(&)[VEC]>(zuq));
+                zuq[VEC] = T(0);
+                if (colok && cb + VEC < W) {
+                    const T up = i > 0 ? us[(i + 2) % 3][0][cb + VEC] : T(0);
+                    zuq[VEC] = ds[i & 1][cb + VEC] + wh0 * (us[i % 3][0][cb + VEC] - up) +
+                               wh1 * (us[i % 3][1][cb + VEC] - un1[VEC - 1]);
+                }
+            }
+            if (i - 1 >= r0) second(i - 1, true, zq, zuq);
+#pragma unroll
+            for (int j = 0; j <= VEC; ++j) {
+                zp[j] = zq[j];
+                if (GAP2) zup[j] = zuq[j];
+            }
         }
 #pragma unroll
         for (int j = 0; j < VEC; ++j) {
@@ -1055,18 +1112,41 @@ __global__ void __launch_bounds__(128, 4) iso2d_pair_kernel(StepArgs A, IsoCall 
     }
     // the last row of the image has no row below
     if (r1 == H && H - 1 >= r0) {
-        T zq[VEC];
+        T zq[VEC + 1];
 #pragma unroll
-        for (int j = 0; j < VEC; ++j) zq[j] = T(0);
-        second(H - 1, false, zq);
+        for (int j = 0; j <= VEC; ++j) zq[j] = T(0);
+        second(H - 1, false, zq, zq);
     }
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (GAP2) {
+        // one slot per row, the sum of its warps in order (as lean_rows)
+        __syncthreads();
+        if ((int)threadIdx.x < r1 - r0) {
+            double gv = 0.0, dv = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+                gv += rowp[threadIdx.x * 8 + 2 * w];
+                dv += rowp[threadIdx.x * 8 + 2 * w + 1];
+            }
+            const int64_t slot = r0 + (int)threadIdx.x;
+            part[slot * 2 + 0] = gv;
+            part[slot * 2 + 1] = dv;
+        }
+    }
     if (!arrive_last(bf.ticket + b, gridDim.x * gridDim.y, &flag)) return;
+    const double gap = GAP2 ? sum_partials(part, H, 2, 0, sh) : 0.0;
+    const double dot = GAP2 ? sum_partials(part, H, 2, 1, sh) : 0.0;
     if (threadIdx.x != 0) return;
     bf.ticket[b] = 0;
     IsoState s2 = st;
     control(s2, im, A.max_iter, false, false, 0.0, 0.0, pin, bf.live);
-    control(s2, im, A.max_iter, false, false, 0.0, 0.0, pin, bf.live);
+    if (GAP2) {
+        // the check is at u' (in U[2]); the update to u'' (in pout) stands unless it passes
+        control(s2, im, A.max_iter, true, true, gap, dot, 2, bf.live);
+        if (s2.status == kLive) s2.fin_par = pout;
+    } else {
+        control(s2, im, A.max_iter, false, false, 0.0, 0.0, pin, bf.live);
+    }
     bf.st[b] = s2;
 }
 
@@ -1934,14 +2014,22 @@ void launch_lean_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoB
 // (the halo of the first iteration is 4 rows), fewer per block while the
 // launch has too few blocks to spread (the tail of a batch).
 template <class T>
-void launch_pair(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
+void launch_pair(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s, bool gap) {
     const int64_t H = A.g.L[0];
-    int rows = sh.rows;
+    int rows = sh.rows < kLeanRowsMax ? sh.rows : kLeanRowsMax;
     while (rows > 8 && A.nimg * ((H + rows - 1) / rows) < tail_blocks()) rows /= 2;
     A.rows = rows;
     const dim3 grid(1, (unsigned)((H + rows - 1) / rows), (unsigned)A.nimg);
-    if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true>, grid, 128, 0, s, A, c, bf);
-    else launch_step(iso2d_pair_kernel<T, false>, grid, 128, 0, s, A, c, bf);
+    if (gap) {
+        // float only: the rings of the double variant pass the static shared-memory limit
+        if constexpr (sizeof(T) == 4) {
+            if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, true>, grid, 128, 0, s, A, c, bf);
+            else launch_step(iso2d_pair_kernel<T, false, true>, grid, 128, 0, s, A, c, bf);
+        }
+    } else {
+        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, false>, grid, 128, 0, s, A, c, bf);
+        else launch_step(iso2d_pair_kernel<T, false, false>, grid, 128, 0, s, A, c, bf);
+    }
 }
 
 template <class T, int VEC>
@@ -2016,8 +2104,8 @@ cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, co
     A.nimg = nimg;
     A.row_part = 0;
     if (nimg <= 0) return cudaSuccess;
-    if (variant == kVariantPair) {
-        launch_pair<T>(sh, A, c, bf, s);
+    if (variant == kVariantPair || variant == kVariantPairGap) {
+        launch_pair<T>(sh, A, c, bf, s, variant == kVariantPairGap);
         return cudaGetLastError();
     }
     StepShape sh2 = sh;
@@ -2170,13 +2258,13 @@ cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBu
                       : step_t<double>(g, c, bf, sh, par, variant, nimg, s);
 }
 
-bool iso_pair_ok(const Geometry &g, const StepShape &sh) {
+bool iso_pair_ok(const Geometry &g, const StepShape &sh, int max_part) {
     static const bool on = [] {
         const char *v = std::getenv("FASTPROX_B200_PAIRS");
         return !(v && v[0] == '0' && v[1] == 0);
     }();
     return on && g.k == 2 && sh.kind == 4 && sh.vec == 4 && sh.bx == 128 && sh.gx == 1 && g.L[1] <= kPairCols &&
-           g.L[0] >= 2;
+           g.L[0] >= 2 && g.L[0] <= max_part;
 }
 
 cudaError_t iso_live_list(const IsoState *st, int64_t B, int *lmap, int *lcnt, cudaStream_t s) {
