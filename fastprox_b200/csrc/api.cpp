@@ -534,7 +534,7 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     }
     // the first iterate of a pair launch whose second iteration carries the
     // check (the final u when it passes)
-    if (op->kind != kAniso && x.dtype == FP_F32 && iso_pair_ok(g, ws->shape_, ws->max_part)) A(&ws->U2, dualb);
+    if (op->kind != kAniso && iso_pair_ok(g, ws->shape_, ws->max_part)) A(&ws->U2, dualb);
     if (op->kind == kAniso) {
         A((void **)&ws->an_img, (size_t)B * sizeof(AnImage));
         A((void **)&ws->an_st, (size_t)B * sizeof(AnState));

@@ -61,7 +61,7 @@ cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBu
 // iso_pair_ok (the lean 2D shape over whole rows) and k + 1 < max_iter:
 // kVariantPair for k = 1 mod 4 (neither has a check), kVariantPairGap for
 // k = 3 mod 4 (the second carries the gap check and the restart test; needs
-// the third dual buffer bf.U[2], float32 only).
+// the third dual buffer bf.U[2]).
 constexpr int kVariantPair = 3;
 constexpr int kVariantPairGap = 4;
 bool iso_pair_ok(const Geometry &g, const StepShape &sh, int max_part);

@@ -835,8 +835,9 @@ __global__ void __launch_bounds__(128, 5) iso2d_lean_kernel(StepArgs A, IsoCall 
 // whole rows and marches them like the lean step, the first iteration in
 // registers as lean_rows does, on its rows and one more above and below, the
 // second one row behind it, with the first's v' (and u') passing between
-// threads through rings of three rows in shared memory (a thread's left and
-// right neighbours in z(v'), z(u')). Only the second's u'', v'' are written.
+// threads by shuffles, and between warps through shared memory (a warp's
+// first and last columns, for its neighbours' z(v'), z(u')). Only the
+// second's u'', v'' are written.
 // Traffic per pixel and two iterations: d, u, v (and alpha) read once over
 // R + 4 rows for R output rows, u'' and v'' written once: about 50 B against
 // 2 x 40 B for two lean steps.
@@ -852,10 +853,11 @@ constexpr int kPairCols = 512;  // columns a block covers: 128 threads x 4
 template <class T, bool ALPHA, bool GAP2>
 __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     constexpr int VEC = 4;
-    constexpr int NU = GAP2 ? 3 : 1;
-    __shared__ __align__(16) T vs[3][2][kPairCols + VEC];   // v' of rows i % 3, both axes
-    __shared__ __align__(16) T us[NU][2][kPairCols + VEC];  // u' of rows i % 3 (GAP2)
-    __shared__ __align__(16) T ds[2][kPairCols + VEC];      // d of rows i % 2
+    // what warps pass on per row (two rows in flight): a warp's first column
+    // (d, v0', v1', u0', u1') to the warp on its left, its last column's v1'
+    // (u1') to the warp on its right
+    __shared__ T xf[2][4][5];
+    __shared__ T xl[2][4][2];
     __shared__ double rowp[GAP2 ? kLeanRowsMax * 8 : 1];
     __shared__ double sh[32];
     __shared__ int flag;
@@ -944,6 +946,7 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
 #pragma unroll
     for (int j = 0; j <= VEC; ++j) zp[j] = zup[j] = T(0);
     double gap_acc = 0.0, dot_acc = 0.0;
+    T xv0p = T(0), xu0p = T(0);  // lane 31: v0', u0' of the right neighbour's first column, row above
 
     // the second iteration on row j from z(v') (and z(u')) of rows j and j + 1
     auto second = [&](int j, bool hasn, const T(&zq)[VEC + 1], const T(&zuq)[VEC + 1]) {
@@ -1043,16 +1046,20 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
             vo0[j] = un0[j] + beta1 * (un0[j] - u0c[j]);
             vo1[j] = un1[j] + beta1 * (un1[j] - u1c[j]);
         }
+        const int w = (int)(threadIdx.x >> 5);
         if (colok) {
-#pragma unroll
-            for (int j = 0; j < VEC; ++j) {
-                vs[i % 3][0][cb + j] = vo0[j];
-                vs[i % 3][1][cb + j] = vo1[j];
+            if (lane == 0) {
+                xf[i & 1][w][0] = dc[0];
+                xf[i & 1][w][1] = vo0[0];
+                xf[i & 1][w][2] = vo1[0];
                 if (GAP2) {
-                    us[i % 3][0][cb + j] = un0[j];
-                    us[i % 3][1][cb + j] = un1[j];
+                    xf[i & 1][w][3] = un0[0];
+                    xf[i & 1][w][4] = un1[0];
                 }
-                ds[i & 1][cb + j] = dc[j];
+            }
+            if (lane == 31) {
+                xl[i & 1][w][0] = vo1[VEC - 1];
+                if (GAP2) xl[i & 1][w][1] = un1[VEC - 1];
             }
             if (GAP2 && i >= r0 && i < r1) {
                 store_pack<T, VEC>(UM0 + off, un0);
@@ -1060,30 +1067,40 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
             }
         }
         __syncthreads();
+        // the left neighbour's last v1' (u1'), and the right neighbour's first column
+        T lv1 = __shfl_up_sync(0xffffffffu, vo1[VEC - 1], 1);
+        T lu1 = GAP2 ? __shfl_up_sync(0xffffffffu, un1[VEC - 1], 1) : T(0);
+        if (lane == 0) {
+            lv1 = w > 0 ? xl[i & 1][w - 1][0] : T(0);
+            if (GAP2) lu1 = w > 0 ? xl[i & 1][w - 1][1] : T(0);
+        }
+        const bool hasx = lane == 31 && colok && cb + VEC < W;
+        T nd = T(0), nv0 = T(0), nv1 = T(0), nu0 = T(0), nu1 = T(0);
+        if (hasx) {
+            nd = xf[i & 1][w + 1][0];
+            nv0 = xf[i & 1][w + 1][1];
+            nv1 = xf[i & 1][w + 1][2];
+            if (GAP2) {
+                nu0 = xf[i & 1][w + 1][3];
+                nu1 = xf[i & 1][w + 1][4];
+            }
+        }
         if (i >= r0) {
             // z(v') and z(u') on row i: own columns, and the right neighbour's first
             T zq[VEC + 1], zuq[VEC + 1], pr[VEC];
 #pragma unroll
             for (int j = 0; j < VEC; ++j) pr[j] = i > 0 ? pv0[j] : T(0);
-            zrow(dc, vo0, pr, vo1, (colok && cb > 0) ? vs[i % 3][1][cb - 1] : T(0),
-                 reinterpret_cast<T(&)[VEC]>(zq));
-            zq[VEC] = T(0);
-            if (colok && cb + VEC < W) {
-                const T up = i > 0 ? vs[(i + 2) % 3][0][cb + VEC] : T(0);
-                zq[VEC] = ds[i & 1][cb + VEC] + wh0 * (vs[i % 3][0][cb + VEC] - up) +
-                          wh1 * (vs[i % 3][1][cb + VEC] - vo1[VEC - 1]);
-            }
+            zrow(dc, vo0, pr, vo1, lv1, reinterpret_cast<T(&)[VEC]>(zq));
+            zq[VEC] = __shfl_down_sync(0xffffffffu, zq[0], 1);
+            if (lane == 31)
+                zq[VEC] = hasx ? nd + wh0 * (nv0 - (i > 0 ? xv0p : T(0))) + wh1 * (nv1 - vo1[VEC - 1]) : T(0);
             if (GAP2) {
 #pragma unroll
                 for (int j = 0; j < VEC; ++j) pr[j] = i > 0 ? pu0[j] : T(0);
-                zrow(dc, un0, pr, un1, (colok && cb > 0) ? us[i % 3][1][cb - 1] : T(0),
-                     reinterpret_cast<T(&)[VEC]>(zuq));
-                zuq[VEC] = T(0);
-                if (colok && cb + VEC < W) {
-                    const T up = i > 0 ? us[(i + 2) % 3][0][cb + VEC] : T(0);
-                    zuq[VEC] = ds[i & 1][cb + VEC] + wh0 * (us[i % 3][0][cb + VEC] - up) +
-                               wh1 * (us[i % 3][1][cb + VEC] - un1[VEC - 1]);
-                }
+                zrow(dc, un0, pr, un1, lu1, reinterpret_cast<T(&)[VEC]>(zuq));
+                zuq[VEC] = __shfl_down_sync(0xffffffffu, zuq[0], 1);
+                if (lane == 31)
+                    zuq[VEC] = hasx ? nd + wh0 * (nu0 - (i > 0 ? xu0p : T(0))) + wh1 * (nu1 - un1[VEC - 1]) : T(0);
             }
             if (i - 1 >= r0) second(i - 1, true, zq, zuq);
 #pragma unroll
@@ -1092,6 +1109,8 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
                 if (GAP2) zup[j] = zuq[j];
             }
         }
+        xv0p = nv0;
+        xu0p = nu0;
 #pragma unroll
         for (int j = 0; j < VEC; ++j) {
             pv0[j] = vo0[j];
@@ -2010,22 +2029,25 @@ void launch_lean_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoB
     else launch_step(iso2d_lean_kernel<T, VEC, ALPHA, false, false>, grid, sh.bx, 0, s, A, c, bf);
 }
 
-// Two plain iterations per launch: blocks of whole rows, at least 8 of them
-// (the halo of the first iteration is 4 rows), fewer per block while the
-// launch has too few blocks to spread (the tail of a batch).
+// Two iterations per launch: blocks of whole rows (the first iteration's
+// halo is 4 rows).
 template <class T>
 void launch_pair(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s, bool gap) {
+    static const int rows_hint = [] {  // tuning hint FASTPROX_B200_PAIR_ROWS
+        const char *v = std::getenv("FASTPROX_B200_PAIR_ROWS");
+        const int r = v ? std::atoi(v) : 0;
+        return (r >= 8 && r <= kLeanRowsMax) ? r : 0;
+    }();
+    (void)sh;
     const int64_t H = A.g.L[0];
-    int rows = sh.rows < kLeanRowsMax ? sh.rows : kLeanRowsMax;
-    while (rows > 8 && A.nimg * ((H + rows - 1) / rows) < tail_blocks()) rows /= 2;
+    // 8 rows per block: on 64 x 512^2 772 images/s, against 760 at 16 and 745 at 32
+    // (more blocks hide more of the loads' latency than the longer halo costs)
+    const int rows = rows_hint ? rows_hint : 8;
     A.rows = rows;
     const dim3 grid(1, (unsigned)((H + rows - 1) / rows), (unsigned)A.nimg);
     if (gap) {
-        // float only: the rings of the double variant pass the static shared-memory limit
-        if constexpr (sizeof(T) == 4) {
-            if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, true>, grid, 128, 0, s, A, c, bf);
-            else launch_step(iso2d_pair_kernel<T, false, true>, grid, 128, 0, s, A, c, bf);
-        }
+        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, true>, grid, 128, 0, s, A, c, bf);
+        else launch_step(iso2d_pair_kernel<T, false, true>, grid, 128, 0, s, A, c, bf);
     } else {
         if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, false>, grid, 128, 0, s, A, c, bf);
         else launch_step(iso2d_pair_kernel<T, false, false>, grid, 128, 0, s, A, c, bf);
