@@ -850,6 +850,36 @@ __global__ void __launch_bounds__(128, 5) iso2d_lean_kernel(StepArgs A, IsoCall 
 // ---------------------------------------------------------------------------
 constexpr int kPairCols = 512;  // columns a block covers: 128 threads x 4
 
+// Asynchronous copies global -> shared of a thread's own data (cp.async),
+// counted per thread in commit groups.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async_small(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "n"(BYTES)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// The pair kernel's row ring: three rows of each thread's inputs (d, v0, v1,
+// u0, u1, alpha: VEC entries each; v1 of the column before, and lane 31's d,
+// v0, v1 of the column after), in flight up to three rows ahead.
+constexpr int kPairRing = 3;
+template <class T, bool ALPHA>
+constexpr size_t pair_slot_bytes() {
+    return (size_t)128 * ((ALPHA ? 6 : 5) * 4 * sizeof(T) + 4 * sizeof(T));
+}
+template <class T, bool ALPHA>
+constexpr size_t pair_ring_bytes() {
+    return kPairRing * pair_slot_bytes<T, ALPHA>();
+}
+
 template <class T, bool ALPHA, bool GAP2>
 __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     constexpr int VEC = 4;
@@ -861,6 +891,7 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
     __shared__ double rowp[GAP2 ? kLeanRowsMax * 8 : 1];
     __shared__ double sh[32];
     __shared__ int flag;
+    extern __shared__ __align__(16) unsigned char pair_ring[];
     asm volatile("griddepcontrol.wait;" ::: "memory");  // a programmatic dependent of the previous step
     const int b = step_image(bf, blockIdx.z);
     if (b < 0) return;
@@ -918,9 +949,55 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
         return al[j] == T(0) ? T(0) : (r <= bnd ? r : bnd);
     };
 
+    // The rows after s0 come through the ring: row r is copied into slot
+    // r % 3 two steps before it is read (issued at step r - 3, read at step
+    // r - 1), each thread copying and reading only its own entries, so no
+    // barrier guards the ring; a slot is refilled one step after it was read.
+    constexpr int NARR = ALPHA ? 6 : 5;
+    constexpr int AB = VEC * (int)sizeof(T);  // bytes of one array's entries per thread
+    const unsigned tid = threadIdx.x;
+    auto slot_arr = [&](int r, int a) -> T * {
+        return reinterpret_cast<T *>(pair_ring + (size_t)(r % kPairRing) * pair_slot_bytes<T, ALPHA>() +
+                                     ((size_t)a * 128 + tid) * AB);
+    };
+    auto slot_sc = [&](int r, int q) -> T * {
+        return reinterpret_cast<T *>(pair_ring + (size_t)(r % kPairRing) * pair_slot_bytes<T, ALPHA>() +
+                                     (size_t)NARR * 128 * AB + ((size_t)tid * 4 + q) * sizeof(T));
+    };
+    auto issue = [&](int r) {  // one commit group per row, empty past the rows this block reads
+        if (r <= s1 + 1 && r < H && colok) {
+            const int o = r * W + cb;
+            const T *src[6] = {D + o, V0 + o, V1 + o, U0 + o, U1 + o, ALPHA ? AL + o : nullptr};
+#pragma unroll
+            for (int a = 0; a < NARR; ++a)
+#pragma unroll
+                for (int q = 0; q < AB; q += 16) cp_async16(reinterpret_cast<char *>(slot_arr(r, a)) + q,
+                                                            reinterpret_cast<const char *>(src[a]) + q);
+            if (cb > 0) cp_async_small<sizeof(T)>(slot_sc(r, 0), V1 + o - 1);
+            if (ext) {
+                cp_async_small<sizeof(T)>(slot_sc(r, 1), D + o + VEC);
+                cp_async_small<sizeof(T)>(slot_sc(r, 2), V0 + o + VEC);
+                cp_async_small<sizeof(T)>(slot_sc(r, 3), V1 + o + VEC);
+            }
+        }
+        cp_async_commit();
+    };
+    auto rd = [&](int r, int a, T(&o)[VEC]) {
+        if (colok) {
+            const T *p = slot_arr(r, a);
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) o[j] = p[j];
+        } else {
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) o[j] = T(0);
+        }
+    };
+    issue(s0 + 1);
+    issue(s0 + 2);
+
     // first iteration: row s0 and the part of row s0 - 1 it needs (lean_rows)
     int off = s0 * W + cb;
-    T dc[VEC], v0c[VEC], v1c[VEC], u0c[VEC], u1c[VEC], zc[VEC], v0p[VEC];
+    T dc[VEC], v0c[VEC], v1c[VEC], u0c[VEC], u1c[VEC], zc[VEC], v0p[VEC], aln[VEC];
     ld(D, off, dc);
     ld(V0, off, v0c);
     ld(V1, off, v1c);
@@ -998,34 +1075,33 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
         }
     };
 
+    if (ALPHA) ld(AL, off, aln);
     for (int i = s0; i <= s1; ++i) {
         const bool hasn = i + 1 < H;
         const int offn = off + W;
-        T dn[VEC], v0n[VEC], v1n[VEC], u0n[VEC], u1n[VEC], zn[VEC];
+        T dn[VEC], v0n[VEC], v1n[VEC], u0n[VEC], u1n[VEC], zn[VEC], al[VEC];
         T nx_v0 = T(0), nx_z = T(0);
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) al[j] = aln[j];
+        cp_async_wait<1>();  // row i + 1 is in (row i + 2 may still be in flight)
         if (hasn) {
-            ld(D, offn, dn);
-            ld(V0, offn, v0n);
-            ld(V1, offn, v1n);
-            ld(U0, offn, u0n);
-            ld(U1, offn, u1n);
-            zrow(dn, v0n, v0c, v1n, (colok && cb > 0) ? V1[offn - 1] : T(0), zn);
+            rd(i + 1, 0, dn);
+            rd(i + 1, 1, v0n);
+            rd(i + 1, 2, v1n);
+            rd(i + 1, 3, u0n);
+            rd(i + 1, 4, u1n);
+            if (ALPHA) rd(i + 1, 5, aln);
+            zrow(dn, v0n, v0c, v1n, (colok && cb > 0) ? *slot_sc(i + 1, 0) : T(0), zn);
             if (ext) {
-                const T dx = D[offn + VEC];
-                nx_v0 = V0[offn + VEC];
-                nx_z = dx + wh0 * (nx_v0 - x_v0) + wh1 * (V1[offn + VEC] - v1n[VEC - 1]);
+                const T dx = *slot_sc(i + 1, 1);
+                nx_v0 = *slot_sc(i + 1, 2);
+                nx_z = dx + wh0 * (nx_v0 - x_v0) + wh1 * (*slot_sc(i + 1, 3) - v1n[VEC - 1]);
             }
         } else {
 #pragma unroll
             for (int j = 0; j < VEC; ++j) zn[j] = u0n[j] = u1n[j] = v0n[j] = v1n[j] = dn[j] = T(0);
         }
-        T al[VEC];
-        if (ALPHA) {
-            if (colok) load_pack<T, VEC>(AL + off, al);
-            else
-#pragma unroll
-                for (int j = 0; j < VEC; ++j) al[j] = T(0);
-        }
+        issue(i + 3);  // into the slot of row i, read at the last step
         T zr = __shfl_down_sync(0xffffffffu, zc[0], 1);
         if (lane == 31) zr = x_z;
         // the first iteration on row i
@@ -1129,6 +1205,7 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
         x_z = nx_z;
         off = offn;
     }
+    cp_async_wait<0>();
     // the last row of the image has no row below
     if (r1 == H && H - 1 >= r0) {
         T zq[VEC + 1];
@@ -2031,6 +2108,25 @@ void launch_lean_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoB
 
 // Two iterations per launch: blocks of whole rows (the first iteration's
 // halo is 4 rows).
+// The pair kernels' ring passes 48 KB in float64: their attribute, once per device.
+template <class T>
+void pair_attr() {
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    const unsigned long long bit = 1ull << dev;
+    if (done.load() & bit) return;
+    cudaFuncSetAttribute(iso2d_pair_kernel<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)pair_ring_bytes<T, true>());
+    cudaFuncSetAttribute(iso2d_pair_kernel<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)pair_ring_bytes<T, false>());
+    cudaFuncSetAttribute(iso2d_pair_kernel<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)pair_ring_bytes<T, true>());
+    cudaFuncSetAttribute(iso2d_pair_kernel<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)pair_ring_bytes<T, false>());
+    done.fetch_or(bit);
+}
+
 template <class T>
 void launch_pair(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s, bool gap) {
     static const int rows_hint = [] {  // tuning hint FASTPROX_B200_PAIR_ROWS
@@ -2045,12 +2141,13 @@ void launch_pair(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuf
     const int rows = rows_hint ? rows_hint : 8;
     A.rows = rows;
     const dim3 grid(1, (unsigned)((H + rows - 1) / rows), (unsigned)A.nimg);
+    pair_attr<T>();
     if (gap) {
-        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, true>, grid, 128, 0, s, A, c, bf);
-        else launch_step(iso2d_pair_kernel<T, false, true>, grid, 128, 0, s, A, c, bf);
+        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, true>, grid, 128, pair_ring_bytes<T, true>(), s, A, c, bf);
+        else launch_step(iso2d_pair_kernel<T, false, true>, grid, 128, pair_ring_bytes<T, false>(), s, A, c, bf);
     } else {
-        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, false>, grid, 128, 0, s, A, c, bf);
-        else launch_step(iso2d_pair_kernel<T, false, false>, grid, 128, 0, s, A, c, bf);
+        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, false>, grid, 128, pair_ring_bytes<T, true>(), s, A, c, bf);
+        else launch_step(iso2d_pair_kernel<T, false, false>, grid, 128, pair_ring_bytes<T, false>(), s, A, c, bf);
     }
 }
 
