@@ -2137,8 +2137,11 @@ void launch_pair(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuf
     (void)sh;
     const int64_t H = A.g.L[0];
     // 12 rows per block: on 64 x 512^2 836 images/s, against 815 at 8 and 822 at 16
-    // (shorter blocks spread better, longer ones recompute less of the halo)
-    const int rows = rows_hint ? rows_hint : 12;
+    // (shorter blocks spread better, longer ones recompute less of the halo);
+    // fewer, down to 4, while the launch has too few blocks to spread (the
+    // tail of a batch, a few images live)
+    int rows = rows_hint ? rows_hint : 12;
+    while (!rows_hint && rows > 4 && A.nimg * ((H + rows - 1) / rows) < tail_blocks()) rows = rows / 2 > 4 ? rows / 2 : 4;
     A.rows = rows;
     const dim3 grid(1, (unsigned)((H + rows - 1) / rows), (unsigned)A.nimg);
     pair_attr<T>();
