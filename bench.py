@@ -38,6 +38,11 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 B, H, W = 64, 512, 512
+# DRAM bytes (read + write) of one launch of the dominant kernel, the pair
+# launch whose second iteration carries the gap check (two iterations over the
+# 64 images), from one ncu capture of this batch: below the 2 x 40 B per pixel
+# of its two iterations, since d, u, v and alpha are read once for both.
+PAIR_TRAFFIC = 357_220_352 + 357_471_232
 GAMMAS = (0.05, 0.1, 0.2)
 TOL, MAX_ITER = 1e-6, 20000
 BYTES_PER_PIXEL_ITER = 40  # d 4 + u 8 + v 8 in, u 8 + v 8 out, alpha 4 (fp32)
@@ -323,7 +328,9 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "bytes_per_pixel_iter": BYTES_PER_PIXEL_ITER,
-                         "traffic": None},
+                         "achieved_over": "the whole call (every kernel and the tail of slow images)",
+                         "traffic": PAIR_TRAFFIC, "traffic_kernel": "iso2d_pair_kernel with the check, per launch",
+                         "algorithmic_bytes_per_launch": 2 * BYTES_PER_PIXEL_ITER * B * H * W},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "images/s", "h2d_bytes_per_step": int(x.nbytes),
                     "d2h_bytes_per_step": int(x.nbytes)},
