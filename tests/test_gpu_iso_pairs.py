@@ -1,12 +1,15 @@
-"""Two plain isotropic iterations in one launch (iso2d_pair_kernel) against
-the same iterations one launch each: the same arithmetic per iteration, so
-the same iterates, iteration counts and gaps. Covers images with and without
-pixel weights, float32 and float64, heights that leave blocks of one to
-sixteen rows and a last block shorter than the rest, widths below the block's
-512 columns, per-image steps (images that stop at different iterations),
-warm starts, and max_iter values that end inside a pair. The one-launch-each
-run is a child process with FASTPROX_B200_PAIRS=0 (the library reads its
-tuning hints once)."""
+"""Two isotropic iterations in one launch (iso2d_pair_kernel: iterations 1
+and 2 mod 4, and 3 and 4 mod 4 with the gap check and restart test in the
+second) against the same iterations one launch each: the same arithmetic per
+iteration and the same order of every sum, so the same iterates, iteration
+counts and gaps, bit for bit. Covers images with and without pixel weights,
+heights that leave blocks of 4 to 12 rows and a last block shorter than the
+rest, images of two and three rows, widths below the block's 512 columns,
+per-image steps (images that stop at different iterations), warm starts, and
+max_iter values that end inside a pair. The float64 cases run single steps
+either way (the float64 lean shape has 2-wide vectors; pairs need 4) and check
+that the switch leaves them alone. The one-launch-each run is a child process
+with FASTPROX_B200_PAIRS=0 (the library reads its tuning hints once)."""
 
 import os
 import pathlib
@@ -25,6 +28,8 @@ CASES = [  # (dtype, B, H, W, alpha, tol, max_iter, warm)
     (np.float64, 2, 5, 64, False, 0.0, 6, False),
     (np.float32, 2, 64, 508, True, 0.0, 7, False),
     (np.float64, 2, 96, 128, False, 1e-8, 3000, True),
+    (np.float32, 3, 2, 40, True, 1e-7, 300, False),
+    (np.float32, 2, 3, 36, False, 0.0, 9, False),
 ]
 
 
