@@ -863,6 +863,13 @@ __device__ __forceinline__ void cp_async_small(void *dst, const void *src) {
                  "l"(src), "n"(BYTES)
                  : "memory");
 }
+// One entry, or zeros when n is 0 (nothing is read then).
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void *dst, const void *src, unsigned n) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "n"(BYTES), "r"(n)
+                 : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
@@ -1704,7 +1711,8 @@ __global__ void __launch_bounds__(256) iso_generic_kernel(StepArgs A, IsoCall c,
 // The 3D step: a block owns a kTY x kTX tile of the (axis 1, axis 2) plane and
 // marches along axis 0 through a chunk of A.rows slices. For each slice it
 // stages d and the dual of the next slice over the tile and a one-entry halo
-// in shared memory (three slices in rotation), forms z of the next slice over
+// in shared memory (four slices in rotation, copied by cp.async three steps
+// ahead), forms z of the next slice over
 // the tile and its forward halo (two slices of z in rotation), and updates the
 // tile at the current slice from z of this slice and of the next. Every array
 // is read from HBM once per iteration; the halo entries are neighbouring
@@ -1715,13 +1723,14 @@ __global__ void __launch_bounds__(256) iso_generic_kernel(StepArgs A, IsoCall c,
 constexpr int k3TX = 32, k3TY = 8;
 constexpr int k3RX = k3TX + 2, k3RY = k3TY + 2, k3R = k3RX * k3RY;  // staged region: tile plus halo
 constexpr int k3ZX = k3TX + 1, k3Z = (k3TY + 1) * k3ZX;              // z: tile plus forward halo
+constexpr int k3Ring = 4;  // staged slices in rotation (two in use, two in flight)
 
 template <class T, bool ALPHA, bool GAP, bool ZIN>
 __global__ void __launch_bounds__(k3TX * k3TY) iso3d_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     constexpr int NA = GAP ? 7 : 4;  // staged arrays: d, v0..v2 (and u0..u2 for the gap)
     extern __shared__ __align__(16) unsigned char i3_smem[];
     T(*reg)[NA][k3R] = reinterpret_cast<T(*)[NA][k3R]>(i3_smem);
-    T(*zs)[GAP ? 2 : 1][k3Z] = reinterpret_cast<T(*)[GAP ? 2 : 1][k3Z]>(i3_smem + 3 * NA * k3R * sizeof(T));
+    T(*zs)[GAP ? 2 : 1][k3Z] = reinterpret_cast<T(*)[GAP ? 2 : 1][k3Z]>(i3_smem + k3Ring * NA * k3R * sizeof(T));
     __shared__ double sh[32];
     __shared__ int flag;
     asm volatile("griddepcontrol.wait;" ::: "memory");  // a programmatic dependent of the previous step
@@ -1757,7 +1766,7 @@ __global__ void __launch_bounds__(k3TX * k3TY) iso3d_kernel(StepArgs A, IsoCall 
     const int y0 = (blockIdx.y % nyt) * k3TY;
     const int s0 = (blockIdx.y / nyt) * A.rows;
     const int s1 = min(D0, s0 + A.rows);
-    auto q3 = [](int sl) { return (sl + 3) % 3; };
+    auto q3 = [](int sl) { return (sl + k3Ring) % k3Ring; };
     // The region entries this thread stages (tid and tid + 256): their
     // offsets in a slice and whether they lie in the image.
     constexpr int kE = (k3R + k3TX * k3TY - 1) / (k3TX * k3TY);
@@ -1770,31 +1779,31 @@ __global__ void __launch_bounds__(k3TX * k3TY) iso3d_kernel(StepArgs A, IsoCall 
         inimg[e] = i < k3R && gy >= 0 && gy < D1 && gx >= 0 && gx < D2;
         poff[e] = inimg[e] ? (int64_t)gy * D2 + gx : 0;
     }
-    // Slices go through registers: the loads of slice sl + 2 are issued
-    // before the work on slice sl and land in shared memory one step later.
-    T pf[kE][NA];
-    auto fetch = [&](int sl) {
+    // Slices come into the ring by cp.async (zeros outside the image), issued
+    // three steps before the work on them: slice sl + 3 goes into the slot of
+    // slice sl - 1 once every thread is past the last step's reads of it.
+    auto issue = [&](int sl) {
+        if (sl <= s1) {
+            T(*r)[k3R] = reg[q3(sl)];
 #pragma unroll
-        for (int e = 0; e < kE; ++e) {
-            const bool in = inimg[e] && sl >= 0 && sl < D0;
-            const int64_t o = in ? (int64_t)sl * S0 + poff[e] : 0;
-            pf[e][0] = in ? D[o] : T(0);
+            for (int e = 0; e < kE; ++e) {
+                const int i = tid + e * k3TX * k3TY;
+                if (i < k3R) {
+                    const bool in = inimg[e] && sl >= 0 && sl < D0;
+                    const int64_t o = in ? (int64_t)sl * S0 + poff[e] : 0;
+                    cp_async_zfill<sizeof(T)>(&r[0][i], D + o, in ? sizeof(T) : 0);
 #pragma unroll
-            for (int a = 0; a < 3; ++a) pf[e][1 + a] = (in && !ZIN) ? V[a * N + o] : T(0);
-            if (GAP)
+                    for (int a = 0; a < 3; ++a)
+                        cp_async_zfill<sizeof(T)>(&r[1 + a][i], V + a * N + o, (in && !ZIN) ? sizeof(T) : 0);
+                    if (GAP)
 #pragma unroll
-                for (int a = 0; a < 3; ++a) pf[e][(GAP ? 4 : 1) + a] = (in && !ZIN) ? U[a * N + o] : T(0);
+                        for (int a = 0; a < 3; ++a)
+                            cp_async_zfill<sizeof(T)>(&r[(GAP ? 4 : 1) + a][i], U + a * N + o,
+                                                      (in && !ZIN) ? sizeof(T) : 0);
+                }
+            }
         }
-    };
-    auto put = [&](int sl) {
-        T(*r)[k3R] = reg[q3(sl)];
-#pragma unroll
-        for (int e = 0; e < kE; ++e) {
-            const int i = tid + e * k3TX * k3TY;
-            if (i < k3R)
-#pragma unroll
-                for (int a = 0; a < NA; ++a) r[a][i] = pf[e][a];
-        }
+        cp_async_commit();
     };
     // z of slice sl (of v, and of u for the gap) over the tile and its forward halo
     auto zslice = [&](int sl) {
@@ -1823,22 +1832,20 @@ __global__ void __launch_bounds__(k3TX * k3TY) iso3d_kernel(StepArgs A, IsoCall 
         for (int a = 0; a < 3; ++a) pu[a] = U[a * N + o];
     };
     double gap_acc = 0.0, dot_acc = 0.0;
-    fetch(s0 - 1);
-    put(s0 - 1);
-    fetch(s0);
-    put(s0);
-    fetch(s0 + 1);
+    issue(s0 - 1);
+    issue(s0);
+    issue(s0 + 1);
+    issue(s0 + 2);
     fetch_u(s0);
+    cp_async_wait<2>();  // slices s0 - 1 and s0 are in
     __syncthreads();
     zslice(s0);
     for (int sl = s0; sl < s1; ++sl) {
-        put(sl + 1);
         T uc[3] = {pu[0], pu[1], pu[2]};
-        if (sl + 1 < s1) {
-            fetch(sl + 2);
-            fetch_u(sl + 1);
-        }
+        if (sl + 1 < s1) fetch_u(sl + 1);
+        cp_async_wait<1>();  // slice sl + 1 is in (sl + 2 may still be in flight)
         __syncthreads();
+        issue(sl + 3);
         zslice(sl + 1);
         __syncthreads();
         if (own) {
@@ -1883,6 +1890,7 @@ __global__ void __launch_bounds__(k3TX * k3TY) iso3d_kernel(StepArgs A, IsoCall 
             }
         }
     }
+    cp_async_wait<0>();
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const unsigned nblk = gridDim.x * gridDim.y;
     const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
@@ -2161,10 +2169,10 @@ void launch_lean(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuf
     else launch_lean_a<T, VEC, false>(sh, A, c, bf, s, variant);
 }
 
-// Dynamic shared memory of the 3D step: three staged slices and two of z.
+// Dynamic shared memory of the 3D step: k3Ring staged slices and two of z.
 template <class T, bool GAP>
 constexpr size_t iso3d_smem() {
-    return (size_t)3 * (GAP ? 7 : 4) * k3R * sizeof(T) + (size_t)2 * (GAP ? 2 : 1) * k3Z * sizeof(T);
+    return (size_t)k3Ring * (GAP ? 7 : 4) * k3R * sizeof(T) + (size_t)2 * (GAP ? 2 : 1) * k3Z * sizeof(T);
 }
 
 // The attribute is per function and device: set once, to the kernel's size.
