@@ -92,6 +92,8 @@ SIGNATURES = {
     "fp_version_string": (C.c_char_p, []),
     "fp_default_threads": (C.c_int, []),
     "fp_b200_workspace_stats": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "fp_b200_workspace_time_steps": (C.c_int, [_P, C.c_int]),
+    "fp_b200_workspace_step_times": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "fp_b200_release_cached": (None, []),
     "fp_b200_batch_create": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int, C.POINTER(_P)]),
     "fp_b200_batch_free": (None, [_P]),

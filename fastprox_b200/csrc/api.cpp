@@ -417,6 +417,8 @@ void free_ws_memory(fp_workspace *ws) {
     for (int i = 0; i < 2; ++i)
         if (ws->ev[i]) cudaEventDestroy(ws->ev[i]);
     ws->ev[0] = ws->ev[1] = nullptr;
+    for (cudaEvent_t e : ws->tev) cudaEventDestroy(e);
+    ws->tev.clear();
 }
 
 // The buffers of a workspace, laid out in one block (256-byte aligned
@@ -947,13 +949,33 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     int par = 0, slot = 0, inflight = 0;
     int64_t launched = 0, steps = 0, lists = 0, nimg = g.B;
     const int64_t cap = (int64_t)max_iter + 1 + 2 * chunk;
+    // step-launch timing: an event pair around each launch, up to kTimed launches
+    constexpr size_t kTimed = 4096;
+    std::vector<int> tkind;
+    for (int k = 0; k < 3; ++k) {
+        ws->tms[k] = 0.0;
+        ws->tcount[k] = 0;
+    }
     bool done = false;
     while (!done) {
         for (int j = 0; j < chunk; ++j) {
             const int pv = pairs ? iso_pair_at(launched, max_iter, ws->U2 != nullptr) : -1;
+            const bool timed = ws->time_steps && tkind.size() < kTimed;
+            if (timed) {
+                while (ws->tev.size() < 2 * (tkind.size() + 1)) {
+                    cudaEvent_t ev = nullptr;
+                    if ((e = cudaEventCreate(&ev)) != cudaSuccess) return cuda_status(e);
+                    ws->tev.push_back(ev);
+                }
+                if ((e = cudaEventRecord(ws->tev[2 * tkind.size()], s)) != cudaSuccess) return cuda_status(e);
+            }
             e = iso_step(ws->dtype, g, c, bf, ws->shape_, par, pv >= 0 ? pv : iso_variant(launched, max_iter, warm),
                          nimg, s);
             if (e != cudaSuccess) return cuda_status(e);
+            if (timed) {
+                if ((e = cudaEventRecord(ws->tev[2 * tkind.size() + 1], s)) != cudaSuccess) return cuda_status(e);
+                tkind.push_back(pv == kVariantPairGap ? 2 : (pv == kVariantPair ? 1 : 0));
+            }
             par ^= 1;
             launched += pv >= 0 ? 2 : 1;
             ++steps;
@@ -983,6 +1005,16 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     }
     ws->launches = steps;
     ws->kernel_launches += steps + lists + 3 + (warm ? 1 : 0) + 1 + ((c.na == 1 && !c.has_alpha) ? 1 : 0);
+    if (!tkind.empty()) {
+        if ((e = cudaEventSynchronize(ws->tev[2 * tkind.size() - 1])) != cudaSuccess) return cuda_status(e);
+        for (size_t k = 0; k < tkind.size(); ++k) {
+            float ms = 0.0f;
+            if ((e = cudaEventElapsedTime(&ms, ws->tev[2 * k], ws->tev[2 * k + 1])) != cudaSuccess)
+                return cuda_status(e);
+            ws->tms[tkind[k]] += ms;
+            ws->tcount[tkind[k]] += 1;
+        }
+    }
     e = iso_finalize(ws->dtype, g, c, bf, zdst, s);
     return cuda_status(e);
 }
@@ -2370,6 +2402,19 @@ FP_API fp_status fp_b200_workspace_stats(const fp_workspace *ws, int64_t *kernel
     if (!ws || !ws->info_valid) return FP_EINVAL;
     if (kernel_launches) *kernel_launches = ws->kernel_launches;
     if (step_launches) *step_launches = ws->launches;
+    return FP_OK;
+}
+
+FP_API fp_status fp_b200_workspace_time_steps(fp_workspace *ws, int on) {
+    if (!ws) return FP_EINVAL;
+    ws->time_steps = on != 0;
+    return FP_OK;
+}
+
+FP_API fp_status fp_b200_workspace_step_times(const fp_workspace *ws, int kind, double *ms, int64_t *launches) {
+    if (!ws || kind < 0 || kind > 2) return FP_EINVAL;
+    if (ms) *ms = ws->tms[kind];
+    if (launches) *launches = ws->tcount[kind];
     return FP_OK;
 }
 

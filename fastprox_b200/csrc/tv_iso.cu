@@ -2113,7 +2113,8 @@ void launch_lean_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoB
 }
 
 // Two iterations per launch: blocks of whole rows (the first iteration's
-// halo is 4 rows).
+// halo is 4 rows) with the lean step's threads per block (the same warps, so
+// the same per-row sums).
 // The pair kernels' ring passes 48 KB in float64: their attribute, once per device.
 template <class T>
 void pair_attr() {
@@ -2140,7 +2141,6 @@ void launch_pair(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuf
         const int r = v ? std::atoi(v) : 0;
         return (r >= 8 && r <= kLeanRowsMax) ? r : 0;
     }();
-    (void)sh;
     const int64_t H = A.g.L[0];
     // 12 rows per block: on 64 x 512^2 836 images/s, against 815 at 8 and 822 at 16
     // (shorter blocks spread better, longer ones recompute less of the halo);
@@ -2152,11 +2152,11 @@ void launch_pair(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuf
     const dim3 grid(1, (unsigned)((H + rows - 1) / rows), (unsigned)A.nimg);
     pair_attr<T>();
     if (gap) {
-        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, true>, grid, 128, pair_ring_bytes<T, true>(), s, A, c, bf);
-        else launch_step(iso2d_pair_kernel<T, false, true>, grid, 128, pair_ring_bytes<T, false>(), s, A, c, bf);
+        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, true>, grid, (unsigned)sh.bx, pair_ring_bytes<T, true>(), s, A, c, bf);
+        else launch_step(iso2d_pair_kernel<T, false, true>, grid, (unsigned)sh.bx, pair_ring_bytes<T, false>(), s, A, c, bf);
     } else {
-        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, false>, grid, 128, pair_ring_bytes<T, true>(), s, A, c, bf);
-        else launch_step(iso2d_pair_kernel<T, false, false>, grid, 128, pair_ring_bytes<T, false>(), s, A, c, bf);
+        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, false>, grid, (unsigned)sh.bx, pair_ring_bytes<T, true>(), s, A, c, bf);
+        else launch_step(iso2d_pair_kernel<T, false, false>, grid, (unsigned)sh.bx, pair_ring_bytes<T, false>(), s, A, c, bf);
     }
 }
 
@@ -2391,7 +2391,7 @@ bool iso_pair_ok(const Geometry &g, const StepShape &sh, int max_part) {
         const char *v = std::getenv("FASTPROX_B200_PAIRS");
         return !(v && v[0] == '0' && v[1] == 0);
     }();
-    return on && g.k == 2 && sh.kind == 4 && sh.vec == 4 && sh.bx == 128 && sh.gx == 1 && g.L[1] <= kPairCols &&
+    return on && g.k == 2 && sh.kind == 4 && sh.vec == 4 && sh.bx <= 128 && sh.gx == 1 && g.L[1] <= kPairCols &&
            g.L[0] >= 2 && g.L[0] <= max_part;
 }
 

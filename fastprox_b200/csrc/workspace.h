@@ -91,6 +91,13 @@ struct fp_workspace {
     int chunk = 8;
     int64_t launches = 0;         // step launches of the last call
     int64_t kernel_launches = 0;  // all kernels of the last call
+    // step-launch timing (fp_b200_workspace_time_steps): an event pair around
+    // each step launch of a call, created on first use; device milliseconds and
+    // launches of the last call by kind (0 single, 1 pair, 2 pair with the check)
+    bool time_steps = false;
+    std::vector<cudaEvent_t> tev;
+    double tms[3] = {0.0, 0.0, 0.0};
+    int64_t tcount[3] = {0, 0, 0};
     // results of the last call
     std::vector<double> gaps, zerrs;
     std::vector<int> iters;

@@ -243,6 +243,16 @@ FP_API int         fp_default_threads(void);
 FP_API fp_status fp_b200_workspace_stats(const fp_workspace *ws, int64_t *kernel_launches,
                                          int64_t *step_launches);
 
+/* Device time of the isotropic step launches of the next prox calls on ws:
+ * with on = 1, each step launch of a call is bracketed by a pair of events on
+ * the workspace's stream (up to 4096 launches per call), which serialises the
+ * launches and adds a little to the call. fp_b200_workspace_step_times then
+ * gives the last call's total milliseconds and launches of one kind: 0 single
+ * iterations, 1 two iterations per launch, 2 two iterations the second of
+ * which carries the gap check. For benchmarks. */
+FP_API fp_status fp_b200_workspace_time_steps(fp_workspace *ws, int on);
+FP_API fp_status fp_b200_workspace_step_times(const fp_workspace *ws, int kind, double *ms, int64_t *launches);
+
 /* Workspaces take their device memory from a stream-ordered pool per device
  * and their pinned host memory from a cache, so creating and freeing one
  * (once per call when fp_prox gets ws = NULL) never synchronises the whole

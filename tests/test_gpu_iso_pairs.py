@@ -73,3 +73,32 @@ if __name__ == "__main__":  # the single-step run (FASTPROX_B200_PAIRS=0 in the 
         z, iters, gaps = _run(i)
         res[f"z{i}"], res[f"it{i}"], res[f"g{i}"] = z, iters, gaps
     np.savez(sys.argv[1], **res)
+
+
+@pytest.mark.gpu
+def test_step_timing_counts_launch_kinds(cuda):
+    """fp_b200_workspace_time_steps: 12 iterations of a batch that never
+    converges run as a cold single step, pairs at iterations 1, 5, 9, pairs
+    with the check at 3 and 7, and single steps from 11 on."""
+    import ctypes as C
+
+    import torch
+    from fastprox_b200 import TVIso, capi, synth
+    L = capi.lib()
+    x = torch.as_tensor(synth.phantom(4, 64, 128, seed=90), device=cuda)
+    op = TVIso(2)
+    ws = op.workspace(x)
+    capi.check(L.fp_b200_workspace_time_steps(ws, 1), "time_steps")
+    op.solve(x, 0.1, tol=0.0, max_iter=12, with_dual=False)
+    ms, n = C.c_double(), C.c_int64()
+    got = []
+    for kind in range(3):
+        capi.check(L.fp_b200_workspace_step_times(ws, kind, C.byref(ms), C.byref(n)), "step_times")
+        got.append((n.value, ms.value))
+    assert got[1][0] == 3 and got[2][0] == 2 and got[0][0] >= 3, got
+    assert all(t > 0.0 for _, t in got), got
+    capi.check(L.fp_b200_workspace_time_steps(ws, 0), "time_steps")
+    op.solve(x, 0.1, tol=0.0, max_iter=12, with_dual=False)
+    capi.check(L.fp_b200_workspace_step_times(ws, 2, C.byref(ms), C.byref(n)), "step_times")
+    assert n.value == 0
+    assert L.fp_b200_workspace_step_times(ws, 3, None, None) == capi.FP_EINVAL
