@@ -875,19 +875,26 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // The pair kernel's row ring: three rows of each thread's inputs (d, v0, v1,
-// u0, u1, alpha: VEC entries each; v1 of the column before, and lane 31's d,
-// v0, v1 of the column after), in flight up to three rows ahead.
+// u0, u1, alpha: VEC entries each; v1 of the column before, lane 31's d, v0,
+// v1 of the column after, and the halo columns' entries of a block's edge
+// threads), in flight up to three rows ahead. Ten scalars per thread with the
+// halo columns, four without (a smaller ring leaves more of the SM's shared
+// storage to the L1 cache: 1% on 64 x 512^2).
 constexpr int kPairRing = 3;
-template <class T, bool ALPHA>
-constexpr size_t pair_slot_bytes() {
-    return (size_t)128 * ((ALPHA ? 6 : 5) * 4 * sizeof(T) + 4 * sizeof(T));
+template <bool WIDE>
+constexpr int pair_scalars() {
+    return WIDE ? 10 : 4;
 }
-template <class T, bool ALPHA>
+template <class T, bool ALPHA, bool WIDE>
+constexpr size_t pair_slot_bytes() {
+    return (size_t)128 * ((ALPHA ? 6 : 5) * 4 * sizeof(T) + pair_scalars<WIDE>() * sizeof(T));
+}
+template <class T, bool ALPHA, bool WIDE>
 constexpr size_t pair_ring_bytes() {
-    return kPairRing * pair_slot_bytes<T, ALPHA>();
+    return kPairRing * pair_slot_bytes<T, ALPHA, WIDE>();
 }
 
-template <class T, bool ALPHA, bool GAP2>
+template <class T, bool ALPHA, bool GAP2, bool WIDE>
 __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     constexpr int VEC = 4;
     // what warps pass on per row (two rows in flight): a warp's first column
@@ -895,6 +902,9 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
     // (u1') to the warp on its right
     __shared__ T xf[2][4][5];
     __shared__ T xl[2][4][2];
+    // the edge threads' halo column (rows wider than a block): v0, v1, u0, u1,
+    // alpha, z and, for the column after the block, v0 and z one further right
+    __shared__ T hst[2][8];
     __shared__ double rowp[GAP2 ? kLeanRowsMax * 8 : 1];
     __shared__ double sh[32];
     __shared__ int flag;
@@ -929,9 +939,17 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
     const T beta2 = (T)((st.tn - 1.0) / tn2);
 
     const int lane = threadIdx.x & 31;
-    const int cb = (int)threadIdx.x * VEC;
+    const int c0 = WIDE ? (int)blockIdx.x * kPairCols : 0;  // the block's first column
+    const int cb = c0 + (int)threadIdx.x * VEC;
     const bool colok = cb < W;
     const bool ext = lane == 31 && cb + VEC < W;  // the next warp's first column (first iteration)
+    // Rows wider than a block: the first iteration also runs on the column
+    // before the block (thread 0: its v1', u1' are the left neighbours of the
+    // second iteration's first column) and the column after it (the last
+    // thread: its v', u' give z(v'), z(u') of the second iteration's right
+    // neighbour), with the arithmetic of the blocks that own those columns.
+    const bool lext = WIDE && threadIdx.x == 0 && c0 > 0;
+    const bool rext = WIDE && threadIdx.x == blockDim.x - 1 && cb + VEC < W;
     const int r0 = blockIdx.y * A.rows;
     const int r1 = min(H, r0 + A.rows);
     const int s0 = r0 > 0 ? r0 - 1 : 0;       // rows of the first iteration: s0 .. s1
@@ -964,12 +982,12 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
     constexpr int AB = VEC * (int)sizeof(T);  // bytes of one array's entries per thread
     const unsigned tid = threadIdx.x;
     auto slot_arr = [&](int r, int a) -> T * {
-        return reinterpret_cast<T *>(pair_ring + (size_t)(r % kPairRing) * pair_slot_bytes<T, ALPHA>() +
+        return reinterpret_cast<T *>(pair_ring + (size_t)(r % kPairRing) * pair_slot_bytes<T, ALPHA, WIDE>() +
                                      ((size_t)a * 128 + tid) * AB);
     };
     auto slot_sc = [&](int r, int q) -> T * {
-        return reinterpret_cast<T *>(pair_ring + (size_t)(r % kPairRing) * pair_slot_bytes<T, ALPHA>() +
-                                     (size_t)NARR * 128 * AB + ((size_t)tid * 4 + q) * sizeof(T));
+        return reinterpret_cast<T *>(pair_ring + (size_t)(r % kPairRing) * pair_slot_bytes<T, ALPHA, WIDE>() +
+                                     (size_t)NARR * 128 * AB + ((size_t)tid * pair_scalars<WIDE>() + q) * sizeof(T));
     };
     auto issue = [&](int r) {  // one commit group per row, empty past the rows this block reads
         if (r <= s1 + 1 && r < H && colok) {
@@ -985,6 +1003,22 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
                 cp_async_small<sizeof(T)>(slot_sc(r, 1), D + o + VEC);
                 cp_async_small<sizeof(T)>(slot_sc(r, 2), V0 + o + VEC);
                 cp_async_small<sizeof(T)>(slot_sc(r, 3), V1 + o + VEC);
+            }
+            if (lext) {  // column c0 - 1 (v1 there is entry 0), and v1 of c0 - 2
+                cp_async_small<sizeof(T)>(slot_sc(r, 4), D + o - 1);
+                cp_async_small<sizeof(T)>(slot_sc(r, 5), V0 + o - 1);
+                cp_async_small<sizeof(T)>(slot_sc(r, 6), U0 + o - 1);
+                cp_async_small<sizeof(T)>(slot_sc(r, 7), U1 + o - 1);
+                if (ALPHA) cp_async_small<sizeof(T)>(slot_sc(r, 8), AL + o - 1);
+                cp_async_small<sizeof(T)>(slot_sc(r, 9), V1 + o - 2);
+            }
+            if (rext) {  // column c0 + 512 (d, v0, v1 there are entries 1-3), and c0 + 513
+                cp_async_small<sizeof(T)>(slot_sc(r, 4), U0 + o + VEC);
+                cp_async_small<sizeof(T)>(slot_sc(r, 5), U1 + o + VEC);
+                if (ALPHA) cp_async_small<sizeof(T)>(slot_sc(r, 6), AL + o + VEC);
+                cp_async_small<sizeof(T)>(slot_sc(r, 7), D + o + VEC + 1);
+                cp_async_small<sizeof(T)>(slot_sc(r, 8), V0 + o + VEC + 1);
+                cp_async_small<sizeof(T)>(slot_sc(r, 9), V1 + o + VEC + 1);
             }
         }
         cp_async_commit();
@@ -1015,12 +1049,39 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
 #pragma unroll
         for (int j = 0; j < VEC; ++j) v0p[j] = T(0);
     zrow(dc, v0c, v0p, v1c, (colok && cb > 0) ? V1[off - 1] : T(0), zc);
-    T x_v0 = T(0), x_z = T(0);
+    T x_v0 = T(0), x_z = T(0), x_d = T(0), x_v1 = T(0);
     if (ext) {
-        const T dx = D[off + VEC];
+        x_d = D[off + VEC];
         x_v0 = V0[off + VEC];
+        x_v1 = V1[off + VEC];
         const T pv = s0 > 0 ? V0[off + VEC - W] : T(0);
-        x_z = dx + wh0 * (x_v0 - pv) + wh1 * (V1[off + VEC] - v1c[VEC - 1]);
+        x_z = x_d + wh0 * (x_v0 - pv) + wh1 * (x_v1 - v1c[VEC - 1]);
+    }
+    // the halo column's row s0 (in shared memory: two threads use it)
+    if (lext) {
+        const int o = off - 1;
+        T *hs = hst[0];
+        hs[0] = V0[o];
+        hs[1] = V1[o];
+        hs[2] = U0[o];
+        hs[3] = U1[o];
+        hs[4] = ALPHA ? AL[o] : T(0);
+        const T pv = s0 > 0 ? V0[o - W] : T(0);
+        hs[5] = D[o] + wh0 * (hs[0] - pv) + wh1 * (hs[1] - V1[o - 1]);
+        hs[6] = hs[7] = T(0);
+    }
+    if (rext) {
+        const int o = off + VEC;
+        T *hs = hst[1];
+        hs[0] = x_v0;
+        hs[1] = x_v1;
+        hs[2] = U0[o];
+        hs[3] = U1[o];
+        hs[4] = ALPHA ? AL[o] : T(0);
+        hs[5] = x_z;
+        hs[6] = V0[o + 1];
+        const T pv = s0 > 0 ? V0[o + 1 - W] : T(0);
+        hs[7] = D[o + 1] + wh0 * (hs[6] - pv) + wh1 * (V1[o + 1] - x_v1);
     }
     // the second iteration's inputs on the row above: v', u', alpha, and z(v'),
     // z(u') on five columns (the last the right neighbour's first)
@@ -1087,7 +1148,7 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
         const bool hasn = i + 1 < H;
         const int offn = off + W;
         T dn[VEC], v0n[VEC], v1n[VEC], u0n[VEC], u1n[VEC], zn[VEC], al[VEC];
-        T nx_v0 = T(0), nx_z = T(0);
+        T nx_v0 = T(0), nx_z = T(0), nx_d = T(0), nx_v1 = T(0);
 #pragma unroll
         for (int j = 0; j < VEC; ++j) al[j] = aln[j];
         cp_async_wait<1>();  // row i + 1 is in (row i + 2 may still be in flight)
@@ -1100,13 +1161,58 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
             if (ALPHA) rd(i + 1, 5, aln);
             zrow(dn, v0n, v0c, v1n, (colok && cb > 0) ? *slot_sc(i + 1, 0) : T(0), zn);
             if (ext) {
-                const T dx = *slot_sc(i + 1, 1);
+                nx_d = *slot_sc(i + 1, 1);
                 nx_v0 = *slot_sc(i + 1, 2);
-                nx_z = dx + wh0 * (nx_v0 - x_v0) + wh1 * (*slot_sc(i + 1, 3) - v1n[VEC - 1]);
+                nx_v1 = *slot_sc(i + 1, 3);
+                nx_z = nx_d + wh0 * (nx_v0 - x_v0) + wh1 * (nx_v1 - v1n[VEC - 1]);
             }
         } else {
 #pragma unroll
             for (int j = 0; j < VEC; ++j) zn[j] = u0n[j] = u1n[j] = v0n[j] = v1n[j] = dn[j] = T(0);
+        }
+        // the first iteration on row i at the halo column, as its owner computes it
+        T hun0 = T(0), hun1 = T(0), hvo0 = T(0), hvo1 = T(0);
+        if (lext || rext) {
+            T *hs = hst[lext ? 0 : 1];  // row i
+            T n[8] = {T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0)};  // row i + 1
+            if (hasn && lext) {  // column c0 - 1
+                n[0] = *slot_sc(i + 1, 5);
+                n[1] = *slot_sc(i + 1, 0);
+                n[2] = *slot_sc(i + 1, 6);
+                n[3] = *slot_sc(i + 1, 7);
+                if (ALPHA) n[4] = *slot_sc(i + 1, 8);
+                n[5] = *slot_sc(i + 1, 4) + wh0 * (n[0] - hs[0]) + wh1 * (n[1] - *slot_sc(i + 1, 9));
+            }
+            if (hasn && rext) {  // column c0 + 512, and v0, z at c0 + 513
+                n[0] = nx_v0;
+                n[1] = nx_v1;
+                n[2] = *slot_sc(i + 1, 4);
+                n[3] = *slot_sc(i + 1, 5);
+                if (ALPHA) n[4] = *slot_sc(i + 1, 6);
+                n[5] = nx_z;
+                n[6] = *slot_sc(i + 1, 8);
+                n[7] = *slot_sc(i + 1, 7) + wh0 * (n[6] - hs[6]) + wh1 * (*slot_sc(i + 1, 9) - nx_v1);
+            }
+            // z there, below it and to its right (this thread's first column
+            // for c0 - 1, column c0 + 513 for c0 + 512)
+            const T zh = hs[5], zhn = n[5], zhr = lext ? zc[0] : hs[7];
+            const T g0 = hasn ? wh0 * (zhn - zh) : T(0);
+            const T g1 = wh1 * (zhr - zh);
+            const T cv0 = hs[0] + tau * g0;
+            const T cv1 = hs[1] + tau * g1;
+            const T nn = cv0 * cv0 + cv1 * cv1;
+            T rp = rad;
+            if (ALPHA) {
+                const T r = rad * hs[4];
+                rp = hs[4] == T(0) ? T(0) : (r <= bnd ? r : bnd);
+            }
+            const T sc = nn > rp * rp ? rp * rsqrt_t(nn) : T(1);
+            hun0 = cv0 * sc;
+            hun1 = cv1 * sc;
+            hvo0 = hun0 + beta1 * (hun0 - hs[2]);
+            hvo1 = hun1 + beta1 * (hun1 - hs[3]);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) hs[q] = n[q];
         }
         issue(i + 3);  // into the slot of row i, read at the last step
         T zr = __shfl_down_sync(0xffffffffu, zc[0], 1);
@@ -1154,12 +1260,18 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
         T lv1 = __shfl_up_sync(0xffffffffu, vo1[VEC - 1], 1);
         T lu1 = GAP2 ? __shfl_up_sync(0xffffffffu, un1[VEC - 1], 1) : T(0);
         if (lane == 0) {
-            lv1 = w > 0 ? xl[i & 1][w - 1][0] : T(0);
-            if (GAP2) lu1 = w > 0 ? xl[i & 1][w - 1][1] : T(0);
+            lv1 = w > 0 ? xl[i & 1][w - 1][0] : (lext ? hvo1 : T(0));
+            if (GAP2) lu1 = w > 0 ? xl[i & 1][w - 1][1] : (lext ? hun1 : T(0));
         }
         const bool hasx = lane == 31 && colok && cb + VEC < W;
         T nd = T(0), nv0 = T(0), nv1 = T(0), nu0 = T(0), nu1 = T(0);
-        if (hasx) {
+        if (rext) {
+            nd = x_d;
+            nv0 = hvo0;
+            nv1 = hvo1;
+            nu0 = hun0;
+            nu1 = hun1;
+        } else if (hasx) {
             nd = xf[i & 1][w + 1][0];
             nv0 = xf[i & 1][w + 1][1];
             nv1 = xf[i & 1][w + 1][2];
@@ -1210,6 +1322,8 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
         }
         x_v0 = nx_v0;
         x_z = nx_z;
+        x_d = nx_d;
+        x_v1 = nx_v1;
         off = offn;
     }
     cp_async_wait<0>();
@@ -1231,14 +1345,16 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
                 gv += rowp[threadIdx.x * 8 + 2 * w];
                 dv += rowp[threadIdx.x * 8 + 2 * w + 1];
             }
-            const int64_t slot = r0 + (int)threadIdx.x;
+            const int64_t slot = WIDE ? (int64_t)(r0 + (int)threadIdx.x) * gridDim.x + blockIdx.x
+                                      : (int64_t)(r0 + (int)threadIdx.x);
             part[slot * 2 + 0] = gv;
             part[slot * 2 + 1] = dv;
         }
     }
     if (!arrive_last(bf.ticket + b, gridDim.x * gridDim.y, &flag)) return;
-    const double gap = GAP2 ? sum_partials(part, H, 2, 0, sh) : 0.0;
-    const double dot = GAP2 ? sum_partials(part, H, 2, 1, sh) : 0.0;
+    const int nslot = H * (int)gridDim.x;
+    const double gap = GAP2 ? sum_partials(part, nslot, 2, 0, sh) : 0.0;
+    const double dot = GAP2 ? sum_partials(part, nslot, 2, 1, sh) : 0.0;
     if (threadIdx.x != 0) return;
     bf.ticket[b] = 0;
     IsoState s2 = st;
@@ -2116,22 +2232,29 @@ void launch_lean_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoB
 // halo is 4 rows) with the lean step's threads per block (the same warps, so
 // the same per-row sums).
 // The pair kernels' ring passes 48 KB in float64: their attribute, once per device.
-template <class T>
-void pair_attr() {
-    static std::atomic<unsigned long long> done{0};
+template <class T, bool ALPHA, bool GAP2, bool WIDE>
+void launch_pair_k(dim3 grid, unsigned bx, cudaStream_t s, const StepArgs &A, const IsoCall &c,
+                   const IsoBuffers &bf) {
+    static std::atomic<unsigned long long> done{0};  // the attribute is per function and device
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
-    const unsigned long long bit = 1ull << dev;
-    if (done.load() & bit) return;
-    cudaFuncSetAttribute(iso2d_pair_kernel<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)pair_ring_bytes<T, true>());
-    cudaFuncSetAttribute(iso2d_pair_kernel<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)pair_ring_bytes<T, false>());
-    cudaFuncSetAttribute(iso2d_pair_kernel<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)pair_ring_bytes<T, true>());
-    cudaFuncSetAttribute(iso2d_pair_kernel<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)pair_ring_bytes<T, false>());
-    done.fetch_or(bit);
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && !(done.load() & (1ull << dev))) {
+        cudaFuncSetAttribute(iso2d_pair_kernel<T, ALPHA, GAP2, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)pair_ring_bytes<T, ALPHA, WIDE>());
+        done.fetch_or(1ull << dev);
+    }
+    launch_step(iso2d_pair_kernel<T, ALPHA, GAP2, WIDE>, grid, bx, pair_ring_bytes<T, ALPHA, WIDE>(), s, A, c, bf);
+}
+
+template <class T, bool WIDE>
+void launch_pair_w(dim3 grid, unsigned bx, cudaStream_t s, const StepArgs &A, const IsoCall &c, const IsoBuffers &bf,
+                   bool gap) {
+    if (gap) {
+        if (c.has_alpha) launch_pair_k<T, true, true, WIDE>(grid, bx, s, A, c, bf);
+        else launch_pair_k<T, false, true, WIDE>(grid, bx, s, A, c, bf);
+    } else {
+        if (c.has_alpha) launch_pair_k<T, true, false, WIDE>(grid, bx, s, A, c, bf);
+        else launch_pair_k<T, false, false, WIDE>(grid, bx, s, A, c, bf);
+    }
 }
 
 template <class T>
@@ -2147,17 +2270,13 @@ void launch_pair(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuf
     // fewer, down to 4, while the launch has too few blocks to spread (the
     // tail of a batch, a few images live)
     int rows = rows_hint ? rows_hint : 12;
-    while (!rows_hint && rows > 4 && A.nimg * ((H + rows - 1) / rows) < tail_blocks()) rows = rows / 2 > 4 ? rows / 2 : 4;
+    while (!rows_hint && rows > 4 && A.nimg * sh.gx * ((H + rows - 1) / rows) < tail_blocks())
+        rows = rows / 2 > 4 ? rows / 2 : 4;
     A.rows = rows;
-    const dim3 grid(1, (unsigned)((H + rows - 1) / rows), (unsigned)A.nimg);
-    pair_attr<T>();
-    if (gap) {
-        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, true>, grid, (unsigned)sh.bx, pair_ring_bytes<T, true>(), s, A, c, bf);
-        else launch_step(iso2d_pair_kernel<T, false, true>, grid, (unsigned)sh.bx, pair_ring_bytes<T, false>(), s, A, c, bf);
-    } else {
-        if (c.has_alpha) launch_step(iso2d_pair_kernel<T, true, false>, grid, (unsigned)sh.bx, pair_ring_bytes<T, true>(), s, A, c, bf);
-        else launch_step(iso2d_pair_kernel<T, false, false>, grid, (unsigned)sh.bx, pair_ring_bytes<T, false>(), s, A, c, bf);
-    }
+    const dim3 grid((unsigned)sh.gx, (unsigned)((H + rows - 1) / rows), (unsigned)A.nimg);
+    // rows wider than a block: the kernel with the halo columns of the first iteration
+    if (sh.gx > 1) launch_pair_w<T, true>(grid, (unsigned)sh.bx, s, A, c, bf, gap);
+    else launch_pair_w<T, false>(grid, (unsigned)sh.bx, s, A, c, bf, gap);
 }
 
 template <class T, int VEC>
@@ -2391,8 +2510,9 @@ bool iso_pair_ok(const Geometry &g, const StepShape &sh, int max_part) {
         const char *v = std::getenv("FASTPROX_B200_PAIRS");
         return !(v && v[0] == '0' && v[1] == 0);
     }();
-    return on && g.k == 2 && sh.kind == 4 && sh.vec == 4 && sh.bx <= 128 && sh.gx == 1 && g.L[1] <= kPairCols &&
-           g.L[0] >= 2 && g.L[0] <= max_part;
+    // one block per row up to 512 columns (the lean step's threads), else blocks of 512 columns
+    return on && g.k == 2 && sh.kind == 4 && sh.vec == 4 && (sh.gx == 1 ? g.L[1] <= kPairCols : sh.bx == 128) &&
+           g.L[0] >= 2 && g.L[0] * sh.gx <= max_part;
 }
 
 cudaError_t iso_live_list(const IsoState *st, int64_t B, int *lmap, int *lcnt, cudaStream_t s) {

@@ -4,7 +4,9 @@ second) against the same iterations one launch each: the same arithmetic per
 iteration and the same order of every sum, so the same iterates, iteration
 counts and gaps, bit for bit. Covers images with and without pixel weights,
 heights that leave blocks of 4 to 12 rows and a last block shorter than the
-rest, images of two and three rows, widths below the block's 512 columns,
+rest, images of two and three rows, widths below the block's 512 columns, widths
+above it (several column blocks; the edge threads recompute the neighbouring
+block's first iteration on the column either side, ragged last block included),
 per-image steps (images that stop at different iterations), warm starts, and
 max_iter values that end inside a pair. The float64 cases run single steps
 either way (the float64 lean shape has 2-wide vectors; pairs need 4) and check
@@ -30,6 +32,9 @@ CASES = [  # (dtype, B, H, W, alpha, tol, max_iter, warm)
     (np.float64, 2, 96, 128, False, 1e-8, 3000, True),
     (np.float32, 3, 2, 40, True, 1e-7, 300, False),
     (np.float32, 2, 3, 36, False, 0.0, 9, False),
+    (np.float32, 2, 40, 1024, True, 1e-7, 400, False),
+    (np.float32, 2, 33, 640, False, 0.0, 9, False),
+    (np.float32, 2, 29, 1540, True, 1e-6, 300, True),
 ]
 
 
