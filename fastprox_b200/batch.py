@@ -64,7 +64,8 @@ class RaggedBatch:
 
     def run(self, steps=8, max_chunks=0):
         """Iterates until some images finish (or, with max_chunks > 0, at most
-        that many chunks of `steps` iterations); returns
+        that many chunks of `steps` steps; a step advances each live image by
+        one iteration, or by four where the pair variants take it); returns
         [(slot, z, gap, iters, converged)]."""
         nf, nl = C.c_int(0), C.c_int(0)
         capi.check(capi.lib().fp_b200_batch_run(self._h, int(steps), int(max_chunks),

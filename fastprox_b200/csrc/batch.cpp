@@ -8,7 +8,9 @@
 // of pixel ranges on the host places them), per-slot constants and state,
 // partial sums and tickets, and two work lists of (image, tile) items, one
 // for rows of a multiple of 4 pixels (16-byte vectors) and one for the rest.
-// A step launches the three kernel variants over each list; chunks of steps
+// A step launches the three kernel variants over each list, and on the
+// 4-wide float list the two pair variants (two iterations per launch, with a
+// third dual buffer for u' of the checked pair); chunks of steps
 // are replayed as CUDA graphs, captured again only when the work lists
 // outgrow their current size class.
 #include <cuda_runtime_api.h>
@@ -66,6 +68,7 @@ struct fp_b200_batch {
     int max_part = 4096;
     // device
     void *d = nullptr, *U[2] = {nullptr, nullptr}, *V[2] = {nullptr, nullptr}, *dual = nullptr;
+    void *U2 = nullptr;  // u' of the pair variants with the check (float)
     IsoImage *img = nullptr;
     IsoState *st = nullptr;
     double *gammas = nullptr, *part = nullptr;
@@ -160,6 +163,7 @@ IsoBuffers buffers(fp_b200_batch *bt) {
         bf.U[i] = bt->U[i];
         bf.V[i] = bt->V[i];
     }
+    bf.U[2] = bt->U2;
     bf.dual = bt->dual;
     bf.alpha = nullptr;
     bf.img = bt->img;
@@ -183,6 +187,7 @@ IsoBuffers slot_buffers(fp_b200_batch *bt, int slot) {
         bf.U[i] = static_cast<char *>(bt->U[i]) + 2 * (size_t)s.off * T;
         bf.V[i] = static_cast<char *>(bt->V[i]) + 2 * (size_t)s.off * T;
     }
+    if (bt->U2) bf.U[2] = static_cast<char *>(bt->U2) + 2 * (size_t)s.off * T;
     bf.dual = static_cast<char *>(bt->dual) + 2 * (size_t)s.off * T;
     bf.img = bt->img + slot;
     bf.st = bt->st + slot;
@@ -276,6 +281,15 @@ cudaError_t launch_steps(fp_b200_batch *bt, int steps) {
     return cudaSuccess;
 }
 
+// kernels one step launches: three variants per non-empty list, two more
+// (the pair variants) on the 4-wide float list
+int launches_per_step(const fp_b200_batch *bt) {
+    int n = 0;
+    if (bt->grid[0] > 0) n += 3 + (bt->U2 && iso_ragged_pairs(bt->dtype, 4) ? 2 : 0);
+    if (bt->grid[1] > 0) n += 3;
+    return n;
+}
+
 void trace(const char *what, cudaError_t e) {
     if (e != cudaSuccess && std::getenv("FASTPROX_B200_DEBUG"))
         std::fprintf(stderr, "fastprox_b200 batch: %s: %s\n", what, cudaGetErrorString(e));
@@ -361,6 +375,7 @@ FP_API fp_status fp_b200_batch_create(const fp_op *op, int64_t max_images, int64
             A(&bt->V[i], 2 * P * T);
         }
         A(&bt->dual, 2 * P * T);
+        if (iso_ragged_pairs(dtype, 4)) A(&bt->U2, 2 * P * T);
         A((void **)&bt->img, S * sizeof(IsoImage));
         A((void **)&bt->st, S * sizeof(IsoState));
         A((void **)&bt->gammas, S * sizeof(double));
@@ -530,7 +545,7 @@ FP_API fp_status fp_b200_batch_run(fp_b200_batch *bt, int steps, int max_chunks,
             trace("run", e);
             if (e != cudaSuccess) return FP_EDEVICE;
             bt->steps_run += steps;
-            bt->kernel_launches += (int64_t)steps * 6;
+            bt->kernel_launches += (int64_t)steps * launches_per_step(bt);
             e = cudaMemcpyAsync(bt->h_st, bt->st, S * sizeof(IsoState), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaMemcpyAsync(bt->h_live, bt->live, sizeof(int), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);

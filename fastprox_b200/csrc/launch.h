@@ -84,6 +84,10 @@ cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const I
 // of `vec` (items[0 .. *n_items), grid >= *n_items blocks).
 cudaError_t iso_ragged_step(int dtype, int vec, const RagItem *items, const int *n_items, int grid,
                             const RagSlot *slots, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s);
+// Whether the ragged step on a list of `vec`-wide rows adds the two pair
+// variants (float, 4-wide rows, pairs not switched off); they need bf.U[2].
+bool iso_ragged_pairs(int dtype, int vec);
+bool pairs_enabled();
 
 // Fills gammas[i] = v for i < n.
 cudaError_t fill_double(double *dst, double v, int64_t n, cudaStream_t s);

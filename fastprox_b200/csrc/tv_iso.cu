@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <type_traits>
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
@@ -894,8 +895,23 @@ constexpr size_t pair_ring_bytes() {
     return kPairRing * pair_slot_bytes<T, ALPHA, WIDE>();
 }
 
-template <class T, bool ALPHA, bool GAP2, bool WIDE>
-__global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+// What one pair pass needs: an image's arrays, the block's rows [r0, r1) and
+// first column c0, the step's constants and the momenta of both iterations.
+template <class T>
+struct PairTile {
+    const T *D, *U0, *V0, *AL;
+    T *UO0, *VO0, *UM0;
+    int64_t N;
+    int H, W, r0, r1, c0;
+    T wh0, wh1, tau, rad, bnd, beta1, beta2;
+};
+
+// Both iterations of a pair launch over one block's rows. ROWSUMS: the second
+// iteration's gap and restart-test sums per row and warp into rowp (the
+// batched launch's per-row slots); else kept per thread in gap_acc, dot_acc
+// over the block's rows (the ragged step's per-tile slot).
+template <class T, bool ALPHA, bool GAP2, bool WIDE, bool ROWSUMS>
+__device__ __forceinline__ void pair_pass(const PairTile<T> &p, double *rowp, double &gap_acc, double &dot_acc) {
     constexpr int VEC = 4;
     // what warps pass on per row (two rows in flight): a warp's first column
     // (d, v0', v1', u0', u1') to the warp on its left, its last column's v1'
@@ -905,41 +921,17 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
     // the edge threads' halo column (rows wider than a block): v0, v1, u0, u1,
     // alpha, z and, for the column after the block, v0 and z one further right
     __shared__ T hst[2][8];
-    __shared__ double rowp[GAP2 ? kLeanRowsMax * 8 : 1];
-    __shared__ double sh[32];
-    __shared__ int flag;
     extern __shared__ __align__(16) unsigned char pair_ring[];
-    asm volatile("griddepcontrol.wait;" ::: "memory");  // a programmatic dependent of the previous step
-    const int b = step_image(bf, blockIdx.z);
-    if (b < 0) return;
-    const IsoState st = bf.st[b];
-    if (st.status != kLive) return;
-    const int it = st.it;
-    if (it <= 0 || (it & 3) != (GAP2 ? 3 : 1) || it + 1 >= A.max_iter || st.zero_in || (GAP2 && !bf.U[2])) {
-        if (threadIdx.x == 0) atomicExch(bf.err, 3);
-        return;
-    }
-    const IsoImage im = bf.img[b];
-    const int H = (int)A.g.L[0], W = (int)A.g.L[1];
-    const int64_t N = A.g.N;
-    const int pin = A.par, pout = A.par ^ 1;
-    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
-    const T *U0 = static_cast<const T *>(bf.U[pin]) + (int64_t)b * 2 * N;
-    const T *V0 = st.vsel ? U0 : static_cast<const T *>(bf.V[pin]) + (int64_t)b * 2 * N;
+    const int H = p.H, W = p.W;
+    const int64_t N = p.N;
+    const T *D = p.D, *U0 = p.U0, *V0 = p.V0, *AL = p.AL;
     const T *U1 = U0 + N, *V1 = V0 + N;
-    T *UO0 = static_cast<T *>(bf.U[pout]) + (int64_t)b * 2 * N;
-    T *VO0 = static_cast<T *>(bf.V[pout]) + (int64_t)b * 2 * N;
+    T *UO0 = p.UO0, *VO0 = p.VO0, *UM0 = p.UM0;
     T *UO1 = UO0 + N, *VO1 = VO0 + N;
-    T *UM0 = GAP2 ? static_cast<T *>(bf.U[2]) + (int64_t)b * 2 * N : nullptr;
-    const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
-    const T wh0 = (T)c.wh[0], wh1 = (T)c.wh[1], tau = (T)c.tau;
-    const T rad = (T)im.radius, bnd = (T)im.bound;
-    const T beta1 = (T)st.beta;
-    const double tn2 = fista_t(st.tn);
-    const T beta2 = (T)((st.tn - 1.0) / tn2);
+    const T wh0 = p.wh0, wh1 = p.wh1, tau = p.tau, rad = p.rad, bnd = p.bnd, beta1 = p.beta1, beta2 = p.beta2;
 
     const int lane = threadIdx.x & 31;
-    const int c0 = WIDE ? (int)blockIdx.x * kPairCols : 0;  // the block's first column
+    const int c0 = WIDE ? p.c0 : 0;  // the block's first column
     const int cb = c0 + (int)threadIdx.x * VEC;
     const bool colok = cb < W;
     const bool ext = lane == 31 && cb + VEC < W;  // the next warp's first column (first iteration)
@@ -950,8 +942,7 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
     // neighbour), with the arithmetic of the blocks that own those columns.
     const bool lext = WIDE && threadIdx.x == 0 && c0 > 0;
     const bool rext = WIDE && threadIdx.x == blockDim.x - 1 && cb + VEC < W;
-    const int r0 = blockIdx.y * A.rows;
-    const int r1 = min(H, r0 + A.rows);
+    const int r0 = p.r0, r1 = p.r1;
     const int s0 = r0 > 0 ? r0 - 1 : 0;       // rows of the first iteration: s0 .. s1
     const int s1 = r1 < H ? r1 : H - 1;
 
@@ -1090,7 +1081,6 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
     for (int j = 0; j < VEC; ++j) pv0[j] = pv1[j] = pu0[j] = pu1[j] = pal[j] = T(0);
 #pragma unroll
     for (int j = 0; j <= VEC; ++j) zp[j] = zup[j] = T(0);
-    double gap_acc = 0.0, dot_acc = 0.0;
     T xv0p = T(0), xu0p = T(0);  // lane 31: v0', u0' of the right neighbour's first column, row above
 
     // the second iteration on row j from z(v') (and z(u')) of rows j and j + 1
@@ -1127,7 +1117,7 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
             store_pack<T, VEC>(VO0 + o, vo0);
             store_pack<T, VEC>(VO1 + o, vo1);
         }
-        if (GAP2) {
+        if (GAP2 && ROWSUMS) {
             // this row's sums over the warp (a fixed tree), per warp in shared
             // memory, as lean_rows: rowp[(row - r0) * 8 + 2 * warp + (0: gap, 1: dot)]
             double gv = gap_acc, dv = dot_acc;
@@ -1334,7 +1324,52 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
         for (int j = 0; j <= VEC; ++j) zq[j] = T(0);
         second(H - 1, false, zq, zq);
     }
+}
+
+template <class T, bool ALPHA, bool GAP2, bool WIDE>
+__global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+    __shared__ double rowp[GAP2 ? kLeanRowsMax * 8 : 1];
+    __shared__ double sh[32];
+    __shared__ int flag;
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // a programmatic dependent of the previous step
+    const int b = step_image(bf, blockIdx.z);
+    if (b < 0) return;
+    const IsoState st = bf.st[b];
+    if (st.status != kLive) return;
+    const int it = st.it;
+    if (it <= 0 || (it & 3) != (GAP2 ? 3 : 1) || it + 1 >= A.max_iter || st.zero_in || (GAP2 && !bf.U[2])) {
+        if (threadIdx.x == 0) atomicExch(bf.err, 3);
+        return;
+    }
+    const IsoImage im = bf.img[b];
+    const int H = (int)A.g.L[0];
+    const int64_t N = A.g.N;
+    const int pin = A.par, pout = A.par ^ 1;
+    PairTile<T> p;
+    p.D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    p.U0 = static_cast<const T *>(bf.U[pin]) + (int64_t)b * 2 * N;
+    p.V0 = st.vsel ? p.U0 : static_cast<const T *>(bf.V[pin]) + (int64_t)b * 2 * N;
+    p.AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
+    p.UO0 = static_cast<T *>(bf.U[pout]) + (int64_t)b * 2 * N;
+    p.VO0 = static_cast<T *>(bf.V[pout]) + (int64_t)b * 2 * N;
+    p.UM0 = GAP2 ? static_cast<T *>(bf.U[2]) + (int64_t)b * 2 * N : nullptr;
+    p.N = N;
+    p.H = H;
+    p.W = (int)A.g.L[1];
+    p.r0 = blockIdx.y * A.rows;
+    p.r1 = min(H, p.r0 + A.rows);
+    p.c0 = WIDE ? (int)blockIdx.x * kPairCols : 0;
+    p.wh0 = (T)c.wh[0];
+    p.wh1 = (T)c.wh[1];
+    p.tau = (T)c.tau;
+    p.rad = (T)im.radius;
+    p.bnd = (T)im.bound;
+    p.beta1 = (T)st.beta;
+    p.beta2 = (T)((st.tn - 1.0) / fista_t(st.tn));
+    double gap_acc = 0.0, dot_acc = 0.0;
+    pair_pass<T, ALPHA, GAP2, WIDE, true>(p, rowp, gap_acc, dot_acc);
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int r0 = p.r0, r1 = p.r1;
     double *part = bf.part + (int64_t)b * bf.max_part * 2;
     if (GAP2) {
         // one slot per row, the sum of its warps in order (as lean_rows)
@@ -1373,14 +1408,27 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
 // The ragged step: images of any size in one arena, a device-resident work
 // list of (image, tile) items, each image at its own iteration with its own
 // buffer parity (its state's fin_par). Three variants (cold start, gap
-// check, plain) are launched per step; an item's block runs only in the
-// variant its image's state asks for.
+// check, plain) are launched per step, and on the list of 4-wide float rows
+// two pair variants after them (two iterations per launch, as the batched
+// pair launch); an item's block runs only in the variant its image's state
+// asks for.
 // ---------------------------------------------------------------------------
+
+// The pair variant an image's state asks for in the ragged step: 0 (iterations
+// 1 and 2 mod 4), 1 (3 and 4 mod 4, with the check), -1 (a single step).
+// As the batched launches: after the cold first iteration, not across
+// max_iter, images of two rows or more.
+__device__ __forceinline__ int ragged_pair_kind(const IsoState &st, const RagSlot &sl) {
+    const int it = st.it;
+    if (it <= 0 || it + 1 >= sl.max_iter || st.zero_in || (it & 1) == 0 || sl.H < 2) return -1;
+    return (it & 3) == 3 ? 1 : 0;
+}
 
 template <class T, int VEC, bool GAP, bool ZIN>
 __global__ void __launch_bounds__(128) iso2d_ragged_kernel(const RagItem *__restrict__ items,
                                                            const int *__restrict__ n_items,
-                                                           const RagSlot *__restrict__ slots, IsoCall c, IsoBuffers bf) {
+                                                           const RagSlot *__restrict__ slots, IsoCall c, IsoBuffers bf,
+                                                           int pairs) {
     __shared__ double sh[32];
     __shared__ int flag;
     if ((int)blockIdx.x >= *n_items) return;
@@ -1389,6 +1437,7 @@ __global__ void __launch_bounds__(128) iso2d_ragged_kernel(const RagItem *__rest
     const RagSlot sl = slots[b];
     const IsoState st = bf.st[b];
     if (st.status != kLive) return;
+    if (pairs && ragged_pair_kind(st, sl) >= 0) return;  // the pair variants take it
     const int it = st.it;
     const bool do_gap = (it > 0 && ((it & 3) == 0 || it == sl.max_iter)) || (it == 0 && st.warm);
     const bool zin = st.zero_in != 0;
@@ -1425,6 +1474,77 @@ __global__ void __launch_bounds__(128) iso2d_ragged_kernel(const RagItem *__rest
     bf.ticket[b] = 0;
     IsoState s2 = st;
     control(s2, im, sl.max_iter, GAP, test, gap, dot, pin, bf.live);
+    bf.st[b] = s2;
+}
+
+// The ragged step's pair variants: an item's tile (the slot's rows x 512
+// columns) of an image whose state asks for two iterations, the batched pair
+// launch's pass; the tile's gap and restart-test sums go to its partial slot.
+template <class T, bool GAP2>
+__global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_ragged_pair_kernel(const RagItem *__restrict__ items,
+                                                                              const int *__restrict__ n_items,
+                                                                              const RagSlot *__restrict__ slots,
+                                                                              IsoBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    if ((int)blockIdx.x >= *n_items) return;
+    const RagItem item = items[blockIdx.x];
+    const int b = item.slot;
+    const RagSlot sl = slots[b];
+    const IsoState st = bf.st[b];
+    if (st.status != kLive || ragged_pair_kind(st, sl) != (GAP2 ? 1 : 0)) return;
+    if (GAP2 && !bf.U[2]) {
+        if (threadIdx.x == 0) atomicExch(bf.err, 3);
+        return;
+    }
+    const IsoImage im = bf.img[b];
+    const int pin = st.fin_par, pout = pin ^ 1;
+    PairTile<T> p;
+    p.D = static_cast<const T *>(bf.d) + sl.off;
+    p.U0 = static_cast<const T *>(bf.U[pin]) + 2 * sl.off;
+    p.V0 = st.vsel ? p.U0 : static_cast<const T *>(bf.V[pin]) + 2 * sl.off;
+    p.AL = nullptr;
+    p.UO0 = static_cast<T *>(bf.U[pout]) + 2 * sl.off;
+    p.VO0 = static_cast<T *>(bf.V[pout]) + 2 * sl.off;
+    p.UM0 = GAP2 ? static_cast<T *>(bf.U[2]) + 2 * sl.off : nullptr;
+    p.N = (int64_t)sl.H * sl.W;
+    p.H = sl.H;
+    p.W = sl.W;
+    p.r0 = item.r0;
+    p.r1 = min(sl.H, item.r0 + sl.rows);
+    p.c0 = item.cs;
+    p.wh0 = (T)sl.wh0;
+    p.wh1 = (T)sl.wh1;
+    p.tau = (T)sl.tau;
+    p.rad = (T)im.radius;
+    p.bnd = (T)im.bound;
+    p.beta1 = (T)st.beta;
+    p.beta2 = (T)((st.tn - 1.0) / fista_t(st.tn));
+    double gap_acc = 0.0, dot_acc = 0.0;
+    pair_pass<T, false, GAP2, true, false>(p, nullptr, gap_acc, dot_acc);
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (GAP2) {
+        const double gsum = block_sum(gap_acc, sh);
+        const double dsum = block_sum(dot_acc, sh);
+        if (threadIdx.x == 0) {
+            part[item.blk * 2 + 0] = gsum;
+            part[item.blk * 2 + 1] = dsum;
+        }
+    }
+    if (!arrive_last(bf.ticket + b, sl.nblk, &flag)) return;
+    const double gap = GAP2 ? sum_partials(part, sl.nblk, 2, 0, sh) : 0.0;
+    const double dot = GAP2 ? sum_partials(part, sl.nblk, 2, 1, sh) : 0.0;
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2 = st;
+    control(s2, im, sl.max_iter, false, false, 0.0, 0.0, pin, bf.live);
+    if (GAP2) {
+        // the check is at u' (in U[2]); the update to u'' (in pout) stands unless it passes
+        control(s2, im, sl.max_iter, true, true, gap, dot, 2, bf.live);
+        if (s2.status == kLive) s2.fin_par = pout;
+    } else {
+        control(s2, im, sl.max_iter, false, false, 0.0, 0.0, pin, bf.live);
+    }
     bf.st[b] = s2;
 }
 
@@ -2408,13 +2528,33 @@ cudaError_t finalize_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf
     return cudaGetLastError();
 }
 
+template <bool GAP2>
+void launch_ragged_pair(const RagItem *items, const int *n_items, int grid, const RagSlot *slots,
+                        const IsoBuffers &bf, cudaStream_t s) {
+    constexpr size_t smem = pair_ring_bytes<float, false, true>();
+    static std::atomic<unsigned long long> done{0};  // the attribute is per function and device
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && !(done.load() & (1ull << dev))) {
+        cudaFuncSetAttribute(iso2d_ragged_pair_kernel<float, GAP2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        done.fetch_or(1ull << dev);
+    }
+    iso2d_ragged_pair_kernel<float, GAP2><<<grid, 128, smem, s>>>(items, n_items, slots, bf);
+}
+
 template <class T, int VEC>
 void launch_ragged_t(const RagItem *items, const int *n_items, int grid, const RagSlot *slots, const IsoCall &c,
-                     const IsoBuffers &bf, cudaStream_t s) {
+                     const IsoBuffers &bf, cudaStream_t s, bool pairs) {
     const int bx = 128;
-    iso2d_ragged_kernel<T, VEC, false, true><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf);
-    iso2d_ragged_kernel<T, VEC, true, false><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf);
-    iso2d_ragged_kernel<T, VEC, false, false><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf);
+    iso2d_ragged_kernel<T, VEC, false, true><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf, pairs);
+    iso2d_ragged_kernel<T, VEC, true, false><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf, pairs);
+    iso2d_ragged_kernel<T, VEC, false, false><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf, pairs);
+    if constexpr (std::is_same<T, float>::value && VEC == 4) {
+        if (pairs) {
+            launch_ragged_pair<false>(items, n_items, grid, slots, bf, s);
+            launch_ragged_pair<true>(items, n_items, grid, slots, bf, s);
+        }
+    }
 }
 
 }  // namespace
@@ -2423,13 +2563,18 @@ cudaError_t iso_ragged_step(int dtype, int vec, const RagItem *items, const int 
                             const RagSlot *slots, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
     if (grid <= 0) return cudaSuccess;
     if (dtype == 1) {
-        if (vec == 4) launch_ragged_t<float, 4>(items, n_items, grid, slots, c, bf, s);
-        else launch_ragged_t<float, 1>(items, n_items, grid, slots, c, bf, s);
+        const bool pairs = iso_ragged_pairs(dtype, vec) && bf.U[2];
+        if (vec == 4) launch_ragged_t<float, 4>(items, n_items, grid, slots, c, bf, s, pairs);
+        else launch_ragged_t<float, 1>(items, n_items, grid, slots, c, bf, s, false);
     } else {
-        if (vec == 2) launch_ragged_t<double, 2>(items, n_items, grid, slots, c, bf, s);
-        else launch_ragged_t<double, 1>(items, n_items, grid, slots, c, bf, s);
+        if (vec == 2) launch_ragged_t<double, 2>(items, n_items, grid, slots, c, bf, s, false);
+        else launch_ragged_t<double, 1>(items, n_items, grid, slots, c, bf, s, false);
     }
     return cudaGetLastError();
+}
+
+bool iso_ragged_pairs(int dtype, int vec) {
+    return pairs_enabled() && dtype == 1 && vec == 4;
 }
 
 int iso_setup_blocks(const Geometry &g) {
@@ -2505,13 +2650,17 @@ cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBu
                       : step_t<double>(g, c, bf, sh, par, variant, nimg, s);
 }
 
-bool iso_pair_ok(const Geometry &g, const StepShape &sh, int max_part) {
-    static const bool on = [] {
+bool pairs_enabled() {
+    static const bool on = [] {  // tuning hint FASTPROX_B200_PAIRS=0: single steps only
         const char *v = std::getenv("FASTPROX_B200_PAIRS");
         return !(v && v[0] == '0' && v[1] == 0);
     }();
+    return on;
+}
+
+bool iso_pair_ok(const Geometry &g, const StepShape &sh, int max_part) {
     // one block per row up to 512 columns (the lean step's threads), else blocks of 512 columns
-    return on && g.k == 2 && sh.kind == 4 && sh.vec == 4 && (sh.gx == 1 ? g.L[1] <= kPairCols : sh.bx == 128) &&
+    return pairs_enabled() && g.k == 2 && sh.kind == 4 && sh.vec == 4 && (sh.gx == 1 ? g.L[1] <= kPairCols : sh.bx == 128) &&
            g.L[0] >= 2 && g.L[0] * sh.gx <= max_part;
 }
 

@@ -274,12 +274,14 @@ FP_API void fp_b200_release_cached(void);
  * contiguous (height, width) arrays (z may be x), copied in now, solved by
  * later runs; tol and max_iter as in fp_prox, per image; FP_ENOMEM when no
  * slot or not enough contiguous pixels are free (admit again after a run has
- * finished others). run: repeats `steps` iterations of every live image (as a
- * captured CUDA graph) until at least one image has finished or none is live;
+ * finished others). run: repeats `steps` steps of every live image (as a
+ * captured CUDA graph; a step advances an image by one iteration, or by four
+ * on float images whose width is a multiple of 4, in two launches of two
+ * iterations each) until at least one image has finished or none is live;
  * writes the finished images' z, and their slots, gaps and iterations (a
  * negative count: stopped at max_iter) into arrays of max_images entries;
  * *nlive, the images still iterating. max_chunks > 0 bounds the chunks of
- * `steps` iterations one run may take (it may then return with none
+ * `steps` steps one run may take (it may then return with none
  * finished, so that a serving loop can admit new images in between). All
  * calls on one batch run on its stream (set_stream; NULL by default) and
  * must not overlap. */
