@@ -419,6 +419,8 @@ void free_ws_memory(fp_workspace *ws) {
     ws->ev[0] = ws->ev[1] = nullptr;
     for (cudaEvent_t e : ws->tev) cudaEventDestroy(e);
     ws->tev.clear();
+    if (ws->an_graph) cudaGraphExecDestroy(ws->an_graph);
+    ws->an_graph = nullptr;
 }
 
 // The buffers of a workspace, laid out in one block (256-byte aligned
@@ -1019,6 +1021,67 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     return cuda_status(e);
 }
 
+// Anisotropic rounds per captured graph, and the solves that use graphs: a
+// round is about 15 launches, most of which exit at once, so a small solve is
+// bound by launch latency (a 64 x 64 image took 150 us a round in plain
+// launches). FASTPROX_B200_AN_GRAPHS=0 keeps plain launches.
+constexpr int kAnChunk = 4;
+constexpr int64_t kAnGraphPixels = int64_t(1) << 22;
+
+bool an_graphs_enabled() {
+    static const bool on = [] {
+        const char *v = std::getenv("FASTPROX_B200_AN_GRAPHS");
+        return !(v && v[0] == '0' && v[1] == 0);
+    }();
+    return on;
+}
+
+bool same_call(const AnCall &a, const AnCall &b) {
+    return a.w[0] == b.w[0] && a.w[1] == b.w[1] && a.w[2] == b.w[2] && a.tol == b.tol && a.max_iter == b.max_iter &&
+           a.step_scale == b.step_scale && a.has_beta == b.has_beta && a.beta_max == b.beta_max && a.N == b.N &&
+           a.has_adbpg == b.has_adbpg && a.has_fdpg3 == b.has_fdpg3 && a.warm == b.warm;
+}
+
+// kAnChunk rounds as one graph launch on s, captured on a private stream when
+// the workspace holds none for these arguments. False: capture failed (the
+// caller launches rounds itself from then on).
+bool an_graph_rounds(fp_workspace *ws, const AnGeom &g, const AnCall &c, const AnBuffers &bf, int64_t nimg,
+                     cudaStream_t s, int64_t *launches, cudaError_t *err) {
+    if (!(ws->an_graph && ws->an_graph_nimg == nimg && ws->an_graph_lmap == bf.lmap && same_call(ws->an_graph_c, c))) {
+        if (ws->an_graph) cudaGraphExecDestroy(ws->an_graph);
+        ws->an_graph = nullptr;
+        cudaStream_t cap = nullptr;
+        if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        cudaGraph_t graph = nullptr;
+        int64_t nl = 0;
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            for (int r = 0; r < kAnChunk && e == cudaSuccess; ++r) e = aniso_round(ws->dtype, g, c, bf, nimg, cap, &nl);
+            const cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
+            if (e == cudaSuccess) e = e2;
+        }
+        cudaStreamDestroy(cap);
+        cudaGraphExec_t exec = nullptr;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        ws->an_graph = exec;
+        ws->an_graph_c = c;
+        ws->an_graph_nimg = nimg;
+        ws->an_graph_lmap = bf.lmap;
+        ws->an_graph_launches = nl;
+    }
+    *err = cudaGraphLaunch(ws->an_graph, s);
+    *launches += ws->an_graph_launches;
+    return true;
+}
+
 fp_status run_aniso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zdst, double tol, int max_iter,
                     bool warm) {
     const Geometry &g0 = ws->g;
@@ -1080,15 +1143,22 @@ fp_status run_aniso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *z
     aniso_prepare(ws->dtype);
     // rounds of launches (an iteration each, with its check, polish and
     // retirement), the live count read back behind two rounds in flight
-    // (over a list of the live images once fewer are live, as in run_iso)
+    // (over a list of the live images once fewer are live, as in run_iso);
+    // after the first, small solves replay rounds in captured chunks
     int slot = 0, inflight = 0;
     int64_t rounds = 0, nimg = g.B;
     const int64_t cap = (int64_t)max_iter + 4;
     bool done = false;
+    bool graphs = an_graphs_enabled() && g.N * g.B <= kAnGraphPixels;
     while (!done) {
-        e = aniso_round(ws->dtype, g, c, bf, nimg, s, &launches);
+        if (graphs && rounds > 0 && an_graph_rounds(ws, g, c, bf, nimg, s, &launches, &e)) {
+            rounds += kAnChunk;
+        } else {
+            if (rounds > 0) graphs = false;
+            e = aniso_round(ws->dtype, g, c, bf, nimg, s, &launches);
+            ++rounds;
+        }
         if (e != cudaSuccess) return cuda_status(e);
-        ++rounds;
         e = cudaMemcpyAsync(ws->h_live + slot, ws->live, sizeof(int), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaEventRecord(ws->ev[slot], s);
         if (e != cudaSuccess) return cuda_status(e);

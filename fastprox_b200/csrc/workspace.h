@@ -98,6 +98,13 @@ struct fp_workspace {
     std::vector<cudaEvent_t> tev;
     double tms[3] = {0.0, 0.0, 0.0};
     int64_t tcount[3] = {0, 0, 0};
+    // small anisotropic solves: a captured chunk of rounds, replayed while the
+    // call's constants, the launched images and the live list are the same
+    cudaGraphExec_t an_graph = nullptr;
+    fpb::AnCall an_graph_c{};
+    int64_t an_graph_nimg = 0;
+    const int *an_graph_lmap = nullptr;
+    int64_t an_graph_launches = 0;  // kernels one replay launches
     // results of the last call
     std::vector<double> gaps, zerrs;
     std::vector<int> iters;
