@@ -174,7 +174,9 @@ def profile_case(kind="iso"):
     solved for exactly 8 iterations: launch 0 is the cold start, launches 4
     and 8 carry gap checks, the rest are plain iterations. aniso: 16 of its
     images, anisotropic with edge weights, solved to gap 1e-6 (every kernel of
-    the method, polish included). iso3d: 8 volumes of 128^3 for 8 iterations."""
+    the method, polish included). iso3d: 8 volumes of 128^3 for 8 iterations.
+    ragged: 64 images of 512^2 in a ragged batch (32-row tiles, plain
+    launches), gamma 0.1, gap 1e-6, at most 200 iterations."""
     import torch
 
     from fastprox_b200 import TVAniso, TVIso, synth
@@ -183,6 +185,19 @@ def profile_case(kind="iso"):
         z, info = TVIso(3).solve(x, 0.1, tol=0.0, max_iter=8, with_dual=False)
         torch.cuda.synchronize()
         print(json.dumps({"profile_case": "iso3d", "iters": int(info.iters)}))
+        return
+    if kind == "ragged":
+        from fastprox_b200.batch import RaggedBatch
+        B, H, W = 64, 512, 512
+        b = RaggedBatch(max_images=B, max_pixels=B * H * W + 4096, rows=32, graphs=False)
+        xs = torch.as_tensor(synth.phantom(B, H, W, seed=0), device="cuda")
+        for i in range(B):
+            b.admit(xs[i], 0.1, 1e-6, max_iter=200)
+        n = 0
+        while b.pending:
+            n += len(b.run(steps=4))
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": "ragged", "finished": n, **b.stats()}))
         return
     if kind == "aniso":
         B = 16
@@ -209,9 +224,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--profile-case", nargs="?", const="iso", default=None, choices=["iso", "aniso", "iso3d"],
+    ap.add_argument("--profile-case", nargs="?", const="iso", default=None, choices=["iso", "aniso", "iso3d", "ragged"],
                     help="iso: one solve of the benchmark batch with 8 iterations (tol 0); aniso: 16 images "
-                         "anisotropic to gap 1e-6; iso3d: 8 x 128^3 with 8 iterations; the cases for ncu captures")
+                         "anisotropic to gap 1e-6; iso3d: 8 x 128^3 with 8 iterations; ragged: 64 x 512^2 in a "
+                         "ragged batch; the cases for ncu captures")
     ap.add_argument("--workload", default="iso512", choices=["iso512", "aniso512", "iso3d", "uneven", "vjp", "serve"],
                     help="iso512 (default, the headline line); the others report the other workloads")
     ap.add_argument("--serve-seconds", type=float, default=20.0)
