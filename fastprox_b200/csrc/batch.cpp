@@ -8,9 +8,10 @@
 // of pixel ranges on the host places them), per-slot constants and state,
 // partial sums and tickets, and two work lists of (image, tile) items, one
 // for rows of a multiple of 4 pixels (16-byte vectors) and one for the rest.
-// A step launches the three kernel variants over each list, and on the
-// 4-wide float list the two pair variants (two iterations per launch, with a
-// third dual buffer for u' of the checked pair); chunks of steps
+// A step launches the single-step kernel over each list (each block in the
+// variant its image's state asks for), and on the 4-wide float list the two
+// pair variants (two iterations per launch, with a third dual buffer for u'
+// of the checked pair); chunks of steps
 // are replayed as CUDA graphs, captured again only when the work lists
 // outgrow their current size class.
 #include <cuda_runtime_api.h>
@@ -281,12 +282,12 @@ cudaError_t launch_steps(fp_b200_batch *bt, int steps) {
     return cudaSuccess;
 }
 
-// kernels one step launches: three variants per non-empty list, two more
-// (the pair variants) on the 4-wide float list
+// kernels one step launches: the single steps on each non-empty list, the
+// two pair variants on the 4-wide float list
 int launches_per_step(const fp_b200_batch *bt) {
     int n = 0;
-    if (bt->grid[0] > 0) n += 3 + (bt->U2 && iso_ragged_pairs(bt->dtype, 4) ? 2 : 0);
-    if (bt->grid[1] > 0) n += 3;
+    if (bt->grid[0] > 0) n += 1 + (bt->U2 && iso_ragged_pairs(bt->dtype, 4) ? 2 : 0);
+    if (bt->grid[1] > 0) n += 1;
     return n;
 }
 

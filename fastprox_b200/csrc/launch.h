@@ -80,8 +80,9 @@ inline int iso_variant(int64_t k, int max_iter, bool warm) {
 cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, void *out,
                          cudaStream_t s);
 
-// One step of a ragged batch: the three kernel variants over the work list
-// of `vec` (items[0 .. *n_items), grid >= *n_items blocks).
+// One step of a ragged batch over the work list of `vec` (items[0 ..
+// *n_items), grid >= *n_items blocks): the single-step launch (each block in
+// the variant its image asks for), then the pair variants where they apply.
 cudaError_t iso_ragged_step(int dtype, int vec, const RagItem *items, const int *n_items, int grid,
                             const RagSlot *slots, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s);
 // Whether the ragged step on a list of `vec`-wide rows adds the two pair

@@ -1407,11 +1407,11 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
 // ---------------------------------------------------------------------------
 // The ragged step: images of any size in one arena, a device-resident work
 // list of (image, tile) items, each image at its own iteration with its own
-// buffer parity (its state's fin_par). Three variants (cold start, gap
-// check, plain) are launched per step, and on the list of 4-wide float rows
-// two pair variants after them (two iterations per launch, as the batched
-// pair launch); an item's block runs only in the variant its image's state
-// asks for.
+// buffer parity (its state's fin_par). One launch of single steps (each
+// block in the variant its image's state asks for: cold start, gap check or
+// plain) per step, and on the list of 4-wide float rows two pair variants
+// after it (two iterations per launch, as the batched pair launch); an
+// image's blocks run in the launch its state asks for.
 // ---------------------------------------------------------------------------
 
 // The pair variant an image's state asks for in the ragged step: 0 (iterations
@@ -1424,24 +1424,13 @@ __device__ __forceinline__ int ragged_pair_kind(const IsoState &st, const RagSlo
     return (it & 3) == 3 ? 1 : 0;
 }
 
+// One single step of an item's tile, in the variant (GAP: gap check; ZIN:
+// cold start from a zero dual) its image's state asks for.
 template <class T, int VEC, bool GAP, bool ZIN>
-__global__ void __launch_bounds__(128) iso2d_ragged_kernel(const RagItem *__restrict__ items,
-                                                           const int *__restrict__ n_items,
-                                                           const RagSlot *__restrict__ slots, IsoCall c, IsoBuffers bf,
-                                                           int pairs) {
-    __shared__ double sh[32];
-    __shared__ int flag;
-    if ((int)blockIdx.x >= *n_items) return;
-    const RagItem item = items[blockIdx.x];
+__device__ __forceinline__ void ragged_single(const RagItem &item, const RagSlot &sl, const IsoState &st,
+                                              const IsoBuffers &bf, double *sh, int *flag) {
     const int b = item.slot;
-    const RagSlot sl = slots[b];
-    const IsoState st = bf.st[b];
-    if (st.status != kLive) return;
-    if (pairs && ragged_pair_kind(st, sl) >= 0) return;  // the pair variants take it
     const int it = st.it;
-    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == sl.max_iter)) || (it == 0 && st.warm);
-    const bool zin = st.zero_in != 0;
-    if (do_gap != GAP || zin != ZIN) return;
     const IsoImage im = bf.img[b];
     const int H = sl.H, W = sl.W;
     const int64_t N = (int64_t)H * W;
@@ -1467,7 +1456,7 @@ __global__ void __launch_bounds__(128) iso2d_ragged_kernel(const RagItem *__rest
         part[item.blk * 2 + 0] = gsum;
         part[item.blk * 2 + 1] = dsum;
     }
-    if (!arrive_last(bf.ticket + b, sl.nblk, &flag)) return;
+    if (!arrive_last(bf.ticket + b, sl.nblk, flag)) return;
     const double gap = GAP ? sum_partials(part, sl.nblk, 2, 0, sh) : 0.0;
     const double dot = test ? sum_partials(part, sl.nblk, 2, 1, sh) : 0.0;
     if (threadIdx.x != 0) return;
@@ -1475,6 +1464,30 @@ __global__ void __launch_bounds__(128) iso2d_ragged_kernel(const RagItem *__rest
     IsoState s2 = st;
     control(s2, im, sl.max_iter, GAP, test, gap, dot, pin, bf.live);
     bf.st[b] = s2;
+}
+
+// The single steps of a ragged step, one launch: each item's block runs the
+// variant its image's state asks for (cold start, gap check or plain), or
+// exits when the pair variants take the image.
+template <class T, int VEC>
+__global__ void __launch_bounds__(128) iso2d_ragged_kernel(const RagItem *__restrict__ items,
+                                                           const int *__restrict__ n_items,
+                                                           const RagSlot *__restrict__ slots, IsoBuffers bf,
+                                                           int pairs) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    if ((int)blockIdx.x >= *n_items) return;
+    const RagItem item = items[blockIdx.x];
+    const RagSlot sl = slots[item.slot];
+    const IsoState st = bf.st[item.slot];
+    if (st.status != kLive) return;
+    if (pairs && ragged_pair_kind(st, sl) >= 0) return;  // the pair variants take it
+    const int it = st.it;
+    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == sl.max_iter)) || (it == 0 && st.warm);
+    const bool zin = st.zero_in != 0;
+    if (zin && !do_gap) ragged_single<T, VEC, false, true>(item, sl, st, bf, sh, &flag);
+    else if (!zin && do_gap) ragged_single<T, VEC, true, false>(item, sl, st, bf, sh, &flag);
+    else if (!zin) ragged_single<T, VEC, false, false>(item, sl, st, bf, sh, &flag);
 }
 
 // The ragged step's pair variants: an item's tile (the slot's rows x 512
@@ -2545,10 +2558,7 @@ void launch_ragged_pair(const RagItem *items, const int *n_items, int grid, cons
 template <class T, int VEC>
 void launch_ragged_t(const RagItem *items, const int *n_items, int grid, const RagSlot *slots, const IsoCall &c,
                      const IsoBuffers &bf, cudaStream_t s, bool pairs) {
-    const int bx = 128;
-    iso2d_ragged_kernel<T, VEC, false, true><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf, pairs);
-    iso2d_ragged_kernel<T, VEC, true, false><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf, pairs);
-    iso2d_ragged_kernel<T, VEC, false, false><<<grid, bx, 0, s>>>(items, n_items, slots, c, bf, pairs);
+    iso2d_ragged_kernel<T, VEC><<<grid, 128, 0, s>>>(items, n_items, slots, bf, pairs);
     if constexpr (std::is_same<T, float>::value && VEC == 4) {
         if (pairs) {
             launch_ragged_pair<false>(items, n_items, grid, slots, bf, s);

@@ -65,8 +65,9 @@ def test_ragged_pairs_match_single_steps(cuda, tmp_path):
             assert np.array_equal(z, zr), (rows, IMAGES[k], np.abs(z - zr).max())
             assert it == int(itr) and bool(conv) == bool(cr), (rows, IMAGES[k], it, itr)
             assert gap == gr or (np.isnan(gap) and np.isnan(gr)), (rows, IMAGES[k], gap, gr)
-        # the pair variants ran: five launches per step on the 4-wide list
-        assert stats["kernel_launches"] > 5 * stats["steps"], stats
+        # the pair variants ran: three launches per step on the 4-wide list
+        # (single steps and two pair variants), one on the other list
+        assert stats["kernel_launches"] > 2 * stats["steps"], stats
 
 
 if __name__ == "__main__":  # the single-step run (FASTPROX_B200_PAIRS=0 in the environment)
