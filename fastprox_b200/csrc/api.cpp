@@ -538,7 +538,6 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     }
     // the first iterate of a pair launch whose second iteration carries the
     // check (the final u when it passes)
-    if (op->kind != kAniso && iso_pair_ok(g, ws->shape_, ws->max_part)) A(&ws->U2, dualb);
     if (op->kind == kAniso) {
         A((void **)&ws->an_img, (size_t)B * sizeof(AnImage));
         A((void **)&ws->an_st, (size_t)B * sizeof(AnState));
@@ -947,7 +946,6 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     // applies (iso_pair_ok).
     const int chunk = ws->chunk > 0 ? ws->chunk : 8;
     const bool pairs = iso_pair_ok(g, ws->shape_, ws->max_part);
-    bf.U[2] = ws->U2;
     int par = 0, slot = 0, inflight = 0;
     int64_t launched = 0, steps = 0, lists = 0, nimg = g.B;
     const int64_t cap = (int64_t)max_iter + 1 + 2 * chunk;
@@ -961,7 +959,7 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     bool done = false;
     while (!done) {
         for (int j = 0; j < chunk; ++j) {
-            const int pv = pairs ? iso_pair_at(launched, max_iter, ws->U2 != nullptr) : -1;
+            const int pv = pairs ? iso_pair_at(launched, max_iter) : -1;
             const bool timed = ws->time_steps && tkind.size() < kTimed;
             if (timed) {
                 while (ws->tev.size() < 2 * (tkind.size() + 1)) {
@@ -1017,7 +1015,11 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
             ws->tcount[tkind[k]] += 1;
         }
     }
-    e = iso_finalize(ws->dtype, g, c, bf, zdst, s);
+    if (pairs) {
+        e = iso_redo(ws->dtype, g, c, bf, s);
+        ws->kernel_launches += 2;
+    }
+    if (e == cudaSuccess) e = iso_finalize(ws->dtype, g, c, bf, zdst, s);
     return cuda_status(e);
 }
 
@@ -1639,7 +1641,6 @@ fp_status deriv_prepare(const fp_op *op, fp_workspace *ws, VjpGeom &vg, VjpBuffe
     bf.d = ws->d;
     bf.U[0] = ws->U[0];
     bf.U[1] = ws->U[1];
-    bf.U[2] = ws->U2;
     bf.img = ws->img;
     bf.st = ws->st;
     bf.alpha = ws->spatial;

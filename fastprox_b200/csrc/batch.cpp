@@ -10,10 +10,9 @@
 // for rows of a multiple of 4 pixels (16-byte vectors) and one for the rest.
 // A step launches the single-step kernel over each list (each block in the
 // variant its image's state asks for), and on the 4-wide float list the two
-// pair variants (two iterations per launch, with a third dual buffer for u'
-// of the checked pair); chunks of steps
-// are replayed as CUDA graphs, captured again only when the work lists
-// outgrow their current size class.
+// pair variants (two iterations per launch); chunks of steps are replayed
+// as CUDA graphs, captured again only when the work lists outgrow their
+// current size class.
 #include <cuda_runtime_api.h>
 
 #include <algorithm>
@@ -69,7 +68,6 @@ struct fp_b200_batch {
     int max_part = 4096;
     // device
     void *d = nullptr, *U[2] = {nullptr, nullptr}, *V[2] = {nullptr, nullptr}, *dual = nullptr;
-    void *U2 = nullptr;  // u' of the pair variants with the check (float)
     IsoImage *img = nullptr;
     IsoState *st = nullptr;
     double *gammas = nullptr, *part = nullptr;
@@ -164,7 +162,6 @@ IsoBuffers buffers(fp_b200_batch *bt) {
         bf.U[i] = bt->U[i];
         bf.V[i] = bt->V[i];
     }
-    bf.U[2] = bt->U2;
     bf.dual = bt->dual;
     bf.alpha = nullptr;
     bf.img = bt->img;
@@ -188,7 +185,6 @@ IsoBuffers slot_buffers(fp_b200_batch *bt, int slot) {
         bf.U[i] = static_cast<char *>(bt->U[i]) + 2 * (size_t)s.off * T;
         bf.V[i] = static_cast<char *>(bt->V[i]) + 2 * (size_t)s.off * T;
     }
-    if (bt->U2) bf.U[2] = static_cast<char *>(bt->U2) + 2 * (size_t)s.off * T;
     bf.dual = static_cast<char *>(bt->dual) + 2 * (size_t)s.off * T;
     bf.img = bt->img + slot;
     bf.st = bt->st + slot;
@@ -286,7 +282,7 @@ cudaError_t launch_steps(fp_b200_batch *bt, int steps) {
 // two pair variants on the 4-wide float list
 int launches_per_step(const fp_b200_batch *bt) {
     int n = 0;
-    if (bt->grid[0] > 0) n += 1 + (bt->U2 && iso_ragged_pairs(bt->dtype, 4) ? 2 : 0);
+    if (bt->grid[0] > 0) n += 1 + (iso_ragged_pairs(bt->dtype, 4) ? 2 : 0);
     if (bt->grid[1] > 0) n += 1;
     return n;
 }
@@ -376,7 +372,6 @@ FP_API fp_status fp_b200_batch_create(const fp_op *op, int64_t max_images, int64
             A(&bt->V[i], 2 * P * T);
         }
         A(&bt->dual, 2 * P * T);
-        if (iso_ragged_pairs(dtype, 4)) A(&bt->U2, 2 * P * T);
         A((void **)&bt->img, S * sizeof(IsoImage));
         A((void **)&bt->st, S * sizeof(IsoState));
         A((void **)&bt->gammas, S * sizeof(double));
@@ -571,8 +566,9 @@ FP_API fp_status fp_b200_batch_run(fp_b200_batch *bt, int steps, int max_chunks,
             g.N = (int64_t)s.H * s.W;
             g.B = 1;
             IsoBuffers bf = slot_buffers(bt, slot);
+            if (e == cudaSuccess) e = iso_redo(bt->dtype, g, c, bf, st);
             if (e == cudaSuccess) e = iso_finalize(bt->dtype, g, c, bf, s.out, st);
-            bt->kernel_launches += 1;
+            bt->kernel_launches += 3;
         }
         if (e == cudaSuccess) e = cudaMemcpyAsync(bt->h_img, bt->img, S * sizeof(IsoImage), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -53,6 +53,9 @@ struct IsoState {
     int zero_in;   // 1: u = v = 0 (cold start, nothing staged)
     int warm;      // 1: the gap is checked before the first iteration
     int fin_par;   // buffer parity holding the final u
+    int redo;      // 1: the final u is one more iteration from the buffers of fin_par, reading v = u when
+                   // redo_vsel (a checked pair's check passed at its first iterate, which it did not store)
+    int redo_vsel;
     double tn;     // fista_t(t) of the next iteration, t its momentum scalar
     double beta;   // (t - 1) / tn of the next iteration
     double gp;     // last gap checked

@@ -11,7 +11,7 @@ namespace fpb {
 // Device buffers of an isotropic solve (see engine.h for the layout).
 struct IsoBuffers {
     void *d = nullptr;          // B x N of T
-    void *U[3] = {nullptr, nullptr, nullptr};  // U[2]: the first iterate of a pair launch (optional)
+    void *U[2] = {nullptr, nullptr};
     void *V[2] = {nullptr, nullptr};
     void *dual = nullptr;       // k x B x N of T
     const void *alpha = nullptr;  // pixel weights (T), N or B x N, or null
@@ -60,21 +60,25 @@ cudaError_t iso_step(int dtype, const Geometry &g, const IsoCall &c, const IsoBu
 // Variants of iso_step running iterations k and k + 1 in one launch, where
 // iso_pair_ok (the lean 2D shape over whole rows) and k + 1 < max_iter:
 // kVariantPair for k = 1 mod 4 (neither has a check), kVariantPairGap for
-// k = 3 mod 4 (the second carries the gap check and the restart test; needs
-// the third dual buffer bf.U[2]).
+// k = 3 mod 4 (the second carries the gap check and the restart test; when
+// it passes, the final u is the first iterate, formed again by iso_redo).
 constexpr int kVariantPair = 3;
 constexpr int kVariantPairGap = 4;
 bool iso_pair_ok(const Geometry &g, const StepShape &sh, int max_part);
-inline int iso_pair_at(int64_t k, int max_iter, bool gap_pairs) {
+inline int iso_pair_at(int64_t k, int max_iter) {
     if (k <= 0 || k + 1 >= max_iter) return -1;
     if ((k & 3) == 1) return kVariantPair;
-    if ((k & 3) == 3 && gap_pairs) return kVariantPairGap;
+    if ((k & 3) == 3) return kVariantPairGap;
     return -1;
 }
 inline int iso_variant(int64_t k, int max_iter, bool warm) {
     if (k == 0) return warm ? 2 : 1;
     return (k % 4 == 0 || k == max_iter) ? 2 : 0;
 }
+// The final u of images whose checked pair launch passed at its first
+// iterate (state redo), formed again from that launch's input buffers; the
+// state then points at it. Before any read of a solve's final dual.
+cudaError_t iso_redo(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s);
 // z = x - G^T q into out (contiguous, device, x's dtype), the dual into
 // bf.dual, for every image by its mode; exact 1D TV for single-axis images.
 cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, void *out,
@@ -86,7 +90,7 @@ cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const I
 cudaError_t iso_ragged_step(int dtype, int vec, const RagItem *items, const int *n_items, int grid,
                             const RagSlot *slots, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s);
 // Whether the ragged step on a list of `vec`-wide rows adds the two pair
-// variants (float, 4-wide rows, pairs not switched off); they need bf.U[2].
+// variants (float, 4-wide rows, pairs not switched off).
 bool iso_ragged_pairs(int dtype, int vec);
 bool pairs_enabled();
 

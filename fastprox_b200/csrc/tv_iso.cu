@@ -135,6 +135,8 @@ __global__ void __launch_bounds__(kScanThreads) scan1_kernel(const T *__restrict
     st.zero_in = 1;
     st.warm = 0;
     st.fin_par = 0;
+    st.redo = 0;
+    st.redo_vsel = 0;
     st.tn = fista_t(1.0);
     st.beta = 0.0;
     st.gp = CUDART_INF;
@@ -844,8 +846,9 @@ __global__ void __launch_bounds__(128, 5) iso2d_lean_kernel(StepArgs A, IsoCall 
 // 2 x 40 B for two lean steps.
 // GAP2: it = 3 mod 4, the second iteration (0 mod 4) carrying the gap check
 // at u' and the restart test, with lean_rows' per-row partial sums; u' is
-// also written to the third dual buffer (U[2]), the final iterate when the
-// check passes (the state's fin_par is then 2).
+// not stored: when the check passes (the final iterate is u'), the state
+// keeps fin_par = the launch's input parity and redo = 1, and iso_redo forms
+// u' again from those untouched buffers before the solve's outputs are read.
 // Each iteration's arithmetic and every sum's order are lean_rows' (the same
 // expressions), so the iterates and the checks are those of two lean steps.
 // ---------------------------------------------------------------------------
@@ -900,7 +903,7 @@ constexpr size_t pair_ring_bytes() {
 template <class T>
 struct PairTile {
     const T *D, *U0, *V0, *AL;
-    T *UO0, *VO0, *UM0;
+    T *UO0, *VO0;
     int64_t N;
     int H, W, r0, r1, c0;
     T wh0, wh1, tau, rad, bnd, beta1, beta2;
@@ -926,7 +929,7 @@ __device__ __forceinline__ void pair_pass(const PairTile<T> &p, double *rowp, do
     const int64_t N = p.N;
     const T *D = p.D, *U0 = p.U0, *V0 = p.V0, *AL = p.AL;
     const T *U1 = U0 + N, *V1 = V0 + N;
-    T *UO0 = p.UO0, *VO0 = p.VO0, *UM0 = p.UM0;
+    T *UO0 = p.UO0, *VO0 = p.VO0;
     T *UO1 = UO0 + N, *VO1 = VO0 + N;
     const T wh0 = p.wh0, wh1 = p.wh1, tau = p.tau, rad = p.rad, bnd = p.bnd, beta1 = p.beta1, beta2 = p.beta2;
 
@@ -1240,10 +1243,6 @@ __device__ __forceinline__ void pair_pass(const PairTile<T> &p, double *rowp, do
                 xl[i & 1][w][0] = vo1[VEC - 1];
                 if (GAP2) xl[i & 1][w][1] = un1[VEC - 1];
             }
-            if (GAP2 && i >= r0 && i < r1) {
-                store_pack<T, VEC>(UM0 + off, un0);
-                store_pack<T, VEC>(UM0 + N + off, un1);
-            }
         }
         __syncthreads();
         // the left neighbour's last v1' (u1'), and the right neighbour's first column
@@ -1337,7 +1336,7 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
     const IsoState st = bf.st[b];
     if (st.status != kLive) return;
     const int it = st.it;
-    if (it <= 0 || (it & 3) != (GAP2 ? 3 : 1) || it + 1 >= A.max_iter || st.zero_in || (GAP2 && !bf.U[2])) {
+    if (it <= 0 || (it & 3) != (GAP2 ? 3 : 1) || it + 1 >= A.max_iter || st.zero_in) {
         if (threadIdx.x == 0) atomicExch(bf.err, 3);
         return;
     }
@@ -1352,7 +1351,6 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
     p.AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
     p.UO0 = static_cast<T *>(bf.U[pout]) + (int64_t)b * 2 * N;
     p.VO0 = static_cast<T *>(bf.V[pout]) + (int64_t)b * 2 * N;
-    p.UM0 = GAP2 ? static_cast<T *>(bf.U[2]) + (int64_t)b * 2 * N : nullptr;
     p.N = N;
     p.H = H;
     p.W = (int)A.g.L[1];
@@ -1395,13 +1393,69 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_pair_kernel(StepArgs 
     IsoState s2 = st;
     control(s2, im, A.max_iter, false, false, 0.0, 0.0, pin, bf.live);
     if (GAP2) {
-        // the check is at u' (in U[2]); the update to u'' (in pout) stands unless it passes
-        control(s2, im, A.max_iter, true, true, gap, dot, 2, bf.live);
-        if (s2.status == kLive) s2.fin_par = pout;
+        // the check is at u'; the update to u'' (in pout) stands unless it
+        // passes, and then the final u is u', formed again from pin
+        control(s2, im, A.max_iter, true, true, gap, dot, pin, bf.live);
+        if (s2.status != kLive) {
+            s2.redo = 1;
+            s2.redo_vsel = st.vsel;
+        }
     } else {
         control(s2, im, A.max_iter, false, false, 0.0, 0.0, pin, bf.live);
     }
     bf.st[b] = s2;
+}
+
+// The final iterate of the images whose checked pair passed at its first
+// iterate u' (state redo): u' formed again from the pair's input buffers (the
+// state's fin_par, reading v = u when redo_vsel) with the pair's first-
+// iteration arithmetic (the same expressions, so the same bits), into the
+// other parity's u; iso2d_redo_state then points fin_par there.
+template <class T, bool ALPHA>
+__global__ void __launch_bounds__(256) iso2d_redo_kernel(Geometry g, IsoCall c, IsoBuffers bf) {
+    const int b = (int)blockIdx.y;
+    const IsoState st = bf.st[b];
+    if (!st.redo) return;
+    const IsoImage im = bf.img[b];
+    const int H = (int)g.L[0], W = (int)g.L[1];
+    const int64_t N = g.N;
+    const int pin = st.fin_par, pout = pin ^ 1;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *U0 = static_cast<const T *>(bf.U[pin]) + (int64_t)b * 2 * N;
+    const T *V0 = st.redo_vsel ? U0 : static_cast<const T *>(bf.V[pin]) + (int64_t)b * 2 * N;
+    const T *V1 = V0 + N;
+    T *UO0 = static_cast<T *>(bf.U[pout]) + (int64_t)b * 2 * N;
+    T *UO1 = UO0 + N;
+    const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
+    const T wh0 = (T)c.wh[0], wh1 = (T)c.wh[1], tau = (T)c.tau;
+    const T rad = (T)im.radius, bnd = (T)im.bound;
+    auto zat = [&](int r, int q) -> T {  // z(v) at (r, q), as the pair's rows form it
+        const int64_t o = (int64_t)r * W + q;
+        const T up = r > 0 ? V0[o - W] : T(0);
+        const T left = q > 0 ? V1[o - 1] : T(0);
+        return D[o] + wh0 * (V0[o] - up) + wh1 * (V1[o] - left);
+    };
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(p / W), q = (int)(p % W);
+        const T z = zat(r, q);
+        const T g0 = r + 1 < H ? wh0 * (zat(r + 1, q) - z) : T(0);
+        const T g1 = q + 1 < W ? wh1 * (zat(r, q + 1) - z) : T(0);
+        const T cv0 = V0[p] + tau * g0;
+        const T cv1 = V1[p] + tau * g1;
+        const T nn = cv0 * cv0 + cv1 * cv1;
+        const T rp = pixel_radius<T, ALPHA>(rad, bnd, AL, p);
+        const T sc = nn > rp * rp ? rp * rsqrt_t(nn) : T(1);
+        UO0[p] = cv0 * sc;
+        UO1[p] = cv1 * sc;
+    }
+}
+
+__global__ void iso2d_redo_state(IsoState *st, int64_t B) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < B && st[i].redo) {
+        st[i].fin_par ^= 1;
+        st[i].redo = 0;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1506,10 +1560,6 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_ragged_pair_kernel(co
     const RagSlot sl = slots[b];
     const IsoState st = bf.st[b];
     if (st.status != kLive || ragged_pair_kind(st, sl) != (GAP2 ? 1 : 0)) return;
-    if (GAP2 && !bf.U[2]) {
-        if (threadIdx.x == 0) atomicExch(bf.err, 3);
-        return;
-    }
     const IsoImage im = bf.img[b];
     const int pin = st.fin_par, pout = pin ^ 1;
     PairTile<T> p;
@@ -1519,7 +1569,6 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_ragged_pair_kernel(co
     p.AL = nullptr;
     p.UO0 = static_cast<T *>(bf.U[pout]) + 2 * sl.off;
     p.VO0 = static_cast<T *>(bf.V[pout]) + 2 * sl.off;
-    p.UM0 = GAP2 ? static_cast<T *>(bf.U[2]) + 2 * sl.off : nullptr;
     p.N = (int64_t)sl.H * sl.W;
     p.H = sl.H;
     p.W = sl.W;
@@ -1552,9 +1601,13 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_ragged_pair_kernel(co
     IsoState s2 = st;
     control(s2, im, sl.max_iter, false, false, 0.0, 0.0, pin, bf.live);
     if (GAP2) {
-        // the check is at u' (in U[2]); the update to u'' (in pout) stands unless it passes
-        control(s2, im, sl.max_iter, true, true, gap, dot, 2, bf.live);
-        if (s2.status == kLive) s2.fin_par = pout;
+        // the check is at u'; the update to u'' (in pout) stands unless it
+        // passes, and then the final u is u', formed again from pin
+        control(s2, im, sl.max_iter, true, true, gap, dot, pin, bf.live);
+        if (s2.status != kLive) {
+            s2.redo = 1;
+            s2.redo_vsel = st.vsel;
+        }
     } else {
         control(s2, im, sl.max_iter, false, false, 0.0, 0.0, pin, bf.live);
     }
@@ -2573,7 +2626,7 @@ cudaError_t iso_ragged_step(int dtype, int vec, const RagItem *items, const int 
                             const RagSlot *slots, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
     if (grid <= 0) return cudaSuccess;
     if (dtype == 1) {
-        const bool pairs = iso_ragged_pairs(dtype, vec) && bf.U[2];
+        const bool pairs = iso_ragged_pairs(dtype, vec);
         if (vec == 4) launch_ragged_t<float, 4>(items, n_items, grid, slots, c, bf, s, pairs);
         else launch_ragged_t<float, 1>(items, n_items, grid, slots, c, bf, s, false);
     } else {
@@ -2676,6 +2729,20 @@ bool iso_pair_ok(const Geometry &g, const StepShape &sh, int max_part) {
 
 cudaError_t iso_live_list(const IsoState *st, int64_t B, int *lmap, int *lcnt, cudaStream_t s) {
     live_list_kernel<<<1, 1024, 0, s>>>(st, B, lmap, lcnt);
+    return cudaGetLastError();
+}
+
+cudaError_t iso_redo(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
+    if (g.k != 2 || g.B <= 0 || g.N <= 0) return cudaSuccess;
+    const dim3 grid((unsigned)std::min<int64_t>((g.N + 255) / 256, 1024), (unsigned)g.B);
+    if (dtype == 1) {
+        if (c.has_alpha) iso2d_redo_kernel<float, true><<<grid, 256, 0, s>>>(g, c, bf);
+        else iso2d_redo_kernel<float, false><<<grid, 256, 0, s>>>(g, c, bf);
+    } else {
+        if (c.has_alpha) iso2d_redo_kernel<double, true><<<grid, 256, 0, s>>>(g, c, bf);
+        else iso2d_redo_kernel<double, false><<<grid, 256, 0, s>>>(g, c, bf);
+    }
+    iso2d_redo_state<<<(unsigned)((g.B + 127) / 128), 128, 0, s>>>(bf.st, g.B);
     return cudaGetLastError();
 }
 

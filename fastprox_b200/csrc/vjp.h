@@ -56,7 +56,7 @@ struct CgState {
 struct VjpBuffers {
     // the forward's point
     const void *d = nullptr;
-    const void *U[3] = {nullptr, nullptr, nullptr};  // the forward's buffers, indexed by its fin_par
+    const void *U[2] = {nullptr, nullptr};  // the forward's buffers, indexed by its fin_par
     const IsoImage *img = nullptr;
     const IsoState *st = nullptr;
     const void *alpha = nullptr;

@@ -42,7 +42,6 @@ struct fp_workspace {
     // device memory
     void *d = nullptr, *stage = nullptr, *dual = nullptr, *spatial = nullptr;
     void *U[2] = {nullptr, nullptr}, *V[2] = {nullptr, nullptr};
-    void *U2 = nullptr;  // the first iterate of a pair launch with the check (iso 2D, when pairs apply)
     fpb::IsoImage *img = nullptr;
     fpb::IsoState *st = nullptr;
     // anisotropic TV: per-image state, the polish's scratch, FDPG-3's scratch

@@ -108,7 +108,7 @@ def serve_stream(reqs, src, budget_bytes=120e9, workers=16, steps=8):
     main = torch.cuda.Stream()
     # worker threads use the device while the batch runs: plain launches
     batch = RaggedBatch(max_images=512, max_pixels=arena_px, graphs=False, stream=main.cuda_stream)
-    arena_bytes = arena_px * 52  # d 4, u and v ping-pong 32, u' of checked pairs 8, dual 8
+    arena_bytes = arena_px * 44  # d 4, u and v ping-pong 32, dual 8
     used = arena_bytes
     lock = threading.Lock()
     streams = [torch.cuda.Stream() for _ in range(workers)]
