@@ -53,7 +53,9 @@ def _run(i):
         dual = info0.dual
     z, info = op.solve(xt, steps, tol=tol, max_iter=max_iter, warm=warm, dual=dual)
     torch.cuda.synchronize()
-    return z.cpu().numpy(), np.asarray(info.image_iters), np.asarray(info.gaps)
+    # the dual too: where a checked pair passed, its first iterate is formed again
+    q = info.dual.cpu().numpy() if hasattr(info.dual, "cpu") else np.asarray(info.dual)
+    return z.cpu().numpy(), np.asarray(info.image_iters), np.asarray(info.gaps), q
 
 
 @pytest.mark.gpu
@@ -65,18 +67,19 @@ def test_pairs_match_single_steps(cuda, tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     ref = np.load(out)
     for i in range(len(CASES)):
-        z, iters, gaps = _run(i)
+        z, iters, gaps, q = _run(i)
         assert np.array_equal(iters, ref[f"it{i}"]), (i, iters, ref[f"it{i}"])
         assert np.array_equal(z, ref[f"z{i}"]), (i, np.abs(z - ref[f"z{i}"]).max())
         assert np.array_equal(gaps, ref[f"g{i}"]), (i, gaps, ref[f"g{i}"])
+        assert np.array_equal(q, ref[f"q{i}"]), (i, np.abs(q - ref[f"q{i}"]).max())
 
 
 if __name__ == "__main__":  # the single-step run (FASTPROX_B200_PAIRS=0 in the environment)
     sys.path.insert(0, str(ROOT))
     res = {}
     for i in range(len(CASES)):
-        z, iters, gaps = _run(i)
-        res[f"z{i}"], res[f"it{i}"], res[f"g{i}"] = z, iters, gaps
+        z, iters, gaps, q = _run(i)
+        res[f"z{i}"], res[f"it{i}"], res[f"g{i}"], res[f"q{i}"] = z, iters, gaps, q
     np.savez(sys.argv[1], **res)
 
 
