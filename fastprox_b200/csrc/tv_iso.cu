@@ -2685,7 +2685,11 @@ StepShape iso_pick_shape(int dtype, const Geometry &g, int rows_hint, int bx_hin
         sh.kind = 5;
         sh.bx = k3TX * k3TY;
         const int64_t xt = (g.L[2] + k3TX - 1) / k3TX, yt = (g.L[1] + k3TY - 1) / k3TY;
-        int64_t rows = rows_hint > 0 ? rows_hint : 8;
+        // 16 slices per block (62.4 volumes/s on 8 x 128^3 against 59.8 at 8,
+        // 62.0 at 32), fewer while a launch would have too few blocks to
+        // spread over the SMs (small volumes)
+        int64_t rows = rows_hint > 0 ? rows_hint : 16;
+        while (rows_hint <= 0 && rows > 4 && xt * yt * ((g.L[0] + rows - 1) / rows) * g.B < tail_blocks()) rows /= 2;
         while (xt * yt * ((g.L[0] + rows - 1) / rows) > 4096) rows *= 2;
         sh.rows = (int)rows;
         sh.gx = (int)xt;
