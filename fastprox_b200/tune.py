@@ -5,7 +5,9 @@ batch and cached per shape class (in-process, and in
 ~/.cache/fastprox_b200/tune.json when that directory is writable). Longer
 tuning solves (48 iterations) with chunks of 1 and 2 steps were measured and
 not kept: they chose 2 steps, 1034 images/s on the uneven batch against 1057
-with the 4 steps these choose.
+with the 4 steps these choose; 64-row tiles were chosen when offered and ran
+935 images/s against 1084 at 32 (short solves favour tiles that long ones,
+with most images retired, cannot fill the SMs with).
 
 A tuning solve runs 16 iterations (tol 0) of every image with each
 candidate; the choice changes how work is tiled and how often the host
