@@ -18,7 +18,13 @@ bytes per launch / its event-timed launch duration) and of the whole call
 measured copy bandwidth; ``cpu_baseline`` the reference C library on the host cores.
 ``--impl reference`` times the reference's own CPU implementation (its C
 library, built from its sources into oracle/_ref) on a bounded sample.
-Multi-GPU: replicas (each rank its own batch, no data-path collective).
+``parity`` compares the images the CPU leg solved with the GPU's results for
+the same images (relative 2-norm error, largest entry error against
+1 + max|x|, iteration counts), and states the error of both against the
+reference run in float64 to gap 1e-12 on one image, beside the GPU's certified
+error for it.
+Multi-GPU: replicas (each rank its own batch, no data-path collective);
+``--gpus N`` without a launcher's environment starts the N ranks itself.
 """
 
 from __future__ import annotations
@@ -27,6 +33,7 @@ import argparse
 import json
 import os
 import pathlib
+import socket
 import statistics
 import subprocess
 import sys
@@ -49,6 +56,20 @@ GAMMAS = (0.05, 0.1, 0.2)
 TOL, MAX_ITER = 1e-6, 20000
 BYTES_PER_PIXEL_ITER = 40  # d 4 + u 8 + v 8 in, u 8 + v 8 out, alpha 4 (fp32)
 WORKLOAD = "tv_iso 2D, 64 x 512^2 fp32 phantom+noise(0.1), pixel weights U[0.5,1.5], gamma {0.05,0.1,0.2}, gap<=1e-6"
+
+
+def launch_replicas(n):
+    """Re-runs this script as n ranks on one node (torch.distributed.run, one
+    process per GPU, rendezvous on 127.0.0.1) with the same arguments; rank 0
+    prints the line. Returns the launcher's exit status."""
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes", "1", "--nproc-per-node", str(n),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(pathlib.Path(__file__).resolve()),
+           *sys.argv[1:]]
+    env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "1"))
+    return subprocess.run(cmd, env=env).returncode
 
 
 def reduce_max_time(t, dist, device):
@@ -160,14 +181,39 @@ def run_reference_arm(args):
         if i >= args.warmup:
             vals.append(v)
     value = statistics.median(vals)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     line = {"metric": "TV-prox images/s at gap<=1e-6 (512^2 fp32)", "value": value, "unit": "images/s",
-            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 3 / value * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": value, "unit": "images/s", "cores": threads, "kind": "reference",
                              "sample": "3 of the 64 images per step (one per gamma), reference fp_prox_steps"},
             "e2e": {"value": value, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def _nrel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def parity(x, alpha, steps, z_gpu, iters_gpu, zerr_gpu, r):
+    """The GPU's results on the images the reference solved (r: the CPU
+    leg's result on the first len(r.iters) images), and the error of both
+    against the reference in float64 at gap 1e-12 on image 0."""
+    from oracle import ref_capi
+    n = len(r.iters)
+    rel = [_nrel(z_gpu[i], r.z[i]) for i in range(n)]
+    emax = float(np.abs(z_gpu[:n].astype(np.float64) - r.z).max() / (1 + np.abs(x[:n]).max()))
+    r64 = ref_capi.solve(x[:1].astype(np.float64), float(steps[0]), iso=True, k=2, spatial=alpha, tol=1e-12,
+                         max_iter=200000)
+    return {"images": n, "gamma": [float(g) for g in steps[:n]], "max_rel_err": max(rel),
+            "rel_err": rel, "max_entry_err": emax,
+            "iters_gpu": [int(i) for i in iters_gpu[:n]], "iters_reference": [int(i) for i in r.iters],
+            "iters_equal": bool(np.array_equal(iters_gpu[:n], r.iters)),
+            "fp64_1e12": {"image": 0, "iters": int(r64.iters[0]), "err_gpu_f32": _nrel(z_gpu[0], r64.z[0]),
+                          "err_reference_f32_input": _nrel(r.z[0], r64.z[0]), "zerr_gpu": float(zerr_gpu[0])}}
 
 
 def profile_case(kind="iso"):
@@ -241,6 +287,8 @@ def main():
         from fastprox_b200 import workloads
         print(json.dumps(getattr(workloads, args.workload)(args)))
         return
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_replicas(args.gpus))
     if args.impl == "reference":
         run_reference_arm(args)
         return
@@ -332,14 +380,16 @@ def main():
     kernel_bytes = 2 * BYTES_PER_PIXEL_ITER * B * H * W  # two iterations over the batch
     achieved_kernel = kernel_bytes / (kernel_us * 1e-6) / 1e9 if kn.value else None
     cpu = None
+    par = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             from oracle import ref_capi
             if ref_capi.available():
-                v, threads, _ = cpu_reference(x, alpha, steps, 3)
+                v, threads, r = cpu_reference(x, alpha, steps, 3)
                 cpu = {"value": v, "unit": "images/s", "cores": threads, "kind": "reference",
                        "sample": "3 of the 64 images (gamma 0.05, 0.1, 0.2), reference C fp_prox_steps, "
                                  "all host threads"}
+                par = parity(x, alpha, steps, out.cpu().numpy(), info.image_iters, info.zerr, r)
         except Exception as e:  # the baseline is reported, not required
             cpu = {"value": None, "unit": "images/s", "cores": None, "kind": "reference", "sample": f"failed: {e}"}
     if rank == 0:
@@ -360,8 +410,11 @@ def main():
                          "kernel_us": kernel_us, "kernel_launches_timed": int(kn.value),
                          "algorithmic_bytes_per_launch": kernel_bytes, "bytes_per_pixel_iter": BYTES_PER_PIXEL_ITER,
                          "traffic": PAIR_TRAFFIC,
+                         "dram_achieved": PAIR_TRAFFIC / (kernel_us * 1e-6) / 1e9 if kn.value else None,
+                         "dram_frac": PAIR_TRAFFIC / (kernel_us * 1e-6) / 1e9 / peak if kn.value else None,
                          "achieved_whole_call": achieved, "frac_whole_call": achieved / peak},
             "cpu_baseline": cpu,
+            "parity": par,
             "e2e": {"value": e2e, "unit": "images/s", "h2d_bytes_per_step": int(x.nbytes),
                     "d2h_bytes_per_step": int(x.nbytes)},
             "gpu_launches": int(launches),

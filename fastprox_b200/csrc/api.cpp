@@ -510,20 +510,13 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
         }
     }
     // per-image state, partials and tickets; launch shape (tuning hints from
-    // the environment: FASTPROX_B200_ROWS, FASTPROX_B200_BX, FASTPROX_B200_VEC)
+    // the environment: FASTPROX_B200_ROWS, FASTPROX_B200_BX, FASTPROX_B200_KIND=1 for the generic step)
     auto env_int = [](const char *n) {
         const char *v = std::getenv(n);
         return v ? std::atoi(v) : 0;
     };
     ws->shape_ = iso_pick_shape(x.dtype, g, env_int("FASTPROX_B200_ROWS"), env_int("FASTPROX_B200_BX"),
                                 env_int("FASTPROX_B200_KIND"));
-    if (const int vh = env_int("FASTPROX_B200_VEC")) {
-        if (ws->shape_.kind == 0 && vh > 0 && vh <= ws->shape_.vec && g.L[1] % vh == 0) {
-            const int64_t cols = (g.L[1] + vh - 1) / vh;
-            ws->shape_.vec = vh;
-            ws->shape_.gx = (int)((cols + ws->shape_.bx - 1) / ws->shape_.bx);
-        }
-    }
     if (const int ch = env_int("FASTPROX_B200_CHUNK")) ws->chunk = ch;
     ws->max_part = std::max(iso_setup_blocks(g), ws->shape_.gx * ws->shape_.gy);
     ws->max_part = std::max(ws->max_part, 4096);

@@ -375,193 +375,12 @@ int64_t tail_blocks() {
 }
 
 // ---------------------------------------------------------------------------
-// The 2D row-marching step: a warp spans 32 * VEC consecutive columns, a
-// block BX * VEC of them, and each thread walks down `rows` rows keeping the
+// The lean 2D step: a warp spans 32 * VEC consecutive columns, a block
+// BX * VEC of them, and each thread walks down `rows` rows keeping the
 // current and next rows of z, u and v in registers, so every array is read
 // from HBM once per iteration (36 B per pixel in FP32: d, u, v in; u, v out).
-// Horizontal neighbours come from the next lane by shuffle; lane 31 reads
-// the first column of the next warp's span itself.
-// ---------------------------------------------------------------------------
-
-template <class T, int VEC>
-struct Row {
-    T v[VEC];
-};
-
-template <class T, int VEC, bool ALPHA>
-__global__ void __launch_bounds__(256) iso2d_march_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
-    __shared__ double sh[32];
-    __shared__ int flag;
-    const int b = step_image(bf, blockIdx.z);
-    if (b < 0) return;
-    const IsoState st = bf.st[b];
-    if (st.status != kLive) return;
-    const IsoImage im = bf.img[b];
-    const int64_t H = A.g.L[0], W = A.g.L[1], N = A.g.N;
-    const int it = st.it;
-    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == A.max_iter)) || (it == 0 && st.warm);
-    const bool do_upd = it < A.max_iter;
-    const bool test = do_upd && (it & 3) == 0;
-    const bool zin = st.zero_in != 0;
-    const int pin = A.par, pout = A.par ^ 1;
-    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
-    const T *U0 = static_cast<const T *>(bf.U[pin]) + (int64_t)b * 2 * N;
-    const T *U1 = U0 + N;
-    const T *V0 = st.vsel ? U0 : static_cast<const T *>(bf.V[pin]) + (int64_t)b * 2 * N;
-    const T *V1 = V0 + N;
-    T *UO0 = static_cast<T *>(bf.U[pout]) + (int64_t)b * 2 * N;
-    T *UO1 = UO0 + N;
-    T *VO0 = static_cast<T *>(bf.V[pout]) + (int64_t)b * 2 * N;
-    T *VO1 = VO0 + N;
-    const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
-    const T wh0 = (T)c.wh[0], wh1 = (T)c.wh[1], tau = (T)c.tau, beta = (T)st.beta;
-    const T rad = (T)im.radius, bnd = (T)im.bound;
-    const int lane = threadIdx.x & 31;
-    const int64_t cb = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * VEC;
-    const bool colok = cb < W;
-    const int64_t r0 = (int64_t)blockIdx.y * A.rows;
-    const int64_t r1 = min(H, r0 + (int64_t)A.rows);
-
-    auto LD = [&](const T *P, int64_t r, bool zero, T(&o)[VEC]) {
-        if (zero || r < 0 || r >= H || !colok) {
-#pragma unroll
-            for (int j = 0; j < VEC; ++j) o[j] = T(0);
-        } else {
-            load_pack<T, VEC>(P + r * W + cb, o);
-        }
-    };
-    auto LS = [&](const T *P, int64_t r, int64_t col, bool zero) -> T {
-        if (zero || r < 0 || r >= H || col < 0 || col >= W) return T(0);
-        return P[r * W + col];
-    };
-    // z at (r, col) from d and a dual field (P0, P1), for one point.
-    auto zpoint = [&](const T *P0, const T *P1, int64_t r, int64_t col, T left1) -> T {
-        const T dd = LS(D, r, col, false);
-        const T a0 = LS(P0, r, col, zin), a0p = LS(P0, r - 1, col, zin);
-        const T a1 = LS(P1, r, col, zin);
-        return dd + wh0 * (a0 - a0p) + wh1 * (a1 - left1);
-    };
-    // z on a row: d + wh0 (p0 - p0prev) + wh1 (p1 - p1 shifted right by one)
-    auto zrow = [&](const T(&dd)[VEC], const T(&p0)[VEC], const T(&p0p)[VEC], const T(&p1)[VEC], T p1l,
-                    T(&z)[VEC]) {
-#pragma unroll
-        for (int j = 0; j < VEC; ++j) {
-            const T left = j == 0 ? p1l : p1[j - 1];
-            z[j] = dd[j] + wh0 * (p0[j] - p0p[j]) + wh1 * (p1[j] - left);
-        }
-    };
-
-    T v0c[VEC], v1c[VEC], u0c[VEC], u1c[VEC], zc[VEC], zuc[VEC];
-    {
-        T v0p[VEC], dc[VEC];
-        LD(V0, r0 - 1, zin, v0p);
-        LD(V0, r0, zin, v0c);
-        LD(V1, r0, zin, v1c);
-        LD(D, r0, false, dc);
-        zrow(dc, v0c, v0p, v1c, LS(V1, r0, cb - 1, zin), zc);
-        LD(U0, r0, zin, u0c);
-        LD(U1, r0, zin, u1c);
-        if (do_gap) {
-            T u0p[VEC];
-            LD(U0, r0 - 1, zin, u0p);
-            zrow(dc, u0c, u0p, u1c, LS(U1, r0, cb - 1, zin), zuc);
-        } else {
-#pragma unroll
-            for (int j = 0; j < VEC; ++j) zuc[j] = T(0);
-        }
-    }
-    double gap_acc = 0.0, dot_acc = 0.0;
-    for (int64_t i = r0; i < r1; ++i) {
-        const bool hasn = i + 1 < H;
-        T dn[VEC], v0n[VEC], v1n[VEC], u0n[VEC], u1n[VEC], zn[VEC], zun[VEC];
-        LD(D, i + 1, false, dn);
-        LD(V0, i + 1, zin, v0n);
-        LD(V1, i + 1, zin, v1n);
-        LD(U0, i + 1, zin, u0n);
-        LD(U1, i + 1, zin, u1n);
-        T al[VEC];
-        if (ALPHA) {
-            if (colok) load_pack<T, VEC>(AL + i * W + cb, al);
-            else
-#pragma unroll
-                for (int j = 0; j < VEC; ++j) al[j] = T(0);
-        }
-        zrow(dn, v0n, v0c, v1n, LS(V1, i + 1, cb - 1, zin), zn);
-        // right neighbour of the last column
-        T zr = __shfl_down_sync(0xffffffffu, zc[0], 1);
-        if (lane == 31 && cb + VEC < W) zr = zpoint(V0, V1, i, cb + VEC, v1c[VEC - 1]);
-        T zur = T(0);
-        if (do_gap) {
-            zrow(dn, u0n, u0c, u1n, LS(U1, i + 1, cb - 1, zin), zun);
-            zur = __shfl_down_sync(0xffffffffu, zuc[0], 1);
-            if (lane == 31 && cb + VEC < W) zur = zpoint(U0, U1, i, cb + VEC, u1c[VEC - 1]);
-        }
-        T uo0[VEC], uo1[VEC], vo0[VEC], vo1[VEC];
-#pragma unroll
-        for (int j = 0; j < VEC; ++j) {
-            const int64_t col = cb + j;
-            const bool hasr = col + 1 < W;
-            const T zright = j + 1 < VEC ? zc[j + 1] : zr;
-            const T g0 = hasn ? wh0 * (zn[j] - zc[j]) : T(0);
-            const T g1 = hasr ? wh1 * (zright - zc[j]) : T(0);
-            const T cv0 = wh0 != T(0) ? v0c[j] + tau * g0 : T(0);
-            const T cv1 = wh1 != T(0) ? v1c[j] + tau * g1 : T(0);
-            const T nr = sqrt_t(cv0 * cv0 + cv1 * cv1);
-            T rp = rad;
-            if (ALPHA) rp = al[j] == T(0) ? T(0) : (rad * al[j] <= bnd ? rad * al[j] : bnd);
-            const T sc = nr > rp ? rp / nr : T(1);
-            const T un0 = cv0 * sc, un1 = cv1 * sc;
-            if (test && colok)
-                dot_acc += (double)((v0c[j] - un0) * (un0 - u0c[j])) + (double)((v1c[j] - un1) * (un1 - u1c[j]));
-            vo0[j] = un0 + beta * (un0 - u0c[j]);
-            vo1[j] = un1 + beta * (un1 - u1c[j]);
-            uo0[j] = un0;
-            uo1[j] = un1;
-            if (do_gap && colok) {
-                const T zuright = j + 1 < VEC ? zuc[j + 1] : zur;
-                const double gu0 = hasn ? (double)(wh0 * (zun[j] - zuc[j])) : 0.0;
-                const double gu1 = hasr ? (double)(wh1 * (zuright - zuc[j])) : 0.0;
-                gap_acc += (double)rp * sqrt(gu0 * gu0 + gu1 * gu1) - (gu0 * (double)u0c[j] + gu1 * (double)u1c[j]);
-            }
-        }
-        if (do_upd && colok) {
-            store_pack<T, VEC>(UO0 + i * W + cb, uo0);
-            store_pack<T, VEC>(UO1 + i * W + cb, uo1);
-            store_pack<T, VEC>(VO0 + i * W + cb, vo0);
-            store_pack<T, VEC>(VO1 + i * W + cb, vo1);
-        }
-#pragma unroll
-        for (int j = 0; j < VEC; ++j) {
-            v0c[j] = v0n[j];
-            v1c[j] = v1n[j];
-            u0c[j] = u0n[j];
-            u1c[j] = u1n[j];
-            zc[j] = zn[j];
-            zuc[j] = do_gap ? zun[j] : T(0);
-        }
-    }
-    const unsigned nblk = gridDim.x * gridDim.y;
-    const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
-    const double gsum = (do_gap ? block_sum(gap_acc, sh) : 0.0);
-    const double dsum = (test ? block_sum(dot_acc, sh) : 0.0);
-    double *part = bf.part + (int64_t)b * bf.max_part * 2;
-    if (threadIdx.x == 0) {
-        part[blk * 2 + 0] = gsum;
-        part[blk * 2 + 1] = dsum;
-    }
-    if (!arrive_last(bf.ticket + b, nblk, &flag)) return;
-    const double gap = do_gap ? sum_partials(part, nblk, 2, 0, sh) : 0.0;
-    const double dot = test ? sum_partials(part, nblk, 2, 1, sh) : 0.0;
-    if (threadIdx.x != 0) return;
-    bf.ticket[b] = 0;
-    IsoState s2 = st;
-    control(s2, im, A.max_iter, do_gap, test, gap, dot, pin, bf.live);
-    bf.st[b] = s2;
-}
-
-// ---------------------------------------------------------------------------
-// The lean 2D step: the row-marching scheme above with the per-pixel work
-// cut to the arithmetic of the iteration. Offsets are 32-bit within an image
+// Horizontal neighbours come from the next lane by shuffle. The per-pixel
+// work is the arithmetic of the iteration. Offsets are 32-bit within an image
 // (images have fewer than 2^31 pixels), row pointers advance by W, the gap
 // and the cold start are compile-time variants (one per block: every live
 // image of a launch shares its branch), the projection multiplies by a
@@ -1615,285 +1434,6 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_ragged_pair_kernel(co
 }
 
 // ---------------------------------------------------------------------------
-// The 2D step with a TMA row pipeline (sm_100a): one elected thread streams
-// whole row segments of d, v, u (and the pixel weights) from HBM into a ring
-// of shared-memory slots with bulk asynchronous copies (cp.async.bulk,
-// completion counted on an mbarrier per slot), several rows ahead of the
-// rows being computed, so the loads in flight are not bounded by registers.
-// The threads compute z for the next row into shared memory, then update the
-// current row with every neighbour read from shared memory, and store u and
-// v straight to HBM. Same arithmetic and control as the kernels above.
-//
-// A block owns a span of SPAN = blockDim.x * VEC columns (plus a halo of one
-// 16-byte vector each side) and walks `rows` rows. Slot s holds row r with
-// (r - r0 + 1) % SLOTS == s; the row a slot holds is known to every thread.
-// Rows outside the image are never copied: they read as zeros.
-// ---------------------------------------------------------------------------
-
-constexpr int kSlots = 4;
-constexpr int kArrays = 6;  // d, v0, v1, u0, u1, alpha
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_addr(dst)),
-        "l"(src), "r"(bytes), "r"(smem_addr(bar))
-        : "memory");
-}
-
-// Waits for the phase of parity `par` of a slot's barrier; false after
-// about a second of polling (the caller then records an error).
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned par) {
-    const uint32_t a = smem_addr(bar);
-    for (int i = 0; i < (1 << 22); ++i) {
-        uint32_t ok;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-            : "=r"(ok)
-            : "r"(a), "r"(par)
-            : "memory");
-        if (ok) return true;
-        if (i > 16) __nanosleep(64);
-    }
-    return false;
-}
-
-template <class T, int VEC, bool ALPHA>
-__global__ void __launch_bounds__(128) iso2d_tma_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ uint64_t bars[kSlots];
-    __shared__ double sh[32];
-    __shared__ int flag;
-    const int b = step_image(bf, blockIdx.z);
-    if (b < 0) return;
-    const IsoState st = bf.st[b];
-    if (st.status != kLive) return;
-    const IsoImage im = bf.img[b];
-    const int64_t H = A.g.L[0], W = A.g.L[1], N = A.g.N;
-    const int it = st.it;
-    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == A.max_iter)) || (it == 0 && st.warm);
-    const bool do_upd = it < A.max_iter;
-    const bool test = do_upd && (it & 3) == 0;
-    const bool zin = st.zero_in != 0;
-    const bool vsel = st.vsel != 0;
-    const int pin = A.par, pout = A.par ^ 1;
-    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
-    const T *U0 = static_cast<const T *>(bf.U[pin]) + (int64_t)b * 2 * N;
-    const T *V0 = static_cast<const T *>(bf.V[pin]) + (int64_t)b * 2 * N;
-    T *UO0 = static_cast<T *>(bf.U[pout]) + (int64_t)b * 2 * N;
-    T *VO0 = static_cast<T *>(bf.V[pout]) + (int64_t)b * 2 * N;
-    const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
-    const T wh0 = (T)c.wh[0], wh1 = (T)c.wh[1], tau = (T)c.tau, beta = (T)st.beta;
-    const T rad = (T)im.radius, bnd = (T)im.bound;
-
-    constexpr int HALO = 16 / sizeof(T);
-    const int span = blockDim.x * VEC;
-    const int RW = span + 2 * HALO;                    // row width in shared memory (elements)
-    const int64_t cs = (int64_t)blockIdx.x * span;     // first column of the span
-    const int64_t c0 = cs - HALO > 0 ? cs - HALO : 0;  // loaded columns [c0, c1)
-    const int64_t c1 = cs + span + HALO < W ? cs + span + HALO : W;
-    const unsigned seg_bytes = (unsigned)((c1 - c0) * (int64_t)sizeof(T));
-    const int soff = (int)(c0 - (cs - HALO));          // shared index of column c0
-    T *slots = reinterpret_cast<T *>(smem_raw);        // [kSlots][kArrays][RW]
-    T *zrow = slots + (size_t)kSlots * kArrays * RW;   // [2][RW] z of v, then [2][RW] z of u
-    const int64_t r0 = (int64_t)blockIdx.y * A.rows;
-    const int64_t r1 = min(H, r0 + (int64_t)A.rows);
-    const bool load_v = !zin && !vsel;
-    const bool load_u = !zin;
-    const unsigned row_bytes = seg_bytes * (1u + (load_v ? 2u : 0u) + (load_u ? 2u : 0u) + (ALPHA ? 1u : 0u));
-    const int tid = threadIdx.x;
-
-    auto slot_of = [&](int64_t r) { return (int)((r - r0 + 1) % kSlots); };
-    auto parity = [&](int64_t r) { return (unsigned)(((r - r0 + 1) / kSlots) & 1); };
-    auto arr = [&](int s, int a) { return slots + ((size_t)s * kArrays + a) * RW; };
-    // the shared row of array a (d 0, v0 1, v1 2, u0 3, u1 4, alpha 5) holding row r,
-    // or null where it reads as zeros (outside the image; u = v = 0 on a cold
-    // start; v = u after a restart)
-    auto row = [&](int64_t r, int a) -> const T * {
-        if (r < 0 || r >= H) return nullptr;
-        if ((a >= 1 && a <= 4) && zin) return nullptr;
-        if ((a == 1 || a == 2) && vsel) a += 2;
-        return arr(slot_of(r), a);
-    };
-    int64_t last_prod = r0 - 2;
-    auto produce = [&](int64_t r) {  // thread 0 only
-        const int s = slot_of(r);
-        uint64_t *bar = &bars[s];
-        last_prod = r;
-        if (r < 0 || r >= H) {
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-            return;
-        }
-        mbar_expect_tx(bar, row_bytes);
-        const int64_t g = r * W + c0;
-        bulk_load(arr(s, 0) + soff, D + g, seg_bytes, bar);
-        if (load_v) {
-            bulk_load(arr(s, 1) + soff, V0 + g, seg_bytes, bar);
-            bulk_load(arr(s, 2) + soff, V0 + N + g, seg_bytes, bar);
-        }
-        if (load_u) {
-            bulk_load(arr(s, 3) + soff, U0 + g, seg_bytes, bar);
-            bulk_load(arr(s, 4) + soff, U0 + N + g, seg_bytes, bar);
-        }
-        if (ALPHA) bulk_load(arr(s, 5) + soff, AL + g, seg_bytes, bar);
-    };
-    if (tid == 0) {
-        for (int i = 0; i < kSlots; ++i) mbar_init(&bars[i], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    if (tid == 0)
-        for (int64_t r = r0 - 1; r < r0 - 1 + kSlots && r <= r1; ++r) produce(r);
-
-    const int64_t cb = cs + (int64_t)tid * VEC;
-    const bool colok = cb < W;
-    const int ib = HALO + tid * VEC;  // shared index of column cb
-    auto ldv = [&](const T *p, T(&o)[VEC]) {
-        if (p && colok) load_pack<T, VEC>(p + ib, o);
-        else
-#pragma unroll
-            for (int j = 0; j < VEC; ++j) o[j] = T(0);
-    };
-    auto lds = [&](const T *p, int64_t col) -> T {  // one column, zero outside
-        if (!p || col < 0 || col >= W) return T(0);
-        return p[col - cs + HALO];
-    };
-    // z of a dual pair (p = 1: v, p = 3: u) on row r, for this thread's columns
-    // and (the last thread) the right halo column
-    auto zfill = [&](int64_t r, int p, T *zdst) {
-        if (r < 0 || r >= H) {
-#pragma unroll
-            for (int j = 0; j < VEC; ++j) zdst[ib + j] = T(0);
-            if (tid == blockDim.x - 1) zdst[HALO + span] = T(0);
-            return;
-        }
-        const T *dr = row(r, 0), *a0 = row(r, p), *a0p = row(r - 1, p), *a1 = row(r, p + 1);
-        T dd[VEC], x0[VEC], x0p[VEC], x1[VEC], z[VEC];
-        ldv(dr, dd);
-        ldv(a0, x0);
-        ldv(a0p, x0p);
-        ldv(a1, x1);
-        T left = lds(a1, cb - 1);
-#pragma unroll
-        for (int j = 0; j < VEC; ++j) {
-            z[j] = colok ? dd[j] + wh0 * (x0[j] - x0p[j]) + wh1 * (x1[j] - left) : T(0);
-            left = x1[j];
-        }
-        if (colok) store_pack<T, VEC>(zdst + ib, z);
-        else
-#pragma unroll
-            for (int j = 0; j < VEC; ++j) zdst[ib + j] = T(0);
-        if (tid == blockDim.x - 1) {
-            const int64_t col = cs + span;
-            zdst[HALO + span] = col < W ? lds(dr, col) + wh0 * (lds(a0, col) - lds(a0p, col)) +
-                                              wh1 * (lds(a1, col) - lds(a1, col - 1))
-                                        : T(0);
-        }
-    };
-    auto zv = [&](int64_t r) { return zrow + (size_t)(r & 1) * RW; };
-    auto zu = [&](int64_t r) { return zrow + (size_t)(2 + (r & 1)) * RW; };
-
-    bool ok = mbar_wait(&bars[slot_of(r0 - 1)], parity(r0 - 1));
-    ok = mbar_wait(&bars[slot_of(r0)], parity(r0)) && ok;
-    zfill(r0, 1, zv(r0));
-    if (do_gap) zfill(r0, 3, zu(r0));
-    double gap_acc = 0.0, dot_acc = 0.0;
-    for (int64_t i = r0; i < r1; ++i) {
-        ok = mbar_wait(&bars[slot_of(i + 1)], parity(i + 1)) && ok;
-        zfill(i + 1, 1, zv(i + 1));
-        if (do_gap) zfill(i + 1, 3, zu(i + 1));
-        ok = __syncthreads_and(ok) != 0;  // block-uniform from here
-        if (!ok) break;
-        if (colok) {
-            const T *zc = zv(i), *zn = zv(i + 1), *zuc = zu(i), *zun = zu(i + 1);
-            T v0[VEC], v1[VEC], u0[VEC], u1[VEC], al[VEC], zcv[VEC], znv[VEC];
-            ldv(row(i, 1), v0);
-            ldv(row(i, 2), v1);
-            ldv(row(i, 3), u0);
-            ldv(row(i, 4), u1);
-            if (ALPHA) ldv(row(i, 5), al);
-            load_pack<T, VEC>(zc + ib, zcv);
-            load_pack<T, VEC>(zn + ib, znv);
-            const T zright = zc[ib + VEC];
-            const bool hasn = i + 1 < H;
-            T uo0[VEC], uo1[VEC], vo0[VEC], vo1[VEC];
-#pragma unroll
-            for (int j = 0; j < VEC; ++j) {
-                const bool hasr = cb + j + 1 < W;
-                const T zr = j + 1 < VEC ? zcv[j + 1] : zright;
-                const T g0 = hasn ? wh0 * (znv[j] - zcv[j]) : T(0);
-                const T g1 = hasr ? wh1 * (zr - zcv[j]) : T(0);
-                const T cv0 = wh0 != T(0) ? v0[j] + tau * g0 : T(0);
-                const T cv1 = wh1 != T(0) ? v1[j] + tau * g1 : T(0);
-                const T nr = sqrt_t(cv0 * cv0 + cv1 * cv1);
-                T rp = rad;
-                if (ALPHA) rp = al[j] == T(0) ? T(0) : (rad * al[j] <= bnd ? rad * al[j] : bnd);
-                const T sc = nr > rp ? rp / nr : T(1);
-                const T un0 = cv0 * sc, un1 = cv1 * sc;
-                if (test) dot_acc += (double)((v0[j] - un0) * (un0 - u0[j])) + (double)((v1[j] - un1) * (un1 - u1[j]));
-                vo0[j] = un0 + beta * (un0 - u0[j]);
-                vo1[j] = un1 + beta * (un1 - u1[j]);
-                uo0[j] = un0;
-                uo1[j] = un1;
-                if (do_gap) {
-                    const T zur = j + 1 < VEC ? zuc[ib + j + 1] : zuc[ib + VEC];
-                    const double gu0 = hasn ? (double)(wh0 * (zun[ib + j] - zuc[ib + j])) : 0.0;
-                    const double gu1 = hasr ? (double)(wh1 * (zur - zuc[ib + j])) : 0.0;
-                    gap_acc += (double)rp * sqrt(gu0 * gu0 + gu1 * gu1) - (gu0 * (double)u0[j] + gu1 * (double)u1[j]);
-                }
-            }
-            if (do_upd) {
-                store_pack<T, VEC>(UO0 + i * W + cb, uo0);
-                store_pack<T, VEC>(UO0 + N + i * W + cb, uo1);
-                store_pack<T, VEC>(VO0 + i * W + cb, vo0);
-                store_pack<T, VEC>(VO0 + N + i * W + cb, vo1);
-            }
-        }
-        __syncthreads();  // rows i - 1 and i and z row i are free
-        if (tid == 0 && i + kSlots - 1 <= r1) produce(i + kSlots - 1);
-    }
-    if (!ok) {
-        // a copy never completed: record it, wait (bounded) for whatever this
-        // block still has in flight, and leave the image's state unchanged
-        if (tid == 0) {
-            atomicExch(bf.err, 1);
-            for (int64_t r = r0 - 1; r <= last_prod; ++r) mbar_wait(&bars[slot_of(r)], parity(r));
-        }
-        return;
-    }
-    const unsigned nblk = gridDim.x * gridDim.y;
-    const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
-    const double gsum = do_gap ? block_sum(gap_acc, sh) : 0.0;
-    const double dsum = test ? block_sum(dot_acc, sh) : 0.0;
-    double *part = bf.part + (int64_t)b * bf.max_part * 2;
-    if (threadIdx.x == 0) {
-        part[blk * 2 + 0] = gsum;
-        part[blk * 2 + 1] = dsum;
-    }
-    if (!arrive_last(bf.ticket + b, nblk, &flag)) return;
-    const double gap = do_gap ? sum_partials(part, nblk, 2, 0, sh) : 0.0;
-    const double dot = test ? sum_partials(part, nblk, 2, 1, sh) : 0.0;
-    if (threadIdx.x != 0) return;
-    bf.ticket[b] = 0;
-    IsoState s2 = st;
-    control(s2, im, A.max_iter, do_gap, test, gap, dot, pin, bf.live);
-    bf.st[b] = s2;
-}
-
-// ---------------------------------------------------------------------------
 // Generic step: one thread per pixel, 2D or 3D, any extents. Neighbours are
 // read through the caches.
 // ---------------------------------------------------------------------------
@@ -2505,27 +2045,6 @@ void launch_3d_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuf
     else launch_3d_v<T, ALPHA, false, false>(grid, A, c, bf, s);
 }
 
-template <class T, int VEC>
-void launch_march(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
-    const dim3 grid(sh.gx, sh.gy, (unsigned)A.nimg);
-    if (c.has_alpha) iso2d_march_kernel<T, VEC, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
-    else iso2d_march_kernel<T, VEC, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
-}
-
-template <class T, int VEC, bool ALPHA>
-void launch_tma(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
-    constexpr int HALO = 16 / sizeof(T);
-    const int RW = sh.bx * VEC + 2 * HALO;
-    const size_t smem = (size_t)(kSlots * kArrays + 4) * RW * sizeof(T);
-    static size_t configured = 0;
-    if (configured < smem) {
-        cudaFuncSetAttribute(iso2d_tma_kernel<T, VEC, ALPHA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = smem;
-    }
-    const dim3 grid(sh.gx, sh.gy, (unsigned)A.nimg);
-    iso2d_tma_kernel<T, VEC, ALPHA><<<grid, sh.bx, smem, s>>>(A, c, bf);
-}
-
 template <class T>
 cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh, int par,
                    int variant, int64_t nimg, cudaStream_t s) {
@@ -2561,14 +2080,6 @@ cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, co
         if (sh.vec == 4) launch_lean<T, 4>(sh2, A, c, bf, s, variant);
         else if (sh.vec == 2) launch_lean<T, 2>(sh2, A, c, bf, s, variant);
         else launch_lean<T, 1>(sh2, A, c, bf, s, variant);
-    } else if (sh.kind == 2) {
-        constexpr int V = 16 / sizeof(T);
-        if (c.has_alpha) launch_tma<T, V, true>(sh, A, c, bf, s);
-        else launch_tma<T, V, false>(sh, A, c, bf, s);
-    } else if (sh.kind == 0) {
-        if (sh.vec == 4) launch_march<T, 4>(sh, A, c, bf, s);
-        else if (sh.vec == 2) launch_march<T, 2>(sh, A, c, bf, s);
-        else launch_march<T, 1>(sh, A, c, bf, s);
     } else {
         const dim3 grid(sh.gx, (unsigned)nimg);
         if (g.k == 2) {
@@ -2651,21 +2162,8 @@ StepShape iso_pick_shape(int dtype, const Geometry &g, int rows_hint, int bx_hin
     StepShape sh;
     const int64_t W = g.k == 2 ? g.L[1] : 0;
     const int vmax = dtype == 1 ? 4 : 2;
-    const int vfull = dtype == 1 ? 4 : 2;  // one 16-byte vector per thread
-    if (g.k == 2 && W >= 32 && W % vfull == 0 && kind_hint == 2) {
-        // TMA row pipeline: spans of at most 512 columns (fp32), 128 threads
-        sh.kind = 2;
-        sh.vec = vfull;
-        const int64_t cols = W / vfull;
-        sh.bx = bx_hint > 0 ? bx_hint : (int)std::min<int64_t>(128, ((cols + 31) / 32) * 32);
-        sh.gx = (int)((cols + sh.bx - 1) / sh.bx);
-        const int64_t H = g.L[0];
-        int rows = rows_hint;
-        if (rows <= 0) rows = (int)std::max<int64_t>(8, std::min<int64_t>(32, H / 16));
-        sh.rows = rows;
-        sh.gy = (int)((H + rows - 1) / rows);
-    } else if (g.k == 2 && W >= 32 && kind_hint != 1) {
-        sh.kind = kind_hint == 3 ? 0 : 4;
+    if (g.k == 2 && W >= 32 && kind_hint != 1) {
+        sh.kind = 4;
         sh.vec = (W % vmax == 0) ? vmax : ((W % 2 == 0) ? 2 : 1);
         const int64_t cols = (W + sh.vec - 1) / sh.vec;
         int bx = bx_hint > 0 ? bx_hint : (int)std::min<int64_t>(128, ((cols + 31) / 32) * 32);
@@ -2811,10 +2309,8 @@ cudaError_t strided_copy(const void *src, int src_dtype, const int64_t *shape, c
 // ---------------------------------------------------------------------------
 // fp_b200_tv_iso_noalloc: the isotropic solve for callers that cannot
 // allocate device memory (see include/fastprox_b200.h). Its scratch is the
-// file-scope array below, resolved to a device address once per device.
+// file-scope array below, whose device address is looked up on every call.
 // ---------------------------------------------------------------------------
-
-#include <mutex>
 
 #include "../../include/fastprox_b200.h"
 
@@ -2823,7 +2319,13 @@ namespace {
 
 constexpr int64_t kNoAllocPixels = int64_t(1) << 20;  // batch x height x width at most
 constexpr int64_t kNoAllocImages = 64;                // batch at most
-constexpr int kNoAllocParts = 1024;                   // partial-sum slots per image
+// Partial-sum slots over all images of a call: enough for one slot per row
+// and column block of every image (the lean step's per-row sums, as fp_prox
+// uses them, so that the sums and the iterates are the same bits), and for
+// the set-up scans and the generic step's blocks: with batch x height x width
+// <= 2^20, batch x height x ceil(width / 128) <= 2^13 + 2^15 for rows of 32
+// or more, 64 x 1024 for narrower ones.
+constexpr int64_t kNoAllocPartSlots = int64_t(1) << 16;
 
 constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
@@ -2838,19 +2340,18 @@ constexpr size_t kOffImg = kOffDual + align256(2 * kNoAllocPixels * 4);
 constexpr size_t kOffSt = kOffImg + align256(kNoAllocImages * sizeof(IsoImage));
 constexpr size_t kOffGam = kOffSt + align256(kNoAllocImages * sizeof(IsoState));
 constexpr size_t kOffPart = kOffGam + align256(kNoAllocImages * sizeof(double));
-constexpr size_t kOffTicket = kOffPart + align256(kNoAllocImages * kNoAllocParts * 2 * sizeof(double));
+constexpr size_t kOffTicket = kOffPart + align256(kNoAllocPartSlots * 2 * sizeof(double));
 constexpr size_t kOffLive = kOffTicket + align256(kNoAllocImages * sizeof(unsigned));
 constexpr size_t kOffErr = kOffLive + 256;
 constexpr size_t kOffRes = kOffErr + 256;  // per image: gap (double), iters (int); then a flag word
 constexpr size_t kNoAllocBytes = kOffRes + align256(kNoAllocImages * (sizeof(double) + sizeof(int)) + 16);
 
-// Every GPU that loads this library holds this array (about 47 MB) until
-// the process exits.
+// About 48 MB. The CUDA runtime loads this file's kernels, and reserves this
+// array with them, on a device the first time anything of the file runs
+// there (lazy module loading): the first isotropic solve or call of the
+// entry point on that device. From then on the array stays reserved there
+// until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
-
-constexpr int kMaxDevices = 64;
-unsigned char *g_scratch_addr[kMaxDevices] = {};
-std::mutex g_scratch_mu;
 
 // Per-image results into the scratch: gap at the input's scale, iterations,
 // and flag bits (1: an image did not converge, 2: an image held an Inf).
@@ -2891,21 +2392,15 @@ extern "C" FP_API fp_status fp_b200_tv_iso_noalloc(const float *x, float *z, int
         return FP_ESHAPE;
     if (!std::isfinite(gamma) || gamma < 0.0 || !(gamma <= 0x1p960)) return FP_EPARAM;
     if (!(tol >= 0.0) || !std::isfinite(tol) || max_iter < 1) return FP_EPARAM;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FP_EDEVICE;
-    unsigned char *base = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_scratch_mu);
-        if (!g_scratch_addr[dev]) {
-            void *p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-                cudaGetLastError();
-                return FP_EDEVICE;
-            }
-            g_scratch_addr[dev] = static_cast<unsigned char *>(p);
-        }
-        base = g_scratch_addr[dev];
+    // The array's address on the current device, looked up on every call (no
+    // cached pointer can outlive a device reset); in host code the array's
+    // name is only a stand-in for it.
+    void *sym = nullptr;
+    if (cudaGetSymbolAddress(&sym, g_noalloc_scratch) != cudaSuccess || !sym) {
+        cudaGetLastError();
+        return FP_EDEVICE;
     }
+    unsigned char *base = static_cast<unsigned char *>(sym);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Geometry g{};
     g.k = 2;
@@ -2939,6 +2434,13 @@ extern "C" FP_API fp_status fp_b200_tv_iso_noalloc(const float *x, float *z, int
     c.alpha_stride = 0;
     c.alpha_max = 0.0;
     c.step_scale = 1.0;
+    // The step's shape and partial-sum slots as a workspace of this geometry
+    // has them (per-row sums of the lean 2D step), so the sums, the stopping
+    // decisions and the iterates are fp_prox's.
+    const StepShape sh = iso_pick_shape(FP_F32, g, 0, 0, 0);
+    int64_t max_part = std::max<int64_t>(iso_setup_blocks(g), (int64_t)sh.gx * sh.gy);
+    if (sh.kind == 4) max_part = std::max<int64_t>(max_part, (int64_t)sh.gx * height);
+    if (batch * max_part > kNoAllocPartSlots) return FP_ESHAPE;
     IsoBuffers bf;
     bf.d = base + kOffD;
     bf.U[0] = base + kOffU0;
@@ -2954,17 +2456,10 @@ extern "C" FP_API fp_status fp_b200_tv_iso_noalloc(const float *x, float *z, int
     bf.ticket = reinterpret_cast<unsigned *>(base + kOffTicket);
     bf.live = reinterpret_cast<int *>(base + kOffLive);
     bf.err = reinterpret_cast<int *>(base + kOffErr);
-    bf.max_part = kNoAllocParts;
+    bf.max_part = (int)max_part;
     double *rg = reinterpret_cast<double *>(base + kOffRes);
     int *ri = reinterpret_cast<int *>(base + kOffRes + kNoAllocImages * sizeof(double));
     int *rflags = ri + kNoAllocImages;
-    StepShape sh = iso_pick_shape(FP_F32, g, 0, 0, 0);
-    if (sh.gx * sh.gy > kNoAllocParts) {  // more rows per block keep the partials within their slots
-        const int per = kNoAllocParts / sh.gx;
-        sh.rows = (int)((height + per - 1) / per);
-        sh.gy = (int)((height + sh.rows - 1) / sh.rows);
-    }
-    if (sh.gx * sh.gy > kNoAllocParts || iso_setup_blocks(g) > kNoAllocParts) return FP_ESHAPE;
     // the scratch keeps the last call's contents: clear what must start at zero
     cudaError_t e = cudaMemsetAsync(bf.ticket, 0, (size_t)batch * sizeof(unsigned), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(bf.live, 0, sizeof(int), s);

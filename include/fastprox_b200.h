@@ -313,9 +313,17 @@ FP_API fp_status fp_b200_batch_stats(const fp_b200_batch *bt, int64_t *kernel_la
  * handler, or latency-bound code that may not call cudaMalloc because it can
  * synchronise the whole device. fp_prox needs a workspace, and creating one
  * allocates; this entry point takes its scratch from a fixed array inside the
- * library instead (about 47 MB, held on every GPU that loads the library until
- * the process exits). It calls no cudaMalloc, cudaFree or other allocating
- * routine.
+ * library instead (about 48 MB). It calls no cudaMalloc, cudaFree or other
+ * allocating routine.
+ *
+ * When the array is reserved: the CUDA runtime loads the library's isotropic
+ * kernels, and reserves the array with them, on a device the first time any
+ * of them runs there (lazy module loading): the first call of this entry
+ * point, or the first isotropic fp_prox, on that device. That first call can
+ * therefore fail with FP_EDEVICE when the device is out of memory. A caller
+ * that must never allocate makes one small call on each device it uses at
+ * start-up (before any stream capture); later calls reserve nothing more. The
+ * array then stays reserved on that device until the process exits.
  *
  * x and z: device pointers on the calling thread's current device to
  * contiguous (batch, height, width) float32 arrays; z may equal x. Unit axis
@@ -324,12 +332,13 @@ FP_API fp_status fp_b200_batch_stats(const fp_b200_batch *bt, int64_t *kernel_la
  * gaps, iters: host arrays of batch entries for the per-image duality gap and
  * iterations, or NULL. Limits: batch <= 64 and batch * height * width <= 2^20
  * (FP_ESHAPE beyond them). Returns FP_OK, FP_ENOTCONV, FP_EINVAL (an image
- * holding +-Inf), FP_EPARAM or FP_EDEVICE.
+ * holding +-Inf), FP_EPARAM or FP_EDEVICE. The results are fp_prox's for the
+ * same input (the same launch shapes and partial sums).
  *
  * Every call shares the one scratch array, which keeps the last call's
  * contents: calls that overlap on the GPU (from two host threads, or on two
- * streams) race and corrupt each other's results; serialise them. The first
- * call on each device looks up the array's device address. */
+ * streams) race and corrupt each other's results; serialise them. The
+ * array's device address is looked up on each call. */
 FP_API fp_status fp_b200_tv_iso_noalloc(const float *x, float *z, int64_t batch, int64_t height, int64_t width,
                                         double gamma, double tol, int max_iter, void *stream, double *gaps,
                                         int *iters);

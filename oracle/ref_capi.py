@@ -63,6 +63,8 @@ def lib():
                               C.POINTER(FpInfo)]
         L.fp_prox_steps.argtypes = [P, C.POINTER(FpArray), C.POINTER(FpArray), C.POINTER(FpArray),
                                     C.POINTER(FpOptions), P]
+        L.fp_prox_conj.argtypes = [P, C.c_double, C.POINTER(FpArray), C.POINTER(FpArray), C.POINTER(FpOptions), P,
+                                   C.POINTER(FpInfo)]
         L.fp_workspace_image_info.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_int),
                                               C.POINTER(C.c_double), C.c_int64]
         L.fp_workspace_get_dual.argtypes = [P, C.POINTER(FpArray)]
@@ -129,10 +131,11 @@ class Result:
 
 
 def solve(x, gamma, *, iso=True, k=2, w=None, spatial=None, tol=1e-6, max_iter=1000, threads=0,
-          steps=None, warm_dual=None, keep=False):
+          steps=None, warm_dual=None, keep=False, conj=False):
     """One reference call on x (batch over leading axes, images the last k).
 
-    ``gamma`` is one step, or ``steps`` one per image (``fp_prox_steps``).
+    ``gamma`` is one step, or ``steps`` one per image (``fp_prox_steps``);
+    with ``conj`` the call is ``fp_prox_conj`` and ``gamma`` its sigma.
     Returns a Result with z (x's dtype), per-image gaps/iters/zerrs and the
     dual (k, *x.shape) in float64, the reference's own form."""
     L = lib()
@@ -150,7 +153,10 @@ def solve(x, gamma, *, iso=True, k=2, w=None, spatial=None, tol=1e-6, max_iter=1
             _check(L.fp_workspace_set_dual(ws, da.ref()), "set_dual")
         z = np.empty_like(x)
         za = _Arr(z)
-        if steps is None:
+        if conj:
+            info = FpInfo()
+            st = L.fp_prox_conj(op, float(gamma), xa.ref(), za.ref(), C.byref(opt), ws, C.byref(info))
+        elif steps is None:
             info = FpInfo()
             st = L.fp_prox(op, float(gamma), xa.ref(), za.ref(), C.byref(opt), ws, C.byref(info))
         else:
@@ -164,9 +170,10 @@ def solve(x, gamma, *, iso=True, k=2, w=None, spatial=None, tol=1e-6, max_iter=1
         _check(L.fp_workspace_image_info(ws, gaps.ctypes.data_as(C.POINTER(C.c_double)),
                                          iters.ctypes.data_as(C.POINTER(C.c_int)),
                                          zerrs.ctypes.data_as(C.POINTER(C.c_double)), B), "image_info")
-        dual = np.empty((k,) + x.shape, np.float64)
-        dd = _Arr(dual)
-        _check(L.fp_workspace_get_dual(ws, dd.ref()), "get_dual")
+        dual = None
+        if not conj:  # the reference keeps no dual of a conjugate call
+            dual = np.empty((k,) + x.shape, np.float64)
+            _check(L.fp_workspace_get_dual(ws, _Arr(dual).ref()), "get_dual")
         res = Result(z, gaps, iters, zerrs, dual, st)
         if keep:
             res._ws, res._op = ws, op

@@ -42,3 +42,24 @@ def test_replica_inputs_differ_per_rank_but_are_seeded():
     a1 = synth.phantom(2, 32, 32, seed=1)
     assert not (a0 == a1).all()
     assert (synth.phantom(2, 32, 32, seed=1) == a1).all()
+
+
+def test_bench_gpus_flag_launches_the_ranks_itself():
+    """bench.py --gpus 2 outside a launcher starts two ranks (rendezvous on
+    127.0.0.1) and rank 0 alone prints one line, for the world of two. The
+    reference arm runs on the host cores, so this needs no GPU."""
+    import json
+    import subprocess
+
+    import pytest
+    from oracle import ref_capi
+    if not ref_capi.available():
+        pytest.skip("reference library not built (make -C oracle)")
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--gpus", "2", "--impl", "reference", "--steps", "1",
+                        "--warmup", "0"], capture_output=True, text=True, timeout=600, env=env, cwd=str(ROOT))
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2
