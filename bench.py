@@ -46,12 +46,13 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 B, H, W = 64, 512, 512
-# DRAM bytes (read + write) of one launch of the dominant kernel, the pair
-# launch whose second iteration carries the gap check (two iterations over the
-# 64 images), from one ncu capture of this batch: below the 2 x 40 B per pixel
-# of its two iterations, since d, u, v and alpha are read once for both and
-# only the second's u, v are written.
-PAIR_TRAFFIC = 366_400_000 + 225_300_000
+# DRAM bytes (read + write) of one launch of the dominant kernel, the quad
+# launch (four iterations over the 64 images, the fourth with the gap check),
+# from one ncu capture of this batch (profiles/): below the 4 x 40 B per pixel
+# of its four iterations, since d, u, v and alpha are read once for all four
+# and only the fourth's u, v are written. None until captured.
+QUAD_TRAFFIC = None
+QUAD_KIND, QUAD_ITERS = 3, 4  # fp_b200_workspace_step_times kind of the quad launch, its iterations
 GAMMAS = (0.05, 0.1, 0.2)
 TOL, MAX_ITER = 1e-6, 20000
 BYTES_PER_PIXEL_ITER = 40  # d 4 + u 8 + v 8 in, u 8 + v 8 out, alpha 4 (fp32)
@@ -216,6 +217,22 @@ def parity(x, alpha, steps, z_gpu, iters_gpu, zerr_gpu, r):
                           "err_reference_f32_input": _nrel(r.z[0], r64.z[0]), "zerr_gpu": float(zerr_gpu[0])}}
 
 
+def uneven_parity(sample):
+    """The uneven workload's ragged results on a seeded sample of its images
+    against the reference C library on the same images (each with its own
+    step and tolerance): relative 2-norm errors and iteration counts."""
+    from oracle import ref_capi
+    if not ref_capi.available():
+        return None
+    errs, its = [], []
+    for i, x, gamma, tol, z, it in sample:
+        r = ref_capi.solve(x[None], gamma, iso=True, k=2, tol=tol, max_iter=5000)
+        errs.append(_nrel(z, r.z[0]))
+        its.append((it, int(r.iters[0])))
+    return {"images": [s[0] for s in sample], "max_rel_err_vs_reference": max(errs), "rel_err": errs,
+            "iters_gpu_vs_reference": its}
+
+
 def profile_case(kind="iso"):
     """iso: the benchmark batch (64 x 512^2, pixel weights, three steps)
     solved for exactly 8 iterations: launch 0 is the cold start, launches 4
@@ -277,7 +294,7 @@ def main():
                          "ragged batch; the cases for ncu captures")
     ap.add_argument("--workload", default="iso512", choices=["iso512", "aniso512", "iso3d", "uneven", "vjp", "serve"],
                     help="iso512 (default, the headline line); the others report the other workloads")
-    ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-workers", type=int, default=16, help="worker streams for anisotropic and 3D requests")
     args = ap.parse_args()
     if args.profile_case:
@@ -285,7 +302,11 @@ def main():
         return
     if args.workload != "iso512" and args.impl == "ours":
         from fastprox_b200 import workloads
-        print(json.dumps(getattr(workloads, args.workload)(args)))
+        res = getattr(workloads, args.workload)(args)
+        sample = res.pop("_sample", None)
+        if sample is not None and not args.no_cpu:
+            res["vs_reference"] = uneven_parity(sample)
+        print(json.dumps(res))
         return
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         sys.exit(launch_replicas(args.gpus))
@@ -368,17 +389,18 @@ def main():
 
     peak, peak_kind = peaks()
     achieved = BYTES_PER_PIXEL_ITER * pix_iters / args.steps / (t / args.steps) / 1e9
-    # The dominant kernel alone (after the timed region): the pair launch whose
-    # second iteration carries the gap check, timed by events the library puts
-    # around each step launch, with all 64 images live (tol 0, 24 iterations).
+    # The dominant kernel alone (after the timed region): the quad launch,
+    # timed by events the library puts around each step launch, with all 64
+    # images live (tol 0, 24 iterations: quads at iterations 1, 5, ..., 17).
     L.fp_b200_workspace_time_steps(ws, 1)
     op.solve(xt, st, tol=0.0, max_iter=24, out=out, with_dual=False)
     L.fp_b200_workspace_time_steps(ws, 0)
     kms, kn = C.c_double(), C.c_int64()
-    L.fp_b200_workspace_step_times(ws, 2, C.byref(kms), C.byref(kn))
+    L.fp_b200_workspace_step_times(ws, QUAD_KIND, C.byref(kms), C.byref(kn))
     kernel_us = kms.value / max(kn.value, 1) * 1e3
-    kernel_bytes = 2 * BYTES_PER_PIXEL_ITER * B * H * W  # two iterations over the batch
+    kernel_bytes = QUAD_ITERS * BYTES_PER_PIXEL_ITER * B * H * W  # four iterations over the batch
     achieved_kernel = kernel_bytes / (kernel_us * 1e-6) / 1e9 if kn.value else None
+    dram = QUAD_TRAFFIC / (kernel_us * 1e-6) / 1e9 if (kn.value and QUAD_TRAFFIC) else None
     cpu = None
     par = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -406,12 +428,12 @@ def main():
                                            "max": int(iters.max())}},
             "roofline": {"bound": "hbm", "achieved": achieved_kernel, "peak": peak, "unit": "GB/s",
                          "frac": achieved_kernel / peak if achieved_kernel else None, "peak_kind": peak_kind,
-                         "kernel": "iso2d_pair_kernel with the check (two iterations per launch, all images live)",
+                         "kernel": "iso2d_quad_kernel (four iterations per launch, the fourth with the gap "
+                                   "check; all images live)",
                          "kernel_us": kernel_us, "kernel_launches_timed": int(kn.value),
                          "algorithmic_bytes_per_launch": kernel_bytes, "bytes_per_pixel_iter": BYTES_PER_PIXEL_ITER,
-                         "traffic": PAIR_TRAFFIC,
-                         "dram_achieved": PAIR_TRAFFIC / (kernel_us * 1e-6) / 1e9 if kn.value else None,
-                         "dram_frac": PAIR_TRAFFIC / (kernel_us * 1e-6) / 1e9 / peak if kn.value else None,
+                         "traffic": QUAD_TRAFFIC, "dram_achieved": dram,
+                         "dram_frac": dram / peak if dram else None,
                          "achieved_whole_call": achieved, "frac_whole_call": achieved / peak},
             "cpu_baseline": cpu,
             "parity": par,

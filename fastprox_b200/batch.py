@@ -18,7 +18,8 @@ from .image_tv import TVIso
 
 
 class RaggedBatch:
-    def __init__(self, max_images, max_pixels, dtype="float32", weights=None, rows=0, stream=None, graphs=True):
+    def __init__(self, max_images, max_pixels, dtype="float32", weights=None, rows=0, stream=None, graphs=True,
+                 quads=True, quad_rows=0):
         import torch
         self.op = TVIso(2, weights)
         self.max_images = int(max_images)
@@ -32,6 +33,7 @@ class RaggedBatch:
             capi.check(capi.lib().fp_b200_batch_set_rows(self._h, int(rows)), "batch_rows")
         if not graphs:
             capi.check(capi.lib().fp_b200_batch_set_graphs(self._h, 0), "batch_graphs")
+        capi.check(capi.lib().fp_b200_batch_set_quads(self._h, int(bool(quads)), int(quad_rows)), "batch_quads")
         self.pending = 0
         self._keep = {}
         self._fin = np.zeros(self.max_images, np.int32)

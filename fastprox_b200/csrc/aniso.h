@@ -67,6 +67,11 @@ struct AnBuffers {
     // a round's images: with lmap, launch slot z runs image lmap[z] for z < *lcnt
     const int *lmap = nullptr;
     const int *lcnt = nullptr;
+    // the fibre-major passes: y of a pass's fibres (B x N), the segment ends of
+    // their scans (value, first entry), the edge weights of strided axes (k x N)
+    void *ys = nullptr, *segv = nullptr;
+    int *segk = nullptr;
+    const void *wt = nullptr;
 };
 
 // CheckSchedule::done (src/ops/tv_aniso.cpp:400-413): after the first two
@@ -89,6 +94,11 @@ __device__ __forceinline__ void check_done(AnState &s, double gp, double target)
 #endif
 
 int an_pixel_blocks(const AnGeom &g);
+// Whether rounds run the fibre-major passes (FASTPROX_B200_AN_FIB=0: the tiled ones).
+bool aniso_fm_enabled();
+// The edge weights beta (k x N of the dtype) of every strided axis into wt,
+// fibre-major (entry i of fibre f of axis a at a N + f L_a + i).
+cudaError_t aniso_weights_fm(int dtype, const AnGeom &g, const void *beta, void *wt, cudaStream_t s);
 cudaError_t aniso_setup(int dtype, const AnGeom &g, const AnCall &c, const AnBuffers &bf, const void *x,
                         cudaStream_t s);
 // A warm start (tv_aniso.cpp:316-320, 436-486, 539-543, 630-684): the dual

@@ -522,6 +522,8 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     ws->max_part = std::max(ws->max_part, 4096);
     if (ws->shape_.kind == 4)  // per-row partial sums of the lean 2D step
         ws->max_part = (int)std::max<int64_t>(ws->max_part, (int64_t)ws->shape_.gx * g.L[0]);
+    if (x.dtype == FP_F32 && g.k == 2)  // per-row, per-strip partial sums of the quad launch
+        ws->max_part = (int)std::max<int64_t>(ws->max_part, iso_quad_parts(g));
     if (op->kind == kAniso) {
         // the untiled fibre passes: a block of 128 fibres per partial, three
         // axes in one launch for FDPG-3
@@ -539,6 +541,10 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
         A((void **)&ws->an_parent, (size_t)B * (size_t)N * sizeof(int));
         A((void **)&ws->an_cnt, (size_t)B * (size_t)N * sizeof(int));
         A((void **)&ws->an_sum, (size_t)B * (size_t)N * sizeof(unsigned long long));
+        A(&ws->an_ys, img);
+        A(&ws->an_segv, img);
+        A((void **)&ws->an_segk, (size_t)B * (size_t)N * sizeof(int));
+        if (!op->spatial.empty()) A(&ws->an_wt, op->spatial.size() * T);
     }
     if (ws->keep) {
         const size_t bn = (size_t)B * (size_t)N, kk = (size_t)g.k;
@@ -599,6 +605,17 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
             if (r == cudaSuccess) r = cudaMemsetAsync(ws->err, 0, 16, ps);
             if (r == cudaSuccess && !spatial_h.empty())
                 r = cudaMemcpyAsync(ws->spatial, spatial_h.data(), spatial_h.size(), cudaMemcpyHostToDevice, ps);
+            if (r == cudaSuccess && ws->an_wt && N > 0) {  // the edge weights of strided axes, fibre-major
+                AnGeom ag{};
+                ag.k = g.k;
+                for (int a = 0; a < 3; ++a) ag.L[a] = a < g.k ? g.L[a] : 1;
+                ag.S[g.k - 1] = 1;
+                for (int a = g.k - 2; a >= 0; --a) ag.S[a] = ag.S[a + 1] * ag.L[a + 1];
+                for (int a = g.k; a < 3; ++a) ag.S[a] = 1;
+                ag.N = N;
+                ag.B = B;
+                r = aniso_weights_fm(x.dtype, ag, ws->spatial, ws->an_wt, ps);
+            }
             return r;
         });
         ws->dev_block = base;
@@ -939,20 +956,22 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     // applies (iso_pair_ok).
     const int chunk = ws->chunk > 0 ? ws->chunk : 8;
     const bool pairs = iso_pair_ok(g, ws->shape_, ws->max_part);
+    const bool quads = iso_quad_ok(ws->dtype, g, ws->max_part);
     int par = 0, slot = 0, inflight = 0;
     int64_t launched = 0, steps = 0, lists = 0, nimg = g.B;
     const int64_t cap = (int64_t)max_iter + 1 + 2 * chunk;
     // step-launch timing: an event pair around each launch, up to kTimed launches
     constexpr size_t kTimed = 4096;
     std::vector<int> tkind;
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 4; ++k) {
         ws->tms[k] = 0.0;
         ws->tcount[k] = 0;
     }
     bool done = false;
     while (!done) {
         for (int j = 0; j < chunk; ++j) {
-            const int pv = pairs ? iso_pair_at(launched, max_iter) : -1;
+            int pv = quads ? iso_quad_at(launched, max_iter) : -1;
+            if (pv < 0 && pairs) pv = iso_pair_at(launched, max_iter);
             const bool timed = ws->time_steps && tkind.size() < kTimed;
             if (timed) {
                 while (ws->tev.size() < 2 * (tkind.size() + 1)) {
@@ -967,10 +986,10 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
             if (e != cudaSuccess) return cuda_status(e);
             if (timed) {
                 if ((e = cudaEventRecord(ws->tev[2 * tkind.size() + 1], s)) != cudaSuccess) return cuda_status(e);
-                tkind.push_back(pv == kVariantPairGap ? 2 : (pv == kVariantPair ? 1 : 0));
+                tkind.push_back(pv == kVariantQuad ? 3 : pv == kVariantPairGap ? 2 : (pv == kVariantPair ? 1 : 0));
             }
             par ^= 1;
-            launched += pv >= 0 ? 2 : 1;
+            launched += pv == kVariantQuad ? 4 : pv >= 0 ? 2 : 1;
             ++steps;
         }
         e = cudaMemcpyAsync(ws->h_live + slot, ws->live, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -1008,9 +1027,9 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
             ws->tcount[tkind[k]] += 1;
         }
     }
-    if (pairs) {
-        e = iso_redo(ws->dtype, g, c, bf, s);
-        ws->kernel_launches += 2;
+    if (pairs || quads) {
+        e = iso_redo(ws->dtype, g, c, bf, s, quads);
+        ws->kernel_launches += quads ? 3 : 2;
     }
     if (e == cudaSuccess) e = iso_finalize(ws->dtype, g, c, bf, zdst, s);
     return cuda_status(e);
@@ -1119,6 +1138,10 @@ fp_status run_aniso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *z
     bf.parent = ws->an_parent;
     bf.sum = ws->an_sum;
     bf.cnt = ws->an_cnt;
+    bf.ys = ws->an_ys;
+    bf.segv = ws->an_segv;
+    bf.segk = ws->an_segk;
+    bf.wt = ws->an_wt;
     bf.img = ws->an_img;
     bf.st = ws->an_st;
     bf.gammas = ws->gammas;
@@ -1874,9 +1897,12 @@ fp_status vjp_impl(const fp_op *op, fp_workspace *ws, const fp_array *ga, fp_arr
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         return cuda_status(e);
     };
+    ws->vjp_gg_img.assign((size_t)g0.B, 0.0);
+    ws->vjp_gw_img.assign((size_t)(g0.B * op->k), 0.0);
     if (ws->identity) {  // gx = g; no parameter gradient; the sigma-derivative NaN (api.cpp:711-716)
         if (fp_status st = copy_or_fill(ws, &g, gx, 0.0, nullptr)) return st;
         gsum = std::numeric_limits<double>::quiet_NaN();
+        ws->vjp_gg_img.assign((size_t)g0.B, gsum);
         return finish();
     }
     if (g0.B * g0.N == 0) return finish();
@@ -1905,10 +1931,14 @@ fp_status vjp_impl(const fp_op *op, fp_workspace *ws, const fp_array *ga, fp_arr
         if (e != cudaSuccess) return cuda_status(e);
         // d/dw_a = -gamma sum_C S_{C,a} g_C; d/dgamma = -sum_a w_a sum_C S_{C,a} g_C
         const auto *hv = reinterpret_cast<const AnVjpImage *>(ws->h_vimg);
+        ws->vjp_gg_img.assign((size_t)g0.B, 0.0);
+        ws->vjp_gw_img.assign((size_t)(g0.B * op->k), 0.0);
         for (int64_t b = 0; b < g0.B; ++b)
             for (int a = 0; a < op->k; ++a) {
                 tot[(size_t)a] -= hv[b].gamma * ws->h_gw[3 * b + a];
                 gsum -= op->w[a] * ws->h_gw[3 * b + a];
+                ws->vjp_gg_img[(size_t)b] -= ws->conj ? 0.0 : op->w[a] * ws->h_gw[3 * b + a];
+                ws->vjp_gw_img[(size_t)(b * op->k + a)] = (ws->conj ? 1.0 : -1.0) * hv[b].gamma * ws->h_gw[3 * b + a];
             }
         if (params) {
             for (int64_t i = 0; i < nb; ++i) tot[(size_t)(op->k + i)] = gb[(size_t)i];
@@ -1936,10 +1966,18 @@ fp_status vjp_impl(const fp_op *op, fp_workspace *ws, const fp_array *ga, fp_arr
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e);
-    for (int64_t b = 0; b < g0.B; ++b) gsum += ws->h_ggam[b];
+    ws->vjp_gg_img.assign((size_t)g0.B, 0.0);
+    ws->vjp_gw_img.assign((size_t)(g0.B * op->k), 0.0);
+    for (int64_t b = 0; b < g0.B; ++b) {
+        gsum += ws->h_ggam[b];
+        ws->vjp_gg_img[(size_t)b] = ws->h_ggam[b];
+    }
     if (params) {
         for (int a = 0; a < op->k; ++a)
-            for (int64_t b = 0; b < g0.B; ++b) tot[(size_t)a] += ws->h_gw[3 * b + a];
+            for (int64_t b = 0; b < g0.B; ++b) {
+                tot[(size_t)a] += ws->h_gw[3 * b + a];
+                ws->vjp_gw_img[(size_t)(b * op->k + a)] = (ws->conj ? -1.0 : 1.0) * ws->h_gw[3 * b + a];
+            }
         for (int64_t i = 0; i < na; ++i) tot[(size_t)(op->k + i)] = ga_host[(size_t)i];
         // the conjugate y - prox(y): -sigma times the parameters' gradients,
         // sigma = 1 for TV (api.cpp:726-730)
@@ -2475,8 +2513,21 @@ FP_API fp_status fp_b200_workspace_time_steps(fp_workspace *ws, int on) {
     return FP_OK;
 }
 
+FP_API fp_status fp_b200_vjp_images(const fp_workspace *ws, double *ggamma, double *gweights, int64_t count) {
+    if (!ws || count < 0) return FP_EINVAL;
+    const int64_t B = (int64_t)ws->vjp_gg_img.size();
+    if (count != B || B != ws->g.B) return FP_EINVAL;
+    const int64_t k = B ? (int64_t)ws->vjp_gw_img.size() / B : 0;
+    for (int64_t b = 0; b < B; ++b) {
+        if (ggamma) ggamma[b] = ws->vjp_gg_img[(size_t)b];
+        if (gweights)
+            for (int64_t a = 0; a < k; ++a) gweights[b * k + a] = ws->vjp_gw_img[(size_t)(b * k + a)];
+    }
+    return FP_OK;
+}
+
 FP_API fp_status fp_b200_workspace_step_times(const fp_workspace *ws, int kind, double *ms, int64_t *launches) {
-    if (!ws || kind < 0 || kind > 2) return FP_EINVAL;
+    if (!ws || kind < 0 || kind > 3) return FP_EINVAL;
     if (ms) *ms = ws->tms[kind];
     if (launches) *launches = ws->tcount[kind];
     return FP_OK;

@@ -9,10 +9,11 @@
 // partial sums and tickets, and two work lists of (image, tile) items, one
 // for rows of a multiple of 4 pixels (16-byte vectors) and one for the rest.
 // A step launches the single-step kernel over each list (each block in the
-// variant its image's state asks for), and on the 4-wide float list the two
-// pair variants (two iterations per launch); chunks of steps are replayed
-// as CUDA graphs, captured again only when the work lists outgrow their
-// current size class.
+// variant its image's state asks for), on the 4-wide float list the two pair
+// variants (two iterations per launch), and over a third list of quad tiles
+// (float rows of a multiple of 4 pixels) the quad (four iterations per
+// launch); chunks of steps are replayed as CUDA graphs, captured again only
+// when the work lists outgrow their current size class.
 #include <cuda_runtime_api.h>
 
 #include <algorithm>
@@ -44,6 +45,7 @@ struct SlotHost {
     int64_t off = 0, len = 0;
     void *out = nullptr;  // the caller's z (device)
     int first_item = 0, n_items = 0, vec = 1;
+    bool quad = false;  // the slot may take quad launches (its redo)
 };
 
 template <class F>
@@ -74,23 +76,25 @@ struct fp_b200_batch {
     unsigned *ticket = nullptr;
     int *live = nullptr, *err = nullptr;
     RagSlot *slots = nullptr;
-    RagItem *items[2] = {nullptr, nullptr};  // [0] vec 4 (or 2 for double), [1] vec 1
-    int *n_items = nullptr;                  // 2 counts
+    RagItem *items[3] = {nullptr, nullptr, nullptr};  // [0] vec 4 (or 2 for double), [1] vec 1, [2] quad tiles
+    int *n_items = nullptr;                           // 3 counts
     std::vector<void *> allocs, pinned;
     // host
     std::vector<Range> free_list;
     std::vector<SlotHost> sh;
     RagSlot *h_slots = nullptr;
-    RagItem *h_items[2] = {nullptr, nullptr};
+    RagItem *h_items[3] = {nullptr, nullptr, nullptr};
     int *h_n = nullptr;
     IsoState *h_st = nullptr;
     IsoImage *h_img = nullptr;
     int *h_live = nullptr;
     bool items_dirty = true;
-    int grid[2] = {0, 0};
-    // graphs of `chunk` steps, keyed by (grid0, grid1, chunk)
-    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
+    int grid[3] = {0, 0, 0};
+    // graphs of `chunk` steps, keyed by (grid0, grid1, grid2, chunk)
+    std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;
     int rows_hint = 0;
+    bool quads = true;  // quad tiles for the float rows of a multiple of 4 pixels (admitted from now on)
+    int quad_rows = 32;
     bool use_graphs = true;
     int64_t steps_run = 0, kernel_launches = 0;
     double wh[2] = {1.0, 1.0}, tau = 0.125;
@@ -231,7 +235,7 @@ IsoCall call_for(fp_b200_batch *bt, const SlotHost &s, double tol, int max_iter)
 
 // the work lists from the slots in use
 void rebuild_items(fp_b200_batch *bt) {
-    int n[2] = {0, 0};
+    int n[3] = {0, 0, 0};
     const int vfull = bt->dtype == FP_F32 ? 4 : 2;
     for (size_t i = 0; i < bt->sh.size(); ++i) {
         SlotHost &s = bt->sh[i];
@@ -245,10 +249,20 @@ void rebuild_items(fp_b200_batch *bt) {
                 if (n[list] < bt->max_items) bt->h_items[list][n[list]++] = RagItem{(int)i, blk, r0, cs};
                 ++blk;
             }
+        if (rs.nquad > 0) {  // quad tiles: qrows rows x iso_quad_warps() strips
+            const int ns = iso_quad_strips(s.W), qw = iso_quad_warps();
+            int qb = 0;
+            for (int r0 = 0; r0 < s.H; r0 += rs.qrows)
+                for (int st0 = 0; st0 < ns; st0 += qw) {
+                    if (n[2] < bt->max_items) bt->h_items[2][n[2]++] = RagItem{(int)i, qb, r0, st0};
+                    ++qb;
+                }
+        }
     }
     bt->h_n[0] = n[0];
     bt->h_n[1] = n[1];
-    for (int l = 0; l < 2; ++l) {
+    bt->h_n[2] = n[2];
+    for (int l = 0; l < 3; ++l) {
         // a size class (a power of two) keeps captured graphs valid while the lists change within it
         int gcls = 0;
         if (n[l] > 0) {
@@ -259,7 +273,7 @@ void rebuild_items(fp_b200_batch *bt) {
         if (n[l]) cudaMemcpyAsync(bt->items[l], bt->h_items[l], (size_t)n[l] * sizeof(RagItem), cudaMemcpyHostToDevice,
                                   bt->stream);
     }
-    cudaMemcpyAsync(bt->n_items, bt->h_n, 2 * sizeof(int), cudaMemcpyHostToDevice, bt->stream);
+    cudaMemcpyAsync(bt->n_items, bt->h_n, 3 * sizeof(int), cudaMemcpyHostToDevice, bt->stream);
     bt->items_dirty = false;
 }
 
@@ -273,6 +287,8 @@ cudaError_t launch_steps(fp_b200_batch *bt, int steps) {
                                         bt->stream);
         if (e == cudaSuccess)
             e = iso_ragged_step(bt->dtype, 1, bt->items[1], bt->n_items + 1, bt->grid[1], bt->slots, c, bf, bt->stream);
+        if (e == cudaSuccess)
+            e = iso_ragged_quad_step(bt->items[2], bt->n_items + 2, bt->grid[2], bt->slots, bf, bt->stream);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -284,6 +300,7 @@ int launches_per_step(const fp_b200_batch *bt) {
     int n = 0;
     if (bt->grid[0] > 0) n += 1 + (iso_ragged_pairs(bt->dtype, 4) ? 2 : 0);
     if (bt->grid[1] > 0) n += 1;
+    if (bt->grid[2] > 0) n += 1;
     return n;
 }
 
@@ -294,7 +311,7 @@ void trace(const char *what, cudaError_t e) {
 
 cudaError_t run_chunk(fp_b200_batch *bt, int steps) {
     if (!bt->use_graphs) return launch_steps(bt, steps);
-    const auto key = std::make_tuple(bt->grid[0], bt->grid[1], steps);
+    const auto key = std::make_tuple(bt->grid[0], bt->grid[1], bt->grid[2], steps);
     auto it = bt->graphs.find(key);
     if (it == bt->graphs.end()) {
         cudaGraph_t graph = nullptr;
@@ -382,10 +399,12 @@ FP_API fp_status fp_b200_batch_create(const fp_op *op, int64_t max_images, int64
         A((void **)&bt->slots, S * sizeof(RagSlot));
         A((void **)&bt->items[0], (size_t)bt->max_items * sizeof(RagItem));
         A((void **)&bt->items[1], (size_t)bt->max_items * sizeof(RagItem));
+        A((void **)&bt->items[2], (size_t)bt->max_items * sizeof(RagItem));
         A((void **)&bt->n_items, 16);
         Hh((void **)&bt->h_slots, S * sizeof(RagSlot));
         Hh((void **)&bt->h_items[0], (size_t)bt->max_items * sizeof(RagItem));
         Hh((void **)&bt->h_items[1], (size_t)bt->max_items * sizeof(RagItem));
+        Hh((void **)&bt->h_items[2], (size_t)bt->max_items * sizeof(RagItem));
         Hh((void **)&bt->h_n, 16);
         Hh((void **)&bt->h_st, S * sizeof(IsoState));
         Hh((void **)&bt->h_img, S * sizeof(IsoImage));
@@ -439,6 +458,13 @@ FP_API fp_status fp_b200_batch_set_graphs(fp_b200_batch *bt, int on) {
     return FP_OK;
 }
 
+FP_API fp_status fp_b200_batch_set_quads(fp_b200_batch *bt, int on, int rows) {
+    if (!bt || rows < 0 || rows > 1024) return FP_EINVAL;
+    bt->quads = on != 0;
+    if (rows > 0) bt->quad_rows = rows;
+    return FP_OK;
+}
+
 FP_API fp_status fp_b200_batch_set_rows(fp_b200_batch *bt, int rows) {
     if (!bt || rows < 0 || rows > 1024) return FP_EINVAL;
     bt->rows_hint = rows;
@@ -487,6 +513,15 @@ FP_API fp_status fp_b200_batch_admit(fp_b200_batch *bt, const void *x, int64_t h
         }
         rs.max_iter = max_iter;
         rs.vec = s.vec;
+        // quad tiles: float rows of a multiple of 4 pixels, two rows or more
+        rs.qrows = bt->quad_rows;
+        rs.nquad = 0;
+        if (bt->quads && iso_ragged_pairs(bt->dtype, s.vec) && width % 4 == 0 && height >= 2) {
+            const int64_t nq = ((height + rs.qrows - 1) / rs.qrows) *
+                               ((iso_quad_strips((int)width) + iso_quad_warps() - 1) / iso_quad_warps());
+            if (nq <= bt->max_part) rs.nquad = (int)nq;
+        }
+        s.quad = rs.nquad > 0;
         rs.wh0 = c.wh[0];
         rs.wh1 = c.wh[1];
         rs.tau = c.tau;
@@ -566,7 +601,7 @@ FP_API fp_status fp_b200_batch_run(fp_b200_batch *bt, int steps, int max_chunks,
             g.N = (int64_t)s.H * s.W;
             g.B = 1;
             IsoBuffers bf = slot_buffers(bt, slot);
-            if (e == cudaSuccess) e = iso_redo(bt->dtype, g, c, bf, st);
+            if (e == cudaSuccess) e = iso_redo(bt->dtype, g, c, bf, st, s.quad);
             if (e == cudaSuccess) e = iso_finalize(bt->dtype, g, c, bf, s.out, st);
             bt->kernel_launches += 3;
         }

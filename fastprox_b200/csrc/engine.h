@@ -53,13 +53,15 @@ struct IsoState {
     int zero_in;   // 1: u = v = 0 (cold start, nothing staged)
     int warm;      // 1: the gap is checked before the first iteration
     int fin_par;   // buffer parity holding the final u
-    int redo;      // 1: the final u is one more iteration from the buffers of fin_par, reading v = u when
-                   // redo_vsel (a checked pair's check passed at its first iterate, which it did not store)
+    int redo;      // the final u is redo more iterations from the buffers of fin_par, reading v = u when
+                   // redo_vsel: 1 (a checked pair's check passed at its first iterate, which it did not
+                   // store) or 3 (a quad's check passed at its third iterate); 0 otherwise
     int redo_vsel;
     double tn;     // fista_t(t) of the next iteration, t its momentum scalar
     double beta;   // (t - 1) / tn of the next iteration
     double gp;     // last gap checked
     double dot;    // last restart dot product
+    double redo_tn, redo_beta;  // tn and beta of the first iteration redone (redo = 3)
 };
 
 struct Geometry {
@@ -96,6 +98,8 @@ struct RagSlot {
     int rows;       // rows per tile
     int vec;        // pixels per thread along a row
     double wh0, wh1, tau;
+    int nquad;      // tiles of the quad launch (0: the image takes no quads)
+    int qrows;      // rows per quad tile
 };
 
 // One tile of the work list: the image's slot, the tile's index within the

@@ -74,10 +74,24 @@ inline int iso_variant(int64_t k, int max_iter, bool warm) {
     if (k == 0) return warm ? 2 : 1;
     return (k % 4 == 0 || k == max_iter) ? 2 : 0;
 }
-// The final u of images whose checked pair launch passed at its first
-// iterate (state redo), formed again from that launch's input buffers; the
-// state then points at it. Before any read of a solve's final dual.
-cudaError_t iso_redo(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s);
+// Iterations k .. k + 3 in one launch (the quad), for k = 1 mod 4 and
+// k + 3 < max_iter where iso_quad_ok (2D float32 rows of a multiple of 4
+// pixels): the fourth carries the gap check of the third iterate and the
+// restart test; when the check passes, the final u is the third iterate,
+// formed again by iso_redo.
+constexpr int kVariantQuad = 5;
+bool iso_quad_ok(int dtype, const Geometry &g, int max_part);
+// Partial-sum slots per image the quad needs (one per row and warp strip).
+int64_t iso_quad_parts(const Geometry &g);
+inline int iso_quad_at(int64_t k, int max_iter) {
+    return (k > 0 && (k & 3) == 1 && k + 3 < max_iter) ? kVariantQuad : -1;
+}
+// The final u of images whose checked pair (or quad) launch passed at its
+// first (third) iterate (state redo), formed again from that launch's input
+// buffers; the state then points at it. Before any read of a solve's final
+// dual. quads: quad launches may have run (they have their own redo launch).
+cudaError_t iso_redo(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s,
+                     bool quads = false);
 // z = x - G^T q into out (contiguous, device, x's dtype), the dual into
 // bf.dual, for every image by its mode; exact 1D TV for single-axis images.
 cudaError_t iso_finalize(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, void *out,
@@ -91,6 +105,16 @@ cudaError_t iso_ragged_step(int dtype, int vec, const RagItem *items, const int 
 // Whether the ragged step on a list of `vec`-wide rows adds the two pair
 // variants (float, 4-wide rows, pairs not switched off).
 bool iso_ragged_pairs(int dtype, int vec);
+// The ragged step's quad launch over its own work list (items[0 .. *n_items),
+// an item a block of quad strips: its slot, its tile index, first row and
+// first strip): four iterations for the images whose state asks for them
+// (slots with nquad > 0, iteration 1 mod 4, not across max_iter); the other
+// launches of the step leave those images alone.
+cudaError_t iso_ragged_quad_step(const RagItem *items, const int *n_items, int grid, const RagSlot *slots,
+                                 const IsoBuffers &bf, cudaStream_t s);
+// Strips of a quad pass over rows of W pixels, and strips per quad block.
+int iso_quad_strips(int W);
+int iso_quad_warps();
 bool pairs_enabled();
 
 // Fills gammas[i] = v for i < n.

@@ -270,7 +270,9 @@ struct NoWeight {
 };
 
 // tv1d_fiber_sink on the fibres of one warp at once: lane t scans fibre t when
-// `act`, every lane of the warp calls it, and n is the same for all. Run one
+// `act`, every lane of the warp calls it, and n is the same for all. COPY: a
+// fibre that is its own prox is written through the sink too (every entry a
+// segment of its own; without COPY the sink's storage is the input's). Run one
 // lane per thread, the scans drift apart and a warp runs each lane's branches
 // in turn; here the warp takes one CondatScan step of every live scan per trip
 // of a loop that all its lanes share, and every step is the same arithmetic,
@@ -279,7 +281,7 @@ struct NoWeight {
 // with zero-weight edges (pieces) run tv1d_fiber_sink after the loop. A scan
 // takes at most 2 (n + 1)^2 steps (every jump moves the segment's start
 // forward, and between jumps k only grows): the loop stops there.
-template <class C, class In, class Sink, class Wt, class Rcp>
+template <class C, bool COPY = false, class In, class Sink, class Wt, class Rcp>
 __device__ __forceinline__ void tv1d_warp(const In &in, const Sink &out, int n, double lam_d, bool has_w, const Wt &w,
                                           const Rcp &rcp, bool act) {
     const C lam = (C)lam_d;
@@ -326,6 +328,10 @@ __device__ __forceinline__ void tv1d_warp(const In &in, const Sink &out, int n, 
     }
     if (fill) out.finish(n);
     if (serial) tv1d_fiber_sink<C>(in, out, n, lam_d, true, w, rcp);
+    if (COPY && act && !fill && !serial) {
+        for (int i = 0; i < n; ++i) out.segment(i, i, (double)in(i));
+        out.finish(n);
+    }
 }
 
 }  // namespace fpb

@@ -667,6 +667,278 @@ __global__ void __launch_bounds__(kTileThreads) an_fdpg3_tile(AnGeom g, AnCall c
 }
 
 // ---------------------------------------------------------------------------
+// Fibre-major passes
+// ---------------------------------------------------------------------------
+//
+// The fibre scans are long serial chains (each step of Condat's scan depends on
+// the last), so a pass is bound by how many fibres an SM keeps in flight. The
+// tiles above hold a block's fibres in shared memory, which caps an SM at a few
+// dozen fibres. These passes keep every fibre of the launch in flight at once
+// (a lane per fibre, 32 fibres a warp, in lockstep) and read the fibres through
+// the L1 cache from a fibre-major copy, where each fibre's entries are
+// contiguous: a lane's reads walk its own few cache lines. A pass is:
+//  * stage: y of every fibre of the axis into ys, fibre-major (entry i of fibre
+//    f at f L + i), through 32 x 32 tiles of shared memory (coalesced both
+//    ways); a contiguous axis (stride 1) is fibre-major already, and its scan
+//    reads the image arrays directly;
+//  * scan: Condat's scan of every fibre (tv1d_warp); a segment writes its value
+//    and its first entry at its last entry (segv, segk); after the scan each
+//    lane fills its fibre's entries from the segment ends, walking back from
+//    the fibre's end, into ys in place (or, for the first pass over a
+//    contiguous axis, straight into u);
+//  * unstage: the results back into the image's layout with the pass's
+//    epilogue (the dual update and the restart test's sums for the second
+//    pass), through the same tiles.
+// The arithmetic of every step is the tiled passes'. The restart test's FP64
+// sums are formed per tile block in a fixed order (its tiles, then the blocks),
+// a partition that depends on the image's shape only.
+// Edge weights along a strided axis are read from a fibre-major copy made once
+// per workspace (an_weights_fm).
+
+// A segment's value and first entry at its last entry; finish fills the
+// fibre's entries, walking the segments back from the fibre's end.
+template <class T>
+struct SegSink {
+    T *val;
+    int *start;
+    T *out;
+    int *err;
+    __device__ __forceinline__ void segment(int k0, int k1, double v) const {
+        val[k1] = (T)v;
+        start[k1] = k0;
+    }
+    __device__ __forceinline__ void finish(int n) const {
+        int e = n - 1;
+        while (e >= 0) {
+            int k0 = start[e];
+            if (k0 < 0 || k0 > e) {  // never written: a broken scan, flagged (the walk still ends)
+                atomicExch(err, 4);
+                k0 = e;
+            }
+            const T v = val[e];
+            for (int i = e; i >= k0; --i) out[i] = v;
+            e = k0 - 1;
+        }
+    }
+};
+
+// Entry i of a fibre-major fibre.
+template <class T>
+struct FmIn {
+    const T *p;
+    __device__ __forceinline__ T operator()(int i) const { return p[i]; }
+};
+// d + w (the first pass) or u - w (the second) of a contiguous fibre.
+template <class T, int PASS>
+struct SumIn {
+    const T *a, *w;
+    __device__ __forceinline__ T operator()(int i) const { return PASS == 1 ? (T)(a[i] + w[i]) : (T)(a[i] - w[i]); }
+};
+
+// Whether pass PASS of a round acts on image b (the stages of an_pass1 / an_pass2).
+template <int PASS>
+__device__ __forceinline__ bool fm_active(const AnState &st, const AnImage &im) {
+    if (st.status != kLive || im.mode != kAnAdbpg) return false;
+    return PASS == 1 ? (st.stage == kStIter || st.stage == kStWarm) : st.stage == kStIter;
+}
+
+constexpr int kFmTile = 32;     // tile of 32 fibres x 32 entries
+constexpr int kFmThreads = 256; // 32 x 8 threads per tile block
+constexpr int kFmScan = 128;    // lanes (fibres) per scan block
+
+__host__ __device__ __forceinline__ int64_t fm_tiles(int64_t nfib, int64_t L) {
+    return ((nfib + kFmTile - 1) / kFmTile) * ((L + kFmTile - 1) / kFmTile);
+}
+
+// ys = y of axis a's fibres, fibre-major (PASS 1: d + w along a1; 2: u - w along a2).
+template <class T, int PASS>
+__global__ void __launch_bounds__(kFmThreads) an_fm_stage(AnGeom g, AnCall c, AnBuffers bf) {
+    __shared__ T tile[kFmTile][kFmTile + 1];
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
+    const AnImage &im = bf.img[b];
+    if (!fm_active<PASS>(bf.st[b], im)) return;
+    const int a = PASS == 1 ? im.a1 : im.a2;
+    const Fib fb = fibers(g, a);
+    const int64_t N = g.N, L = fb.L;
+    const T *P0 = static_cast<const T *>(PASS == 1 ? bf.d : bf.u) + (int64_t)b * N;
+    const T *Wv = static_cast<const T *>(bf.wv) + (int64_t)b * g.k * N;
+    T *Y = static_cast<T *>(bf.ys) + (int64_t)b * N;
+    auto src = [&](int64_t o) -> T { return PASS == 1 ? (T)(P0[o] + Wv[o]) : (T)(P0[o] - Wv[o]); };
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int64_t neg = (L + kFmTile - 1) / kFmTile, nt = fm_tiles(fb.nfib, L);
+    for (int64_t t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int64_t f0 = (t / neg) * kFmTile, i0 = (t % neg) * kFmTile;
+#pragma unroll
+        for (int r = 0; r < kFmTile; r += 8) {  // along the fibres (adjacent fibres are adjacent in memory)
+            const int64_t f = f0 + tx, i = i0 + ty + r;
+            tile[ty + r][tx] = (f < fb.nfib && i < L) ? src(fb.base(f) + i * fb.s) : T(0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kFmTile; r += 8) {  // along each fibre
+            const int64_t f = f0 + ty + r, i = i0 + tx;
+            if (f < fb.nfib && i < L) Y[f * L + i] = tile[tx][ty + r];
+        }
+        __syncthreads();
+    }
+}
+
+// Condat's scan of every fibre of the pass's axis, a lane per fibre.
+// DIRECT: the axis is contiguous and the scan reads the image arrays (d + w,
+// or u - w); the first pass then fills u, the second ys.
+template <class T, int PASS, bool DIRECT>
+__global__ void __launch_bounds__(kFmScan) an_fm_scan(AnGeom g, AnCall c, AnBuffers bf) {
+    extern __shared__ __align__(16) unsigned char an_fm_smem[];
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
+    const AnImage &im = bf.img[b];
+    if (!fm_active<PASS>(bf.st[b], im)) return;
+    const int a = PASS == 1 ? im.a1 : im.a2;
+    const Fib fb = fibers(g, a);
+    const int L = (int)fb.L;
+    T *rc = reinterpret_cast<T *>(an_fm_smem);  // 1/m, m <= L
+    {
+        const DivRecip<T> div;
+        for (int m = threadIdx.x; m <= L; m += blockDim.x) rc[m] = m ? div(m) : T(0);
+    }
+    __syncthreads();
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool act = f < fb.nfib;
+    const int64_t N = g.N, fo = act ? f * L : 0;  // fibre-major offset (the image offset when DIRECT)
+    T *Y = static_cast<T *>(bf.ys) + (int64_t)b * N + fo;
+    T *out = (DIRECT && PASS == 1) ? static_cast<T *>(bf.u) + (int64_t)b * N + fo : Y;
+    const SegSink<T> sink{static_cast<T *>(bf.segv) + (int64_t)b * N + fo, bf.segk + (int64_t)b * N + fo, out, bf.err};
+    const double lam = im.lam[a];
+    const TableRecip<T> rcp{rc};
+    auto run = [&](const auto &in) {
+        if (c.has_beta) {
+            const T *bw = static_cast<const T *>(fb.s == 1 ? bf.beta : bf.wt) + (int64_t)a * c.N + fo;
+            tv1d_warp<T, true>(in, sink, L, lam, true, FmIn<T>{bw}, rcp, act);
+        } else {
+            tv1d_warp<T, true>(in, sink, L, lam, false, NoWeight{}, rcp, act);
+        }
+    };
+    if (DIRECT) {
+        const T *P0 = static_cast<const T *>(PASS == 1 ? bf.d : bf.u) + (int64_t)b * N + fo;
+        const T *Wv = static_cast<const T *>(bf.wv) + (int64_t)b * g.k * N + fo;
+        run(SumIn<T, PASS>{P0, Wv});
+    } else {
+        run(FmIn<T>{Y});
+    }
+}
+
+// The scan's results back into the image's layout. PASS 1: u = z. PASS 2:
+// z, and the dual update with the extrapolation (an_pass2's); the last block
+// of the image runs the restart test and advances the iteration.
+template <class T, int PASS>
+__global__ void __launch_bounds__(kFmThreads) an_fm_unstage(AnGeom g, AnCall c, AnBuffers bf) {
+    __shared__ T tile[kFmTile][kFmTile + 1];
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = round_image(bf, blockIdx.y);
+    if (b < 0) return;
+    const AnState st = bf.st[b];
+    const AnImage &im = bf.img[b];
+    if (!fm_active<PASS>(st, im)) return;
+    const int a = PASS == 1 ? im.a1 : im.a2;
+    const Fib fb = fibers(g, a);
+    const int64_t N = g.N, L = fb.L;
+    const T *Y = static_cast<const T *>(bf.ys) + (int64_t)b * N;
+    T *U = static_cast<T *>(bf.u) + (int64_t)b * N;
+    T *Wv = static_cast<T *>(bf.wv) + (int64_t)b * g.k * N;
+    T *Yd = static_cast<T *>(bf.y) + (int64_t)b * g.k * N;
+    T *Z = static_cast<T *>(bf.z) + (int64_t)b * N;
+    const bool test = st.it % kCheck == 0;
+    const T beta = (T)st.beta;
+    double up = 0.0;
+    auto put = [&](int64_t o, T z) {
+        if (PASS == 1) {
+            U[o] = z;
+        } else {
+            const T v = U[o] - Wv[o];
+            const T yn = z - v;
+            const T y = Yd[o], w = Wv[o];
+            if (test) up += (double)((w - yn) * (yn - y));
+            Wv[o] = yn + beta * (yn - y);
+            Yd[o] = yn;
+            Z[o] = z;
+        }
+    };
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    if (fb.s == 1) {  // fibre-major is the image's layout
+        for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x)
+            put(p, Y[p]);
+    } else {
+        const int64_t neg = (L + kFmTile - 1) / kFmTile, nt = fm_tiles(fb.nfib, L);
+        for (int64_t t = blockIdx.x; t < nt; t += gridDim.x) {
+            const int64_t f0 = (t / neg) * kFmTile, i0 = (t % neg) * kFmTile;
+#pragma unroll
+            for (int r = 0; r < kFmTile; r += 8) {  // along each fibre
+                const int64_t f = f0 + ty + r, i = i0 + tx;
+                tile[ty + r][tx] = (f < fb.nfib && i < L) ? Y[f * L + i] : T(0);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < kFmTile; r += 8) {  // along the fibres
+                const int64_t f = f0 + tx, i = i0 + ty + r;
+                if (f < fb.nfib && i < L) put(fb.base(f) + i * fb.s, tile[tx][ty + r]);
+            }
+            __syncthreads();
+        }
+    }
+    if (PASS == 1) return;
+    double dot, unused;
+    if (!reduce2(bf, b, blockIdx.x, gridDim.x, test ? up : 0.0, 0.0, sh, &flag, dot, unused)) return;
+    AnState s2 = st;
+    s2.since += 1;
+    double t = s2.tn;
+    if (test && dot > 0.0 && s2.since >= s2.last) {
+        s2.last = s2.since;
+        s2.since = 0;
+        s2.restart = 1;
+        t = 1.0;
+    } else {
+        s2.restart = 0;
+    }
+    s2.it += 1;
+    const double tn = fista_t(t);
+    s2.beta = (t - 1.0) / tn;
+    s2.tn = tn;
+    if (s2.it == s2.chk_next || s2.it == c.max_iter) s2.stage = kStCheck;
+    bf.st[b] = s2;
+}
+
+// The edge weights of every strided axis, fibre-major (once per workspace).
+template <class T>
+__global__ void __launch_bounds__(kFmThreads) an_weights_fm(AnGeom g, const T *__restrict__ beta, T *__restrict__ wt) {
+    __shared__ T tile[kFmTile][kFmTile + 1];
+    const int a = blockIdx.y;
+    const Fib fb = fibers(g, a);
+    if (fb.s == 1) return;
+    const int64_t N = g.N, L = fb.L;
+    const T *Bw = beta + (int64_t)a * N;
+    T *Wt = wt + (int64_t)a * N;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int64_t neg = (L + kFmTile - 1) / kFmTile, nt = fm_tiles(fb.nfib, L);
+    for (int64_t t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int64_t f0 = (t / neg) * kFmTile, i0 = (t % neg) * kFmTile;
+#pragma unroll
+        for (int r = 0; r < kFmTile; r += 8) {
+            const int64_t f = f0 + tx, i = i0 + ty + r;
+            tile[ty + r][tx] = (f < fb.nfib && i < L) ? Bw[fb.base(f) + i * fb.s] : T(0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kFmTile; r += 8) {
+            const int64_t f = f0 + ty + r, i = i0 + tx;
+            if (f < fb.nfib && i < L) Wt[f * L + i] = tile[tx][ty + r];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Warm starts (tv_aniso.cpp:316-320, 436-486, 539-543, 630-684)
 // ---------------------------------------------------------------------------
 
@@ -1435,6 +1707,15 @@ TileCfg tile_cfg(const AnGeom &g, const AnCall &c, int64_t nimg, size_t &smem) {
     return tc;
 }
 
+// The fibre-major scan keeps its table of 1/m (m <= L) in the default 48 KB
+// of shared memory.
+template <class T>
+bool fm_fits(const AnGeom &g) {
+    for (int a = 0; a < g.k; ++a)
+        if ((size_t)(g.L[a] + 1) * sizeof(T) > 48 * 1024) return false;
+    return true;
+}
+
 template <class T>
 cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, int64_t nimg, cudaStream_t s,
                    int64_t *launches) {
@@ -1449,7 +1730,39 @@ cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, int64
     int64_t nfmax = 0;
     for (int a = 0; a < g.k; ++a) nfmax = std::max(nfmax, nf[a]);
     const unsigned fbk = (unsigned)((nfmax + 127) / 128);
-    if (c.has_adbpg) {
+    if (c.has_adbpg && aniso_fm_enabled() && fm_fits<T>(g)) {
+        // the fibre-major passes: the active axes (the same for every image of
+        // the call), a1 the one of smaller stride
+        int act[3], n = 0;
+        for (int a = 0; a < g.k; ++a)
+            if (c.w[a] > 0.0 && g.L[a] > 1) act[n++] = a;
+        const int a1 = g.S[act[0]] < g.S[act[1]] ? act[0] : act[1], a2 = a1 == act[0] ? act[1] : act[0];
+        auto tiles_grid = [&](int a) {
+            if (g.S[a] == 1) return (unsigned)std::min<int64_t>((g.N + kFmThreads - 1) / kFmThreads, 1024);
+            return (unsigned)std::min<int64_t>(fm_tiles(nf[a], g.L[a]), 1024);
+        };
+        auto scan_grid = [&](int a) { return dim3((unsigned)((nf[a] + kFmScan - 1) / kFmScan), B); };
+        auto scan_smem = [&](int a) { return (size_t)(g.L[a] + 1) * sizeof(T); };
+        if (g.S[a1] == 1) {
+            an_fm_scan<T, 1, true><<<scan_grid(a1), kFmScan, scan_smem(a1), s>>>(g, c, bf);
+            nl += 1;
+        } else {
+            an_fm_stage<T, 1><<<dim3(tiles_grid(a1), B), kFmThreads, 0, s>>>(g, c, bf);
+            an_fm_scan<T, 1, false><<<scan_grid(a1), kFmScan, scan_smem(a1), s>>>(g, c, bf);
+            an_fm_unstage<T, 1><<<dim3(tiles_grid(a1), B), kFmThreads, 0, s>>>(g, c, bf);
+            nl += 3;
+        }
+        if (g.S[a2] == 1) {
+            an_fm_scan<T, 2, true><<<scan_grid(a2), kFmScan, scan_smem(a2), s>>>(g, c, bf);
+            nl += 1;
+        } else {
+            an_fm_stage<T, 2><<<dim3(tiles_grid(a2), B), kFmThreads, 0, s>>>(g, c, bf);
+            an_fm_scan<T, 2, false><<<scan_grid(a2), kFmScan, scan_smem(a2), s>>>(g, c, bf);
+            nl += 2;
+        }
+        an_fm_unstage<T, 2><<<dim3(tiles_grid(a2), B), kFmThreads, 0, s>>>(g, c, bf);
+        nl += 1;
+    } else if (c.has_adbpg) {
         size_t smem = 0;
         const TileCfg tc = tile_cfg<T>(g, c, nimg, smem);
         bool tiled = true;
@@ -1538,6 +1851,26 @@ cudaError_t output_t(const AnGeom &g, const AnBuffers &bf, void *out, cudaStream
 }
 
 }  // namespace
+
+bool aniso_fm_enabled() {
+    static const bool on = [] {  // tuning hint FASTPROX_B200_AN_FIB=0: the tiled passes
+        const char *v = std::getenv("FASTPROX_B200_AN_FIB");
+        return !(v && v[0] == '0' && v[1] == 0);
+    }();
+    return on;
+}
+
+cudaError_t aniso_weights_fm(int dtype, const AnGeom &g, const void *beta, void *wt, cudaStream_t s) {
+    int64_t nt = 1;
+    for (int a = 0; a < g.k; ++a) nt = std::max<int64_t>(nt, fm_tiles(g.N / g.L[a], g.L[a]));
+    const dim3 grid((unsigned)std::min<int64_t>(nt, 4096), (unsigned)g.k);
+    if (dtype == 1)
+        an_weights_fm<float><<<grid, kFmThreads, 0, s>>>(g, static_cast<const float *>(beta), static_cast<float *>(wt));
+    else
+        an_weights_fm<double>
+            <<<grid, kFmThreads, 0, s>>>(g, static_cast<const double *>(beta), static_cast<double *>(wt));
+    return cudaGetLastError();
+}
 
 int an_pixel_blocks(const AnGeom &g) {
     int64_t nb = (g.N + kThreads * 4 - 1) / (kThreads * 4);

@@ -1234,7 +1234,7 @@ template <class T, bool ALPHA>
 __global__ void __launch_bounds__(256) iso2d_redo_kernel(Geometry g, IsoCall c, IsoBuffers bf) {
     const int b = (int)blockIdx.y;
     const IsoState st = bf.st[b];
-    if (!st.redo) return;
+    if (st.redo != 1) return;
     const IsoImage im = bf.img[b];
     const int H = (int)g.L[0], W = (int)g.L[1];
     const int64_t N = g.N;
@@ -1278,6 +1278,373 @@ __global__ void iso2d_redo_state(IsoState *st, int64_t B) {
 }
 
 // ---------------------------------------------------------------------------
+// Four iterations in one pass over memory (the quad launch).
+//
+// Iterations it .. it + 3 with it = 1 mod 4: the first three carry no check
+// and no restart test, the fourth (it + 3 = 0 mod 4) carries the gap check
+// of the state it starts from (the third iterate) and the restart test, so
+// nothing global is decided inside the pass, and the momenta of all four are
+// the ones the per-image control would set ((tn - 1) / fista_t(tn), tn
+// advanced by fista_t). Only the fourth iterate's u, v are written; when the
+// check passes, the final iterate is the third's u, formed again by the redo
+// variant of this kernel from the pass's untouched input buffers (state
+// redo = 3).
+//
+// Layout: each warp owns a strip of the image: a window of 64 columns (two
+// per lane) marching down the block's rows, whose middle 56 columns it writes;
+// one iteration needs one column of the previous iterate on each side, so the
+// four iterations need 4 columns of halo on each side, and strips overlap by
+// 8 columns (rows of any width; the halo columns are recomputed, their loads
+// mostly hit L2). Warps never wait on each other: the iterations pass between
+// lanes by shuffles only. A warp's rows are staged in a ring of shared memory
+// by cp.async (every lane copies 16-byte pieces of the window's rows, three
+// rows ahead of the row being read), v and u in four slots, d and the pixel
+// radii (gamma alpha_p capped at bound, formed once per row, used by all four
+// iterations) in eight.
+//
+// At step s iteration l (1..4) updates row s - l: it forms z of its input
+// (iteration l - 1's output, or the staged row for l = 1) on row s - l + 1,
+// the row iteration l - 1 has just produced, and updates row s - l from z on
+// that row and on its own row (kept from the last step) and its carried input
+// row. Each iteration is active only on the rows the block's output rows
+// depend on: r0 - (4 - l) .. r1 + (4 - l).
+// The per-pixel arithmetic is the lean step's (the same expressions), so the
+// iterates are those of four single steps while the restart decisions agree;
+// the gap and restart-test sums are formed per row and strip (a lane's two
+// columns, then the warp's tree) into H x strips slots, summed in order by the
+// image's last block: a fixed order of its own (an image gives the same bits
+// alone and in any batch).
+// Traffic per pixel and four iterations: d, u, v, alpha read once (rows of a
+// block's halo again, from L2 mostly), u, v written once: about 40 B against
+// 4 x 40 B for four single steps.
+// ---------------------------------------------------------------------------
+constexpr int kQuadWin = 64;                        // window columns of a warp: two per lane
+constexpr int kQuadHalo = 4;                        // one column per iteration on each side
+constexpr int kQuadOut = kQuadWin - 2 * kQuadHalo;  // columns a warp writes
+constexpr int kQuadWarps = 4;                       // strips side by side per block
+constexpr int kQuadAhead = 3;                       // rows in flight beyond the row being read
+constexpr int kQuadSlotsUV = 4;                     // ring rows of v0, v1, u0, u1 (read at their own step)
+constexpr int kQuadSlotsD = 8;                      // ring rows of d and the radii (read by all four iterations)
+constexpr int kQuadRingFloats = kQuadSlotsUV * 4 * kQuadWin + kQuadSlotsD * 2 * kQuadWin;
+constexpr size_t kQuadSmem = (size_t)kQuadWarps * kQuadRingFloats * sizeof(float);
+
+__host__ __device__ constexpr int quad_strips(int W) { return (W + kQuadOut - 1) / kQuadOut; }
+
+__device__ __forceinline__ void cp_async16_zfill(void *dst, const void *src, unsigned n) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(n)
+                 : "memory");
+}
+
+// What one quad pass needs: an image's arrays (v = u when vsel), its
+// geometry, the block's rows [r0, r1) and first strip, the step's constants,
+// the momenta of the four iterations, and where the per-row sums go.
+struct QuadTile {
+    const float *D, *U0, *V0, *AL;
+    float *UO0, *VO0;
+    int64_t N;
+    int H, W, r0, r1, strip0;
+    float wh0, wh1, tau, rad, bnd;
+    float beta[4];
+    double *rowpart;  // ROWSUMS: the image's per-row, per-strip slots
+};
+
+// The momenta of four iterations from the state's tn and beta, as the
+// control would set them.
+__device__ __forceinline__ void quad_betas(double tn, double beta0, float (&beta)[4]) {
+    beta[0] = (float)beta0;
+#pragma unroll
+    for (int l = 1; l < 4; ++l) {
+        const double t2 = fista_t(tn);
+        beta[l] = (float)((tn - 1.0) / t2);
+        tn = t2;
+    }
+}
+
+// The march of one warp's strip (see above). REDO: three iterations, the
+// third's u written. ROWSUMS: each row's gap and restart-test sums over the
+// strip into p.rowpart[row x strips + strip] (the batched launch); else they
+// accumulate per lane in gsum, dsum over the block's rows (the ragged step's
+// per-tile slot).
+template <bool ALPHA, bool REDO, bool ROWSUMS>
+__device__ __forceinline__ void quad_pass(const QuadTile &p, int strip, double &gsum, double &dsum) {
+    constexpr int LV = REDO ? 3 : 4;  // iterations of the pass
+    extern __shared__ __align__(16) float quad_ring[];
+    const int H = p.H, W = p.W, r0 = p.r0, r1 = p.r1;
+    const int64_t N = p.N;
+    const float *D = p.D, *U0 = p.U0, *V0 = p.V0, *AL = p.AL;
+    const float *U1 = U0 + N, *V1 = V0 + N;
+    float *UO0 = p.UO0, *VO0 = p.VO0;
+    float *UO1 = UO0 + N, *VO1 = VO0 + N;
+    const float wh0 = p.wh0, wh1 = p.wh1, tau = p.tau, rad = p.rad, bnd = p.bnd;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nstrips = quad_strips(W);
+    float *ring = quad_ring + warp * kQuadRingFloats;
+    float *ruv = ring;                                  // [slot][v0, v1, u0, u1][64]
+    float *rd = ring + kQuadSlotsUV * 4 * kQuadWin;     // [slot][d, radius][64]
+    const int C0 = strip * kQuadOut - kQuadHalo;        // the window's first column (a multiple of 4)
+    const int wc = 2 * lane;                            // this lane's first window column
+    const int col = C0 + wc;
+    const bool colin = col >= 0 && col < W;             // both columns (W and col are even)
+    const bool hasr0 = col + 1 < W, hasr1 = col + 2 < W;
+    const bool outcol = lane >= kQuadHalo / 2 && lane < 32 - kQuadHalo / 2 && colin;  // written columns
+    const int sb = max(0, r0 - LV), se = r1 + LV - 1;   // steps: input rows sb .. se
+    auto issue = [&](int q) {
+        if (q <= se) {
+            const bool rowin = q < H;
+            const int64_t ro = (int64_t)q * W;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {  // 64 pieces of v0, v1, u0, u1: two per lane
+                const int k = lane + 32 * h, a = k >> 4, ch = k & 15;
+                const int cc = C0 + 4 * ch;
+                const bool ok = rowin && cc >= 0 && cc < W;
+                const float *base = a == 0 ? V0 : a == 1 ? V1 : a == 2 ? U0 : U1;
+                cp_async16_zfill(ruv + ((q & (kQuadSlotsUV - 1)) * 4 + a) * kQuadWin + 4 * ch,
+                                 base + (ok ? ro + cc : 0), ok ? 16u : 0u);
+            }
+            if (ALPHA || lane < 16) {  // d (and alpha): one piece per lane
+                const int a = lane >> 4, ch = lane & 15;
+                const int cc = C0 + 4 * ch;
+                const bool ok = rowin && cc >= 0 && cc < W;
+                const float *base = a == 0 ? D : AL;
+                cp_async16_zfill(rd + ((q & (kQuadSlotsD - 1)) * 2 + a) * kQuadWin + 4 * ch,
+                                 base + (ok ? ro + cc : 0), ok ? 16u : 0u);
+            }
+        }
+        cp_async_commit();
+    };
+    auto ld2 = [](const float *q, float (&o)[2]) {
+        const float2 v = *reinterpret_cast<const float2 *>(q);
+        o[0] = v.x;
+        o[1] = v.y;
+    };
+    // Level l's carried input row (iteration l's input v, u on the row
+    // after the one it updated last, and z of them); zero above the image.
+    float cv0[LV][2], cv1[LV][2], cu0[LV][2], cu1[LV][2], cz[LV][2];
+    float czu[2] = {0.f, 0.f};  // the check: z of the third iterate's u on the carried row
+#pragma unroll
+    for (int l = 0; l < LV; ++l)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) cv0[l][j] = cv1[l][j] = cu0[l][j] = cu1[l][j] = cz[l][j] = 0.f;
+    for (int q = 0; q < kQuadAhead; ++q) issue(sb + q);
+    for (int s = sb; s <= se; ++s) {
+        __syncwarp();  // every lane is past its reads of the slots refilled now
+        issue(s + kQuadAhead);
+        cp_async_wait<kQuadAhead>();
+        __syncwarp();  // row s is in, from every lane's copies
+        // the staged row s: the first iteration's new input row
+        float nv0[2], nv1[2], nu0[2], nu1[2], vleft = 0.f;
+        if (s < H) {
+            const float *rs = ruv + (s & (kQuadSlotsUV - 1)) * 4 * kQuadWin;
+            ld2(rs + 0 * kQuadWin + wc, nv0);
+            ld2(rs + 1 * kQuadWin + wc, nv1);
+            ld2(rs + 2 * kQuadWin + wc, nu0);
+            ld2(rs + 3 * kQuadWin + wc, nu1);
+            if (lane > 0) vleft = rs[1 * kQuadWin + wc - 1];
+            if (ALPHA) {  // alpha -> the pixel radius, in place (this lane's own entries)
+                float *ra = rd + ((s & (kQuadSlotsD - 1)) * 2 + 1) * kQuadWin + wc;
+                float al[2], rp[2];
+                ld2(ra, al);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const float r = rad * al[j];
+                    rp[j] = al[j] == 0.f ? 0.f : (r <= bnd ? r : bnd);
+                }
+                *reinterpret_cast<float2 *>(ra) = make_float2(rp[0], rp[1]);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 2; ++j) nv0[j] = nv1[j] = nu0[j] = nu1[j] = 0.f;
+        }
+#pragma unroll
+        for (int l = 0; l < LV; ++l) {
+            const int r = s - l - 1;  // the row iteration l + 1 updates
+            // z of this level's input on row r + 1 (iteration l's output there)
+            const int rn = r + 1;
+            float dn[2] = {0.f, 0.f};
+            if (rn >= sb && rn < H) ld2(rd + ((rn & (kQuadSlotsD - 1)) * 2 + 0) * kQuadWin + wc, dn);
+            float left = l == 0 ? vleft : __shfl_up_sync(0xffffffffu, nv1[1], 1);
+            if (l > 0 && lane == 0) left = 0.f;
+            float nz[2];
+            nz[0] = dn[0] + wh0 * (nv0[0] - cv0[l][0]) + wh1 * (nv1[0] - left);
+            nz[1] = dn[1] + wh0 * (nv0[1] - cv0[l][1]) + wh1 * (nv1[1] - nv1[0]);
+            float nzu[2] = {0.f, 0.f};
+            const bool check = !REDO && l == LV - 1;
+            if (check) {  // z of the third iterate's u on row r + 1
+                float lu = __shfl_up_sync(0xffffffffu, nu1[1], 1);
+                if (lane == 0) lu = 0.f;
+                nzu[0] = dn[0] + wh0 * (nu0[0] - cu0[l][0]) + wh1 * (nu1[0] - lu);
+                nzu[1] = dn[1] + wh0 * (nu0[1] - cu0[l][1]) + wh1 * (nu1[1] - nu1[0]);
+            }
+            float ou0[2] = {0.f, 0.f}, ou1[2] = {0.f, 0.f}, ov0[2] = {0.f, 0.f}, ov1[2] = {0.f, 0.f};
+            const int lo = max(0, r0 - (LV - 1 - l)), hi = min(H, r1 + (LV - 1 - l));
+            const bool act = r >= lo && r < hi;  // the same for the whole warp
+            float zr = __shfl_down_sync(0xffffffffu, cz[l][0], 1);
+            float zur = check ? __shfl_down_sync(0xffffffffu, czu[0], 1) : 0.f;
+            if (lane == 31) zr = zur = 0.f;
+            if (act) {
+                const bool hasn = r + 1 < H;
+                float rp[2] = {rad, rad};
+                if (ALPHA) ld2(rd + ((r & (kQuadSlotsD - 1)) * 2 + 1) * kQuadWin + wc, rp);
+                double gacc = 0.0, dacc = 0.0;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const bool hasr = j == 0 ? hasr0 : hasr1;
+                    const float zright = j == 0 ? cz[l][1] : zr;
+                    const float g0 = hasn ? wh0 * (nz[j] - cz[l][j]) : 0.f;
+                    const float g1 = hasr ? wh1 * (zright - cz[l][j]) : 0.f;
+                    const float a0 = cv0[l][j] + tau * g0;
+                    const float a1 = cv1[l][j] + tau * g1;
+                    const float nn = a0 * a0 + a1 * a1;
+                    const float sc = nn > rp[j] * rp[j] ? rp[j] * rsqrtf(nn) : 1.f;
+                    float un0 = a0 * sc, un1 = a1 * sc;
+                    if (!colin) un0 = un1 = 0.f;  // outside the image the dual is zero
+                    if (check && outcol) {
+                        dacc += (double)((cv0[l][j] - un0) * (un0 - cu0[l][j]) +
+                                         (cv1[l][j] - un1) * (un1 - cu1[l][j]));
+                        const float zuright = j == 0 ? czu[1] : zur;
+                        const float gu0 = hasn ? wh0 * (nzu[j] - czu[j]) : 0.f;
+                        const float gu1 = hasr ? wh1 * (zuright - czu[j]) : 0.f;
+                        gacc += (double)(rp[j] * sqrtf(gu0 * gu0 + gu1 * gu1) -
+                                         (gu0 * cu0[l][j] + gu1 * cu1[l][j]));
+                    }
+                    ou0[j] = un0;
+                    ou1[j] = un1;
+                    ov0[j] = un0 + p.beta[l] * (un0 - cu0[l][j]);
+                    ov1[j] = un1 + p.beta[l] * (un1 - cu1[l][j]);
+                }
+                if (check) {
+                    if (ROWSUMS) {
+                        // this row's sums over the strip (a fixed tree) into its slot
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) {
+                            gacc += __shfl_down_sync(0xffffffffu, gacc, o);
+                            dacc += __shfl_down_sync(0xffffffffu, dacc, o);
+                        }
+                        if (lane == 0) {
+                            double *part = p.rowpart + ((int64_t)r * nstrips + strip) * 2;
+                            part[0] = gacc;
+                            part[1] = dacc;
+                        }
+                    } else {
+                        gsum += gacc;
+                        dsum += dacc;
+                    }
+                }
+                if (l == LV - 1 && outcol) {  // the pass's output row (r0 <= r < r1 here)
+                    const int64_t o = (int64_t)r * W + col;
+                    *reinterpret_cast<float2 *>(UO0 + o) = make_float2(ou0[0], ou0[1]);
+                    *reinterpret_cast<float2 *>(UO1 + o) = make_float2(ou1[0], ou1[1]);
+                    if (!REDO) {
+                        *reinterpret_cast<float2 *>(VO0 + o) = make_float2(ov0[0], ov0[1]);
+                        *reinterpret_cast<float2 *>(VO1 + o) = make_float2(ov1[0], ov1[1]);
+                    }
+                }
+            }
+            // carry: this level's input row becomes the one of row r + 1;
+            // the next level's new input row is this level's output on row r
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                cv0[l][j] = nv0[j];
+                cv1[l][j] = nv1[j];
+                cu0[l][j] = nu0[j];
+                cu1[l][j] = nu1[j];
+                cz[l][j] = nz[j];
+                if (check) czu[j] = nzu[j];
+                nv0[j] = ov0[j];
+                nv1[j] = ov1[j];
+                nu0[j] = ou0[j];
+                nu1[j] = ou1[j];
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+
+// The per-image control after a quad pass: three plain iterations, then the
+// fourth with the check at the third iterate and the restart test; the update
+// to the fourth (in the other parity) stands unless the check passes, and then
+// the final u is the third's, formed again from pin by the redo.
+__device__ __forceinline__ void quad_control(const IsoState &st, const IsoImage &im, int max_iter, double gap,
+                                             double dot, int pin, int *live, IsoState *out) {
+    IsoState s2 = st;
+    for (int l = 0; l < 3; ++l) control(s2, im, max_iter, false, false, 0.0, 0.0, pin, live);
+    control(s2, im, max_iter, true, true, gap, dot, pin, live);
+    if (s2.status != kLive) {
+        s2.redo = 3;
+        s2.redo_vsel = st.vsel;
+        s2.redo_tn = st.tn;
+        s2.redo_beta = st.beta;
+    }
+    *out = s2;
+}
+
+// REDO: the final iterate (the third's u) of images whose quad's check passed
+// (state redo == 3), from that quad's input buffers (fin_par, v = u when
+// redo_vsel) and momenta (redo_tn, redo_beta), into the other parity's u.
+template <bool ALPHA, bool REDO>
+__global__ void __launch_bounds__(32 * kQuadWarps, 4) iso2d_quad_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    if (!REDO) asm volatile("griddepcontrol.wait;" ::: "memory");  // a programmatic dependent of the previous step
+    const int b = REDO ? (int)blockIdx.z : step_image(bf, blockIdx.z);
+    if (b < 0) return;
+    const IsoState st = bf.st[b];
+    if (REDO) {
+        if (st.redo != 3) return;
+    } else {
+        if (st.status != kLive) return;
+        const int it = st.it;
+        if (it <= 0 || (it & 3) != 1 || it + 3 >= A.max_iter || st.zero_in) {
+            if (threadIdx.x == 0) atomicExch(bf.err, 3);
+            return;
+        }
+    }
+    const IsoImage im = bf.img[b];
+    const int H = (int)A.g.L[0], W = (int)A.g.L[1];
+    const int64_t N = A.g.N;
+    const int pin = REDO ? st.fin_par : A.par, pout = pin ^ 1;
+    const bool vsel = REDO ? st.redo_vsel != 0 : st.vsel != 0;
+    QuadTile p;
+    p.D = static_cast<const float *>(bf.d) + (int64_t)b * N;
+    p.U0 = static_cast<const float *>(bf.U[pin]) + (int64_t)b * 2 * N;
+    p.V0 = vsel ? p.U0 : static_cast<const float *>(bf.V[pin]) + (int64_t)b * 2 * N;
+    p.AL = ALPHA ? static_cast<const float *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
+    p.UO0 = static_cast<float *>(bf.U[pout]) + (int64_t)b * 2 * N;
+    p.VO0 = static_cast<float *>(bf.V[pout]) + (int64_t)b * 2 * N;
+    p.N = N;
+    p.H = H;
+    p.W = W;
+    p.r0 = (int)blockIdx.y * A.rows;
+    p.r1 = min(H, p.r0 + A.rows);
+    p.strip0 = (int)blockIdx.x * kQuadWarps;
+    p.wh0 = (float)c.wh[0];
+    p.wh1 = (float)c.wh[1];
+    p.tau = (float)c.tau;
+    p.rad = (float)im.radius;
+    p.bnd = (float)im.bound;
+    quad_betas(REDO ? st.redo_tn : st.tn, REDO ? st.redo_beta : st.beta, p.beta);
+    p.rowpart = bf.part + (int64_t)b * bf.max_part * 2;
+    const int nstrips = quad_strips(W);
+    const int strip = p.strip0 + (int)(threadIdx.x >> 5);
+    double gs = 0.0, ds = 0.0;
+    if (strip < nstrips) quad_pass<ALPHA, REDO, true>(p, strip, gs, ds);
+    if (REDO) return;
+    __syncthreads();
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (!arrive_last(bf.ticket + b, gridDim.x * gridDim.y, &flag)) return;
+    const int nslot = H * nstrips;
+    const double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    const double gap = sum_partials(part, nslot, 2, 0, sh);
+    const double dot = sum_partials(part, nslot, 2, 1, sh);
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2;
+    quad_control(st, im, A.max_iter, gap, dot, pin, bf.live, &s2);
+    bf.st[b] = s2;
+}
+
+// ---------------------------------------------------------------------------
 // The ragged step: images of any size in one arena, a device-resident work
 // list of (image, tile) items, each image at its own iteration with its own
 // buffer parity (its state's fin_par). One launch of single steps (each
@@ -1286,6 +1653,13 @@ __global__ void iso2d_redo_state(IsoState *st, int64_t B) {
 // after it (two iterations per launch, as the batched pair launch); an
 // image's blocks run in the launch its state asks for.
 // ---------------------------------------------------------------------------
+
+// Whether the ragged step's quad launch takes an image (four iterations from
+// iteration 1 mod 4, not across max_iter; slots with quad tiles only).
+__device__ __forceinline__ bool ragged_quad_ok(const IsoState &st, const RagSlot &sl) {
+    const int it = st.it;
+    return sl.nquad > 0 && it > 0 && (it & 3) == 1 && it + 3 < sl.max_iter && !st.zero_in && sl.H >= 2;
+}
 
 // The pair variant an image's state asks for in the ragged step: 0 (iterations
 // 1 and 2 mod 4), 1 (3 and 4 mod 4, with the check), -1 (a single step).
@@ -1354,6 +1728,7 @@ __global__ void __launch_bounds__(128) iso2d_ragged_kernel(const RagItem *__rest
     const RagSlot sl = slots[item.slot];
     const IsoState st = bf.st[item.slot];
     if (st.status != kLive) return;
+    if (ragged_quad_ok(st, sl)) return;                  // the quad takes it
     if (pairs && ragged_pair_kind(st, sl) >= 0) return;  // the pair variants take it
     const int it = st.it;
     const bool do_gap = (it > 0 && ((it & 3) == 0 || it == sl.max_iter)) || (it == 0 && st.warm);
@@ -1378,7 +1753,7 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_ragged_pair_kernel(co
     const int b = item.slot;
     const RagSlot sl = slots[b];
     const IsoState st = bf.st[b];
-    if (st.status != kLive || ragged_pair_kind(st, sl) != (GAP2 ? 1 : 0)) return;
+    if (st.status != kLive || ragged_quad_ok(st, sl) || ragged_pair_kind(st, sl) != (GAP2 ? 1 : 0)) return;
     const IsoImage im = bf.img[b];
     const int pin = st.fin_par, pout = pin ^ 1;
     PairTile<T> p;
@@ -1430,6 +1805,65 @@ __global__ void __launch_bounds__(128, GAP2 ? 3 : 4) iso2d_ragged_pair_kernel(co
     } else {
         control(s2, im, sl.max_iter, false, false, 0.0, 0.0, pin, bf.live);
     }
+    bf.st[b] = s2;
+}
+
+// The ragged step's quad variant: an item's block of strips (the slot's quad
+// rows x kQuadWarps strips) of an image whose state asks for four iterations;
+// the block's gap and restart-test sums (each lane's over the block's rows,
+// then the block's tree) go to the item's partial slot, summed in order by
+// the image's last block.
+__global__ void __launch_bounds__(32 * kQuadWarps, 4) iso2d_ragged_quad_kernel(const RagItem *__restrict__ items,
+                                                                              const int *__restrict__ n_items,
+                                                                              const RagSlot *__restrict__ slots,
+                                                                              IsoBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    if ((int)blockIdx.x >= *n_items) return;
+    const RagItem item = items[blockIdx.x];
+    const int b = item.slot;
+    const RagSlot sl = slots[b];
+    const IsoState st = bf.st[b];
+    if (st.status != kLive || !ragged_quad_ok(st, sl)) return;
+    const IsoImage im = bf.img[b];
+    const int pin = st.fin_par, pout = pin ^ 1;
+    QuadTile p;
+    p.D = static_cast<const float *>(bf.d) + sl.off;
+    p.U0 = static_cast<const float *>(bf.U[pin]) + 2 * sl.off;
+    p.V0 = st.vsel ? p.U0 : static_cast<const float *>(bf.V[pin]) + 2 * sl.off;
+    p.AL = nullptr;
+    p.UO0 = static_cast<float *>(bf.U[pout]) + 2 * sl.off;
+    p.VO0 = static_cast<float *>(bf.V[pout]) + 2 * sl.off;
+    p.N = (int64_t)sl.H * sl.W;
+    p.H = sl.H;
+    p.W = sl.W;
+    p.r0 = item.r0;
+    p.r1 = min(sl.H, item.r0 + sl.qrows);
+    p.strip0 = item.cs;
+    p.wh0 = (float)sl.wh0;
+    p.wh1 = (float)sl.wh1;
+    p.tau = (float)sl.tau;
+    p.rad = (float)im.radius;
+    p.bnd = (float)im.bound;
+    quad_betas(st.tn, st.beta, p.beta);
+    p.rowpart = nullptr;
+    const int strip = p.strip0 + (int)(threadIdx.x >> 5);
+    double gs = 0.0, ds = 0.0;
+    if (strip < quad_strips(sl.W)) quad_pass<false, false, false>(p, strip, gs, ds);
+    const double gsum = block_sum(gs, sh);
+    const double dsum = block_sum(ds, sh);
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[item.blk * 2 + 0] = gsum;
+        part[item.blk * 2 + 1] = dsum;
+    }
+    if (!arrive_last(bf.ticket + b, sl.nquad, &flag)) return;
+    const double gap = sum_partials(part, sl.nquad, 2, 0, sh);
+    const double dot = sum_partials(part, sl.nquad, 2, 1, sh);
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2;
+    quad_control(st, im, sl.max_iter, gap, dot, pin, bf.live, &s2);
     bf.st[b] = s2;
 }
 
@@ -2045,6 +2479,24 @@ void launch_3d_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuf
     else launch_3d_v<T, ALPHA, false, false>(grid, A, c, bf, s);
 }
 
+// The quad launch: blocks of kQuadWarps strips and `rows` rows (32; fewer,
+// down to 8, while the launch has too few blocks to spread over the SMs).
+void launch_quad(StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
+    static const int rows_hint = [] {  // tuning hint FASTPROX_B200_QUAD_ROWS
+        const char *v = std::getenv("FASTPROX_B200_QUAD_ROWS");
+        const int r = v ? std::atoi(v) : 0;
+        return (r >= 4 && r <= 256) ? r : 0;
+    }();
+    const int64_t H = A.g.L[0];
+    const int gx = (quad_strips((int)A.g.L[1]) + kQuadWarps - 1) / kQuadWarps;
+    int rows = rows_hint ? rows_hint : 32;
+    while (!rows_hint && rows > 8 && A.nimg * gx * ((H + rows - 1) / rows) < tail_blocks()) rows /= 2;
+    A.rows = rows;
+    const dim3 grid((unsigned)gx, (unsigned)((H + rows - 1) / rows), (unsigned)A.nimg);
+    if (c.has_alpha) launch_step(iso2d_quad_kernel<true, false>, grid, 32 * kQuadWarps, kQuadSmem, s, A, c, bf);
+    else launch_step(iso2d_quad_kernel<false, false>, grid, 32 * kQuadWarps, kQuadSmem, s, A, c, bf);
+}
+
 template <class T>
 cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, const StepShape &sh, int par,
                    int variant, int64_t nimg, cudaStream_t s) {
@@ -2056,6 +2508,13 @@ cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, co
     A.nimg = nimg;
     A.row_part = 0;
     if (nimg <= 0) return cudaSuccess;
+    if (variant == kVariantQuad) {
+        if constexpr (std::is_same<T, float>::value) {
+            launch_quad(A, c, bf, s);
+            return cudaGetLastError();
+        }
+        return cudaErrorInvalidValue;
+    }
     if (variant == kVariantPair || variant == kVariantPairGap) {
         launch_pair<T>(sh, A, c, bf, s, variant == kVariantPairGap);
         return cudaGetLastError();
@@ -2151,6 +2610,16 @@ bool iso_ragged_pairs(int dtype, int vec) {
     return pairs_enabled() && dtype == 1 && vec == 4;
 }
 
+cudaError_t iso_ragged_quad_step(const RagItem *items, const int *n_items, int grid, const RagSlot *slots,
+                                 const IsoBuffers &bf, cudaStream_t s) {
+    if (grid <= 0) return cudaSuccess;
+    iso2d_ragged_quad_kernel<<<grid, 32 * kQuadWarps, kQuadSmem, s>>>(items, n_items, slots, bf);
+    return cudaGetLastError();
+}
+
+int iso_quad_strips(int W) { return quad_strips(W); }
+int iso_quad_warps() { return kQuadWarps; }
+
 int iso_setup_blocks(const Geometry &g) {
     int64_t nb = (g.N + kScanThreads * 8 - 1) / (kScanThreads * 8);
     if (nb > 128) nb = 128;
@@ -2234,8 +2703,36 @@ cudaError_t iso_live_list(const IsoState *st, int64_t B, int *lmap, int *lcnt, c
     return cudaGetLastError();
 }
 
-cudaError_t iso_redo(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
+bool iso_quad_ok(int dtype, const Geometry &g, int max_part) {
+    static const bool on = [] {  // tuning hint FASTPROX_B200_QUADS=0: no quad launches
+        const char *v = std::getenv("FASTPROX_B200_QUADS");
+        return !(v && v[0] == '0' && v[1] == 0);
+    }();
+    return on && pairs_enabled() && dtype == 1 && g.k == 2 && g.L[1] >= 4 && g.L[1] % 4 == 0 && g.L[0] >= 2 &&
+           g.L[0] * g.L[1] < (int64_t(1) << 31) && iso_quad_parts(g) <= max_part;
+}
+
+int64_t iso_quad_parts(const Geometry &g) {
+    return g.k == 2 ? g.L[0] * (int64_t)quad_strips((int)std::min<int64_t>(g.L[1], 1 << 30)) : 0;
+}
+
+cudaError_t iso_redo(int dtype, const Geometry &g, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s,
+                     bool quads) {
     if (g.k != 2 || g.B <= 0 || g.N <= 0) return cudaSuccess;
+    if (quads && dtype == 1) {
+        // the quad's redo: three iterations over whole images, blocks of 32 rows
+        StepArgs A;
+        A.g = g;
+        A.max_iter = c.max_iter;
+        A.par = 0;
+        A.rows = 32;
+        A.nimg = g.B;
+        A.row_part = 0;
+        const int gx = (quad_strips((int)g.L[1]) + kQuadWarps - 1) / kQuadWarps;
+        const dim3 grid((unsigned)gx, (unsigned)((g.L[0] + A.rows - 1) / A.rows), (unsigned)g.B);
+        if (c.has_alpha) iso2d_quad_kernel<true, true><<<grid, 32 * kQuadWarps, kQuadSmem, s>>>(A, c, bf);
+        else iso2d_quad_kernel<false, true><<<grid, 32 * kQuadWarps, kQuadSmem, s>>>(A, c, bf);
+    }
     const dim3 grid((unsigned)std::min<int64_t>((g.N + 255) / 256, 1024), (unsigned)g.B);
     if (dtype == 1) {
         if (c.has_alpha) iso2d_redo_kernel<float, true><<<grid, 256, 0, s>>>(g, c, bf);

@@ -51,6 +51,8 @@ struct fp_workspace {
     uint8_t *an_flag = nullptr;
     int *an_parent = nullptr, *an_cnt = nullptr;
     unsigned long long *an_sum = nullptr;
+    void *an_ys = nullptr, *an_segv = nullptr, *an_wt = nullptr;  // the fibre-major passes
+    int *an_segk = nullptr;
     double *gammas = nullptr;
     double *part = nullptr;
     unsigned *ticket = nullptr;
@@ -95,8 +97,8 @@ struct fp_workspace {
     // launches of the last call by kind (0 single, 1 pair, 2 pair with the check)
     bool time_steps = false;
     std::vector<cudaEvent_t> tev;
-    double tms[3] = {0.0, 0.0, 0.0};
-    int64_t tcount[3] = {0, 0, 0};
+    double tms[4] = {0.0, 0.0, 0.0, 0.0};
+    int64_t tcount[4] = {0, 0, 0, 0};
     // small anisotropic solves: a captured chunk of rounds, replayed while the
     // call's constants, the launched images and the live list are the same
     cudaGraphExec_t an_graph = nullptr;
@@ -113,6 +115,9 @@ struct fp_workspace {
     bool warm = false, seeded = false, dual_valid = false, valid = false;
     double deriv_tol = 0.0;
     int deriv_max_iter = 10000;
+    // the last fp_vjp's gradients per image: the step's (B) and the axis
+    // weights' (B x k), before their sums over the batch
+    std::vector<double> vjp_gg_img, vjp_gw_img;
     double deriv_residual = 0.0;
     int deriv_iters = 0;
 };

@@ -12,8 +12,11 @@ Serving (``serve_stream``):
   into free slots as they arrive, iterating together with those already on
   the GPU, leaving as each meets its own gap; their dual state stays on the
   device for the whole solve.
-* anisotropic and 3D requests run as their own calls on a pool of worker
-  streams, so their kernels overlap with the batch's.
+* anisotropic and 3D requests of the same shape that wait together are
+  stacked into one batch on the device (one call, one step per image, each
+  image stopped at its own gap; the 3D volumes are all 128^3, so they batch
+  whenever several wait), run on a pool of worker streams, so their kernels
+  overlap with the ragged batch's.
 * admission is capped by an HBM budget: a request waits while the memory its
   solve needs (its workspace, or its share of the batch arena) would exceed it.
 * the batch runs a bounded number of iterations per loop pass, so arrivals
@@ -93,14 +96,63 @@ def _solve_one(r):
     return z[0], info
 
 
+def solve_group(group, ops=None):
+    """One call for requests of the same kind and shape: their images stacked
+    into one batch on the device, one step per image (fp_prox_steps), each
+    image stopped at its own gap. ops caches an operator per kind (its
+    workspaces per batch shape). Returns the results in the group's order."""
+    import torch
+
+    from .image_tv import TVAniso, TVIso
+    kind = group[0].kind
+    if ops is None:
+        ops = {}
+    op = ops.get(kind)
+    if op is None:
+        op = ops[kind] = TVIso(3) if kind == "iso3d" else (TVIso(2) if kind == "iso2d" else TVAniso(2))
+    x = torch.stack([r.x for r in group])
+    steps = torch.tensor([r.gamma for r in group], dtype=torch.float64, device=x.device)
+    z, info = op.solve(x, steps, tol=group[0].tol, max_iter=5000, with_dual=False)
+    return [z[i] for i in range(len(group))], info
+
+
+class Admission:
+    """HBM-budget admission: a request is admitted while the device memory
+    its solve needs (its workspace, or its share of a batch arena) fits under
+    the budget next to what is already admitted; it waits otherwise, and its
+    bytes return to the budget when it finishes. Host-side accounting only,
+    thread-safe (workers release from their threads)."""
+
+    def __init__(self, budget_bytes, reserved=0):
+        self.budget = float(budget_bytes)
+        self.used = float(reserved)
+        self.peak = self.used
+        self._lock = threading.Lock()
+
+    def try_admit(self, nbytes):
+        with self._lock:
+            if self.used + nbytes > self.budget:
+                return False
+            self.used += nbytes
+            self.peak = max(self.peak, self.used)
+            return True
+
+    def release(self, nbytes):
+        with self._lock:
+            self.used -= nbytes
+            if self.used < -1e-6:
+                raise RuntimeError("admission released more than it admitted")
+
+
 def _ws_bytes(r):
     n = r.side ** 3 if r.kind == "iso3d" else r.side * r.side
     k = 3 if r.kind == "iso3d" else 2
     return n * 4 * (3 + 5 * k) + n * 24
 
 
-def serve_stream(reqs, src, budget_bytes=120e9, workers=16, steps=8):
-    """Continuous batching. Returns per-request latencies (s) and the span."""
+def serve_stream(reqs, src, budget_bytes=120e9, workers=16, steps=8, group_max=8, keep=False):
+    """Continuous batching. Returns per-request latencies (s) and the span;
+    with keep, each request's result stays in r.z."""
     import torch
 
     from .batch import RaggedBatch
@@ -109,20 +161,23 @@ def serve_stream(reqs, src, budget_bytes=120e9, workers=16, steps=8):
     # worker threads use the device while the batch runs: plain launches
     batch = RaggedBatch(max_images=512, max_pixels=arena_px, graphs=False, stream=main.cuda_stream)
     arena_bytes = arena_px * 44  # d 4, u and v ping-pong 32, dual 8
-    used = arena_bytes
-    lock = threading.Lock()
+    adm = Admission(budget_bytes, reserved=arena_bytes)
     streams = [torch.cuda.Stream() for _ in range(workers)]
     tls = threading.local()
     counter = iter(range(1 << 30))
 
-    def work(r, ready):
+    def work(group, ready):
         if not hasattr(tls, "s"):
             tls.s = streams[next(counter) % workers]
+            tls.ops = {}
         tls.s.wait_event(ready)
         with torch.cuda.stream(tls.s):
-            z, info = _solve_one(r)
+            zs, _ = solve_group(group, tls.ops)
             tls.s.synchronize()
-        return r
+        if keep:
+            for r, z in zip(group, zs):
+                r.z = z
+        return group
 
     pool = cf.ThreadPoolExecutor(workers)
     futures = {}
@@ -142,6 +197,7 @@ def serve_stream(reqs, src, budget_bytes=120e9, workers=16, steps=8):
             waiting.append(r)
             nxt += 1
         still = []
+        groups = {}
         for r in waiting:
             if r.kind == "iso2d":
                 slot = batch.admit(r.x, r.gamma, r.tol, max_iter=5000)
@@ -150,30 +206,38 @@ def serve_stream(reqs, src, budget_bytes=120e9, workers=16, steps=8):
                 else:
                     inflight[slot] = r
             else:
-                with lock:
-                    ok = used + r.bytes <= budget_bytes
-                    if ok:
-                        used += r.bytes
-                if ok:
-                    ready = torch.cuda.Event()
-                    ready.record(main)
-                    futures[pool.submit(work, r, ready)] = r
+                # anisotropic and 3D requests of one shape waiting together
+                # solve as one batch (up to group_max), admitted as one
+                g = groups.setdefault((r.kind, r.side), [])
+                if len(g) < group_max:
+                    g.append(r)
                 else:
                     still.append(r)
-        waiting = still
+        for g in groups.values():
+            nbytes = sum(r.bytes for r in g)
+            if adm.try_admit(nbytes):
+                ready = torch.cuda.Event()
+                ready.record(main)
+                futures[pool.submit(work, g, ready)] = (g, nbytes)
+            else:
+                still.extend(g)
+        waiting = sorted(still, key=lambda q: q.i)
         if batch.pending:
             for slot, z, gap, it, conv in batch.run(steps=steps, max_chunks=1):
                 r = inflight.pop(slot)
+                if keep:
+                    r.z = z
                 lat[r.i] = time.perf_counter() - t0 - r.t
                 done += 1
         finished = [f for f in futures if f.done()]
         for f in finished:
-            r = futures.pop(f)
+            g, nbytes = futures.pop(f)
             f.result()
-            lat[r.i] = time.perf_counter() - t0 - r.t
-            with lock:
-                used -= r.bytes
-            done += 1
+            tnow = time.perf_counter() - t0
+            for r in g:
+                lat[r.i] = tnow - r.t
+            adm.release(nbytes)
+            done += len(g)
         if not batch.pending and not finished and not (nxt < len(reqs) and reqs[nxt].t <= now):
             time.sleep(0.0005)
     span = time.perf_counter() - t0

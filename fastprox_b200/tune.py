@@ -10,9 +10,10 @@ with the 4 steps these choose; 64-row tiles were chosen when offered and ran
 with most images retired, cannot fill the SMs with).
 
 A tuning solve runs 16 iterations (tol 0) of every image with each
-candidate; the choice changes how work is tiled and how often the host
-polls, never the iterations of an image (the same tiling is then used for
-every image of that class, so results stay reproducible).
+candidate (tile height, steps per chunk, temporal-blocking depth); the
+choice changes how work is tiled and how often the host polls, never the
+iterations of an image (the same tiling is then used for every image of that
+class, so results stay reproducible).
 """
 
 from __future__ import annotations
@@ -25,6 +26,7 @@ import time
 
 ROWS = (8, 16, 32)
 STEPS = (4, 8, 16)
+DEPTHS = (2, 4)  # iterations per launch in steady state: pairs, or quads
 _CACHE: dict = {}
 _PATH = pathlib.Path(os.environ.get("FASTPROX_B200_TUNE", str(pathlib.Path.home() / ".cache" / "fastprox_b200"
                                                                 / "tune.json")))
@@ -55,29 +57,32 @@ def _save():
 
 
 def tune(images, max_pixels, retune=False):
-    """images: [(x (H, W) CUDA tensor, gamma, tol)]. Returns {'rows', 'steps'}."""
+    """images: [(x (H, W) CUDA tensor, gamma, tol)]. Returns {'rows', 'steps',
+    'depth'}: the tile height, the steps per chunk, and the temporal-blocking
+    depth (2: pair launches, 4: quad launches where the rows allow)."""
     import torch
 
     from .batch import RaggedBatch
     _load()
-    key = shape_class([tuple(x.shape[-2:]) for x, _, _ in images])
+    key = shape_class([tuple(x.shape[-2:]) for x, _, _ in images]) + "_d"
     if key in _CACHE and not retune:
         return _CACHE[key]
     best, best_t = None, math.inf
-    for rows in ROWS:
-        for steps in STEPS:
-            b = RaggedBatch(len(images), max_pixels, rows=rows)
-            for x, g, _ in images:
-                b.admit(x, g, 0.0, max_iter=16)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            while b.pending:
-                b.run(steps=steps)
-            torch.cuda.synchronize()
-            t = time.perf_counter() - t0
-            if t < best_t:
-                best, best_t = {"rows": rows, "steps": steps}, t
-            del b
+    for depth in DEPTHS:
+        for rows in ROWS:
+            for steps in STEPS:
+                b = RaggedBatch(len(images), max_pixels, rows=rows, quads=depth == 4)
+                for x, g, _ in images:
+                    b.admit(x, g, 0.0, max_iter=16)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                while b.pending:
+                    b.run(steps=steps)
+                torch.cuda.synchronize()
+                t = time.perf_counter() - t0
+                if t < best_t:
+                    best, best_t = {"rows": rows, "steps": steps, "depth": depth}, t
+                del b
     _CACHE[key] = best
     _save()
     return best

@@ -8,9 +8,11 @@ dict (bench.py --workload NAME):
   ragged batch (tuned tiling, captured graphs) against the plain per-image
   loop of fp_prox calls.
 * ``vjp``       (16, 3, 256, 256) fp32 phantom + noise(0.1), gamma 0.1, loss = MSE
-  to the clean phantom: forward + implicit VJP time and memory, the VJP
-  against the reference's fp_vjp and float64 central differences, against
-  400 unrolled FISTA iterations in torch autograd.
+  to the clean phantom: forward + implicit VJP time and memory against 400
+  unrolled FISTA iterations in torch autograd; then (vjp_checks) the VJP
+  against float64 central differences on 32 directions and the float32
+  gradient's error against the float64 one (tests/test_gpu_vjp.py checks it
+  against the reference's fp_vjp).
 * ``serve``     Poisson arrivals of denoising requests (see serve.py).
 Seeded synthetic data throughout.
 """
@@ -110,7 +112,7 @@ def uneven(args):
     tune_s = time.perf_counter() - t0
 
     def ragged():
-        b = RaggedBatch(len(xs), cap, rows=choice["rows"])
+        b = RaggedBatch(len(xs), cap, rows=choice["rows"], quads=choice.get("depth", 4) == 4)
         outs = [torch.empty_like(x) for x in xs]
         e0, e1 = _events()
         e0.record()
@@ -146,7 +148,64 @@ def uneven(args):
             "speedup_vs_plain": t_plain / t_rag, "seconds": t_rag, "plain_seconds": t_plain,
             "tuned": choice, "tune_seconds": tune_s, "converged": int(sum(c for _, c in res)),
             "max_rel_diff_vs_plain": max(errs), "achieved_GBs": 36 * pix_iters / t_rag / 1e9,
-            "kernel_launches": st["kernel_launches"], "graph_steps": st["steps"], "pixels": total_px}
+            "kernel_launches": st["kernel_launches"], "graph_steps": st["steps"], "pixels": total_px,
+            # a seeded sample of the ragged results, for a comparison with the
+            # reference (bench.py; not part of the printed line)
+            "_sample": [(int(i), imgs[i], float(gammas[i]), float(tols[i]), outs[i].cpu().numpy(), int(res[i][0]))
+                        for i in np.random.default_rng(5).choice(len(xs), 8, replace=False)]}
+
+
+def vjp_checks(noisy, clean, gamma=0.1, ndir=32, h=1e-6, seed=1, tol64=1e-12):
+    """The implicit VJP of the (B, C, H, W) workload's loss (MSE to the clean
+    phantom) checked three ways, all in float64 on the GPU unless stated:
+    * central differences: for ndir random unit directions d (seeded), the
+      VJP's <gx, d> against (<g, z(x + h d)> - <g, z(x - h d)>) / 2h, g the
+      loss's cotangent at z, solves at gap tol64 (and the same for gamma);
+    * the float32 solve at gap 1e-6 and its VJP against the float64 one: the
+      error of the float32 gradient, stated (its flat regions are read off an
+      iterate certified to about 1e-3 relative, so small regions can differ).
+    Returns the worst relative errors."""
+    import torch
+
+    from .image_tv import TVIso
+    from .torch import tv_iso
+    x64 = torch.as_tensor(noisy, device="cuda").double()
+    c64 = torch.as_tensor(clean, device="cuda").double()
+    n = x64.numel()
+
+    def grads(x, c, tol, dtype):
+        xr = x.to(dtype).clone().requires_grad_(True)
+        g = torch.tensor(gamma, device="cuda", dtype=dtype, requires_grad=True)
+        z = tv_iso(xr, g, tol=tol, max_iter=10 ** 6, deriv_tol=1e-12 if dtype == torch.float64 else None)
+        loss = ((z - c.to(dtype)) ** 2).mean()
+        loss.backward()
+        return z.detach(), xr.grad.detach().double(), float(g.grad)
+
+    z64, gx64, gg64 = grads(x64, c64, tol64, torch.float64)
+    cot = 2.0 * (z64 - c64) / n  # d loss / dz at the float64 solution
+    img = tuple(x64.shape[-2:])
+    xb = x64.reshape((-1,) + img)
+    cb = cot.reshape((-1,) + img)
+    op = TVIso(2)
+
+    def fwd(xx, gam):
+        return op.solve(xx, gam, tol=tol64, max_iter=10 ** 6, with_dual=False)[0]
+
+    rng = np.random.default_rng(seed)
+    worst_fd = 0.0
+    for _ in range(ndir):
+        d = torch.as_tensor(rng.normal(size=xb.shape), device="cuda")
+        d = d / d.norm()
+        fd = float(((fwd(xb + h * d, gamma) - fwd(xb - h * d, gamma)) * cb).sum()) / (2 * h)
+        an = float((gx64.reshape(xb.shape) * d).sum())
+        worst_fd = max(worst_fd, abs(fd - an) / max(abs(an), 1e-12 * float(gx64.norm())))
+    fdg = float(((fwd(xb, gamma + h) - fwd(xb, gamma - h)) * cb).sum()) / (2 * h)
+    err_gamma = abs(fdg - gg64) / max(abs(fdg), 1e-300)
+    _, gx32, gg32 = grads(x64, c64, 1e-6, torch.float32)
+    return {"fd_directions": ndir, "fd_h": h, "fd_max_rel_err": worst_fd, "fd_gamma_rel_err": err_gamma,
+            "tol": tol64,
+            "f32_vs_f64_gx_rel_err": float((gx32 - gx64).norm() / gx64.norm()),
+            "f32_vs_f64_ggamma_rel_err": abs(gg32 - gg64) / max(abs(gg64), 1e-300)}
 
 
 def vjp(args):
@@ -190,10 +249,13 @@ def vjp(args):
     torch.cuda.synchronize()
     t_unrolled = e0.elapsed_time(e1) / 1e3
     peak_unrolled = torch.cuda.max_memory_allocated() - base
-    return {"workload": "vjp", "metric": "forward+backward seconds, (16,3,256,256) fp32, implicit VJP",
-            "value": t_ours, "unit": "s", "peak_torch_bytes": int(peak_ours),
-            "unrolled400_seconds": t_unrolled, "unrolled400_peak_bytes": int(peak_unrolled),
-            "loss": float(loss.detach()), "loss_unrolled400": float(loss_u.detach()), "ggamma": float(gg)}
+    out = {"workload": "vjp", "metric": "forward+backward seconds, (16,3,256,256) fp32, implicit VJP",
+           "value": t_ours, "unit": "s", "peak_torch_bytes": int(peak_ours),
+           "unrolled400_seconds": t_unrolled, "unrolled400_peak_bytes": int(peak_unrolled),
+           "loss": float(loss.detach()), "loss_unrolled400": float(loss_u.detach()), "ggamma": float(gg)}
+    if not getattr(args, "no_checks", False):
+        out["checks"] = vjp_checks(noisy.reshape(16, 3, 256, 256), clean.reshape(16, 3, 256, 256))
+    return out
 
 
 def _unrolled_fista(x, gamma, iters):

@@ -249,8 +249,16 @@ FP_API fp_status fp_b200_workspace_stats(const fp_workspace *ws, int64_t *kernel
  * launches and adds a little to the call. fp_b200_workspace_step_times then
  * gives the last call's total milliseconds and launches of one kind: 0 single
  * iterations, 1 two iterations per launch, 2 two iterations the second of
- * which carries the gap check. For benchmarks. */
+ * which carries the gap check, 3 four iterations per launch (the fourth with
+ * the gap check). For benchmarks. */
 FP_API fp_status fp_b200_workspace_time_steps(fp_workspace *ws, int on);
+/* The last fp_vjp (or fp_vjp_device) on ws, per image, before its sums over
+ * the batch: ggamma[b] the gradient of image b's step, gweights[b k + a] that
+ * of axis weight a from image b (k = the operator's ndim); either may be NULL.
+ * For callers with one step per image (fp_prox_steps), whose gradient
+ * fp_vjp returns summed. count must be the batch size (FP_EINVAL otherwise, or
+ * before any fp_vjp). No counterpart in the reference ABI. */
+FP_API fp_status fp_b200_vjp_images(const fp_workspace *ws, double *ggamma, double *gweights, int64_t count);
 FP_API fp_status fp_b200_workspace_step_times(const fp_workspace *ws, int kind, double *ms, int64_t *launches);
 
 /* Workspaces take their device memory from a stream-ordered pool per device
@@ -297,6 +305,10 @@ FP_API fp_status fp_b200_batch_set_graphs(fp_b200_batch *bt, int on);
 /* Rows per tile of images admitted from now on (0: chosen from the image
  * height); the tuner sets it. */
 FP_API fp_status fp_b200_batch_set_rows(fp_b200_batch *bt, int rows);
+/* Quad launches (four iterations per launch) for the float images of rows of a
+ * multiple of 4 pixels admitted from now on: on (default) or off, and the rows
+ * of a quad tile (0 keeps the current, 32 by default). For the tuner. */
+FP_API fp_status fp_b200_batch_set_quads(fp_b200_batch *bt, int on, int rows);
 FP_API fp_status fp_b200_batch_admit(fp_b200_batch *bt, const void *x, int64_t height, int64_t width, double gamma,
                                      double tol, int max_iter, void *z, int *slot);
 FP_API fp_status fp_b200_batch_run(fp_b200_batch *bt, int steps, int max_chunks, int *finished, double *gaps,

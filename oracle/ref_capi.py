@@ -187,9 +187,12 @@ def solve(x, gamma, *, iso=True, k=2, w=None, spatial=None, tol=1e-6, max_iter=1
             L.fp_op_free(op)
 
 
-def vjp(res: Result, g, nparams: int):
-    """fp_vjp at a kept Result: (gx, ggamma, gparams)."""
+def vjp(res: Result, g, nparams: int, deriv_tol=None):
+    """fp_vjp at a kept Result: (gx, ggamma, gparams); deriv_tol sets the
+    derivative's solve tolerance first (fp_workspace_set_deriv_tol)."""
     L = lib()
+    if deriv_tol is not None:
+        _check(L.fp_workspace_set_deriv_tol(res._ws, float(deriv_tol), 1000000), "deriv_tol")
     g = np.ascontiguousarray(g, res.z.dtype)
     gx = np.empty_like(g)
     gp = np.zeros(nparams, np.float64)

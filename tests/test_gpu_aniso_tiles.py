@@ -1,11 +1,15 @@
-"""The tiled fibre passes of anisotropic TV (a block's fibres in shared
-memory, scanned by one warp in lockstep) against the untiled passes (one
-thread per fibre over global memory), which run the same arithmetic: a few
-iterations of each on the same inputs give the same iterates. Fibres of every
+"""The fibre passes of anisotropic TV in their three forms, which run the
+same arithmetic, against each other: the fibre-major passes (the default: a
+lane per fibre over a fibre-major copy of the fibres, every fibre of the
+launch in flight), the tiled passes (a block's fibres in shared memory,
+scanned by one warp in lockstep; FASTPROX_B200_AN_FIB=0) and the untiled
+passes (one thread per fibre over global memory; also
+FASTPROX_B200_TILES=0). A few iterations of each on the same inputs give the
+same iterates, up to the order of the restart test's sums. Fibres of every
 kind share a warp: ordinary ones, constant ones (their own prox), ones with a
 zero-weight edge (independent pieces) and, without edge weights, steps large
-enough that a fibre's prox is its mean. The untiled run is a child process
-with FASTPROX_B200_TILES=0 (the library reads its tuning hints once)."""
+enough that a fibre's prox is its mean. The other forms run in child
+processes (the library reads its tuning hints once)."""
 
 import os
 import pathlib
@@ -47,26 +51,34 @@ def _run(dtype, edge, iters):
 CASES = [(np.float64, False), (np.float64, True), (np.float32, False), (np.float32, True)]
 
 
+def _arm(tmp_path, name, iters, **env):
+    out = tmp_path / f"{name}.npz"
+    r = subprocess.run([sys.executable, str(pathlib.Path(__file__)), str(out), str(iters)], cwd=ROOT,
+                       env=dict(os.environ, **env), capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return np.load(out)
+
+
+def _close(z, zu, dtype, what):
+    assert z.dtype == zu.dtype
+    scale = 1.0 + np.abs(zu).max()
+    # the same arithmetic: equal up to the order of the restart test's sums
+    tol = 1e-13 if dtype == np.float64 else 1e-6
+    assert np.abs(z - zu).max() <= tol * scale, (what, dtype, np.abs(z - zu).max())
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("iters", [1, 6])
-def test_tiled_passes_match_untiled(cuda, tmp_path, iters):
-    env = dict(os.environ, FASTPROX_B200_TILES="0")
-    out = tmp_path / "untiled.npz"
-    r = subprocess.run([sys.executable, str(pathlib.Path(__file__)), str(out), str(iters)], cwd=ROOT, env=env,
-                       capture_output=True, text=True, timeout=600)
-    assert r.returncode == 0, r.stdout + r.stderr
-    ref = np.load(out)
+def test_fibre_pass_forms_agree(cuda, tmp_path, iters):
+    untiled = _arm(tmp_path, "untiled", iters, FASTPROX_B200_AN_FIB="0", FASTPROX_B200_TILES="0")
+    tiled = _arm(tmp_path, "tiled", iters, FASTPROX_B200_AN_FIB="0")
     for i, (dtype, edge) in enumerate(CASES):
         z = _run(dtype, edge, iters)
-        zu = ref[f"z{i}"]
-        assert z.dtype == zu.dtype
-        scale = 1.0 + np.abs(zu).max()
-        # the same arithmetic: equal up to the order of the restart test's sums
-        tol = 1e-13 if dtype == np.float64 else 1e-6
-        assert np.abs(z - zu).max() <= tol * scale, (dtype, edge, np.abs(z - zu).max())
+        _close(z, untiled[f"z{i}"], dtype, ("fibre-major", edge))
+        _close(tiled[f"z{i}"], untiled[f"z{i}"], dtype, ("tiled", edge))
 
 
-if __name__ == "__main__":  # the untiled run (FASTPROX_B200_TILES=0 in the environment)
+if __name__ == "__main__":  # one form (its switches in the environment)
     sys.path.insert(0, str(ROOT))
     n = int(sys.argv[2])
     np.savez(sys.argv[1], **{f"z{i}": _run(dt, e, n) for i, (dt, e) in enumerate(CASES)})

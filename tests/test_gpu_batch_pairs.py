@@ -1,6 +1,9 @@
 """The ragged batch's pair variants (two iterations per launch on images with
 rows of a multiple of 4 float pixels) against the same batch in single steps:
-the same iterates, gaps and iteration counts, bit for bit. The images cover
+the same iterates, gaps and iteration counts, bit for bit (quads off in both).
+Its quad launches (four iterations per launch) against pairs: the same
+iterates and iteration counts, the gaps to rounding (their sums are formed
+per quad tile). The images cover
 one and several 512-column tiles across (the pair pass's halo columns at the
 tile edges), a ragged last tile, a single row and widths off the 4-wide list
 (single steps either way), per-image steps and tolerances, and max_iter values
@@ -29,11 +32,11 @@ IMAGES = [  # (H, W, gamma, tol, max_iter)
 ]
 
 
-def _run(rows, steps):
+def _run(rows, steps, quads=False):
     import torch
     from fastprox_b200 import synth
     from fastprox_b200.batch import RaggedBatch
-    b = RaggedBatch(max_images=16, max_pixels=600_000, rows=rows)
+    b = RaggedBatch(max_images=16, max_pixels=600_000, rows=rows, quads=quads)
     owner = {}
     for k, (h, w, g, t, mi) in enumerate(IMAGES):
         x = torch.as_tensor(synth.phantom(1, h, w, seed=90 + k)[0], device="cuda")
@@ -68,6 +71,18 @@ def test_ragged_pairs_match_single_steps(cuda, tmp_path):
         # the pair variants ran: three launches per step on the 4-wide list
         # (single steps and two pair variants), one on the other list
         assert stats["kernel_launches"] > 2 * stats["steps"], stats
+
+
+@pytest.mark.gpu
+def test_ragged_quads_match_pairs(cuda):
+    for rows, steps in CONFIGS:
+        ref, _ = _run(rows, steps, quads=False)
+        got, stats = _run(rows, steps, quads=True)
+        for k, ((z, gap, it, conv), (zr, gr, itr, cr)) in enumerate(zip(got, ref)):
+            assert it == itr and conv == cr, (rows, IMAGES[k], it, itr)
+            assert np.array_equal(z, zr), (rows, IMAGES[k], np.abs(z - zr).max())
+            assert gap == gr or abs(gap - gr) <= 1e-12 * abs(gr) or (np.isnan(gap) and np.isnan(gr)), \
+                (rows, IMAGES[k], gap, gr)
 
 
 if __name__ == "__main__":  # the single-step run (FASTPROX_B200_PAIRS=0 in the environment)

@@ -100,3 +100,38 @@ def test_repeatable_and_autograd(cuda):
     (zt * torch.as_tensor(g, device=cuda)).sum().backward()
     assert np.array_equal(xt.grad.cpu().numpy(), a1)
     assert abs(float(gam.grad) - g1) <= 1e-6 * (1 + abs(g1))
+
+
+def test_loss_gradient_against_reference_and_differences(cuda):
+    """The differentiation workload's shape in small, (2, 3, 64, 64) phantoms +
+    noise 0.1, gamma 0.1, loss = MSE to the clean phantom, through the torch
+    wrapper: the float64 VJP in x and gamma against the reference's fp_vjp at
+    the same kept point (tol 1e-12) and against float64 central differences on
+    32 random directions (h = 1e-6, within 1e-4); the float32 gradient's error
+    against the float64 one is stated (its flat regions come from an iterate
+    certified to about 1e-3 relative at tol 1e-6)."""
+    import torch
+    from fastprox_b200 import synth
+    from fastprox_b200.torch import tv_iso
+    from fastprox_b200.workloads import vjp_checks
+    from oracle import ref_capi
+    if not ref_capi.available():
+        pytest.skip("reference library not built")
+    noisy, clean = synth.phantom(6, 64, 64, seed=11, sigma=0.1, clean=True)
+    noisy, clean = noisy.reshape(2, 3, 64, 64), clean.reshape(2, 3, 64, 64)
+    res = vjp_checks(noisy, clean, ndir=32)
+    assert res["fd_max_rel_err"] <= 1e-4, res
+    assert res["fd_gamma_rel_err"] <= 1e-4, res
+    assert res["f32_vs_f64_gx_rel_err"] <= 0.2, res  # stated, see the docstring
+    x = torch.as_tensor(noisy, device=cuda).double().requires_grad_(True)
+    c = torch.as_tensor(clean, device=cuda).double()
+    g = torch.tensor(0.1, device=cuda, dtype=torch.float64, requires_grad=True)
+    z = tv_iso(x, g, tol=1e-12, max_iter=10 ** 6, deriv_tol=1e-12)
+    ((z - c) ** 2).mean().backward()
+    cot = (2.0 * (z.detach() - c) / z.numel()).reshape(6, 64, 64).cpu().numpy()
+    r = ref_capi.solve(noisy.reshape(6, 64, 64).astype(np.float64), 0.1, iso=True, tol=1e-12, max_iter=10 ** 6,
+                       keep=True)
+    gxr, ggr, _ = ref_capi.vjp(r, cot, 2, deriv_tol=1e-12)
+    ref_capi.release(r)
+    assert _nrel(x.grad.reshape(6, 64, 64).cpu().numpy(), gxr) <= 1e-6
+    assert abs(float(g.grad) - ggr) <= 1e-6 * (1 + abs(ggr))
