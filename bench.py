@@ -235,8 +235,9 @@ def uneven_parity(sample):
 
 def profile_case(kind="iso"):
     """iso: the benchmark batch (64 x 512^2, pixel weights, three steps)
-    solved for exactly 8 iterations: launch 0 is the cold start, launches 4
-    and 8 carry gap checks, the rest are plain iterations. aniso: 16 of its
+    solved for exactly 12 iterations: the cold start, quad launches at
+    iterations 1 and 5 (four iterations each, the fourth with the gap check),
+    a pair at 9 and single steps at 11 and 12 (the check at max_iter). aniso: 16 of its
     images, anisotropic with edge weights, solved to gap 1e-6 (every kernel of
     the method, polish included). iso3d: 8 volumes of 128^3 for 8 iterations.
     ragged: 64 images of 512^2 in a ragged batch (32-row tiles, plain
@@ -276,7 +277,7 @@ def profile_case(kind="iso"):
     xt = torch.as_tensor(x, device="cuda")
     st = torch.as_tensor(steps, device="cuda")
     op = TVIso(2, pixel_weights=alpha)
-    z, info = op.solve(xt, st, tol=0.0, max_iter=8, with_dual=False)
+    z, info = op.solve(xt, st, tol=0.0, max_iter=12, with_dual=False)
     torch.cuda.synchronize()
     print(json.dumps({"profile_case": True, "iters": int(info.iters)}))
 
@@ -289,7 +290,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--profile-case", nargs="?", const="iso", default=None, choices=["iso", "aniso", "iso3d", "ragged"],
-                    help="iso: one solve of the benchmark batch with 8 iterations (tol 0); aniso: 16 images "
+                    help="iso: one solve of the benchmark batch with 12 iterations (tol 0); aniso: 16 images "
                          "anisotropic to gap 1e-6; iso3d: 8 x 128^3 with 8 iterations; ragged: 64 x 512^2 in a "
                          "ragged batch; the cases for ncu captures")
     ap.add_argument("--workload", default="iso512", choices=["iso512", "aniso512", "iso3d", "uneven", "vjp", "serve"],

@@ -1244,7 +1244,11 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
     Arr st;
     Geometry g0;
     if (fp_status s = image_geometry(*op, x, g0)) return s;
-    std::vector<double> host_steps;
+    // The steps per image, read into the workspace's pinned buffer (a call
+    // with a workspace allocates nothing on the host either), or into a local
+    // one when the call builds its own workspace.
+    std::vector<double> local_steps;
+    double *host_steps = nullptr;
     bool device_steps = false;
     if (sa) {
         if (fp_status s = to_arr(sa, st)) return s;
@@ -1254,25 +1258,31 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
         if (fp_status s = check_output(&st, out)) return s;
         // every step checked before any work
         const int64_t B = g0.B;
-        host_steps.resize((size_t)B);
+        if (ws) {
+            host_steps = ws->h_gam;
+        } else {
+            local_steps.resize((size_t)std::max<int64_t>(B, 1));
+            host_steps = local_steps.data();
+        }
         if (st.device == FP_DEVICE_CPU) {
-            std::vector<int64_t> idx((size_t)std::max(1, (int)sa->ndim), 0);
+            int64_t idx[FP_MAX_NDIM] = {0};
             for (int64_t i = 0; i < B; ++i) {
                 int64_t off = 0;
-                for (int d = 0; d < sa->ndim; ++d) off += idx[(size_t)d] * st.strides[d];
+                for (int d = 0; d < sa->ndim; ++d) off += idx[d] * st.strides[d];
                 const char *p = st.data + off * (int64_t)st.itemsize();
-                host_steps[(size_t)i] = st.dtype == FP_F32 ? (double)*reinterpret_cast<const float *>(p)
-                                                           : *reinterpret_cast<const double *>(p);
+                host_steps[i] = st.dtype == FP_F32 ? (double)*reinterpret_cast<const float *>(p)
+                                                   : *reinterpret_cast<const double *>(p);
                 for (int d = sa->ndim - 1; d >= 0; --d) {
-                    if (++idx[(size_t)d] < st.shape[d]) break;
-                    idx[(size_t)d] = 0;
+                    if (++idx[d] < st.shape[d]) break;
+                    idx[d] = 0;
                 }
             }
         } else {
             device_steps = true;  // read into the workspace below, checked before any work
         }
         if (!device_steps)
-            for (double v : host_steps) {
+            for (int64_t i = 0; i < B; ++i) {
+                const double v = host_steps[i];
                 if (!std::isfinite(v) || v < 0) return FP_EPARAM;
                 if (step_scale > 0.0 && !(v * step_scale <= kMaxScaledStep)) return FP_EPARAM;
             }
@@ -1355,8 +1365,8 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
                                  ws->stream);
         if (e0 == cudaSuccess) e0 = cudaStreamSynchronize(ws->stream);
         if (e0 != cudaSuccess) return cuda_status(e0);
-        host_steps.assign(ws->h_gam, ws->h_gam + ws->g.B);
-        for (double v : host_steps) {
+        for (int64_t i = 0; i < ws->g.B; ++i) {
+            const double v = ws->h_gam[i];
             if (!std::isfinite(v) || v < 0) return FP_EPARAM;
             if (step_scale > 0.0 && !(v * step_scale <= kMaxScaledStep)) return FP_EPARAM;
         }
@@ -1385,15 +1395,15 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
         } else {
             // pack through the pinned staging buffer
             if (cudaStreamSynchronize(s) != cudaSuccess) return FP_EDEVICE;
-            std::vector<int64_t> idx((size_t)x.ndim, 0);
+            int64_t idx[FP_MAX_NDIM] = {0};
             char *hs = static_cast<char *>(ws->h_stage);
             for (int64_t i = 0; i < total; ++i) {
                 int64_t off = 0;
-                for (int d = 0; d < x.ndim; ++d) off += idx[(size_t)d] * x.strides[d];
+                for (int d = 0; d < x.ndim; ++d) off += idx[d] * x.strides[d];
                 std::memcpy(hs + i * (int64_t)T, x.data + off * (int64_t)T, T);
                 for (int d = x.ndim - 1; d >= 0; --d) {
-                    if (++idx[(size_t)d] < x.shape[d]) break;
-                    idx[(size_t)d] = 0;
+                    if (++idx[d] < x.shape[d]) break;
+                    idx[d] = 0;
                 }
             }
             e = cudaMemcpyAsync(ws->d, hs, (size_t)total * T, cudaMemcpyHostToDevice, s);
@@ -1418,8 +1428,8 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
     if (e != cudaSuccess) return cuda_status(e);
     // Steps per image
     if (sa && !device_steps) {
-        std::memcpy(ws->h_gam, host_steps.data(), host_steps.size() * sizeof(double));
-        e = cudaMemcpyAsync(ws->gammas, ws->h_gam, host_steps.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (host_steps != ws->h_gam) std::memcpy(ws->h_gam, host_steps, (size_t)g.B * sizeof(double));
+        e = cudaMemcpyAsync(ws->gammas, ws->h_gam, (size_t)g.B * sizeof(double), cudaMemcpyHostToDevice, s);
     } else if (!sa) {
         e = fill_double(ws->gammas, identity ? 0.0 : gamma, g.B, s);
     }
@@ -1458,15 +1468,15 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
                 e = cudaMemcpyAsync(ws->h_stage, zdst, (size_t)total * T, cudaMemcpyDeviceToHost, s);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(s);
                 if (e == cudaSuccess) {
-                    std::vector<int64_t> idx((size_t)out.ndim, 0);
+                    int64_t idx[FP_MAX_NDIM] = {0};
                     const char *hs = static_cast<const char *>(ws->h_stage);
                     for (int64_t i = 0; i < total; ++i) {
                         int64_t off = 0;
-                        for (int d = 0; d < out.ndim; ++d) off += idx[(size_t)d] * out.strides[d];
+                        for (int d = 0; d < out.ndim; ++d) off += idx[d] * out.strides[d];
                         std::memcpy(out.data + off * (int64_t)T, hs + i * (int64_t)T, T);
                         for (int d = out.ndim - 1; d >= 0; --d) {
-                            if (++idx[(size_t)d] < out.shape[d]) break;
-                            idx[(size_t)d] = 0;
+                            if (++idx[d] < out.shape[d]) break;
+                            idx[d] = 0;
                         }
                     }
                 }
