@@ -105,6 +105,8 @@ SIGNATURES = {
     "fp_b200_batch_run": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int),
                                     C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "fp_b200_batch_stats": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "fp_b200_op_tv_iso_huber": (C.c_int, [C.c_int, _A, _A, C.c_double, C.POINTER(_P)]),
+    "fp_b200_op_tv_aniso_huber": (C.c_int, [C.c_int, _A, _A, C.c_double, C.POINTER(_P)]),
     "fp_b200_batch_set_quads": (C.c_int, [_P, C.c_int, C.c_int]),
     "fp_b200_vjp_images": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]),
     "fp_b200_tv_iso_noalloc": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int,

@@ -356,12 +356,47 @@ FP_API void fp_op_free(fp_op *op) { delete op; }
 
 FP_API int64_t fp_op_nparams(const fp_op *op) {
     if (!op) return 0;
-    return op->k + (int64_t)op->spatial.size();
+    return op->k + (int64_t)op->spatial.size() + (op->huber ? 1 : 0);
 }
 
 FP_API const char *fp_op_name(const fp_op *op) {
     if (!op) return "";
+    if (op->huber) return op->kind == kIso ? "tv_iso_huber" : "tv_aniso_huber";
     return op->kind == kIso ? "tv_iso" : "tv_aniso";
+}
+
+// Huber-smoothed TV: the TV operators' parameter rules and a smoothing delta,
+// finite and > 0 (the Huber function's, fp_op_huber).
+FP_API fp_status fp_b200_op_tv_iso_huber(int ndim, const fp_array *axis_weights, const fp_array *pixel_weights,
+                                         double delta, fp_op **out) {
+    return guard([&] {
+        if (!out) return FP_EINVAL;
+        *out = nullptr;
+        if (!std::isfinite(delta) || !(delta > 0.0)) return FP_EPARAM;
+        fp_status s = pixel_weights ? fp_op_tv_iso_weighted(ndim, axis_weights, pixel_weights, out)
+                                    : fp_op_tv_iso(ndim, axis_weights, out);
+        if (s == FP_OK) {
+            (*out)->huber = true;
+            (*out)->delta = delta;
+        }
+        return s;
+    });
+}
+
+FP_API fp_status fp_b200_op_tv_aniso_huber(int ndim, const fp_array *axis_weights, const fp_array *edge_weights,
+                                           double delta, fp_op **out) {
+    return guard([&] {
+        if (!out) return FP_EINVAL;
+        *out = nullptr;
+        if (!std::isfinite(delta) || !(delta > 0.0)) return FP_EPARAM;
+        fp_status s = edge_weights ? fp_op_tv_aniso_weighted(ndim, axis_weights, edge_weights, out)
+                                   : fp_op_tv_aniso(ndim, axis_weights, out);
+        if (s == FP_OK) {
+            (*out)->huber = true;
+            (*out)->delta = delta;
+        }
+        return s;
+    });
 }
 
 FP_API int fp_device_available(fp_device dev) {
@@ -516,15 +551,15 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
         return v ? std::atoi(v) : 0;
     };
     ws->shape_ = iso_pick_shape(x.dtype, g, env_int("FASTPROX_B200_ROWS"), env_int("FASTPROX_B200_BX"),
-                                env_int("FASTPROX_B200_KIND"));
+                                op->huber ? 1 : env_int("FASTPROX_B200_KIND"));
     if (const int ch = env_int("FASTPROX_B200_CHUNK")) ws->chunk = ch;
     ws->max_part = std::max(iso_setup_blocks(g), ws->shape_.gx * ws->shape_.gy);
     ws->max_part = std::max(ws->max_part, 4096);
     if (ws->shape_.kind == 4)  // per-row partial sums of the lean 2D step
         ws->max_part = (int)std::max<int64_t>(ws->max_part, (int64_t)ws->shape_.gx * g.L[0]);
-    if (x.dtype == FP_F32 && g.k == 2)  // per-row, per-strip partial sums of the quad launch
+    if (x.dtype == FP_F32 && g.k == 2 && !op->huber)  // per-row, per-strip partial sums of the quad launch
         ws->max_part = (int)std::max<int64_t>(ws->max_part, iso_quad_parts(g));
-    if (op->kind == kAniso) {
+    if (op->kind == kAniso && !op->huber) {
         // the untiled fibre passes: a block of 128 fibres per partial, three
         // axes in one launch for FDPG-3
         int64_t nfmax = 0;
@@ -533,7 +568,7 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
     }
     // the first iterate of a pair launch whose second iteration carries the
     // check (the final u when it passes)
-    if (op->kind == kAniso) {
+    if (op->kind == kAniso && !op->huber) {
         A((void **)&ws->an_img, (size_t)B * sizeof(AnImage));
         A((void **)&ws->an_st, (size_t)B * sizeof(AnState));
         A(&ws->an_scratch, img);
@@ -585,7 +620,7 @@ fp_status fpb_workspace_build(const fp_op *op, const Arr &x, const fp_options &o
         H((void **)&ws->h_ggam, (size_t)B * sizeof(double));
         H((void **)&ws->h_gw, (size_t)B * 3 * sizeof(double));
     }
-    if (op->kind == kAniso) {
+    if (op->kind == kAniso && !op->huber) {
         H((void **)&ws->h_an_img, (size_t)B * sizeof(AnImage));
         H((void **)&ws->h_an_st, (size_t)B * sizeof(AnState));
     }
@@ -924,6 +959,8 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     c.alpha_stride = 0;
     c.alpha_max = op->smax;
     c.step_scale = std::max({op->w[0], op->w[1], op->w[2]}) * (op->spatial.empty() ? 1.0 : op->smax);
+    c.huber = op->huber ? (op->kind == kIso ? 1 : 2) : 0;
+    c.delta = op->delta;
 
     IsoBuffers bf;
     bf.d = ws->d;
@@ -956,7 +993,7 @@ fp_status run_iso(fp_workspace *ws, const fp_op *op, const void *xsrc, void *zds
     // applies (iso_pair_ok).
     const int chunk = ws->chunk > 0 ? ws->chunk : 8;
     const bool pairs = iso_pair_ok(g, ws->shape_, ws->max_part);
-    const bool quads = iso_quad_ok(ws->dtype, g, ws->max_part);
+    const bool quads = !c.huber && iso_quad_ok(ws->dtype, g, ws->max_part);
     int par = 0, slot = 0, inflight = 0;
     int64_t launched = 0, steps = 0, lists = 0, nimg = g.B;
     const int64_t cap = (int64_t)max_iter + 1 + 2 * chunk;
@@ -1439,7 +1476,7 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
     // at the end of the solve (stage, or V[1] when stage holds y)
     const bool direct_out = !ws->host_mode && out.contiguous();
     void *zdst = direct_out ? out.data : (conj ? ws->V[1] : ws->stage);
-    if (op->kind == kIso) {
+    if (op->kind == kIso || op->huber) {  // Huber-smoothed TV, either form, runs in the isotropic engine
         if (fp_status st2 = run_iso(ws, op, xsrc, zdst, o.tol, o.max_iter, warm)) return st2;
     } else {
         if (fp_status st2 = run_aniso(ws, op, xsrc, zdst, o.tol, o.max_iter, warm)) return st2;
@@ -1449,7 +1486,7 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
         if (e != cudaSuccess) return cuda_status(e);
     }
     // Results back to the host
-    if (op->kind == kIso) {
+    if (op->kind == kIso || op->huber) {
         e = cudaMemcpyAsync(ws->h_img, ws->img, (size_t)g.B * sizeof(IsoImage), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(ws->h_st, ws->st, (size_t)g.B * sizeof(IsoState), cudaMemcpyDeviceToHost, s);
@@ -1505,7 +1542,7 @@ fp_status prox_impl(const fp_op *op, double step, const fp_array *xa, fp_array *
     double gsum = 0.0;
     int imax = 0;
     for (int64_t b = 0; b < g.B; ++b) {
-        if (op->kind == kAniso) {
+        if (op->kind == kAniso && !op->huber) {
             const AnImage &im = ws->h_an_img[b];
             const AnState &sst = ws->h_an_st[b];
             double gap = 0.0, gap_s = 0.0;
@@ -1630,6 +1667,7 @@ fp_status param_array(const fp_array *a, int64_t m, Arr &t) {
 // structure, built once per kept call (the reference's TVIso::save,
 // src/ops/tv_iso.cpp:551-631, done lazily).
 fp_status deriv_prepare(const fp_op *op, fp_workspace *ws, VjpGeom &vg, VjpBuffers &bf) {
+    if (op->huber) return FP_EINVAL;  // the derivatives of Huber-smoothed TV are not built
     const Geometry &g0 = ws->g;
     cudaStream_t s = ws->stream;
     const int64_t total = g0.B * g0.N;

@@ -86,6 +86,8 @@ struct IsoCall {
     int na;                // active axes (the same for every image of gamma > 0)
     int act_axis;          // the active axis when na == 1
     double w_act;          // its weight
+    int huber;             // Huber-smoothed TV: 0 none, 1 isotropic, 2 anisotropic (per axis component)
+    double delta;          // its smoothing delta (at the input's scale)
 };
 
 // One image of a ragged batch: its shape, its place in the arena (pixel

@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(kScanThreads) scan1_kernel(const T *__restrict
     if (im.flags & 2) im.mode = kModeInf;
     else if (im.flags & 1) im.mode = kModeNan;
     else if (!act) im.mode = kModeIdentity;
-    else im.mode = (c.na == 1 && !c.has_alpha) ? kModeTv1d : kModeFdpg;
+    else im.mode = (c.na == 1 && !c.has_alpha && !c.huber) ? kModeTv1d : kModeFdpg;
     if (im.mode == kModeFdpg || im.mode == kModeTv1d) {
         // rescale_exponent (src/ops/image_util.hpp:56-65)
         const double gamma = im.gamma_in;
@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kScanThreads) scan3_kernel(const T *__restrict
     const double gamma_s = ldexp(im.gamma_in, -im.e);
     double gamma = gamma_s * c.wmax;  // tv_iso.cpp:445-447
     const double bound = 2.0 * imb / c.whmin + DBL_MIN;
-    if (!(gamma <= bound) && !c.has_alpha) gamma = bound;
+    if (!(gamma <= bound) && !c.has_alpha && !c.huber) gamma = bound;  // (no such cap for Huber-smoothed TV)
     im.bound = bound;
     im.radius = gamma;
     IsoState &st = bf.st[b];
@@ -256,11 +256,18 @@ __global__ void warm_kernel(Geometry g, IsoCall c, IsoBuffers bf, int par) {
             u[a] = v;
             nn += v * v;
         }
-        const T rp = pixel_radius<T, ALPHA>(rad, bnd, al, p);
-        const T nr = sqrt_t(nn);
-        if (nr > rp) {
-            const T sc = rp / nr;
-            for (int a = 0; a < g.k; ++a) u[a] *= sc;
+        if (c.huber == 2) {  // anisotropic Huber: a box per component, its edge weight's radius
+            for (int a = 0; a < g.k; ++a) {
+                const T ra = ALPHA ? rad * static_cast<const T *>(bf.alpha)[(int64_t)a * N + p] : rad;
+                u[a] = u[a] > ra ? ra : (u[a] < -ra ? -ra : u[a]);
+            }
+        } else {
+            const T rp = c.huber ? (ALPHA ? rad * al[p] : rad) : pixel_radius<T, ALPHA>(rad, bnd, al, p);
+            const T nr = sqrt_t(nn);
+            if (nr > rp) {
+                const T sc = rp / nr;
+                for (int a = 0; a < g.k; ++a) u[a] *= sc;
+            }
         }
         for (int a = 0; a < g.k; ++a) {
             U[a * N + p] = u[a];
@@ -1984,6 +1991,199 @@ __global__ void __launch_bounds__(256) iso_generic_kernel(StepArgs A, IsoCall c,
 }
 
 // ---------------------------------------------------------------------------
+// Huber-smoothed TV (the reference's planned analysis prior, stage 1:
+// ROADMAP.md "Stage 1, Huber-smoothed TV"): isotropic
+// gamma sum_p alpha_p h(|(W D z)_p|), anisotropic gamma sum_{a,p}
+// beta_{a,p} h(|w_a (D_a z)_p|), h the Huber function of fp_op_huber
+// (src/ops/pointwise.cpp:189-206: t^2 / (2 delta) up to delta, t - delta / 2
+// beyond). Its dual adds delta |q_p|^2 / (2 gamma alpha_p) (per component for
+// the anisotropic form) to the TV dual: strongly convex, so dual FISTA with a
+// constant momentum (V-FISTA, kappa = 1 + gamma alpha_max L / delta) converges
+// linearly, with no restarts. At the solved scale, with u = wmax q and radius
+// r = gamma wmax alpha: the step is u+ = P_r((v + tau G_h z(v)) / (1 + tau
+// delta / (r wmax))), the projection onto the ball (isotropic) or the box per
+// component (anisotropic); the gap sums, per pixel (per component),
+// (r / wmax) h(wmax |g|) - <g, u> + delta |u|^2 / (2 r wmax) with g = G_h z(u):
+// each a Fenchel-Young gap, so |z - z*|^2 <= 2 gap as for TV. The arithmetic is
+// the generic step's (one thread per pixel, 2D and 3D); the gap test every
+// fourth iteration and at max_iter, as for TV.
+// ---------------------------------------------------------------------------
+
+template <class T>
+__device__ __forceinline__ double huber_h(double t, double dl) {
+    return t <= dl ? t * t / (2.0 * dl) : t - 0.5 * dl;
+}
+
+template <class T, int K, bool SW, bool ANISO>
+__global__ void __launch_bounds__(256) huber_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+    __shared__ double sh[32];
+    __shared__ int flag;
+    const int b = step_image(bf, blockIdx.y);
+    if (b < 0) return;
+    const IsoState st = bf.st[b];
+    if (st.status != kLive) return;
+    const IsoImage im = bf.img[b];
+    const int64_t N = A.g.N;
+    const int it = st.it;
+    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == A.max_iter)) || (it == 0 && st.warm);
+    const bool do_upd = it < A.max_iter;
+    const bool zin = st.zero_in != 0;
+    const int pin = A.par, pout = A.par ^ 1;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *U = static_cast<const T *>(bf.U[pin]) + (int64_t)b * K * N;
+    const T *V = static_cast<const T *>(bf.V[pin]) + (int64_t)b * K * N;
+    T *UO = static_cast<T *>(bf.U[pout]) + (int64_t)b * K * N;
+    T *VO = static_cast<T *>(bf.V[pout]) + (int64_t)b * K * N;
+    const T *SWp = SW ? static_cast<const T *>(bf.alpha) : nullptr;  // pixel (N) or edge (K N) weights
+    T wh[K];
+    int64_t L[K], S[K];
+    for (int a = 0; a < K; ++a) {
+        wh[a] = (T)c.wh[a];
+        L[a] = A.g.L[a];
+    }
+    S[K - 1] = 1;
+    for (int a = K - 2; a >= 0; --a) S[a] = S[a + 1] * L[a + 1];
+    const T tau = (T)c.tau, beta = (T)st.beta, rad = (T)im.radius, wm = (T)c.wmax;
+    const T dl = (T)ldexp(c.delta, -im.e);
+    const double dld = ldexp(c.delta, -im.e), wmd = c.wmax;
+    auto zat = [&](const T *P, int64_t q, const int64_t *co) -> T {
+        T z = D[q];
+        for (int a = 0; a < K; ++a) {
+            if (wh[a] == T(0)) continue;
+            const T cur = zin ? T(0) : P[a * N + q];
+            const T prev = (zin || co[a] == 0) ? T(0) : P[a * N + q - S[a]];
+            z += wh[a] * (cur - prev);
+        }
+        return z;
+    };
+    double gap_acc = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        int64_t co[K];
+        for (int a = 0; a < K; ++a) co[a] = (p / S[a]) % L[a];
+        T r[K];  // the radius of the pixel (of each component, anisotropic)
+        for (int a = 0; a < K; ++a) r[a] = SW ? rad * SWp[(ANISO ? (int64_t)a * N : 0) + p] : rad;
+        const T z0 = zat(V, p, co);
+        T gv[K];
+        for (int a = 0; a < K; ++a) {
+            gv[a] = T(0);
+            if (wh[a] != T(0) && co[a] + 1 < L[a]) {
+                int64_t cn[K];
+                for (int e = 0; e < K; ++e) cn[e] = co[e];
+                cn[a] += 1;
+                gv[a] = wh[a] * (zat(V, p + S[a], cn) - z0);
+            }
+        }
+        T cv[K], uc[K], vc[K];
+        for (int a = 0; a < K; ++a) {
+            uc[a] = zin ? T(0) : U[a * N + p];
+            vc[a] = zin ? T(0) : V[a * N + p];
+            cv[a] = wh[a] != T(0) ? vc[a] + tau * gv[a] : T(0);
+        }
+        if (ANISO) {
+            for (int a = 0; a < K; ++a) {
+                if (!(r[a] > T(0))) {
+                    cv[a] = T(0);
+                    continue;
+                }
+                cv[a] *= r[a] * wm / (r[a] * wm + tau * dl);
+                cv[a] = cv[a] > r[a] ? r[a] : (cv[a] < -r[a] ? -r[a] : cv[a]);
+            }
+        } else if (!(r[0] > T(0))) {
+            for (int a = 0; a < K; ++a) cv[a] = T(0);
+        } else {
+            const T sc0 = r[0] * wm / (r[0] * wm + tau * dl);
+            T nn = T(0);
+            for (int a = 0; a < K; ++a) {
+                cv[a] *= sc0;
+                nn += cv[a] * cv[a];
+            }
+            const T nr = sqrt_t(nn);
+            if (nr > r[0]) {
+                const T sc = r[0] / nr;
+                for (int a = 0; a < K; ++a) cv[a] *= sc;
+            }
+        }
+        if (do_upd)
+            for (int a = 0; a < K; ++a) {
+                VO[a * N + p] = cv[a] + beta * (cv[a] - uc[a]);
+                UO[a * N + p] = cv[a];
+            }
+        if (do_gap) {
+            const T zu0 = zat(U, p, co);
+            double gu[K];
+            for (int a = 0; a < K; ++a) {
+                gu[a] = 0.0;
+                if (wh[a] != T(0) && co[a] + 1 < L[a]) {
+                    int64_t cn[K];
+                    for (int e = 0; e < K; ++e) cn[e] = co[e];
+                    cn[a] += 1;
+                    gu[a] = (double)(wh[a] * (zat(U, p + S[a], cn) - zu0));
+                }
+            }
+            if (ANISO) {
+                for (int a = 0; a < K; ++a) {
+                    const double ra = (double)r[a], ua = (double)uc[a];
+                    if (ra > 0.0) gap_acc += ra / wmd * huber_h<T>(wmd * fabs(gu[a]), dld) - gu[a] * ua +
+                                             dld * ua * ua / (2.0 * ra * wmd);
+                }
+            } else if ((double)r[0] > 0.0) {
+                double nn = 0.0, pu = 0.0, uu = 0.0;
+                for (int a = 0; a < K; ++a) {
+                    nn += gu[a] * gu[a];
+                    pu += gu[a] * (double)uc[a];
+                    uu += (double)uc[a] * (double)uc[a];
+                }
+                const double r0 = (double)r[0];
+                gap_acc += r0 / wmd * huber_h<T>(wmd * sqrt(nn), dld) - pu + dld * uu / (2.0 * r0 * wmd);
+            }
+        }
+    }
+    const unsigned nblk = gridDim.x;
+    const double gsum = do_gap ? block_sum(gap_acc, sh) : 0.0;
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 2 + 0] = gsum;
+        part[blockIdx.x * 2 + 1] = 0.0;
+    }
+    if (!arrive_last(bf.ticket + b, nblk, &flag)) return;
+    const double gap = do_gap ? sum_partials(part, nblk, 2, 0, sh) : 0.0;
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2 = st;
+    if (do_gap) {
+        s2.gp = gap;
+        if (gap <= im.target || s2.it >= A.max_iter) {
+            s2.status = gap <= im.target ? kConverged : kNotConv;
+            s2.fin_par = pin;
+            atomicSub(bf.live, 1);
+            bf.st[b] = s2;
+            return;
+        }
+    }
+    s2.since += 1;
+    s2.vsel = 0;
+    s2.zero_in = 0;
+    s2.it += 1;  // the momentum stays the constant set at the set-up
+    s2.fin_par = pin ^ 1;
+    bf.st[b] = s2;
+}
+
+// The set-up's last step for Huber-smoothed TV: the constant momentum of
+// V-FISTA, (sqrt(kappa) - 1) / (sqrt(kappa) + 1), kappa = 1 + r_max wmax /
+// (tau delta) at the solved scale (r_max the largest radius).
+__global__ void huber_momentum(IsoCall c, IsoBuffers bf, int64_t B) {
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    const IsoImage im = bf.img[b];
+    if (im.mode != kModeFdpg) return;
+    const double rmax = im.radius * (c.has_alpha ? c.alpha_max : 1.0);
+    const double dl = ldexp(c.delta, -im.e);
+    const double kappa = 1.0 + rmax * c.wmax / (c.tau * dl);
+    const double sk = sqrt(kappa);
+    bf.st[b].beta = (sk - 1.0) / (sk + 1.0);
+}
+
+// ---------------------------------------------------------------------------
 // The 3D step: a block owns a kTY x kTX tile of the (axis 1, axis 2) plane and
 // marches along axis 0 through a chunk of A.rows slices. For each slice it
 // stages d and the dual of the next slice over the tile and a one-entry halo
@@ -2350,6 +2550,7 @@ cudaError_t setup_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, c
         if (c.has_alpha) warm_kernel<T, true><<<wg, 256, 0, s>>>(g, c, bf, par);
         else warm_kernel<T, false><<<wg, 256, 0, s>>>(g, c, bf, par);
     }
+    if (c.huber) huber_momentum<<<(unsigned)((g.B + 127) / 128), 128, 0, s>>>(c, bf, g.B);
     return cudaGetLastError();
 }
 
@@ -2508,6 +2709,28 @@ cudaError_t step_t(const Geometry &g, const IsoCall &c, const IsoBuffers &bf, co
     A.nimg = nimg;
     A.row_part = 0;
     if (nimg <= 0) return cudaSuccess;
+    if (c.huber) {  // Huber-smoothed TV: its own step, one thread per pixel
+        const dim3 grid(sh.gx, (unsigned)nimg);
+        const bool sw = c.has_alpha != 0;
+        if (g.k == 2) {
+            if (c.huber == 2) {
+                if (sw) huber_kernel<T, 2, true, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
+                else huber_kernel<T, 2, false, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
+            } else {
+                if (sw) huber_kernel<T, 2, true, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
+                else huber_kernel<T, 2, false, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
+            }
+        } else {
+            if (c.huber == 2) {
+                if (sw) huber_kernel<T, 3, true, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
+                else huber_kernel<T, 3, false, true><<<grid, sh.bx, 0, s>>>(A, c, bf);
+            } else {
+                if (sw) huber_kernel<T, 3, true, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
+                else huber_kernel<T, 3, false, false><<<grid, sh.bx, 0, s>>>(A, c, bf);
+            }
+        }
+        return cudaGetLastError();
+    }
     if (variant == kVariantQuad) {
         if constexpr (std::is_same<T, float>::value) {
             launch_quad(A, c, bf, s);

@@ -25,6 +25,8 @@ struct fp_op {
     std::vector<double> spatial;  // pixel weights (iso, N) or edge weights (aniso, k N), C order
     int64_t sshape[3] = {1, 1, 1};
     double smax = 0.0;
+    bool huber = false;  // Huber-smoothed TV (fp_b200_op_tv_iso_huber / _aniso_huber), smoothing delta
+    double delta = 0.0;
 };
 
 // One array shape, dtype and device; calls on it must not overlap. Every

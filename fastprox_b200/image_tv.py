@@ -49,6 +49,7 @@ def _is_scalar(g):
 
 class _ImageOp:
     iso = True
+    delta = None  # Huber-smoothed TV: its smoothing delta
 
     def __init__(self, ndim=2, weights=None, spatial=None):
         L = capi.lib()
@@ -56,7 +57,12 @@ class _ImageOp:
         self._op = C.c_void_p()
         w = None if weights is None else np.ascontiguousarray(np.atleast_1d(np.asarray(weights, np.float64)))
         wref = None if w is None else capi.ArrayRef(w)
-        if spatial is None:
+        if self.delta is not None:
+            sp = None if spatial is None else capi.ArrayRef(np.ascontiguousarray(np.asarray(spatial, np.float64)))
+            f = L.fp_b200_op_tv_iso_huber if self.iso else L.fp_b200_op_tv_aniso_huber
+            st = f(self.k, None if wref is None else wref.ref(), None if sp is None else sp.ref(), float(self.delta),
+                   C.byref(self._op))
+        elif spatial is None:
             f = L.fp_op_tv_iso if self.iso else L.fp_op_tv_aniso
             st = f(self.k, None if wref is None else wref.ref(), C.byref(self._op))
         else:
@@ -164,6 +170,24 @@ class TVAniso(_ImageOp):
     iso = False
 
     def __init__(self, ndim=2, weights=None, edge_weights=None):
+        super().__init__(ndim, weights, edge_weights)
+
+
+class TVIsoHuber(_ImageOp):
+    """Huber-smoothed isotropic TV: gamma sum_p alpha_p h_delta(|(W D z)_p|)."""
+    iso = True
+
+    def __init__(self, ndim=2, weights=None, pixel_weights=None, delta=1e-2):
+        self.delta = float(delta)
+        super().__init__(ndim, weights, pixel_weights)
+
+
+class TVAnisoHuber(_ImageOp):
+    """Huber-smoothed anisotropic TV: gamma sum_{a,p} beta_{a,p} h_delta(|w_a (D_a z)_p|)."""
+    iso = False
+
+    def __init__(self, ndim=2, weights=None, edge_weights=None, delta=1e-2):
+        self.delta = float(delta)
         super().__init__(ndim, weights, edge_weights)
 
 

@@ -316,6 +316,25 @@ FP_API fp_status fp_b200_batch_run(fp_b200_batch *bt, int steps, int max_chunks,
 FP_API fp_status fp_b200_batch_stats(const fp_b200_batch *bt, int64_t *kernel_launches, int64_t *steps,
                                      int64_t *free_pixels);
 
+/* Huber-smoothed TV, the reference's planned first analysis prior (its
+ * ROADMAP.md, "Stage 1, Huber-smoothed TV": fp_op_tv_iso_huber,
+ * fp_op_tv_aniso_huber; designed there, not in its code). Isotropic:
+ * g(z) = sum_p alpha_p h(|(W D z)_p|); anisotropic:
+ * g(z) = sum_a sum_p beta[a, p] h(|w_a (D_a z)_p|); h the Huber function of
+ * fp_op_huber (include/fastprox.h:129-131) with smoothing delta, finite and
+ * > 0 (FP_EPARAM otherwise). Weights, shapes and errors as fp_op_tv_iso[_weighted]
+ * and fp_op_tv_aniso[_weighted] (pixel_weights / edge_weights may be NULL).
+ * fp_prox / fp_prox_steps solve it by dual FISTA with a constant momentum
+ * (the dual is strongly convex: linear convergence), stopped on the same
+ * duality gap, |z - z*|^2 <= 2 gap; the dual returned is q with
+ * x - z = sum_a w_a D_a^T q_a. theta = the axis weights, the pixel or edge
+ * weights, then delta. The derivatives (fp_vjp, fp_jvp, the structure
+ * queries) are not built for it: FP_EINVAL. */
+FP_API fp_status fp_b200_op_tv_iso_huber(int ndim, const fp_array *axis_weights, const fp_array *pixel_weights,
+                                         double delta, fp_op **out);
+FP_API fp_status fp_b200_op_tv_aniso_huber(int ndim, const fp_array *axis_weights, const fp_array *edge_weights,
+                                           double delta, fp_op **out);
+
 /* Isotropic 2D TV prox of a small float32 batch without allocating any
  * memory. No counterpart in the reference ABI.
  *

@@ -1,6 +1,7 @@
 """Ragged batches (fp_b200_batch_*): images of mixed sizes, steps and
-tolerances in one set of launches, against the per-image solve (fp_prox);
-the same bits for an image alone and in a mix; continuous admission."""
+tolerances in one set of launches, against the per-image solve (fp_prox) and
+against the reference C library on the same images; the same bits for an
+image alone and in a mix; continuous admission."""
 
 import numpy as np
 import pytest
@@ -48,6 +49,25 @@ def test_matches_per_image_solves(cuda):
         assert conv == info.converged
         assert _nrel(z, zr[0]) <= 1e-5, (x.shape, _nrel(z, zr[0]))
         assert abs(it - int(info.image_iters[0])) <= max(4, 0.2 * it), (x.shape, it, info.image_iters)
+
+
+def test_matches_reference_library(cuda):
+    """Each image of the mixed batch (its own step and tolerance, with quads
+    and pairs where its rows allow) against the reference's fp_prox on the
+    same float32 input: 1e-5 relative, the float32 parity tolerance."""
+    from fastprox_b200.batch import RaggedBatch
+    from oracle import ref_capi
+    if not ref_capi.available():
+        pytest.skip("reference library not built")
+    imgs = _images(cuda)
+    b = RaggedBatch(max_images=16, max_pixels=200_000)
+    slots = [b.admit(x, g, t, max_iter=5000) for x, g, t in imgs]
+    res = _run_all(b)
+    for (x, g, t), s in zip(imgs, slots):
+        r = ref_capi.solve(x.cpu().numpy()[None], g, iso=True, k=2, tol=t, max_iter=5000)
+        z = res[s][0].double().cpu().numpy()
+        err = float(np.linalg.norm(z - r.z[0]) / max(np.linalg.norm(r.z[0]), 1e-300))
+        assert err <= 1e-5, (x.shape, err)
 
 
 def test_alone_equals_in_the_mix_and_continuous_admission(cuda):

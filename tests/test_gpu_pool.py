@@ -61,3 +61,28 @@ def test_reused_workspaces_and_streams(cuda):
     capi.lib().fp_b200_release_cached()
     z, it = _solve(*cases[2])
     assert _nrel(z, ref[2][0]) == 0.0 and it == ref[2][1]
+
+
+def test_prox_with_a_workspace_reserves_no_device_memory(cuda):
+    """The reference's rule that a prox call given a workspace allocates
+    nothing (its allocation counter, tests/c/test_core.cpp:40-66; device rule
+    docs/spec.md:887): after the workspace exists and one call has run (the
+    library's kernels loaded), further calls, isotropic and anisotropic, with
+    one step or one per image, leave the device's free memory unchanged."""
+    import torch
+    from fastprox_b200 import TVAniso, TVIso, synth
+    x = torch.as_tensor(synth.phantom(3, 96, 128, seed=50), device=cuda)
+    steps = torch.tensor([0.05, 0.1, 0.2], dtype=torch.float64, device=cuda)
+    ops = [TVIso(2), TVAniso(2), TVIso(2, pixel_weights=synth.pixel_weights((96, 128), seed=51))]
+    out = torch.empty_like(x)
+    for op in ops:
+        op.solve(x, 0.1, tol=1e-5, max_iter=2000, out=out, with_dual=False)
+        op.solve(x, steps, tol=1e-5, max_iter=2000, out=out, with_dual=False)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        for op in ops:
+            op.solve(x, 0.1, tol=1e-5, max_iter=2000, out=out, with_dual=False)
+            op.solve(x, steps, tol=1e-5, max_iter=2000, out=out, with_dual=False)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
