@@ -2931,7 +2931,8 @@ bool iso_quad_ok(int dtype, const Geometry &g, int max_part) {
         const char *v = std::getenv("FASTPROX_B200_QUADS");
         return !(v && v[0] == '0' && v[1] == 0);
     }();
-    return on && pairs_enabled() && dtype == 1 && g.k == 2 && g.L[1] >= 4 && g.L[1] % 4 == 0 && g.L[0] >= 2 &&
+    // rows narrower than 32 pixels keep the generic step (its gap terms in FP64)
+    return on && pairs_enabled() && dtype == 1 && g.k == 2 && g.L[1] >= 32 && g.L[1] % 4 == 0 && g.L[0] >= 2 &&
            g.L[0] * g.L[1] < (int64_t(1) << 31) && iso_quad_parts(g) <= max_part;
 }
 

@@ -155,12 +155,17 @@ def uneven(args):
                         for i in np.random.default_rng(5).choice(len(xs), 8, replace=False)]}
 
 
-def vjp_checks(noisy, clean, gamma=0.1, ndir=32, h=1e-6, seed=1, tol64=1e-12):
+def vjp_checks(noisy, clean, gamma=0.1, ndir=32, h=1e-5, seed=1, tol64=1e-12):
     """The implicit VJP of the (B, C, H, W) workload's loss (MSE to the clean
     phantom) checked three ways, all in float64 on the GPU unless stated:
     * central differences: for ndir random unit directions d (seeded), the
       VJP's <gx, d> against (<g, z(x + h d)> - <g, z(x - h d)>) / 2h, g the
-      loss's cotangent at z, solves at gap tol64 (and the same for gamma);
+      loss's cotangent at z (and the same for gamma). Both sides run the same
+      fixed number of iterations, twice those of the solve to gap tol64: a
+      stop at different checks on the two sides would put the solver's own
+      error, divided by 2h, into the difference. Each direction's error is
+      relative to max(|<gx, d>|, 0.1 |gx| / sqrt(n)), a tenth of a random
+      direction's typical derivative;
     * the float32 solve at gap 1e-6 and its VJP against the float64 one: the
       error of the float32 gradient, stated (its flat regions are read off an
       iterate certified to about 1e-3 relative, so small regions can differ).
@@ -187,18 +192,20 @@ def vjp_checks(noisy, clean, gamma=0.1, ndir=32, h=1e-6, seed=1, tol64=1e-12):
     xb = x64.reshape((-1,) + img)
     cb = cot.reshape((-1,) + img)
     op = TVIso(2)
+    fixed = 2 * op.solve(xb, gamma, tol=tol64, max_iter=10 ** 6, with_dual=False)[1].iters
 
     def fwd(xx, gam):
-        return op.solve(xx, gam, tol=tol64, max_iter=10 ** 6, with_dual=False)[0]
+        return op.solve(xx, gam, tol=0.0, max_iter=fixed, with_dual=False)[0]
 
     rng = np.random.default_rng(seed)
     worst_fd = 0.0
+    floor = 0.1 * float(gx64.norm()) / math.sqrt(n)
     for _ in range(ndir):
         d = torch.as_tensor(rng.normal(size=xb.shape), device="cuda")
         d = d / d.norm()
         fd = float(((fwd(xb + h * d, gamma) - fwd(xb - h * d, gamma)) * cb).sum()) / (2 * h)
         an = float((gx64.reshape(xb.shape) * d).sum())
-        worst_fd = max(worst_fd, abs(fd - an) / max(abs(an), 1e-12 * float(gx64.norm())))
+        worst_fd = max(worst_fd, abs(fd - an) / max(abs(an), floor))
     fdg = float(((fwd(xb, gamma + h) - fwd(xb, gamma - h)) * cb).sum()) / (2 * h)
     err_gamma = abs(fdg - gg64) / max(abs(fdg), 1e-300)
     _, gx32, gg32 = grads(x64, c64, 1e-6, torch.float32)

@@ -149,3 +149,12 @@ for kind in range(4):
     got.append(n.value)
 assert got[1] == 3 and got[2] == 2 and got[0] >= 3 and got[3] == 0, got
 """
+
+
+if __name__ == "__main__":  # one arm (its switches in the environment)
+    sys.path.insert(0, str(ROOT))
+    res = {}
+    for i in range(len(CASES)):
+        z, it, g, q = _run(i)
+        res.update({f"z{i}": z, f"it{i}": it, f"g{i}": g, f"q{i}": q})
+    np.savez(sys.argv[1], **res)

@@ -159,7 +159,11 @@ def test_certified_errors_match_reference(cuda, name):
     if x.dtype == np.float64:
         np.testing.assert_allclose(info.zerr, zr, rtol=1e-6, atol=1e-300)
     else:
-        np.testing.assert_allclose(info.zerr, zr, rtol=0.25, atol=1e-7)
+        # float32 iterates resolve a gap to about 2e-8 |x|^2 (each pixel's term
+        # rounded to float32 before its FP64 sum), i.e. r = sqrt(2 gap) / |x| to
+        # about 2e-4: a polished anisotropic image whose gap is below that may
+        # read 0 here and a rounding-level value in the reference's FP64 iterates
+        np.testing.assert_allclose(info.zerr, zr, rtol=0.25, atol=2e-4)
 
 
 @pytest.mark.parametrize("name", sorted(n for n, c in REF.items() if "sigma" in c))
@@ -196,8 +200,12 @@ def test_conjugate_matches_reference(cuda, name):
                                          zerr.ctypes.data_as(C.POINTER(C.c_double)), B), "image_info")
     if not f32:
         assert np.array_equal(its, c["iters"]), (its, c["iters"])
-        np.testing.assert_allclose(gaps, c["gaps"], rtol=1e-6, atol=1e-300)
-        np.testing.assert_allclose(zerr, c["zerrs"], rtol=1e-6, atol=1e-300)
+        # the prox behind the conjugate solves y / sigma: a gap below 1e-13 of
+        # its |y / sigma|^2 / 2 is at the rounding of the FP64 sums (a polished
+        # anisotropic point), and r = sqrt(2 gap) / |y / sigma| then below 5e-7
+        half = 0.5 * ((c["x"].astype(np.float64) / float(c["sigma"])) ** 2).reshape(B, -1).sum(1)
+        np.testing.assert_allclose(gaps, c["gaps"], rtol=1e-6, atol=1e-13 * half.min())
+        np.testing.assert_allclose(zerr, c["zerrs"], rtol=1e-6, atol=5e-7)
 
 
 @pytest.mark.parametrize("name", sorted(n for n in REF if n.startswith("rescale_")))
