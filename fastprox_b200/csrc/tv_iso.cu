@@ -1344,13 +1344,13 @@ __device__ __forceinline__ void cp_async16_zfill(void *dst, const void *src, uns
 }
 
 // What one quad pass needs: an image's arrays (v = u when vsel), its
-// geometry, the block's rows [r0, r1) and first strip, the step's constants,
-// the momenta of the four iterations, and where the per-row sums go.
+// geometry, the step's constants, the momenta of the four iterations, and
+// where the per-row sums go.
 struct QuadTile {
     const float *D, *U0, *V0, *AL;
     float *UO0, *VO0;
     int64_t N;
-    int H, W, r0, r1, strip0;
+    int H, W;
     float wh0, wh1, tau, rad, bnd;
     float beta[4];
     double *rowpart;  // ROWSUMS: the image's per-row, per-strip slots
@@ -1368,24 +1368,155 @@ __device__ __forceinline__ void quad_betas(double tn, double beta0, float (&beta
     }
 }
 
-// The march of one warp's strip (see above). REDO: three iterations, the
-// third's u written. ROWSUMS: each row's gap and restart-test sums over the
-// strip into p.rowpart[row x strips + strip] (the batched launch); else they
-// accumulate per lane in gsum, dsum over the block's rows (the ragged step's
-// per-tile slot).
+// One warp's march over a strip, rows [r0, r1) out. The pass's state: per
+// level l, the input row above the one it takes next (v, u of it and z of
+// v), carried from step to step; the check's z of u on that row.
+template <int LV>
+struct QuadCarry {
+    float cv0[LV][2], cv1[LV][2], cu0[LV][2], cu1[LV][2], cz[LV][2];
+    float czu[2];
+};
+
+// One step s of the march: stage row s, then iteration l + 1 (l = 0 ..
+// LV - 1) updates row s - l - 1 from its input rows s - l - 1 (carried) and
+// s - l (the staged row for l = 0, else iteration l's output of this step).
+// OUT: the last level's row is an output row of the tile (stores, and the
+// check's sums); before that (the first 2 LV steps) the levels run on the rows
+// above the tile with the same arithmetic and nothing leaves the warp. Rows
+// outside the image have d = v = u = 0 and radius 0, so their updates give
+// u = v = 0 (the zero padding of the divergence) without a branch; a lane's
+// columns outside the image likewise. The left neighbour of a lane's first
+// column and the right one of its second come by shuffle; lane 0 and lane 31
+// read their own values there, which is wrong for their columns but only
+// moves one column inward per iteration, within the window's 4-column halo.
+template <bool ALPHA, bool REDO, bool ROWSUMS, bool OUT, int LV>
+__device__ __forceinline__ void quad_step(const QuadTile &p, QuadCarry<LV> &q, int s, int strip, float *ruv,
+                                          float *rd, int wc, bool outcol, float wh1r1, double &gsum, double &dsum,
+                                          float *uo, float *vo) {
+    const int H = p.H, W = p.W;
+    const float wh0 = p.wh0, wh1 = p.wh1, tau = p.tau;
+    auto ld2 = [](const float *a, float (&o)[2]) {
+        const float2 v = *reinterpret_cast<const float2 *>(a);
+        o[0] = v.x;
+        o[1] = v.y;
+    };
+    float nv0[2], nv1[2], nu0[2], nu1[2];
+    {
+        const float *rs = ruv + (s & (kQuadSlotsUV - 1)) * 4 * kQuadWin + wc;
+        ld2(rs + 0 * kQuadWin, nv0);
+        ld2(rs + 1 * kQuadWin, nv1);
+        ld2(rs + 2 * kQuadWin, nu0);
+        ld2(rs + 3 * kQuadWin, nu1);
+    }
+#pragma unroll
+    for (int l = 0; l < LV; ++l) {
+        const int rn = s - l, r = rn - 1;  // this level's new input row; the row it updates
+        float dn[2];
+        ld2(rd + (rn & (kQuadSlotsD - 1)) * 2 * kQuadWin + wc, dn);
+        const float left = __shfl_up_sync(0xffffffffu, nv1[1], 1);
+        float nz[2];
+        nz[0] = dn[0] + wh0 * (nv0[0] - q.cv0[l][0]) + wh1 * (nv1[0] - left);
+        nz[1] = dn[1] + wh0 * (nv0[1] - q.cv0[l][1]) + wh1 * (nv1[1] - nv1[0]);
+        const bool last = l == LV - 1;
+        const bool check = !REDO && last;
+        float nzu[2] = {0.f, 0.f};
+        if (check) {  // z of the third iterate's u on row rn
+            const float lu = __shfl_up_sync(0xffffffffu, nu1[1], 1);
+            nzu[0] = dn[0] + wh0 * (nu0[0] - q.cu0[l][0]) + wh1 * (nu1[0] - lu);
+            nzu[1] = dn[1] + wh0 * (nu0[1] - q.cu0[l][1]) + wh1 * (nu1[1] - nu1[0]);
+        }
+        const float wh0n = rn < H ? wh0 : 0.f;  // no vertical difference on the image's last row
+        const float zr = __shfl_down_sync(0xffffffffu, q.cz[l][0], 1);
+        const float zur = check ? __shfl_down_sync(0xffffffffu, q.czu[0], 1) : 0.f;
+        float rp[2];
+        ld2(rd + ((r & (kQuadSlotsD - 1)) * 2 + 1) * kQuadWin + wc, rp);
+        float ou0[2], ou1[2], ov0[2], ov1[2];
+        double gacc = 0.0, dacc = 0.0;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const float whr = j == 0 ? wh1 : wh1r1;
+            const float zright = j == 0 ? q.cz[l][1] : zr;
+            const float g0 = wh0n * (nz[j] - q.cz[l][j]);
+            const float g1 = whr * (zright - q.cz[l][j]);
+            const float a0 = q.cv0[l][j] + tau * g0;
+            const float a1 = q.cv1[l][j] + tau * g1;
+            const float nn = a0 * a0 + a1 * a1;
+            const float sc = nn > rp[j] * rp[j] ? rp[j] * rsqrtf(nn) : 1.f;
+            const float un0 = a0 * sc, un1 = a1 * sc;
+            if (check && OUT && outcol) {
+                dacc += (double)((q.cv0[l][j] - un0) * (un0 - q.cu0[l][j]) +
+                                 (q.cv1[l][j] - un1) * (un1 - q.cu1[l][j]));
+                const float zuright = j == 0 ? q.czu[1] : zur;
+                const float gu0 = wh0n * (nzu[j] - q.czu[j]);
+                const float gu1 = whr * (zuright - q.czu[j]);
+                gacc += (double)(rp[j] * sqrtf(gu0 * gu0 + gu1 * gu1) -
+                                 (gu0 * q.cu0[l][j] + gu1 * q.cu1[l][j]));
+            }
+            ou0[j] = un0;
+            ou1[j] = un1;
+            ov0[j] = un0 + p.beta[l] * (un0 - q.cu0[l][j]);
+            ov1[j] = un1 + p.beta[l] * (un1 - q.cu1[l][j]);
+        }
+        if (OUT && last) {
+            if (check) {
+                if (ROWSUMS) {
+                    // this row's sums over the strip (a fixed tree) into its slot
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        gacc += __shfl_down_sync(0xffffffffu, gacc, o);
+                        dacc += __shfl_down_sync(0xffffffffu, dacc, o);
+                    }
+                    if ((threadIdx.x & 31) == 0) {
+                        double *part = p.rowpart + ((int64_t)r * quad_strips(W) + strip) * 2;
+                        part[0] = gacc;
+                        part[1] = dacc;
+                    }
+                } else {
+                    gsum += gacc;
+                    dsum += dacc;
+                }
+            }
+            if (outcol) {  // the pass's output row
+                const int64_t o = (int64_t)r * W;
+                *reinterpret_cast<float2 *>(uo + o) = make_float2(ou0[0], ou0[1]);
+                *reinterpret_cast<float2 *>(uo + p.N + o) = make_float2(ou1[0], ou1[1]);
+                if (!REDO) {
+                    *reinterpret_cast<float2 *>(vo + o) = make_float2(ov0[0], ov0[1]);
+                    *reinterpret_cast<float2 *>(vo + p.N + o) = make_float2(ov1[0], ov1[1]);
+                }
+            }
+        }
+        // carry: this level's input row becomes the one above its next; the
+        // next level's new input row is this level's output
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            q.cv0[l][j] = nv0[j];
+            q.cv1[l][j] = nv1[j];
+            q.cu0[l][j] = nu0[j];
+            q.cu1[l][j] = nu1[j];
+            q.cz[l][j] = nz[j];
+            if (check) q.czu[j] = nzu[j];
+            nv0[j] = ov0[j];
+            nv1[j] = ov1[j];
+            nu0[j] = ou0[j];
+            nu1[j] = ou1[j];
+        }
+    }
+}
+
+// The march of one warp over strip `strip`, output rows [r0, r1): steps
+// r0 - LV .. r1 + LV - 1, a row staged per step (three ahead), the first 2 LV
+// steps before any output row. REDO: three iterations, the third's u written.
+// ROWSUMS: each output row's gap and restart-test sums over the strip into
+// p.rowpart[row x strips + strip] (the batched launch); else they accumulate
+// per lane in gsum, dsum (the ragged step's per-tile slot).
 template <bool ALPHA, bool REDO, bool ROWSUMS>
-__device__ __forceinline__ void quad_pass(const QuadTile &p, int strip, double &gsum, double &dsum) {
+__device__ __forceinline__ void quad_pass(const QuadTile &p, int strip, int r0, int r1, double &gsum,
+                                          double &dsum) {
     constexpr int LV = REDO ? 3 : 4;  // iterations of the pass
     extern __shared__ __align__(16) float quad_ring[];
-    const int H = p.H, W = p.W, r0 = p.r0, r1 = p.r1;
-    const int64_t N = p.N;
-    const float *D = p.D, *U0 = p.U0, *V0 = p.V0, *AL = p.AL;
-    const float *U1 = U0 + N, *V1 = V0 + N;
-    float *UO0 = p.UO0, *VO0 = p.VO0;
-    float *UO1 = UO0 + N, *VO1 = VO0 + N;
-    const float wh0 = p.wh0, wh1 = p.wh1, tau = p.tau, rad = p.rad, bnd = p.bnd;
+    const int H = p.H, W = p.W;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nstrips = quad_strips(W);
     float *ring = quad_ring + warp * kQuadRingFloats;
     float *ruv = ring;                                  // [slot][v0, v1, u0, u1][64]
     float *rd = ring + kQuadSlotsUV * 4 * kQuadWin;     // [slot][d, radius][64]
@@ -1393,177 +1524,77 @@ __device__ __forceinline__ void quad_pass(const QuadTile &p, int strip, double &
     const int wc = 2 * lane;                            // this lane's first window column
     const int col = C0 + wc;
     const bool colin = col >= 0 && col < W;             // both columns (W and col are even)
-    const bool hasr0 = col + 1 < W, hasr1 = col + 2 < W;
     const bool outcol = lane >= kQuadHalo / 2 && lane < 32 - kQuadHalo / 2 && colin;  // written columns
-    const int sb = max(0, r0 - LV), se = r1 + LV - 1;   // steps: input rows sb .. se
-    auto issue = [&](int q) {
-        if (q <= se) {
-            const bool rowin = q < H;
-            const int64_t ro = (int64_t)q * W;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {  // 64 pieces of v0, v1, u0, u1: two per lane
-                const int k = lane + 32 * h, a = k >> 4, ch = k & 15;
-                const int cc = C0 + 4 * ch;
-                const bool ok = rowin && cc >= 0 && cc < W;
-                const float *base = a == 0 ? V0 : a == 1 ? V1 : a == 2 ? U0 : U1;
-                cp_async16_zfill(ruv + ((q & (kQuadSlotsUV - 1)) * 4 + a) * kQuadWin + 4 * ch,
-                                 base + (ok ? ro + cc : 0), ok ? 16u : 0u);
-            }
-            if (ALPHA || lane < 16) {  // d (and alpha): one piece per lane
-                const int a = lane >> 4, ch = lane & 15;
-                const int cc = C0 + 4 * ch;
-                const bool ok = rowin && cc >= 0 && cc < W;
-                const float *base = a == 0 ? D : AL;
-                cp_async16_zfill(rd + ((q & (kQuadSlotsD - 1)) * 2 + a) * kQuadWin + 4 * ch,
-                                 base + (ok ? ro + cc : 0), ok ? 16u : 0u);
-            }
+    const float wh1r1 = col + 2 < W ? p.wh1 : 0.f;      // the second column's right difference
+    const float radl = colin ? p.rad : 0.f;             // the radius of this lane's columns (no pixel weights)
+    // the copies: 16-byte pieces of the window's rows, a piece per lane and
+    // array; pieces outside the image are zero-filled (from a valid address)
+    const int ch = lane & 15, half = lane >> 4;
+    const int cc = C0 + 4 * ch;
+    const bool colok = cc >= 0 && cc < W;
+    const int ccs = colok ? cc : 0;
+    const float *src_v = (half ? p.V0 + p.N : p.V0) + ccs;
+    const float *src_u = (half ? p.U0 + p.N : p.U0) + ccs;
+    const float *src_d = (half ? p.AL : p.D) + ccs;
+    float *dst_v = ruv + half * kQuadWin + 4 * ch;
+    float *dst_u = ruv + (2 + half) * kQuadWin + 4 * ch;
+    float *dst_d = rd + half * kQuadWin + 4 * ch;
+    const bool copy_d = ALPHA || half == 0;
+    auto issue = [&](int row, int se) {
+        if (row <= se) {
+            const bool rowin = (unsigned)row < (unsigned)H;
+            const int64_t ro = (int64_t)(rowin ? row : 0) * W;
+            const unsigned n = rowin && colok ? 16u : 0u;
+            cp_async16_zfill(dst_v + (row & (kQuadSlotsUV - 1)) * 4 * kQuadWin, src_v + ro, n);
+            cp_async16_zfill(dst_u + (row & (kQuadSlotsUV - 1)) * 4 * kQuadWin, src_u + ro, n);
+            if (copy_d) cp_async16_zfill(dst_d + (row & (kQuadSlotsD - 1)) * 2 * kQuadWin, src_d + ro, n);
         }
         cp_async_commit();
     };
-    auto ld2 = [](const float *q, float (&o)[2]) {
-        const float2 v = *reinterpret_cast<const float2 *>(q);
-        o[0] = v.x;
-        o[1] = v.y;
-    };
-    // Level l's carried input row (iteration l's input v, u on the row
-    // after the one it updated last, and z of them); zero above the image.
-    float cv0[LV][2], cv1[LV][2], cu0[LV][2], cu1[LV][2], cz[LV][2];
-    float czu[2] = {0.f, 0.f};  // the check: z of the third iterate's u on the carried row
+    QuadCarry<LV> q;
 #pragma unroll
     for (int l = 0; l < LV; ++l)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) cv0[l][j] = cv1[l][j] = cu0[l][j] = cu1[l][j] = cz[l][j] = 0.f;
-    for (int q = 0; q < kQuadAhead; ++q) issue(sb + q);
-    for (int s = sb; s <= se; ++s) {
+        for (int j = 0; j < 2; ++j) q.cv0[l][j] = q.cv1[l][j] = q.cu0[l][j] = q.cu1[l][j] = q.cz[l][j] = 0.f;
+    q.czu[0] = q.czu[1] = 0.f;
+    float *uo = p.UO0 + (colin ? col : 0), *vo = p.VO0 + (colin ? col : 0);
+    const int sb = r0 - LV, se = r1 + LV - 1;
+    for (int k = 0; k < kQuadAhead; ++k) issue(sb + k, se);
+    // stage row s: wait for its copies, then the radius row in place (this
+    // lane's own entries): gamma alpha capped at the bound, 0 where alpha is 0
+    // or outside the image
+    auto stage = [&](int s) {
         __syncwarp();  // every lane is past its reads of the slots refilled now
-        issue(s + kQuadAhead);
+        issue(s + kQuadAhead, se);
         cp_async_wait<kQuadAhead>();
         __syncwarp();  // row s is in, from every lane's copies
-        // the staged row s: the first iteration's new input row
-        float nv0[2], nv1[2], nu0[2], nu1[2], vleft = 0.f;
-        if (s < H) {
-            const float *rs = ruv + (s & (kQuadSlotsUV - 1)) * 4 * kQuadWin;
-            ld2(rs + 0 * kQuadWin + wc, nv0);
-            ld2(rs + 1 * kQuadWin + wc, nv1);
-            ld2(rs + 2 * kQuadWin + wc, nu0);
-            ld2(rs + 3 * kQuadWin + wc, nu1);
-            if (lane > 0) vleft = rs[1 * kQuadWin + wc - 1];
-            if (ALPHA) {  // alpha -> the pixel radius, in place (this lane's own entries)
-                float *ra = rd + ((s & (kQuadSlotsD - 1)) * 2 + 1) * kQuadWin + wc;
-                float al[2], rp[2];
-                ld2(ra, al);
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const float r = rad * al[j];
-                    rp[j] = al[j] == 0.f ? 0.f : (r <= bnd ? r : bnd);
-                }
-                *reinterpret_cast<float2 *>(ra) = make_float2(rp[0], rp[1]);
-            }
+        float *ra = rd + ((s & (kQuadSlotsD - 1)) * 2 + 1) * kQuadWin + wc;
+        float rp[2];
+        if (ALPHA) {
+            const float2 al = *reinterpret_cast<const float2 *>(ra);
+            const float r0f = p.rad * al.x, r1f = p.rad * al.y;
+            rp[0] = al.x == 0.f ? 0.f : (r0f <= p.bnd ? r0f : p.bnd);
+            rp[1] = al.y == 0.f ? 0.f : (r1f <= p.bnd ? r1f : p.bnd);
         } else {
-#pragma unroll
-            for (int j = 0; j < 2; ++j) nv0[j] = nv1[j] = nu0[j] = nu1[j] = 0.f;
+            rp[0] = rp[1] = (unsigned)s < (unsigned)H ? radl : 0.f;
         }
-#pragma unroll
-        for (int l = 0; l < LV; ++l) {
-            const int r = s - l - 1;  // the row iteration l + 1 updates
-            // z of this level's input on row r + 1 (iteration l's output there)
-            const int rn = r + 1;
-            float dn[2] = {0.f, 0.f};
-            if (rn >= sb && rn < H) ld2(rd + ((rn & (kQuadSlotsD - 1)) * 2 + 0) * kQuadWin + wc, dn);
-            float left = l == 0 ? vleft : __shfl_up_sync(0xffffffffu, nv1[1], 1);
-            if (l > 0 && lane == 0) left = 0.f;
-            float nz[2];
-            nz[0] = dn[0] + wh0 * (nv0[0] - cv0[l][0]) + wh1 * (nv1[0] - left);
-            nz[1] = dn[1] + wh0 * (nv0[1] - cv0[l][1]) + wh1 * (nv1[1] - nv1[0]);
-            float nzu[2] = {0.f, 0.f};
-            const bool check = !REDO && l == LV - 1;
-            if (check) {  // z of the third iterate's u on row r + 1
-                float lu = __shfl_up_sync(0xffffffffu, nu1[1], 1);
-                if (lane == 0) lu = 0.f;
-                nzu[0] = dn[0] + wh0 * (nu0[0] - cu0[l][0]) + wh1 * (nu1[0] - lu);
-                nzu[1] = dn[1] + wh0 * (nu0[1] - cu0[l][1]) + wh1 * (nu1[1] - nu1[0]);
-            }
-            float ou0[2] = {0.f, 0.f}, ou1[2] = {0.f, 0.f}, ov0[2] = {0.f, 0.f}, ov1[2] = {0.f, 0.f};
-            const int lo = max(0, r0 - (LV - 1 - l)), hi = min(H, r1 + (LV - 1 - l));
-            const bool act = r >= lo && r < hi;  // the same for the whole warp
-            float zr = __shfl_down_sync(0xffffffffu, cz[l][0], 1);
-            float zur = check ? __shfl_down_sync(0xffffffffu, czu[0], 1) : 0.f;
-            if (lane == 31) zr = zur = 0.f;
-            if (act) {
-                const bool hasn = r + 1 < H;
-                float rp[2] = {rad, rad};
-                if (ALPHA) ld2(rd + ((r & (kQuadSlotsD - 1)) * 2 + 1) * kQuadWin + wc, rp);
-                double gacc = 0.0, dacc = 0.0;
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const bool hasr = j == 0 ? hasr0 : hasr1;
-                    const float zright = j == 0 ? cz[l][1] : zr;
-                    const float g0 = hasn ? wh0 * (nz[j] - cz[l][j]) : 0.f;
-                    const float g1 = hasr ? wh1 * (zright - cz[l][j]) : 0.f;
-                    const float a0 = cv0[l][j] + tau * g0;
-                    const float a1 = cv1[l][j] + tau * g1;
-                    const float nn = a0 * a0 + a1 * a1;
-                    const float sc = nn > rp[j] * rp[j] ? rp[j] * rsqrtf(nn) : 1.f;
-                    float un0 = a0 * sc, un1 = a1 * sc;
-                    if (!colin) un0 = un1 = 0.f;  // outside the image the dual is zero
-                    if (check && outcol) {
-                        dacc += (double)((cv0[l][j] - un0) * (un0 - cu0[l][j]) +
-                                         (cv1[l][j] - un1) * (un1 - cu1[l][j]));
-                        const float zuright = j == 0 ? czu[1] : zur;
-                        const float gu0 = hasn ? wh0 * (nzu[j] - czu[j]) : 0.f;
-                        const float gu1 = hasr ? wh1 * (zuright - czu[j]) : 0.f;
-                        gacc += (double)(rp[j] * sqrtf(gu0 * gu0 + gu1 * gu1) -
-                                         (gu0 * cu0[l][j] + gu1 * cu1[l][j]));
-                    }
-                    ou0[j] = un0;
-                    ou1[j] = un1;
-                    ov0[j] = un0 + p.beta[l] * (un0 - cu0[l][j]);
-                    ov1[j] = un1 + p.beta[l] * (un1 - cu1[l][j]);
-                }
-                if (check) {
-                    if (ROWSUMS) {
-                        // this row's sums over the strip (a fixed tree) into its slot
-#pragma unroll
-                        for (int o = 16; o > 0; o >>= 1) {
-                            gacc += __shfl_down_sync(0xffffffffu, gacc, o);
-                            dacc += __shfl_down_sync(0xffffffffu, dacc, o);
-                        }
-                        if (lane == 0) {
-                            double *part = p.rowpart + ((int64_t)r * nstrips + strip) * 2;
-                            part[0] = gacc;
-                            part[1] = dacc;
-                        }
-                    } else {
-                        gsum += gacc;
-                        dsum += dacc;
-                    }
-                }
-                if (l == LV - 1 && outcol) {  // the pass's output row (r0 <= r < r1 here)
-                    const int64_t o = (int64_t)r * W + col;
-                    *reinterpret_cast<float2 *>(UO0 + o) = make_float2(ou0[0], ou0[1]);
-                    *reinterpret_cast<float2 *>(UO1 + o) = make_float2(ou1[0], ou1[1]);
-                    if (!REDO) {
-                        *reinterpret_cast<float2 *>(VO0 + o) = make_float2(ov0[0], ov0[1]);
-                        *reinterpret_cast<float2 *>(VO1 + o) = make_float2(ov1[0], ov1[1]);
-                    }
-                }
-            }
-            // carry: this level's input row becomes the one of row r + 1;
-            // the next level's new input row is this level's output on row r
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                cv0[l][j] = nv0[j];
-                cv1[l][j] = nv1[j];
-                cu0[l][j] = nu0[j];
-                cu1[l][j] = nu1[j];
-                cz[l][j] = nz[j];
-                if (check) czu[j] = nzu[j];
-                nv0[j] = ov0[j];
-                nv1[j] = ov1[j];
-                nu0[j] = ou0[j];
-                nu1[j] = ou1[j];
-            }
-        }
+        *reinterpret_cast<float2 *>(ra) = make_float2(rp[0], rp[1]);
+    };
+    int s = sb;
+    for (; s < r0 + LV; ++s) {  // the rows above the tile
+        stage(s);
+        quad_step<ALPHA, REDO, ROWSUMS, false, LV>(p, q, s, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
+    }
+    for (; s + 1 <= se; s += 2) {  // output rows, two steps per trip
+        stage(s);
+        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
+        stage(s + 1);
+        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s + 1, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo,
+                                                  vo);
+    }
+    if (s <= se) {
+        stage(s);
+        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
     }
     cp_async_wait<0>();
 }
@@ -1622,9 +1653,6 @@ __global__ void __launch_bounds__(32 * kQuadWarps, 4) iso2d_quad_kernel(StepArgs
     p.N = N;
     p.H = H;
     p.W = W;
-    p.r0 = (int)blockIdx.y * A.rows;
-    p.r1 = min(H, p.r0 + A.rows);
-    p.strip0 = (int)blockIdx.x * kQuadWarps;
     p.wh0 = (float)c.wh[0];
     p.wh1 = (float)c.wh[1];
     p.tau = (float)c.tau;
@@ -1632,10 +1660,15 @@ __global__ void __launch_bounds__(32 * kQuadWarps, 4) iso2d_quad_kernel(StepArgs
     p.bnd = (float)im.bound;
     quad_betas(REDO ? st.redo_tn : st.tn, REDO ? st.redo_beta : st.beta, p.beta);
     p.rowpart = bf.part + (int64_t)b * bf.max_part * 2;
-    const int nstrips = quad_strips(W);
-    const int strip = p.strip0 + (int)(threadIdx.x >> 5);
+    // the block's warps take consecutive tiles (strip, band of A.rows rows) of
+    // the image, strips fastest
+    const int nstrips = quad_strips(W), nbands = (H + A.rows - 1) / A.rows;
+    const int t = (int)blockIdx.x * kQuadWarps + (int)(threadIdx.x >> 5);
     double gs = 0.0, ds = 0.0;
-    if (strip < nstrips) quad_pass<ALPHA, REDO, true>(p, strip, gs, ds);
+    if (t < nstrips * nbands) {
+        const int band = t / nstrips, r0 = band * A.rows;
+        quad_pass<ALPHA, REDO, true>(p, t - band * nstrips, r0, min(H, r0 + A.rows), gs, ds);
+    }
     if (REDO) return;
     __syncthreads();
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
@@ -1844,9 +1877,6 @@ __global__ void __launch_bounds__(32 * kQuadWarps, 4) iso2d_ragged_quad_kernel(c
     p.N = (int64_t)sl.H * sl.W;
     p.H = sl.H;
     p.W = sl.W;
-    p.r0 = item.r0;
-    p.r1 = min(sl.H, item.r0 + sl.qrows);
-    p.strip0 = item.cs;
     p.wh0 = (float)sl.wh0;
     p.wh1 = (float)sl.wh1;
     p.tau = (float)sl.tau;
@@ -1854,9 +1884,9 @@ __global__ void __launch_bounds__(32 * kQuadWarps, 4) iso2d_ragged_quad_kernel(c
     p.bnd = (float)im.bound;
     quad_betas(st.tn, st.beta, p.beta);
     p.rowpart = nullptr;
-    const int strip = p.strip0 + (int)(threadIdx.x >> 5);
+    const int strip = item.cs + (int)(threadIdx.x >> 5);
     double gs = 0.0, ds = 0.0;
-    if (strip < quad_strips(sl.W)) quad_pass<false, false, false>(p, strip, gs, ds);
+    if (strip < quad_strips(sl.W)) quad_pass<false, false, false>(p, strip, item.r0, min(sl.H, item.r0 + sl.qrows), gs, ds);
     const double gsum = block_sum(gs, sh);
     const double dsum = block_sum(ds, sh);
     double *part = bf.part + (int64_t)b * bf.max_part * 2;
@@ -2688,12 +2718,12 @@ void launch_quad(StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_
         const int r = v ? std::atoi(v) : 0;
         return (r >= 4 && r <= 256) ? r : 0;
     }();
-    const int64_t H = A.g.L[0];
-    const int gx = (quad_strips((int)A.g.L[1]) + kQuadWarps - 1) / kQuadWarps;
+    const int64_t H = A.g.L[0], ns = quad_strips((int)A.g.L[1]);
+    auto blocks = [&](int rows) { return (ns * ((H + rows - 1) / rows) + kQuadWarps - 1) / kQuadWarps; };
     int rows = rows_hint ? rows_hint : 32;
-    while (!rows_hint && rows > 8 && A.nimg * gx * ((H + rows - 1) / rows) < tail_blocks()) rows /= 2;
+    while (!rows_hint && rows > 8 && A.nimg * blocks(rows) < tail_blocks()) rows /= 2;
     A.rows = rows;
-    const dim3 grid((unsigned)gx, (unsigned)((H + rows - 1) / rows), (unsigned)A.nimg);
+    const dim3 grid((unsigned)blocks(rows), 1, (unsigned)A.nimg);
     if (c.has_alpha) launch_step(iso2d_quad_kernel<true, false>, grid, 32 * kQuadWarps, kQuadSmem, s, A, c, bf);
     else launch_step(iso2d_quad_kernel<false, false>, grid, 32 * kQuadWarps, kQuadSmem, s, A, c, bf);
 }
@@ -2952,8 +2982,8 @@ cudaError_t iso_redo(int dtype, const Geometry &g, const IsoCall &c, const IsoBu
         A.rows = 32;
         A.nimg = g.B;
         A.row_part = 0;
-        const int gx = (quad_strips((int)g.L[1]) + kQuadWarps - 1) / kQuadWarps;
-        const dim3 grid((unsigned)gx, (unsigned)((g.L[0] + A.rows - 1) / A.rows), (unsigned)g.B);
+        const int64_t tiles = quad_strips((int)g.L[1]) * ((g.L[0] + A.rows - 1) / A.rows);
+        const dim3 grid((unsigned)((tiles + kQuadWarps - 1) / kQuadWarps), 1, (unsigned)g.B);
         if (c.has_alpha) iso2d_quad_kernel<true, true><<<grid, 32 * kQuadWarps, kQuadSmem, s>>>(A, c, bf);
         else iso2d_quad_kernel<false, true><<<grid, 32 * kQuadWarps, kQuadSmem, s>>>(A, c, bf);
     }
