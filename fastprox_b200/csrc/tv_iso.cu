@@ -1368,13 +1368,45 @@ __device__ __forceinline__ void quad_betas(double tn, double beta0, float (&beta
     }
 }
 
+// Packed float pairs (a lane's two columns): sm_100's f32x2 arithmetic, each
+// half one IEEE float32 operation rounded to nearest (the same result as the
+// scalar operation; nothing is fused that the scalar steps do not fuse).
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {  // a - b
+    float2 d;
+    asm("{.reg .b64 a, b, d;\n\t"
+        "mov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
+        "sub.rn.f32x2 d, a, b;\n\tmov.b64 {%0, %1}, d;}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {  // a b
+    float2 d;
+    asm("{.reg .b64 a, b, d;\n\t"
+        "mov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
+        "mul.rn.f32x2 d, a, b;\n\tmov.b64 {%0, %1}, d;}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {  // a b + c, one rounding
+    float2 d;
+    asm("{.reg .b64 a, b, c, d;\n\t"
+        "mov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\tmov.b64 c, {%6, %7};\n\t"
+        "fma.rn.f32x2 d, a, b, c;\n\tmov.b64 {%0, %1}, d;}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
 // One warp's march over a strip, rows [r0, r1) out. The pass's state: per
 // level l, the input row above the one it takes next (v, u of it and z of
-// v), carried from step to step; the check's z of u on that row.
+// v), carried from step to step; the check's z of u on that row. Each entry
+// is a lane's two columns.
 template <int LV>
 struct QuadCarry {
-    float cv0[LV][2], cv1[LV][2], cu0[LV][2], cu1[LV][2], cz[LV][2];
-    float czu[2];
+    float2 cv0[LV], cv1[LV], cu0[LV], cu1[LV], cz[LV];
+    float2 czu;
 };
 
 // One step s of the march: stage row s, then iteration l + 1 (l = 0 ..
@@ -1389,76 +1421,69 @@ struct QuadCarry {
 // column and the right one of its second come by shuffle; lane 0 and lane 31
 // read their own values there, which is wrong for their columns but only
 // moves one column inward per iteration, within the window's 4-column halo.
+// The arithmetic per pixel is the single step's (iso2d_lean_kernel), operation
+// for operation, with each multiply-add the single step's compiler fuses
+// written as one fused operation here.
 template <bool ALPHA, bool REDO, bool ROWSUMS, bool OUT, int LV>
 __device__ __forceinline__ void quad_step(const QuadTile &p, QuadCarry<LV> &q, int s, int strip, float *ruv,
                                           float *rd, int wc, bool outcol, float wh1r1, double &gsum, double &dsum,
                                           float *uo, float *vo) {
     const int H = p.H, W = p.W;
-    const float wh0 = p.wh0, wh1 = p.wh1, tau = p.tau;
-    auto ld2 = [](const float *a, float (&o)[2]) {
-        const float2 v = *reinterpret_cast<const float2 *>(a);
-        o[0] = v.x;
-        o[1] = v.y;
-    };
-    float nv0[2], nv1[2], nu0[2], nu1[2];
-    {
-        const float *rs = ruv + (s & (kQuadSlotsUV - 1)) * 4 * kQuadWin + wc;
-        ld2(rs + 0 * kQuadWin, nv0);
-        ld2(rs + 1 * kQuadWin, nv1);
-        ld2(rs + 2 * kQuadWin, nu0);
-        ld2(rs + 3 * kQuadWin, nu1);
-    }
+    const float2 W0 = make_float2(p.wh0, p.wh0), W1 = make_float2(p.wh1, p.wh1), WR = make_float2(p.wh1, wh1r1);
+    const float2 TAU = make_float2(p.tau, p.tau);
+    auto ld2 = [](const float *a) { return *reinterpret_cast<const float2 *>(a); };
+    const float *rs = ruv + (s & (kQuadSlotsUV - 1)) * 4 * kQuadWin + wc;
+    float2 nv0 = ld2(rs + 0 * kQuadWin), nv1 = ld2(rs + 1 * kQuadWin);
+    float2 nu0 = ld2(rs + 2 * kQuadWin), nu1 = ld2(rs + 3 * kQuadWin);
 #pragma unroll
     for (int l = 0; l < LV; ++l) {
         const int rn = s - l, r = rn - 1;  // this level's new input row; the row it updates
-        float dn[2];
-        ld2(rd + (rn & (kQuadSlotsD - 1)) * 2 * kQuadWin + wc, dn);
-        const float left = __shfl_up_sync(0xffffffffu, nv1[1], 1);
-        float nz[2];
-        nz[0] = dn[0] + wh0 * (nv0[0] - q.cv0[l][0]) + wh1 * (nv1[0] - left);
-        nz[1] = dn[1] + wh0 * (nv0[1] - q.cv0[l][1]) + wh1 * (nv1[1] - nv1[0]);
+        const float2 dn = ld2(rd + (rn & (kQuadSlotsD - 1)) * 2 * kQuadWin + wc);
+        const float left = __shfl_up_sync(0xffffffffu, nv1.y, 1);
+        // z = d + wh0 (v0 - v0 above) + wh1 (v1 - v1 left)
+        const float2 nz = fma2(W1, sub2(nv1, make_float2(left, nv1.x)), fma2(W0, sub2(nv0, q.cv0[l]), dn));
         const bool last = l == LV - 1;
         const bool check = !REDO && last;
-        float nzu[2] = {0.f, 0.f};
+        float2 nzu = make_float2(0.f, 0.f);
         if (check) {  // z of the third iterate's u on row rn
-            const float lu = __shfl_up_sync(0xffffffffu, nu1[1], 1);
-            nzu[0] = dn[0] + wh0 * (nu0[0] - q.cu0[l][0]) + wh1 * (nu1[0] - lu);
-            nzu[1] = dn[1] + wh0 * (nu0[1] - q.cu0[l][1]) + wh1 * (nu1[1] - nu1[0]);
+            const float lu = __shfl_up_sync(0xffffffffu, nu1.y, 1);
+            nzu = fma2(W1, sub2(nu1, make_float2(lu, nu1.x)), fma2(W0, sub2(nu0, q.cu0[l]), dn));
         }
-        const float wh0n = rn < H ? wh0 : 0.f;  // no vertical difference on the image's last row
-        const float zr = __shfl_down_sync(0xffffffffu, q.cz[l][0], 1);
-        const float zur = check ? __shfl_down_sync(0xffffffffu, q.czu[0], 1) : 0.f;
-        float rp[2];
-        ld2(rd + ((r & (kQuadSlotsD - 1)) * 2 + 1) * kQuadWin + wc, rp);
-        float ou0[2], ou1[2], ov0[2], ov1[2];
-        double gacc = 0.0, dacc = 0.0;
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const float whr = j == 0 ? wh1 : wh1r1;
-            const float zright = j == 0 ? q.cz[l][1] : zr;
-            const float g0 = wh0n * (nz[j] - q.cz[l][j]);
-            const float g1 = whr * (zright - q.cz[l][j]);
-            const float a0 = q.cv0[l][j] + tau * g0;
-            const float a1 = q.cv1[l][j] + tau * g1;
-            const float nn = a0 * a0 + a1 * a1;
-            const float sc = nn > rp[j] * rp[j] ? rp[j] * rsqrtf(nn) : 1.f;
-            const float un0 = a0 * sc, un1 = a1 * sc;
-            if (check && OUT && outcol) {
-                dacc += (double)((q.cv0[l][j] - un0) * (un0 - q.cu0[l][j]) +
-                                 (q.cv1[l][j] - un1) * (un1 - q.cu1[l][j]));
-                const float zuright = j == 0 ? q.czu[1] : zur;
-                const float gu0 = wh0n * (nzu[j] - q.czu[j]);
-                const float gu1 = whr * (zuright - q.czu[j]);
-                gacc += (double)(rp[j] * sqrtf(gu0 * gu0 + gu1 * gu1) -
-                                 (gu0 * q.cu0[l][j] + gu1 * q.cu1[l][j]));
-            }
-            ou0[j] = un0;
-            ou1[j] = un1;
-            ov0[j] = un0 + p.beta[l] * (un0 - q.cu0[l][j]);
-            ov1[j] = un1 + p.beta[l] * (un1 - q.cu1[l][j]);
-        }
+        const float wh0n = rn < H ? p.wh0 : 0.f;  // no vertical difference on the image's last row
+        const float2 W0N = make_float2(wh0n, wh0n);
+        const float zr = __shfl_down_sync(0xffffffffu, q.cz[l].x, 1);
+        const float2 rp = ld2(rd + ((r & (kQuadSlotsD - 1)) * 2 + 1) * kQuadWin + wc);
+        const float2 g0 = mul2(W0N, sub2(nz, q.cz[l]));
+        const float2 g1 = mul2(WR, sub2(make_float2(q.cz[l].y, zr), q.cz[l]));
+        const float2 a0 = fma2(TAU, g0, q.cv0[l]);
+        const float2 a1 = fma2(TAU, g1, q.cv1[l]);
+        const float2 nn = fma2(a0, a0, mul2(a1, a1));
+        const float2 rr = mul2(rp, rp);
+        const float2 pr = mul2(rp, make_float2(rsqrtf(nn.x), rsqrtf(nn.y)));
+        const float2 sc = make_float2(nn.x > rr.x ? pr.x : 1.f, nn.y > rr.y ? pr.y : 1.f);
+        const float2 un0 = mul2(a0, sc), un1 = mul2(a1, sc);
+        const float2 B = make_float2(p.beta[l], p.beta[l]);
+        const float2 ov0 = fma2(B, sub2(un0, q.cu0[l]), un0);
+        const float2 ov1 = fma2(B, sub2(un1, q.cu1[l]), un1);
         if (OUT && last) {
             if (check) {
+                // the restart test's dot (v - u_new)(u_new - u) and the gap at
+                // the third iterate u with z of it
+                const float2 dd = fma2(sub2(q.cv0[l], un0), sub2(un0, q.cu0[l]),
+                                       mul2(sub2(q.cv1[l], un1), sub2(un1, q.cu1[l])));
+                const float zur = __shfl_down_sync(0xffffffffu, q.czu.x, 1);
+                const float2 gu0 = mul2(W0N, sub2(nzu, q.czu));
+                const float2 gu1 = mul2(WR, sub2(make_float2(q.czu.y, zur), q.czu));
+                const float2 gg = fma2(gu0, gu0, mul2(gu1, gu1));
+                const float2 in = fma2(gu0, q.cu0[l], mul2(gu1, q.cu1[l]));
+                const float t0 = fmaf(rp.x, sqrtf(gg.x), -in.x), t1 = fmaf(rp.y, sqrtf(gg.y), -in.y);
+                double gacc = 0.0, dacc = 0.0;
+                if (outcol) {
+                    dacc = (double)dd.x;
+                    gacc = (double)t0;
+                    dacc += (double)dd.y;
+                    gacc += (double)t1;
+                }
                 if (ROWSUMS) {
                     // this row's sums over the strip (a fixed tree) into its slot
 #pragma unroll
@@ -1478,29 +1503,26 @@ __device__ __forceinline__ void quad_step(const QuadTile &p, QuadCarry<LV> &q, i
             }
             if (outcol) {  // the pass's output row
                 const int64_t o = (int64_t)r * W;
-                *reinterpret_cast<float2 *>(uo + o) = make_float2(ou0[0], ou0[1]);
-                *reinterpret_cast<float2 *>(uo + p.N + o) = make_float2(ou1[0], ou1[1]);
+                *reinterpret_cast<float2 *>(uo + o) = un0;
+                *reinterpret_cast<float2 *>(uo + p.N + o) = un1;
                 if (!REDO) {
-                    *reinterpret_cast<float2 *>(vo + o) = make_float2(ov0[0], ov0[1]);
-                    *reinterpret_cast<float2 *>(vo + p.N + o) = make_float2(ov1[0], ov1[1]);
+                    *reinterpret_cast<float2 *>(vo + o) = ov0;
+                    *reinterpret_cast<float2 *>(vo + p.N + o) = ov1;
                 }
             }
         }
         // carry: this level's input row becomes the one above its next; the
         // next level's new input row is this level's output
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            q.cv0[l][j] = nv0[j];
-            q.cv1[l][j] = nv1[j];
-            q.cu0[l][j] = nu0[j];
-            q.cu1[l][j] = nu1[j];
-            q.cz[l][j] = nz[j];
-            if (check) q.czu[j] = nzu[j];
-            nv0[j] = ov0[j];
-            nv1[j] = ov1[j];
-            nu0[j] = ou0[j];
-            nu1[j] = ou1[j];
-        }
+        q.cv0[l] = nv0;
+        q.cv1[l] = nv1;
+        q.cu0[l] = nu0;
+        q.cu1[l] = nu1;
+        q.cz[l] = nz;
+        if (check) q.czu = nzu;
+        nv0 = ov0;
+        nv1 = ov1;
+        nu0 = un0;
+        nu1 = un1;
     }
 }
 
@@ -1553,10 +1575,8 @@ __device__ __forceinline__ void quad_pass(const QuadTile &p, int strip, int r0, 
     };
     QuadCarry<LV> q;
 #pragma unroll
-    for (int l = 0; l < LV; ++l)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) q.cv0[l][j] = q.cv1[l][j] = q.cu0[l][j] = q.cu1[l][j] = q.cz[l][j] = 0.f;
-    q.czu[0] = q.czu[1] = 0.f;
+    for (int l = 0; l < LV; ++l) q.cv0[l] = q.cv1[l] = q.cu0[l] = q.cu1[l] = q.cz[l] = make_float2(0.f, 0.f);
+    q.czu = make_float2(0.f, 0.f);
     float *uo = p.UO0 + (colin ? col : 0), *vo = p.VO0 + (colin ? col : 0);
     const int sb = r0 - LV, se = r1 + LV - 1;
     for (int k = 0; k < kQuadAhead; ++k) issue(sb + k, se);
