@@ -1425,9 +1425,9 @@ struct QuadCarry {
 // for operation, with each multiply-add the single step's compiler fuses
 // written as one fused operation here.
 template <bool ALPHA, bool REDO, bool ROWSUMS, bool OUT, int LV>
-__device__ __forceinline__ void quad_step(const QuadTile &p, QuadCarry<LV> &q, int s, int strip, float *ruv,
-                                          float *rd, int wc, bool outcol, float wh1r1, double &gsum, double &dsum,
-                                          float *uo, float *vo) {
+__device__ __forceinline__ void quad_step(const QuadTile &p, QuadCarry<LV> &q, int s, int ustart, int strip,
+                                          float *ruv, float *rd, int wc, bool outcol, float wh1r1, double &gsum,
+                                          double &dsum, float *uo, float *vo) {
     const int H = p.H, W = p.W;
     const float2 W0 = make_float2(p.wh0, p.wh0), W1 = make_float2(p.wh1, p.wh1), WR = make_float2(p.wh1, wh1r1);
     const float2 TAU = make_float2(p.tau, p.tau);
@@ -1453,18 +1453,27 @@ __device__ __forceinline__ void quad_step(const QuadTile &p, QuadCarry<LV> &q, i
         const float2 W0N = make_float2(wh0n, wh0n);
         const float zr = __shfl_down_sync(0xffffffffu, q.cz[l].x, 1);
         const float2 rp = ld2(rd + ((r & (kQuadSlotsD - 1)) * 2 + 1) * kQuadWin + wc);
-        const float2 g0 = mul2(W0N, sub2(nz, q.cz[l]));
-        const float2 g1 = mul2(WR, sub2(make_float2(q.cz[l].y, zr), q.cz[l]));
-        const float2 a0 = fma2(TAU, g0, q.cv0[l]);
-        const float2 a1 = fma2(TAU, g1, q.cv1[l]);
-        const float2 nn = fma2(a0, a0, mul2(a1, a1));
-        const float2 rr = mul2(rp, rp);
-        const float2 pr = mul2(rp, make_float2(rsqrtf(nn.x), rsqrtf(nn.y)));
-        const float2 sc = make_float2(nn.x > rr.x ? pr.x : 1.f, nn.y > rr.y ? pr.y : 1.f);
-        const float2 un0 = mul2(a0, sc), un1 = mul2(a1, sc);
-        const float2 B = make_float2(p.beta[l], p.beta[l]);
-        const float2 ov0 = fma2(B, sub2(un0, q.cu0[l]), un0);
-        const float2 ov1 = fma2(B, sub2(un1, q.cu1[l]), un1);
+        float2 un0, un1, ov0, ov1;
+        // above the tile, level l's updates are first needed at step ustart + 2 l
+        // (their rows feed the output rows' halo); before it only its z and
+        // carried rows are kept, and its output is not read
+        if (OUT || s >= ustart + 2 * l) {
+            const float2 g0 = mul2(W0N, sub2(nz, q.cz[l]));
+            const float2 g1 = mul2(WR, sub2(make_float2(q.cz[l].y, zr), q.cz[l]));
+            const float2 a0 = fma2(TAU, g0, q.cv0[l]);
+            const float2 a1 = fma2(TAU, g1, q.cv1[l]);
+            const float2 nn = fma2(a0, a0, mul2(a1, a1));
+            const float2 rr = mul2(rp, rp);
+            const float2 pr = mul2(rp, make_float2(rsqrtf(nn.x), rsqrtf(nn.y)));
+            const float2 sc = make_float2(nn.x > rr.x ? pr.x : 1.f, nn.y > rr.y ? pr.y : 1.f);
+            un0 = mul2(a0, sc);
+            un1 = mul2(a1, sc);
+            const float2 B = make_float2(p.beta[l], p.beta[l]);
+            ov0 = fma2(B, sub2(un0, q.cu0[l]), un0);
+            ov1 = fma2(B, sub2(un1, q.cu1[l]), un1);
+        } else {
+            un0 = un1 = ov0 = ov1 = make_float2(0.f, 0.f);
+        }
         if (OUT && last) {
             if (check) {
                 // the restart test's dot (v - u_new)(u_new - u) and the gap at
@@ -1578,7 +1587,7 @@ __device__ __forceinline__ void quad_pass(const QuadTile &p, int strip, int r0, 
     for (int l = 0; l < LV; ++l) q.cv0[l] = q.cv1[l] = q.cu0[l] = q.cu1[l] = q.cz[l] = make_float2(0.f, 0.f);
     q.czu = make_float2(0.f, 0.f);
     float *uo = p.UO0 + (colin ? col : 0), *vo = p.VO0 + (colin ? col : 0);
-    const int sb = r0 - LV, se = r1 + LV - 1;
+    const int sb = r0 - LV, se = r1 + LV - 1, ustart = r0 - LV + 2;
     for (int k = 0; k < kQuadAhead; ++k) issue(sb + k, se);
     // stage row s: wait for its copies, then the radius row in place (this
     // lane's own entries): gamma alpha capped at the bound, 0 where alpha is 0
@@ -1603,18 +1612,18 @@ __device__ __forceinline__ void quad_pass(const QuadTile &p, int strip, int r0, 
     int s = sb;
     for (; s < r0 + LV; ++s) {  // the rows above the tile
         stage(s);
-        quad_step<ALPHA, REDO, ROWSUMS, false, LV>(p, q, s, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
+        quad_step<ALPHA, REDO, ROWSUMS, false, LV>(p, q, s, ustart, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
     }
     for (; s + 1 <= se; s += 2) {  // output rows, two steps per trip
         stage(s);
-        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
+        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s, ustart, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
         stage(s + 1);
-        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s + 1, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo,
-                                                  vo);
+        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s + 1, ustart, strip, ruv, rd, wc, outcol, wh1r1, gsum,
+                                                  dsum, uo, vo);
     }
     if (s <= se) {
         stage(s);
-        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
+        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s, ustart, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
     }
     cp_async_wait<0>();
 }
@@ -2730,18 +2739,41 @@ void launch_3d_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuf
     else launch_3d_v<T, ALPHA, false, false>(grid, A, c, bf, s);
 }
 
-// The quad launch: blocks of kQuadWarps strips and `rows` rows (32; fewer,
-// down to 8, while the launch has too few blocks to spread over the SMs).
+// The quad launch: blocks of kQuadWarps tiles (a strip by `rows` rows). A
+// tile's march takes rows + 8 steps and the SMs hold a fixed number of
+// blocks at once, so the rows are chosen (8 to 64, in steps of 4) for the
+// fewest waves of resident blocks times steps per tile: 48 on 64 images of
+// 512^2 (three waves of 56 steps, against five of 40 at 32 rows), 8 for one
+// image (a single wave of short tiles).
 void launch_quad(StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
     static const int rows_hint = [] {  // tuning hint FASTPROX_B200_QUAD_ROWS
         const char *v = std::getenv("FASTPROX_B200_QUAD_ROWS");
         const int r = v ? std::atoi(v) : 0;
         return (r >= 4 && r <= 256) ? r : 0;
     }();
+    static const int64_t slots = [] {  // resident quad blocks on the device
+        int dev = 0, sms = 148, per = 4;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, iso2d_quad_kernel<true, false>, 32 * kQuadWarps,
+                                                          kQuadSmem) != cudaSuccess || per < 1)
+            per = 4;
+        cudaGetLastError();
+        return (int64_t)sms * per;
+    }();
     const int64_t H = A.g.L[0], ns = quad_strips((int)A.g.L[1]);
     auto blocks = [&](int rows) { return (ns * ((H + rows - 1) / rows) + kQuadWarps - 1) / kQuadWarps; };
-    int rows = rows_hint ? rows_hint : 32;
-    while (!rows_hint && rows > 8 && A.nimg * blocks(rows) < tail_blocks()) rows /= 2;
+    int rows = rows_hint;
+    if (!rows) {
+        double best = 0.0;
+        for (int r = 8; r <= 64; r += 4) {
+            const int64_t waves = (A.nimg * blocks(r) + slots - 1) / slots;
+            const double cost = (double)waves * (double)(std::min<int64_t>(r, H) + 8);
+            if (!rows || cost < best) {
+                rows = r;
+                best = cost;
+            }
+        }
+    }
     A.rows = rows;
     const dim3 grid((unsigned)blocks(rows), 1, (unsigned)A.nimg);
     if (c.has_alpha) launch_step(iso2d_quad_kernel<true, false>, grid, 32 * kQuadWarps, kQuadSmem, s, A, c, bf);
