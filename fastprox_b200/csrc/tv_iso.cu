@@ -397,8 +397,16 @@ int64_t tail_blocks() {
 
 template <class T>
 __device__ __forceinline__ T rsqrt_t(T v);
+// float: the hardware reciprocal square root (rsqrtf's result on normal
+// numbers) with arguments below the smallest normal float taken as that
+// smallest normal (no rescaling of subnormal arguments; at a zero radius the
+// projection's scale stays rp times a finite number, 0)
 template <>
-__device__ __forceinline__ float rsqrt_t<float>(float v) { return rsqrtf(v); }
+__device__ __forceinline__ float rsqrt_t<float>(float v) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(fmaxf(v, FLT_MIN)));
+    return r;
+}
 template <>
 __device__ __forceinline__ double rsqrt_t<double>(double v) { return rsqrt(v); }
 
@@ -1335,7 +1343,30 @@ constexpr int kQuadSlotsD = 8;                      // ring rows of d and the ra
 constexpr int kQuadRingFloats = kQuadSlotsUV * 4 * kQuadWin + kQuadSlotsD * 2 * kQuadWin;
 constexpr size_t kQuadSmem = (size_t)kQuadWarps * kQuadRingFloats * sizeof(float);
 
-__host__ __device__ constexpr int quad_strips(int W) { return (W + kQuadOut - 1) / kQuadOut; }
+// Strips of a row of W columns: one window when W <= 64 (its edges are the
+// image's, so it needs no halo); else a first window at column 0 writing
+// columns 0 .. 59 (no halo on the image's edge), windows at 56 k writing
+// 56 k + 4 .. 56 k + 59, and a last window ending at column W writing the rest
+// (9 strips for a row of 512, against 10 with a halo on every side).
+__host__ __device__ constexpr int quad_strips(int W) {
+    return W <= kQuadWin ? 1
+                         : 2 + ((W - 2 * (kQuadWin - kQuadHalo) > 0)
+                                    ? (W - 2 * (kQuadWin - kQuadHalo) + kQuadOut - 1) / kQuadOut
+                                    : 0);
+}
+// Strip k's window (first column, a multiple of 4) and the columns it writes.
+__host__ __device__ inline void quad_strip_cols(int W, int k, int &c0, int &lo, int &hi) {
+    const int n = quad_strips(W);
+    if (n == 1) {
+        c0 = 0, lo = 0, hi = W;
+    } else if (k == 0) {
+        c0 = 0, lo = 0, hi = kQuadWin - kQuadHalo;
+    } else if (k < n - 1) {
+        c0 = k * kQuadOut, lo = c0 + kQuadHalo, hi = c0 + kQuadWin - kQuadHalo;
+    } else {
+        c0 = W - kQuadWin, lo = (n - 2) * kQuadOut + kQuadWin - kQuadHalo, hi = W;
+    }
+}
 
 __device__ __forceinline__ void cp_async16_zfill(void *dst, const void *src, unsigned n) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
@@ -1426,8 +1457,8 @@ struct QuadCarry {
 // written as one fused operation here.
 template <bool ALPHA, bool REDO, bool ROWSUMS, bool OUT, int LV>
 __device__ __forceinline__ void quad_step(const QuadTile &p, QuadCarry<LV> &q, int s, int ustart, int strip,
-                                          float *ruv, float *rd, int wc, bool outcol, float wh1r1, double &gsum,
-                                          double &dsum, float *uo, float *vo) {
+                                          float *ruv, float *rd, int wc, bool outcol, bool ledge, float wh1r1,
+                                          double &gsum, double &dsum, float *uo, float *vo) {
     const int H = p.H, W = p.W;
     const float2 W0 = make_float2(p.wh0, p.wh0), W1 = make_float2(p.wh1, p.wh1), WR = make_float2(p.wh1, wh1r1);
     const float2 TAU = make_float2(p.tau, p.tau);
@@ -1439,14 +1470,16 @@ __device__ __forceinline__ void quad_step(const QuadTile &p, QuadCarry<LV> &q, i
     for (int l = 0; l < LV; ++l) {
         const int rn = s - l, r = rn - 1;  // this level's new input row; the row it updates
         const float2 dn = ld2(rd + (rn & (kQuadSlotsD - 1)) * 2 * kQuadWin + wc);
-        const float left = __shfl_up_sync(0xffffffffu, nv1.y, 1);
+        const float sl = __shfl_up_sync(0xffffffffu, nv1.y, 1);
+        const float left = ledge ? 0.f : sl;
         // z = d + wh0 (v0 - v0 above) + wh1 (v1 - v1 left)
         const float2 nz = fma2(W1, sub2(nv1, make_float2(left, nv1.x)), fma2(W0, sub2(nv0, q.cv0[l]), dn));
         const bool last = l == LV - 1;
         const bool check = !REDO && last;
         float2 nzu = make_float2(0.f, 0.f);
         if (check) {  // z of the third iterate's u on row rn
-            const float lu = __shfl_up_sync(0xffffffffu, nu1.y, 1);
+            const float slu = __shfl_up_sync(0xffffffffu, nu1.y, 1);
+            const float lu = ledge ? 0.f : slu;
             nzu = fma2(W1, sub2(nu1, make_float2(lu, nu1.x)), fma2(W0, sub2(nu0, q.cu0[l]), dn));
         }
         const float wh0n = rn < H ? p.wh0 : 0.f;  // no vertical difference on the image's last row
@@ -1464,7 +1497,7 @@ __device__ __forceinline__ void quad_step(const QuadTile &p, QuadCarry<LV> &q, i
             const float2 a1 = fma2(TAU, g1, q.cv1[l]);
             const float2 nn = fma2(a0, a0, mul2(a1, a1));
             const float2 rr = mul2(rp, rp);
-            const float2 pr = mul2(rp, make_float2(rsqrtf(nn.x), rsqrtf(nn.y)));
+            const float2 pr = mul2(rp, make_float2(rsqrt_t(nn.x), rsqrt_t(nn.y)));
             const float2 sc = make_float2(nn.x > rr.x ? pr.x : 1.f, nn.y > rr.y ? pr.y : 1.f);
             un0 = mul2(a0, sc);
             un1 = mul2(a1, sc);
@@ -1551,11 +1584,13 @@ __device__ __forceinline__ void quad_pass(const QuadTile &p, int strip, int r0, 
     float *ring = quad_ring + warp * kQuadRingFloats;
     float *ruv = ring;                                  // [slot][v0, v1, u0, u1][64]
     float *rd = ring + kQuadSlotsUV * 4 * kQuadWin;     // [slot][d, radius][64]
-    const int C0 = strip * kQuadOut - kQuadHalo;        // the window's first column (a multiple of 4)
+    int C0, lo, hi;  // the window's first column (a multiple of 4); the columns it writes
+    quad_strip_cols(W, strip, C0, lo, hi);
     const int wc = 2 * lane;                            // this lane's first window column
     const int col = C0 + wc;
-    const bool colin = col >= 0 && col < W;             // both columns (W and col are even)
-    const bool outcol = lane >= kQuadHalo / 2 && lane < 32 - kQuadHalo / 2 && colin;  // written columns
+    const bool colin = col < W;                         // both columns (W and col are even)
+    const bool outcol = col >= lo && col < hi;          // written columns (lo, hi multiples of 4)
+    const bool ledge = C0 == 0 && lane == 0;            // column 0: its left neighbour is the zero padding
     const float wh1r1 = col + 2 < W ? p.wh1 : 0.f;      // the second column's right difference
     const float radl = colin ? p.rad : 0.f;             // the radius of this lane's columns (no pixel weights)
     // the copies: 16-byte pieces of the window's rows, a piece per lane and
@@ -1612,18 +1647,12 @@ __device__ __forceinline__ void quad_pass(const QuadTile &p, int strip, int r0, 
     int s = sb;
     for (; s < r0 + LV; ++s) {  // the rows above the tile
         stage(s);
-        quad_step<ALPHA, REDO, ROWSUMS, false, LV>(p, q, s, ustart, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
+        quad_step<ALPHA, REDO, ROWSUMS, false, LV>(p, q, s, ustart, strip, ruv, rd, wc, outcol, ledge, wh1r1, gsum, dsum, uo, vo);
     }
-    for (; s + 1 <= se; s += 2) {  // output rows, two steps per trip
+    for (; s <= se; ++s) {  // output rows
         stage(s);
-        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s, ustart, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
-        stage(s + 1);
-        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s + 1, ustart, strip, ruv, rd, wc, outcol, wh1r1, gsum,
+        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s, ustart, strip, ruv, rd, wc, outcol, ledge, wh1r1, gsum,
                                                   dsum, uo, vo);
-    }
-    if (s <= se) {
-        stage(s);
-        quad_step<ALPHA, REDO, ROWSUMS, true, LV>(p, q, s, ustart, strip, ruv, rd, wc, outcol, wh1r1, gsum, dsum, uo, vo);
     }
     cp_async_wait<0>();
 }
