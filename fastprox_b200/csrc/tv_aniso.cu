@@ -735,6 +735,25 @@ struct SumIn {
     __device__ __forceinline__ T operator()(int i) const { return PASS == 1 ? (T)(a[i] + w[i]) : (T)(a[i] - w[i]); }
 };
 
+// A prefetch into L1 of the next 128 bytes of each of a fibre's input streams
+// (up to three; null: none) when the scan's front enters a new 128-byte block:
+// the lanes of a lockstep warp cross into new cache lines at different steps,
+// and a line read on demand stalls the whole warp.
+__device__ __forceinline__ void prefetch_l1(const void *a) { asm volatile("prefetch.global.L1 [%0];" ::"l"(a)); }
+template <class T>
+struct FmPrefetch {
+    const T *p0, *p1, *p2;
+    int n;
+    __device__ __forceinline__ void operator()(int i) const {
+        constexpr int E = 128 / (int)sizeof(T);
+        if ((i & (E - 1)) == 0 && i + E < n) {
+            prefetch_l1(p0 + i + E);
+            if (p1) prefetch_l1(p1 + i + E);
+            if (p2) prefetch_l1(p2 + i + E);
+        }
+    }
+};
+
 // Whether pass PASS of a round acts on image b (the stages of an_pass1 / an_pass2).
 template <int PASS>
 __device__ __forceinline__ bool fm_active(const AnState &st, const AnImage &im) {
@@ -811,20 +830,20 @@ __global__ void __launch_bounds__(kFmScan) an_fm_scan(AnGeom g, AnCall c, AnBuff
     const SegSink<T> sink{static_cast<T *>(bf.segv) + (int64_t)b * N + fo, bf.segk + (int64_t)b * N + fo, out, bf.err};
     const double lam = im.lam[a];
     const TableRecip<T> rcp{rc};
-    auto run = [&](const auto &in) {
+    auto run = [&](const auto &in, const T *s0, const T *s1) {
         if (c.has_beta) {
             const T *bw = static_cast<const T *>(fb.s == 1 ? bf.beta : bf.wt) + (int64_t)a * c.N + fo;
-            tv1d_warp<T, true>(in, sink, L, lam, true, FmIn<T>{bw}, rcp, act);
+            tv1d_warp<T, true>(in, sink, L, lam, true, FmIn<T>{bw}, rcp, act, FmPrefetch<T>{s0, s1, bw, L});
         } else {
-            tv1d_warp<T, true>(in, sink, L, lam, false, NoWeight{}, rcp, act);
+            tv1d_warp<T, true>(in, sink, L, lam, false, NoWeight{}, rcp, act, FmPrefetch<T>{s0, s1, nullptr, L});
         }
     };
     if (DIRECT) {
         const T *P0 = static_cast<const T *>(PASS == 1 ? bf.d : bf.u) + (int64_t)b * N + fo;
         const T *Wv = static_cast<const T *>(bf.wv) + (int64_t)b * g.k * N + fo;
-        run(SumIn<T, PASS>{P0, Wv});
+        run(SumIn<T, PASS>{P0, Wv}, P0, Wv);
     } else {
-        run(FmIn<T>{Y});
+        run(FmIn<T>{Y}, Y, nullptr);
     }
 }
 
