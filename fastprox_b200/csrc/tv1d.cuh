@@ -281,15 +281,9 @@ struct NoWeight {
 // with zero-weight edges (pieces) run tv1d_fiber_sink after the loop. A scan
 // takes at most 2 (n + 1)^2 steps (every jump moves the segment's start
 // forward, and between jumps k only grows): the loop stops there.
-struct NoPrefetch {
-    __device__ __forceinline__ void operator()(int) const {}
-};
-
-// pf(i) is called when a scan first reaches entry i (its front), for a
-// prefetch of the inputs ahead of it.
-template <class C, bool COPY = false, class In, class Sink, class Wt, class Rcp, class Pf = NoPrefetch>
+template <class C, bool COPY = false, class In, class Sink, class Wt, class Rcp>
 __device__ __forceinline__ void tv1d_warp(const In &in, const Sink &out, int n, double lam_d, bool has_w, const Wt &w,
-                                          const Rcp &rcp, bool act, const Pf &pf = Pf()) {
+                                          const Rcp &rcp, bool act) {
     const C lam = (C)lam_d;
     C range = C(0), wmax = C(0);
     bool cut = false;
@@ -327,14 +321,9 @@ __device__ __forceinline__ void tv1d_warp(const In &in, const Sink &out, int n, 
     CondatScan<C> st;
     st.start();
     const long long steps = 2ll * (long long)(n + 1) * (long long)(n + 1);
-    int front = 0;
     for (long long it = 0; it < steps && __any_sync(0xffffffffu, live); ++it) {
         if (!live) continue;
         const int i = st.next(n);
-        if (i > front) {
-            front = i;
-            pf(i);
-        }
         live = !st.step(n, (C)in(i), rad(i), rcp(st.len(n)), out);
     }
     if (fill) out.finish(n);

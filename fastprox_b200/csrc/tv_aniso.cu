@@ -735,25 +735,6 @@ struct SumIn {
     __device__ __forceinline__ T operator()(int i) const { return PASS == 1 ? (T)(a[i] + w[i]) : (T)(a[i] - w[i]); }
 };
 
-// A prefetch into L1 of the next 128 bytes of each of a fibre's input streams
-// (up to three; null: none) when the scan's front enters a new 128-byte block:
-// the lanes of a lockstep warp cross into new cache lines at different steps,
-// and a line read on demand stalls the whole warp.
-__device__ __forceinline__ void prefetch_l1(const void *a) { asm volatile("prefetch.global.L1 [%0];" ::"l"(a)); }
-template <class T>
-struct FmPrefetch {
-    const T *p0, *p1, *p2;
-    int n;
-    __device__ __forceinline__ void operator()(int i) const {
-        constexpr int E = 128 / (int)sizeof(T);
-        if ((i & (E - 1)) == 0 && i + E < n) {
-            prefetch_l1(p0 + i + E);
-            if (p1) prefetch_l1(p1 + i + E);
-            if (p2) prefetch_l1(p2 + i + E);
-        }
-    }
-};
-
 // Whether pass PASS of a round acts on image b (the stages of an_pass1 / an_pass2).
 template <int PASS>
 __device__ __forceinline__ bool fm_active(const AnState &st, const AnImage &im) {
@@ -763,7 +744,8 @@ __device__ __forceinline__ bool fm_active(const AnState &st, const AnImage &im) 
 
 constexpr int kFmTile = 32;     // tile of 32 fibres x 32 entries
 constexpr int kFmThreads = 256; // 32 x 8 threads per tile block
-constexpr int kFmScan = 128;    // lanes (fibres) per scan block
+constexpr int kFmScan = 128;    // threads per scan block
+constexpr int kFmLanes = 8;     // fibres per warp of a scan block (its other lanes idle)
 
 __host__ __device__ __forceinline__ int64_t fm_tiles(int64_t nfib, int64_t L) {
     return ((nfib + kFmTile - 1) / kFmTile) * ((L + kFmTile - 1) / kFmTile);
@@ -822,28 +804,29 @@ __global__ void __launch_bounds__(kFmScan) an_fm_scan(AnGeom g, AnCall c, AnBuff
         for (int m = threadIdx.x; m <= L; m += blockDim.x) rc[m] = m ? div(m) : T(0);
     }
     __syncthreads();
-    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool act = f < fb.nfib;
+    const int lane = threadIdx.x & 31;
+    const int64_t f = ((int64_t)blockIdx.x * (kFmScan / 32) + (threadIdx.x >> 5)) * kFmLanes + lane;
+    const bool act = lane < kFmLanes && f < fb.nfib;
     const int64_t N = g.N, fo = act ? f * L : 0;  // fibre-major offset (the image offset when DIRECT)
     T *Y = static_cast<T *>(bf.ys) + (int64_t)b * N + fo;
     T *out = (DIRECT && PASS == 1) ? static_cast<T *>(bf.u) + (int64_t)b * N + fo : Y;
     const SegSink<T> sink{static_cast<T *>(bf.segv) + (int64_t)b * N + fo, bf.segk + (int64_t)b * N + fo, out, bf.err};
     const double lam = im.lam[a];
     const TableRecip<T> rcp{rc};
-    auto run = [&](const auto &in, const T *s0, const T *s1) {
+    auto run = [&](const auto &in) {
         if (c.has_beta) {
             const T *bw = static_cast<const T *>(fb.s == 1 ? bf.beta : bf.wt) + (int64_t)a * c.N + fo;
-            tv1d_warp<T, true>(in, sink, L, lam, true, FmIn<T>{bw}, rcp, act, FmPrefetch<T>{s0, s1, bw, L});
+            tv1d_warp<T, true>(in, sink, L, lam, true, FmIn<T>{bw}, rcp, act);
         } else {
-            tv1d_warp<T, true>(in, sink, L, lam, false, NoWeight{}, rcp, act, FmPrefetch<T>{s0, s1, nullptr, L});
+            tv1d_warp<T, true>(in, sink, L, lam, false, NoWeight{}, rcp, act);
         }
     };
     if (DIRECT) {
         const T *P0 = static_cast<const T *>(PASS == 1 ? bf.d : bf.u) + (int64_t)b * N + fo;
         const T *Wv = static_cast<const T *>(bf.wv) + (int64_t)b * g.k * N + fo;
-        run(SumIn<T, PASS>{P0, Wv}, P0, Wv);
+        run(SumIn<T, PASS>{P0, Wv});
     } else {
-        run(FmIn<T>{Y}, Y, nullptr);
+        run(FmIn<T>{Y});
     }
 }
 
@@ -1760,7 +1743,8 @@ cudaError_t round_t(const AnGeom &g, const AnCall &c, const AnBuffers &bf, int64
             if (g.S[a] == 1) return (unsigned)std::min<int64_t>((g.N + kFmThreads - 1) / kFmThreads, 1024);
             return (unsigned)std::min<int64_t>(fm_tiles(nf[a], g.L[a]), 1024);
         };
-        auto scan_grid = [&](int a) { return dim3((unsigned)((nf[a] + kFmScan - 1) / kFmScan), B); };
+        constexpr int per = kFmScan / 32 * kFmLanes;  // fibres per scan block
+        auto scan_grid = [&](int a) { return dim3((unsigned)((nf[a] + per - 1) / per), B); };
         auto scan_smem = [&](int a) { return (size_t)(g.L[a] + 1) * sizeof(T); };
         if (g.S[a1] == 1) {
             an_fm_scan<T, 1, true><<<scan_grid(a1), kFmScan, scan_smem(a1), s>>>(g, c, bf);

@@ -82,6 +82,14 @@ class _ImageOp:
         except Exception:
             pass
 
+    def release(self):
+        """Frees the cached workspaces (created again on the next solve): for
+        callers that solve many shapes with one operator."""
+        L = capi.lib()
+        for ws in self._ws.values():
+            L.fp_workspace_free(ws)
+        self._ws.clear()
+
     @property
     def nparams(self):
         return int(capi.lib().fp_op_nparams(self._op))

@@ -99,8 +99,10 @@ def _solve_one(r):
 def solve_group(group, ops=None):
     """One call for requests of the same kind and shape: their images stacked
     into one batch on the device, one step per image (fp_prox_steps), each
-    image stopped at its own gap. ops caches an operator per kind (its
-    workspaces per batch shape). Returns the results in the group's order."""
+    image stopped at its own gap. ops caches an operator per kind; its
+    workspace is freed after the call (the memory pool makes that cheap), so
+    that the device memory held is the admitted requests', whatever shapes
+    have come before. Returns the results in the group's order."""
     import torch
 
     from .image_tv import TVAniso, TVIso
@@ -113,6 +115,7 @@ def solve_group(group, ops=None):
     x = torch.stack([r.x for r in group])
     steps = torch.tensor([r.gamma for r in group], dtype=torch.float64, device=x.device)
     z, info = op.solve(x, steps, tol=group[0].tol, max_iter=5000, with_dual=False)
+    op.release()
     return [z[i] for i in range(len(group))], info
 
 
