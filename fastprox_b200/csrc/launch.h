@@ -33,7 +33,7 @@ struct IsoBuffers {
 // Launch shape of the step kernel, picked per geometry (and by the tuner).
 struct StepShape {
     int kind = 4;   // 1: generic (one thread per pixel), 4: 2D lean row-marching, 5: 3D slice-marching tiles
-    int vec = 1;    // pixels per thread along the contiguous axis (2D)
+    int vec = 1;    // pixels per thread along the contiguous axis (2D; 3D: 2 for the two-voxel step)
     int bx = 128;   // threads per block
     int rows = 16;  // rows per block (2D), slices per block (3D)
     int gx = 1, gy = 1;  // blocks per image = gx * gy

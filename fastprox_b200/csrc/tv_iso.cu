@@ -2474,6 +2474,260 @@ __global__ void __launch_bounds__(k3TX * k3TY) iso3d_kernel(StepArgs A, IsoCall 
 }
 
 // ---------------------------------------------------------------------------
+// The 3D step with two voxels per thread (float32, rows of an even number of
+// voxels): a block owns a k3VY x k3VX tile of the (axis 1, axis 2) plane, a
+// warp a row of it, a lane two adjacent voxels, and marches along axis 0
+// like iso3d_kernel. The staged region (the tile and a one-entry halo) comes
+// in by 8-byte cp.async pieces (the halo columns by 4-byte ones), z of the
+// next slice is formed by each thread at its own two voxels (the forward halo
+// row and column by the first 41 threads), so no index is divided and each
+// copy and each piece of arithmetic serves two voxels. The per-voxel
+// arithmetic is iso3d_kernel's, expression for expression; its sums run in an
+// order of their own (per thread over its voxels and slices, then the block),
+// fixed by the volume's shape.
+// ---------------------------------------------------------------------------
+constexpr int k3VX = 64, k3VY = 8;        // tile: 64 voxels of axis 2 (two per lane) by 8 of axis 1 (a warp each)
+constexpr int k3VRS = k3VX + 4;           // staged row stride: column c (-1 .. 64) at c + 2, interior 8-byte aligned
+constexpr int k3VRows = k3VY + 2;         // staged rows -1 .. 8
+constexpr int k3VR = k3VRows * k3VRS;     // staged entries per array and slice
+constexpr int k3VZS = k3VX + 2;           // z row stride (columns 0 .. 64)
+constexpr int k3VZ = (k3VY + 1) * k3VZS;  // z of a slice: rows 0 .. 8
+constexpr int k3VPairs = k3VRows * (k3VX / 2);  // 8-byte staging pieces per array and slice (320)
+constexpr int k3VHalo = k3VRows * 2;            // 4-byte halo-column pieces (20)
+
+template <bool GAP>
+constexpr size_t iso3d_v2_smem() {
+    return (size_t)k3Ring * (GAP ? 7 : 4) * k3VR * sizeof(float) + (size_t)2 * (GAP ? 2 : 1) * k3VZ * sizeof(float);
+}
+
+template <bool ALPHA, bool GAP, bool ZIN>
+__global__ void __launch_bounds__(k3VX / 2 * k3VY) iso3d_v2_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+    using T = float;
+    constexpr int NA = GAP ? 7 : 4;  // staged arrays: d, v0..v2 (and u0..u2 for the gap)
+    constexpr int NT = k3VX / 2 * k3VY;
+    extern __shared__ __align__(16) unsigned char i3v_smem[];
+    T(*reg)[NA][k3VR] = reinterpret_cast<T(*)[NA][k3VR]>(i3v_smem);
+    T(*zs)[GAP ? 2 : 1][k3VZ] = reinterpret_cast<T(*)[GAP ? 2 : 1][k3VZ]>(i3v_smem + k3Ring * NA * k3VR * sizeof(T));
+    __shared__ double sh[32];
+    __shared__ int flag;
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // a programmatic dependent of the previous step
+    const int b = step_image(bf, blockIdx.z);
+    if (b < 0) return;
+    const IsoState st = bf.st[b];
+    if (st.status != kLive) return;
+    const int it = st.it;
+    const bool do_gap = (it > 0 && ((it & 3) == 0 || it == A.max_iter)) || (it == 0 && st.warm);
+    const bool zin = st.zero_in != 0;
+    if (do_gap != GAP || zin != ZIN) {
+        if (threadIdx.x == 0) atomicExch(bf.err, 3);
+        return;
+    }
+    const IsoImage im = bf.img[b];
+    const int D0 = (int)A.g.L[0], D1 = (int)A.g.L[1], D2 = (int)A.g.L[2];
+    const int64_t N = A.g.N;
+    const int64_t S0 = (int64_t)D1 * D2;
+    const bool do_upd = it < A.max_iter;
+    const bool test = do_upd && (it & 3) == 0;
+    const int pin = A.par, pout = A.par ^ 1;
+    const T *D = static_cast<const T *>(bf.d) + (int64_t)b * N;
+    const T *U = static_cast<const T *>(bf.U[pin]) + (int64_t)b * 3 * N;
+    const T *V = st.vsel ? U : static_cast<const T *>(bf.V[pin]) + (int64_t)b * 3 * N;
+    T *UO = static_cast<T *>(bf.U[pout]) + (int64_t)b * 3 * N;
+    T *VO = static_cast<T *>(bf.V[pout]) + (int64_t)b * 3 * N;
+    const T *AL = ALPHA ? static_cast<const T *>(bf.alpha) + (int64_t)b * c.alpha_stride : nullptr;
+    const T wh0 = (T)c.wh[0], wh1 = (T)c.wh[1], wh2 = (T)c.wh[2];
+    const T tau = (T)c.tau, beta = (T)st.beta, rad = (T)im.radius, bnd = (T)im.bound;
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+    const int x0 = blockIdx.x * k3VX;
+    const int nyt = (D1 + k3VY - 1) / k3VY;
+    const int y0 = (blockIdx.y % nyt) * k3VY;
+    const int s0 = (blockIdx.y / nyt) * A.rows;
+    const int s1 = min(D0, s0 + A.rows);
+    auto q3 = [](int sl) { return (sl + k3Ring) % k3Ring; };
+    // This thread's staging pieces: 8-byte pieces tid and tid + NT (of 320),
+    // a 4-byte halo piece tid (of 20); offsets in a slice, whether in the
+    // image, and where they go in a staged array.
+    int64_t po[3];
+    bool pin_[3];
+    int pj[3];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const int q = tid + e * NT;
+        const int r = q / (k3VX / 2), cp = q % (k3VX / 2);  // constant divisors (powers of two)
+        const int gy = y0 - 1 + r, gx = x0 + 2 * cp;
+        pin_[e] = q < k3VPairs && gy >= 0 && gy < D1 && gx < D2;
+        po[e] = pin_[e] ? (int64_t)gy * D2 + gx : 0;
+        pj[e] = r * k3VRS + 2 + 2 * cp;
+    }
+    {
+        const int r = tid >> 1, side = tid & 1;
+        const int gy = y0 - 1 + r, gx = side ? x0 + k3VX : x0 - 1;
+        pin_[2] = tid < k3VHalo && gy >= 0 && gy < D1 && gx >= 0 && gx < D2;
+        po[2] = pin_[2] ? (int64_t)gy * D2 + gx : 0;
+        pj[2] = r * k3VRS + (side ? k3VX + 2 : 1);
+    }
+    // Slices come into the ring by cp.async (zeros outside the image), issued
+    // three steps before the work on them: slice sl + 3 goes into the slot of
+    // slice sl - 1 once every thread is past the last step's reads of it.
+    auto issue = [&](int sl) {
+        if (sl <= s1) {
+            T(*r)[k3VR] = reg[q3(sl)];
+            const bool sin = sl >= 0 && sl < D0;
+            const int64_t so = sin ? (int64_t)sl * S0 : 0;
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                if (tid + e * NT < k3VPairs) {
+                    const bool in = pin_[e] && sin;
+                    const int64_t o = in ? so + po[e] : 0;
+                    cp_async_zfill<8>(&r[0][pj[e]], D + o, in ? 8u : 0u);
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                        cp_async_zfill<8>(&r[1 + a][pj[e]], V + a * N + o, (in && !ZIN) ? 8u : 0u);
+                    if (GAP)
+#pragma unroll
+                        for (int a = 0; a < 3; ++a)
+                            cp_async_zfill<8>(&r[(GAP ? 4 : 1) + a][pj[e]], U + a * N + o, (in && !ZIN) ? 8u : 0u);
+                }
+            }
+            if (tid < k3VHalo) {
+                const bool in = pin_[2] && sin;
+                const int64_t o = in ? so + po[2] : 0;
+                cp_async_zfill<4>(&r[0][pj[2]], D + o, in ? 4u : 0u);
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    cp_async_zfill<4>(&r[1 + a][pj[2]], V + a * N + o, (in && !ZIN) ? 4u : 0u);
+                if (GAP)
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                        cp_async_zfill<4>(&r[(GAP ? 4 : 1) + a][pj[2]], U + a * N + o, (in && !ZIN) ? 4u : 0u);
+            }
+        }
+        cp_async_commit();
+    };
+    // z of slice sl (of v, and of u for the gap) at entry (row zy, column zx)
+    // of the tile and its forward halo: iso3d_kernel's expression
+    auto zat = [&](int sl, int zy, int zx) {
+        const T(*r)[k3VR] = reg[q3(sl)];
+        const T(*rp)[k3VR] = reg[q3(sl - 1)];
+        T(*z)[k3VZ] = zs[sl & 1];
+        const int i = zy * k3VZS + zx;
+        const int j = (zy + 1) * k3VRS + zx + 2;
+        z[0][i] = r[0][j] + wh0 * (r[1][j] - rp[1][j]) + wh1 * (r[2][j] - r[2][j - k3VRS]) +
+                  wh2 * (r[3][j] - r[3][j - 1]);
+        if (GAP)
+            z[GAP ? 1 : 0][i] = r[0][j] + wh0 * (r[4][j] - rp[4][j]) + wh1 * (r[5][j] - r[5][j - k3VRS]) +
+                                wh2 * (r[6][j] - r[6][j - 1]);
+    };
+    auto zslice = [&](int sl) {
+        zat(sl, w, 2 * l);
+        zat(sl, w, 2 * l + 1);
+        if (tid < 32) {  // the forward halo row
+            zat(sl, k3VY, 2 * tid);
+            zat(sl, k3VY, 2 * tid + 1);
+        } else if (tid < 32 + k3VY + 1) {  // the forward halo column, rows 0 .. 8
+            zat(sl, tid - 32, k3VX);
+        }
+    };
+    const int gy = y0 + w, gx = x0 + 2 * l;
+    const bool own = gy < D1 && gx < D2;  // both voxels (D2 even)
+    const int64_t ooff = own ? (int64_t)gy * D2 + gx : 0;
+    // u at this thread's voxels of a slice (the gap variant stages it)
+    float2 pu[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    auto fetch_u = [&](int sl) {
+        if (GAP || ZIN || !own || sl >= s1) return;
+        const int64_t o = (int64_t)sl * S0 + ooff;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) pu[a] = *reinterpret_cast<const float2 *>(U + a * N + o);
+    };
+    double gap_acc = 0.0, dot_acc = 0.0;
+#pragma unroll
+    for (int q = -1; q <= k3Ring - 2; ++q) issue(s0 + q);
+    fetch_u(s0);
+    cp_async_wait<k3Ring - 2>();  // slices s0 - 1 and s0 are in
+    __syncthreads();
+    zslice(s0);
+    for (int sl = s0; sl < s1; ++sl) {
+        const float2 uc2[3] = {pu[0], pu[1], pu[2]};
+        if (sl + 1 < s1) fetch_u(sl + 1);
+        cp_async_wait<k3Ring - 3>();  // slice sl + 1 is in (the later ones may still be in flight)
+        __syncthreads();
+        issue(sl + k3Ring - 1);
+        zslice(sl + 1);
+        __syncthreads();
+        if (own) {
+            const T(*r)[k3VR] = reg[q3(sl)];
+            const T(*zc)[k3VZ] = zs[sl & 1];
+            const T(*zn)[k3VZ] = zs[(sl + 1) & 1];
+            const int64_t o = (int64_t)sl * S0 + ooff;
+            const bool h0 = sl + 1 < D0, h1 = gy + 1 < D1;
+            T vo[2][3], uo[2][3];
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int i = w * k3VZS + 2 * l + e, j = (w + 1) * k3VRS + 2 * l + e + 2;
+                const bool h2 = gx + e + 1 < D2;
+                T uc[3] = {e ? uc2[0].y : uc2[0].x, e ? uc2[1].y : uc2[1].x, e ? uc2[2].y : uc2[2].x};
+                const T z0 = zc[0][i];
+                const T g0 = h0 ? wh0 * (zn[0][i] - z0) : T(0);
+                const T g1 = h1 ? wh1 * (zc[0][i + k3VZS] - z0) : T(0);
+                const T g2 = h2 ? wh2 * (zc[0][i + 1] - z0) : T(0);
+                T vc[3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    vc[a] = r[1 + a][j];
+                    if (GAP) uc[a] = r[(GAP ? 4 : 1) + a][j];
+                }
+                const T cv0 = wh0 != T(0) ? vc[0] + tau * g0 : T(0);
+                const T cv1 = wh1 != T(0) ? vc[1] + tau * g1 : T(0);
+                const T cv2 = wh2 != T(0) ? vc[2] + tau * g2 : T(0);
+                const T nn = cv0 * cv0 + cv1 * cv1 + cv2 * cv2;
+                const T rp = pixel_radius<T, ALPHA>(rad, bnd, AL, o + e);
+                const T sc = nn > rp * rp ? rp * rsqrt_t(nn) : T(1);
+                const T un[3] = {cv0 * sc, cv1 * sc, cv2 * sc};
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    if (test) dot_acc += (double)((vc[a] - un[a]) * (un[a] - uc[a]));
+                    vo[e][a] = un[a] + beta * (un[a] - uc[a]);
+                    uo[e][a] = un[a];
+                }
+                if (GAP) {
+                    const T zu = zc[GAP ? 1 : 0][i];
+                    const T gu0 = h0 ? wh0 * (zn[GAP ? 1 : 0][i] - zu) : T(0);
+                    const T gu1 = h1 ? wh1 * (zc[GAP ? 1 : 0][i + k3VZS] - zu) : T(0);
+                    const T gu2 = h2 ? wh2 * (zc[GAP ? 1 : 0][i + 1] - zu) : T(0);
+                    gap_acc += (double)(rp * sqrt_t(gu0 * gu0 + gu1 * gu1 + gu2 * gu2) -
+                                        (gu0 * uc[0] + gu1 * uc[1] + gu2 * uc[2]));
+                }
+            }
+            if (do_upd)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    *reinterpret_cast<float2 *>(VO + a * N + o) = make_float2(vo[0][a], vo[1][a]);
+                    *reinterpret_cast<float2 *>(UO + a * N + o) = make_float2(uo[0][a], uo[1][a]);
+                }
+        }
+    }
+    cp_async_wait<0>();
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const unsigned nblk = gridDim.x * gridDim.y;
+    const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
+    const double gsum = GAP ? block_sum(gap_acc, sh) : 0.0;
+    const double dsum = test ? block_sum(dot_acc, sh) : 0.0;
+    double *part = bf.part + (int64_t)b * bf.max_part * 2;
+    if (threadIdx.x == 0) {
+        part[blk * 2 + 0] = gsum;
+        part[blk * 2 + 1] = dsum;
+    }
+    if (!arrive_last(bf.ticket + b, nblk, &flag)) return;
+    const double gap = GAP ? sum_partials(part, nblk, 2, 0, sh) : 0.0;
+    const double dot = test ? sum_partials(part, nblk, 2, 1, sh) : 0.0;
+    if (threadIdx.x != 0) return;
+    bf.ticket[b] = 0;
+    IsoState s2 = st;
+    control(s2, im, A.max_iter, GAP, test, gap, dot, pin, bf.live);
+    bf.st[b] = s2;
+}
+
+// ---------------------------------------------------------------------------
 // Finalisation: z = d - G^T u (tv_iso.cpp:484-487, 539) back at the input's
 // scale (tv_iso.cpp:403-413), the dual q = u / wmax 2^e into bf.dual.
 // ---------------------------------------------------------------------------
@@ -2760,9 +3014,29 @@ void launch_3d_v(const dim3 &grid, StepArgs A, const IsoCall &c, const IsoBuffer
     launch_step(iso3d_kernel<T, ALPHA, GAP, ZIN>, grid, k3TX * k3TY, iso3d_smem<T, GAP>(), s, A, c, bf);
 }
 
+template <bool ALPHA, bool GAP, bool ZIN>
+void launch_3d_v2(const dim3 &grid, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s) {
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && !(done.load() & (1ull << dev))) {
+        cudaFuncSetAttribute(iso3d_v2_kernel<ALPHA, GAP, ZIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)iso3d_v2_smem<GAP>());
+        done.fetch_or(1ull << dev);
+    }
+    launch_step(iso3d_v2_kernel<ALPHA, GAP, ZIN>, grid, k3VX / 2 * k3VY, iso3d_v2_smem<GAP>(), s, A, c, bf);
+}
+
 template <class T, bool ALPHA>
 void launch_3d_a(const StepShape &sh, StepArgs A, const IsoCall &c, const IsoBuffers &bf, cudaStream_t s, int variant) {
     const dim3 grid(sh.gx, sh.gy, (unsigned)A.nimg);
+    if constexpr (std::is_same<T, float>::value) {
+        if (sh.vec == 2) {  // two voxels per thread (iso_pick_shape)
+            if (variant == 1) launch_3d_v2<ALPHA, false, true>(grid, A, c, bf, s);
+            else if (variant == 2) launch_3d_v2<ALPHA, true, false>(grid, A, c, bf, s);
+            else launch_3d_v2<ALPHA, false, false>(grid, A, c, bf, s);
+            return;
+        }
+    }
     if (variant == 1) launch_3d_v<T, ALPHA, false, true>(grid, A, c, bf, s);
     else if (variant == 2) launch_3d_v<T, ALPHA, true, false>(grid, A, c, bf, s);
     else launch_3d_v<T, ALPHA, false, false>(grid, A, c, bf, s);
@@ -2961,6 +3235,14 @@ int iso_setup_blocks(const Geometry &g) {
     return (int)nb;
 }
 
+bool iso3d_v2_enabled() {
+    static const bool on = [] {
+        const char *v = std::getenv("FASTPROX_B200_3D_V2");
+        return !(v && v[0] == '0' && v[1] == 0);
+    }();
+    return on;
+}
+
 StepShape iso_pick_shape(int dtype, const Geometry &g, int rows_hint, int bx_hint, int kind_hint) {
     StepShape sh;
     const int64_t W = g.k == 2 ? g.L[1] : 0;
@@ -2984,8 +3266,12 @@ StepShape iso_pick_shape(int dtype, const Geometry &g, int rows_hint, int bx_hin
         // slices; chunks short enough for a few blocks per SM, at most 4096
         // blocks per image (the partial sums)
         sh.kind = 5;
-        sh.bx = k3TX * k3TY;
-        const int64_t xt = (g.L[2] + k3TX - 1) / k3TX, yt = (g.L[1] + k3TY - 1) / k3TY;
+        // float32 volumes with rows of an even number of voxels: two voxels per
+        // thread (iso3d_v2_kernel; tuning hint FASTPROX_B200_3D_V2=0: one)
+        sh.vec = (dtype == 1 && g.L[2] % 2 == 0 && iso3d_v2_enabled()) ? 2 : 1;
+        const int tx = sh.vec == 2 ? k3VX : k3TX, ty = sh.vec == 2 ? k3VY : k3TY;
+        sh.bx = sh.vec == 2 ? k3VX / 2 * k3VY : k3TX * k3TY;
+        const int64_t xt = (g.L[2] + tx - 1) / tx, yt = (g.L[1] + ty - 1) / ty;
         // 16 slices per block (62.4 volumes/s on 8 x 128^3 against 59.8 at 8,
         // 62.0 at 32), fewer while a launch would have too few blocks to
         // spread over the SMs (small volumes)
