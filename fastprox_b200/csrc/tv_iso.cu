@@ -2501,7 +2501,7 @@ constexpr size_t iso3d_v2_smem() {
 }
 
 template <bool ALPHA, bool GAP, bool ZIN>
-__global__ void __launch_bounds__(k3VX / 2 * k3VY) iso3d_v2_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
+__global__ void __launch_bounds__(k3VX / 2 * k3VY, 4) iso3d_v2_kernel(StepArgs A, IsoCall c, IsoBuffers bf) {
     using T = float;
     constexpr int NA = GAP ? 7 : 4;  // staged arrays: d, v0..v2 (and u0..u2 for the gap)
     constexpr int NT = k3VX / 2 * k3VY;
