@@ -309,23 +309,40 @@ __device__ __forceinline__ void tv1d_warp(const In &in, const Sink &out, int n, 
     // Below 2 range no radius reaches its clamp (2 max(j, 1) range), so the
     // clamp can be skipped when that holds for every live fibre of the warp.
     const bool clamp = has_w && __any_sync(0xffffffffu, live && lam * wmax > C(2) * range);
-    auto rad = [&](int j) -> C {
-        if (!has_w) return l;
-        if (j >= n - 1) return C(0);
-        const C r = lam * (C)w(j);
-        if (!clamp) return r;
-        const int jj = (j + 1 < n - 1 - j) ? j + 1 : n - 1 - j;
-        const C cap = C(2) * (C)(jj > 0 ? jj : 1) * range;
-        return r < cap ? r : cap;
-    };
     CondatScan<C> st;
     st.start();
-    const long long steps = 2ll * (long long)(n + 1) * (long long)(n + 1);
-    for (long long it = 0; it < steps && __any_sync(0xffffffffu, live); ++it) {
-        if (!live) continue;
-        const int i = st.next(n);
-        live = !st.step(n, (C)in(i), rad(i), rcp(st.len(n)), out);
-    }
+    // The loop, specialised on the radius form (warp-uniform: no weights, the
+    // weights' radii, or those capped at the clamp), so that a step's radius
+    // takes no branch. A scan takes fewer than 2 (n + 1)^2 steps, which fits an
+    // int for fibres of up to 32766 entries (a long counter beyond).
+    auto scan = [&](auto rad, auto count) {
+        using Cnt = decltype(count);
+        const Cnt steps = (Cnt)2 * (Cnt)(n + 1) * (Cnt)(n + 1);
+        for (Cnt it = 0; it < steps && __any_sync(0xffffffffu, live); ++it) {
+            if (!live) continue;
+            const int i = st.next(n);
+            live = !st.step(n, (C)in(i), rad(i), rcp(st.len(n)), out);
+        }
+    };
+    auto run = [&](auto count) {
+        if (!has_w) {
+            scan([l](int) { return l; }, count);
+        } else if (!clamp) {
+            scan([&](int j) -> C { return j >= n - 1 ? C(0) : lam * (C)w(j); }, count);
+        } else {
+            scan(
+                [&](int j) -> C {
+                    if (j >= n - 1) return C(0);
+                    const C r = lam * (C)w(j);
+                    const int jj = (j + 1 < n - 1 - j) ? j + 1 : n - 1 - j;
+                    const C cap = C(2) * (C)(jj > 0 ? jj : 1) * range;
+                    return r < cap ? r : cap;
+                },
+                count);
+        }
+    };
+    if (n <= 32766) run(0);
+    else run(0ll);
     if (fill) out.finish(n);
     if (serial) tv1d_fiber_sink<C>(in, out, n, lam_d, true, w, rcp);
     if (COPY && act && !fill && !serial) {
