@@ -269,6 +269,8 @@ struct NoWeight {
     __device__ __forceinline__ double operator()(int) const { return 1.0; }
 };
 
+constexpr int kScanUnroll = 4;  // scan steps per trip of tv1d_warp's loop
+
 // tv1d_fiber_sink on the fibres of one warp at once: lane t scans fibre t when
 // `act`, every lane of the warp calls it, and n is the same for all. COPY: a
 // fibre that is its own prox is written through the sink too (every entry a
@@ -313,15 +315,22 @@ __device__ __forceinline__ void tv1d_warp(const In &in, const Sink &out, int n, 
     st.start();
     // The loop, specialised on the radius form (warp-uniform: no weights, the
     // weights' radii, or those capped at the clamp), so that a step's radius
-    // takes no branch. A scan takes fewer than 2 (n + 1)^2 steps, which fits an
+    // takes no branch, and four steps per trip (on 64 x 512^2 with edge weights
+    // 195 images/s at one step per trip, 206 at two, 227 at four). A scan takes fewer than 2 (n + 1)^2 steps, which fits an
     // int for fibres of up to 32766 entries (a long counter beyond).
     auto scan = [&](auto rad, auto count) {
         using Cnt = decltype(count);
         const Cnt steps = (Cnt)2 * (Cnt)(n + 1) * (Cnt)(n + 1);
-        for (Cnt it = 0; it < steps && __any_sync(0xffffffffu, live); ++it) {
-            if (!live) continue;
-            const int i = st.next(n);
-            live = !st.step(n, (C)in(i), rad(i), rcp(st.len(n)), out);
+        // kScanUnroll steps of every live scan per trip (a lane whose scan ends
+        // within a trip takes no further step), one vote per trip
+        for (Cnt it = 0; it < steps && __any_sync(0xffffffffu, live); it += kScanUnroll) {
+#pragma unroll
+            for (int u = 0; u < kScanUnroll; ++u) {
+                if (live) {
+                    const int i = st.next(n);
+                    live = !st.step(n, (C)in(i), rad(i), rcp(st.len(n)), out);
+                }
+            }
         }
     };
     auto run = [&](auto count) {
