@@ -171,7 +171,7 @@ struct Shifted {
 };
 template <class S>
 struct ShiftedSink {
-    S s;
+    const S &s;  // the sink itself (a sink may count what it is given)
     int o;
     __device__ __forceinline__ void segment(int k0, int k1, double v) const { s.segment(k0 + o, k1 + o, v); }
 };

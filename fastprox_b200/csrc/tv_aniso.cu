@@ -681,11 +681,10 @@ __global__ void __launch_bounds__(kTileThreads) an_fdpg3_tile(AnGeom g, AnCall c
 //    f at f L + i), through 32 x 32 tiles of shared memory (coalesced both
 //    ways); a contiguous axis (stride 1) is fibre-major already, and its scan
 //    reads the image arrays directly;
-//  * scan: Condat's scan of every fibre (tv1d_warp); a segment writes its value
-//    and its first entry at its last entry (segv, segk); after the scan each
-//    lane fills its fibre's entries from the segment ends, walking back from
-//    the fibre's end, into ys in place (or, for the first pass over a
-//    contiguous axis, straight into u);
+//  * scan: Condat's scan of every fibre (tv1d_warp); each segment's last entry
+//    and value go to a list in the order the scan emits them (segk, segv);
+//    after the scan each lane fills its fibre's entries from the list, into ys
+//    in place (or, for the first pass over a contiguous axis, straight into u);
 //  * unstage: the results back into the image's layout with the pass's
 //    epilogue (the dual update and the restart test's sums for the second
 //    pass), through the same tiles.
@@ -695,30 +694,39 @@ __global__ void __launch_bounds__(kTileThreads) an_fdpg3_tile(AnGeom g, AnCall c
 // Edge weights along a strided axis are read from a fibre-major copy made once
 // per workspace (an_weights_fm).
 
-// A segment's value and first entry at its last entry; finish fills the
-// fibre's entries, walking the segments back from the fibre's end.
+// The segments of a fibre's scan as a list in the order the scan emits them,
+// which is their order along the fibre (a segment, once emitted, is final:
+// the scan goes on from the entry after its end): entry q of the list holds
+// the q-th segment's last entry and value. finish walks the list forwards and
+// fills the fibre's entries; each segment's list entry is read one segment
+// ahead, so the reads do not wait on one another.
 template <class T>
 struct SegSink {
     T *val;
-    int *start;
+    int *end;
     T *out;
     int *err;
-    __device__ __forceinline__ void segment(int k0, int k1, double v) const {
-        val[k1] = (T)v;
-        start[k1] = k0;
+    mutable int cnt = 0;  // segments emitted
+    __device__ __forceinline__ void segment(int, int k1, double v) const {
+        val[cnt] = (T)v;
+        end[cnt] = k1;
+        ++cnt;
     }
     __device__ __forceinline__ void finish(int n) const {
-        int e = n - 1;
-        while (e >= 0) {
-            int k0 = start[e];
-            if (k0 < 0 || k0 > e) {  // never written: a broken scan, flagged (the walk still ends)
-                atomicExch(err, 4);
-                k0 = e;
-            }
-            const T v = val[e];
-            for (int i = e; i >= k0; --i) out[i] = v;
-            e = k0 - 1;
+        int prev = -1;
+        int e = cnt > 0 ? end[0] : -1;
+        T v = cnt > 0 ? val[0] : T(0);
+        for (int q = 0; q < cnt; ++q) {
+            const int en = q + 1 < cnt ? end[q + 1] : -1;
+            const T vn = q + 1 < cnt ? val[q + 1] : T(0);
+            if (e <= prev || e >= n) break;  // not in order: a broken scan, flagged below
+            for (int i = prev + 1; i <= e; ++i) out[i] = v;
+            prev = e;
+            e = en;
+            v = vn;
         }
+        if (prev != n - 1) atomicExch(err, 4);
+        cnt = 0;
     }
 };
 
