@@ -1341,8 +1341,12 @@ __global__ void __launch_bounds__(128) an_mark(AnGeom g, AnCall c, AnBuffers bf,
     uint8_t *F = bf.flag + (int64_t)b * N + base;
     const uint8_t bit = (uint8_t)(1u << a);
     double acc = 0.0;
+    // zp of the edge's first entry is carried in a register from the last
+    // edge (which may have changed it), so no step waits on its own store
+    T zc = ZP[0];
     for (int64_t l = 0; l + 1 < fb.L; ++l) {
         const int64_t o = l * s;
+        T zn = ZP[o + s];
         acc += (double)Q[o];
         const double pe = -acc;
         const double lb = Bw ? lam * (double)Bw[o] : lam;
@@ -1351,10 +1355,13 @@ __global__ void __launch_bounds__(128) an_mark(AnGeom g, AnCall c, AnBuffers bf,
             F[o] |= bit;
         } else {
             const double ls = copysign(lb, pe);
-            ZP[o] = (T)((double)ZP[o] + ls);
-            ZP[o + s] = (T)((double)ZP[o + s] - ls);
+            zc = (T)((double)zc + ls);
+            zn = (T)((double)zn - ls);
         }
+        ZP[o] = zc;
+        zc = zn;
     }
+    ZP[(fb.L - 1) * s] = zc;
 }
 
 __device__ __forceinline__ int uf_find(int *P, int i) {
