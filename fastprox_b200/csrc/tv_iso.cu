@@ -2548,22 +2548,22 @@ __global__ void __launch_bounds__(k3VX / 2 * k3VY, 4) iso3d_v2_kernel(StepArgs A
     // a 4-byte halo piece tid (of 20); offsets in a slice, whether in the
     // image, and where they go in a staged array.
     int64_t po[3];
-    bool pin_[3];
+    bool pok[3];
     int pj[3];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
         const int q = tid + e * NT;
         const int r = q / (k3VX / 2), cp = q % (k3VX / 2);  // constant divisors (powers of two)
         const int gy = y0 - 1 + r, gx = x0 + 2 * cp;
-        pin_[e] = q < k3VPairs && gy >= 0 && gy < D1 && gx < D2;
-        po[e] = pin_[e] ? (int64_t)gy * D2 + gx : 0;
+        pok[e] = q < k3VPairs && gy >= 0 && gy < D1 && gx < D2;
+        po[e] = pok[e] ? (int64_t)gy * D2 + gx : 0;
         pj[e] = r * k3VRS + 2 + 2 * cp;
     }
     {
         const int r = tid >> 1, side = tid & 1;
         const int gy = y0 - 1 + r, gx = side ? x0 + k3VX : x0 - 1;
-        pin_[2] = tid < k3VHalo && gy >= 0 && gy < D1 && gx >= 0 && gx < D2;
-        po[2] = pin_[2] ? (int64_t)gy * D2 + gx : 0;
+        pok[2] = tid < k3VHalo && gy >= 0 && gy < D1 && gx >= 0 && gx < D2;
+        po[2] = pok[2] ? (int64_t)gy * D2 + gx : 0;
         pj[2] = r * k3VRS + (side ? k3VX + 2 : 1);
     }
     // Slices come into the ring by cp.async (zeros outside the image), issued
@@ -2577,7 +2577,7 @@ __global__ void __launch_bounds__(k3VX / 2 * k3VY, 4) iso3d_v2_kernel(StepArgs A
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 if (tid + e * NT < k3VPairs) {
-                    const bool in = pin_[e] && sin;
+                    const bool in = pok[e] && sin;
                     const int64_t o = in ? so + po[e] : 0;
                     cp_async_zfill<8>(&r[0][pj[e]], D + o, in ? 8u : 0u);
 #pragma unroll
@@ -2590,7 +2590,7 @@ __global__ void __launch_bounds__(k3VX / 2 * k3VY, 4) iso3d_v2_kernel(StepArgs A
                 }
             }
             if (tid < k3VHalo) {
-                const bool in = pin_[2] && sin;
+                const bool in = pok[2] && sin;
                 const int64_t o = in ? so + po[2] : 0;
                 cp_async_zfill<4>(&r[0][pj[2]], D + o, in ? 4u : 0u);
 #pragma unroll
