@@ -3,9 +3,9 @@ open, against the reference C library (the checker, oracle/_ref, built from the
 reference's sources) through the C ABI on CUDA tensors:
 
 * the 64 x 512^2 benchmark's own kind of images: isotropic TV with one
-  pixel-weight map for the batch and gamma 0.05 / 0.1 / 0.2 (the pair launches,
-  their checks and the redo of a passing check), anisotropic TV with edge
-  weights and the polish;
+  pixel-weight map for the batch and gamma 0.05 / 0.1 / 0.2 (the quad launches
+  of four iterations, their checks and the redo of a passing check), anisotropic
+  TV with edge weights and the polish;
 * rows wider than one 512-column block (the WIDE pair launch, halo columns);
 * the error against the reference run in float64 to gap 1e-12, stated beside
   the certified error zerr, which must bound it;
